@@ -1,0 +1,208 @@
+/*
+ * sphere_b200.h -- C ABI of the B200-native DEM time step.
+ *
+ * The reference (19revey/sphere) has no library boundary for its time step:
+ * python/sphere.py:4482-4540 (sim.run) writes input/<sid>.bin and executes the
+ * `sphere` binary, whose DEM::startTime loop (src/device.cu:826-2677) runs the
+ * step kernels.  This header is the in-process replacement for that process
+ * boundary.  Each entry point below names the reference code it replaces.
+ *
+ * Conventions
+ *  - Plain C types only; every pointer is a caller-owned HOST buffer that is
+ *    read or written only during the call.
+ *  - Array layouts are the .bin v2.15 block layouts (src/file_io.cpp:420-731):
+ *    x = [np][4] (x, y, z, radius), vel = [np][4] (vx, vy, vz, fixvel),
+ *    xyzsum/force/angpos/angvel/torque = [np][3], energies = [np].
+ *  - Every function returns an SphStatus code (0 = OK) and never calls exit().
+ *  - One handle is bound to one device and one CUDA stream; calls on a handle
+ *    must not overlap.  Handles are independent of each other.
+ *  - Several independent boxes ("ensemble") may share one handle: their
+ *    particles are concatenated in box order and stepped by the same kernel
+ *    launches.  A single simulation is the nboxes == 1 case.
+ */
+#ifndef SPHERE_B200_H_
+#define SPHERE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPH_NC 32          /* contact slots per particle, src/constants.h:21 (NC) */
+#define SPH_MAXWALLS 6     /* src/constants.h:12 (MAXWALLS) */
+#define SPH_BIN_VERSION 2.15 /* src/version.h:5 (VERSION) */
+
+typedef enum SphStatus {
+    SPH_OK = 0,
+    SPH_ERR_INPUT = 1,        /* invalid argument or scene (src/sphere.cpp:145-345 checks) */
+    SPH_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    SPH_ERR_NC_OVERFLOW = 3,  /* a particle had more than SPH_NC contacts */
+    SPH_ERR_OUT_OF_GRID = 4,  /* a particle left the sorting grid */
+    SPH_ERR_NAN = 5,          /* a non-finite particle position */
+    SPH_ERR_NOMEM = 6,        /* device or host allocation failed */
+    SPH_ERR_STATE = 7,        /* call out of order (e.g. step before upload) */
+    SPH_ERR_UNSUPPORTED = 8   /* feature outside this library's scope */
+} SphStatus;
+
+/* Arithmetic of the step. */
+typedef enum SphPrecision {
+    SPH_PREC_FP64 = 0,   /* all state and contact arithmetic in FP64 */
+    SPH_PREC_MIXED = 1   /* FP64 geometry, history and integration; FP32 contact law */
+} SphPrecision;
+
+/* How vector lengths are evaluated.  The reference's length()
+ * (src/vector_arithmetic.h:317-324) is sqrtf() of an FP64 dot product, i.e. the
+ * length is rounded to FP32.  SPH_LEN_REFERENCE reproduces that bit for bit;
+ * SPH_LEN_FP64 takes the square root in FP64. */
+typedef enum SphLengthMode {
+    SPH_LEN_REFERENCE = 0,
+    SPH_LEN_FP64 = 1
+} SphLengthMode;
+
+/* Global physical parameters: src/datatypes.h:74-101 (struct Params), same
+ * field order, without nb0 (a per-box count below). */
+typedef struct SphParams {
+    double g[3];
+    double k_n, k_t, k_r, E;
+    double gamma_n, gamma_t, gamma_r;
+    double mu_s, mu_d, mu_r;
+    double gamma_wn, gamma_wt, mu_ws, mu_wd;
+    double rho;
+    uint32_t contactmodel;  /* 1, 2 or 3 */
+    uint32_t pad0;
+    double kappa, db, V_b;
+    double lambda_bar, sigma_b, tau_b;
+    double sigma0_A, sigma0_f;
+} SphParams;
+
+/* Sorting grid: src/datatypes.h:44-50 (struct Grid). */
+typedef struct SphGrid {
+    double origo[3];
+    double L[3];
+    uint32_t num[3];
+    int32_t periodic;   /* 0: walls, 1: x and y periodic, 2: x periodic */
+    int32_t adaptive;   /* 1: L[2] follows wall 0 (src/device.cu:363-393) */
+    int32_t pad0;
+} SphGrid;
+
+/* Dynamic walls: src/datatypes.h:103-109 (struct Walls).  nx[i] = normal xyz
+ * and position; mvfd[i] = mass, velocity, force, normal stress. */
+typedef struct SphWalls {
+    uint32_t nw;
+    int32_t wmode[SPH_MAXWALLS];   /* 0 fixed, 1 stress, 2 velocity, 3 stress + shear */
+    uint32_t pad0;
+    double nx[SPH_MAXWALLS][4];
+    double mvfd[SPH_MAXWALLS][4];
+    double tau_x;
+} SphWalls;
+
+/* One independent simulation box. */
+typedef struct SphBox {
+    SphGrid grid;
+    SphParams params;
+    SphWalls walls;
+    double dt;          /* time.dt */
+    double t_current;   /* time.current at the start of the next step */
+    uint32_t np;        /* particles in this box */
+    uint32_t nb0;       /* bonds in this box (params.nb0) */
+} SphBox;
+
+/* Host particle arrays (all boxes concatenated), .bin block layouts. */
+typedef struct SphParticles {
+    double *x;       /* [np][4] */
+    double *xyzsum;  /* [np][3] */
+    double *vel;     /* [np][4] */
+    double *force;   /* [np][3] */
+    double *angpos;  /* [np][3] */
+    double *angvel;  /* [np][3] */
+    double *torque;  /* [np][3] */
+    double *es_dot, *es, *ev_dot, *ev, *p;  /* [np] */
+} SphParticles;
+
+/* Host bond arrays (all boxes concatenated), .bin layouts
+ * (src/file_io.cpp:228-250).  Particle indexes are local to the box. */
+typedef struct SphBonds {
+    uint32_t *pairs;   /* [nb0][2] */
+    double *delta_n;   /* [nb0] */
+    double *delta_t;   /* [nb0][3] */
+    double *omega_n;   /* [nb0] */
+    double *omega_t;   /* [nb0][3] */
+} SphBonds;
+
+typedef struct SphHandle SphHandle;
+
+/* Create a handle for `nboxes` boxes on CUDA device `device` (-1: current).
+ * Replaces DEM::DEM + initializeGPU + transferToConstantDeviceMemory +
+ * allocateGlobalDeviceMemory (src/sphere.cpp:16-95, src/device.cu:58-480),
+ * with checkValues (src/sphere.cpp:145-345) applied to every box. */
+int sph_create(const SphBox *boxes, uint32_t nboxes, int precision,
+               int length_mode, int device, SphHandle **out);
+
+/* Copy particle (and bond, may be NULL when no box has bonds) state to the
+ * device; contact lists are emptied and tangential histories zeroed.
+ * Replaces transferToGlobalDeviceMemory (src/device.cu:660-746). */
+int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b);
+
+/* Run `nsteps` iterations of the DEM::startTime loop body for fluid == 0
+ * (src/device.cu:1039-1200 and 2423-2538): cell hash, sort, reorder,
+ * topology, interact, bonds, integrate, wall sums and integrateWalls, then
+ * time.current += dt.  Returns the first device error seen in these steps;
+ * a step that overflowed a contact list is still completed. */
+int sph_step(SphHandle *h, uint64_t nsteps);
+
+/* Output-cadence driver for a single box, replacing the loop control of
+ * src/device.cu:1031, 2536-2537 and 2569: runs steps while
+ * *time_current <= time_total, adding dt to *time_current and *filetimeclock
+ * after each step exactly as the reference does, and returns after the step
+ * where *filetimeclock >= file_dt (the caller then writes an output file and
+ * zeroes *filetimeclock) or when the run is over.  *steps_done receives the
+ * number of steps run; at most max_steps are run. */
+int sph_advance(SphHandle *h, double time_total, double file_dt,
+                double *time_current, double *filetimeclock,
+                uint64_t max_steps, uint64_t *steps_done);
+
+/* Copy the current particle/bond state to host arrays (any pointer may be
+ * NULL to skip it).  Replaces transferFromGlobalDeviceMemory
+ * (src/device.cu:747-822). */
+int sph_download(SphHandle *h, SphParticles *p, SphBonds *b);
+
+/* Current per-box grid, walls and time (wall positions, velocities and
+ * forces after integrateWalls; L[2] after an adaptive-grid update). */
+int sph_get_boxes(SphHandle *h, SphBox *boxes);
+
+/* Contact bookkeeping in the reference's slot form (src/device.cu:428-432):
+ * contacts [np][NC] (partner index local to the box, np_box = empty),
+ * delta_t [np][NC][4], distmod [np][NC][4] (periodic shift xyz, partner
+ * radius).  Any pointer may be NULL. */
+int sph_get_contacts(SphHandle *h, uint32_t *contacts, double *delta_t,
+                     double *distmod);
+
+/* Cell-sort products of the last step (src/sorting.cuh:25-132,
+ * src/device.cu:1059-1107): per-particle cell id [np] (in original order),
+ * sorted permutation [np] (gridParticleIndex), cellStart/cellEnd
+ * [total cells] with 0xffffffff for empty cells.  Indexes are global over
+ * the concatenated boxes; cell ids are offset by the box's first cell. */
+int sph_get_sort(SphHandle *h, uint32_t *cell_id, uint32_t *perm,
+                 uint32_t *cell_start, uint32_t *cell_end);
+uint64_t sph_total_cells(const SphHandle *h);
+
+/* Live directed contacts after the last step (each pair counted twice,
+ * once per particle row); used for the roofline byte count. */
+int sph_count_contacts(SphHandle *h, uint64_t *ncontacts);
+
+/* Kernel launches issued by this handle since creation. */
+uint64_t sph_kernel_launches(const SphHandle *h);
+
+/* Message of the last error on this handle (or a static message for a NULL
+ * handle).  Returns the number of characters written. */
+int sph_last_error(const SphHandle *h, char *buf, size_t n);
+const char *sph_status_string(int status);
+
+void sph_destroy(SphHandle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPHERE_B200_H_ */

@@ -1,0 +1,191 @@
+"""TEST INFRASTRUCTURE ONLY: Python driver of the CPU oracles.
+
+Two CPU implementations of the reference's DEM step share one state layout
+(oracle/sphere_oracle.h):
+  * 'oracle' -- oracle/_build/libsphere_oracle.so, the C restatement
+    (oracle/sphere_oracle.c);
+  * 'ref'    -- oracle/_ref/libsphere_ref.so, the reference's own kernels
+    compiled for the CPU (oracle/ref_emu/ref_harness.cpp).
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline/reference
+legs use this module, as the checker; the product never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy
+
+from sphere_b200._abi import NC, SphBox, box_from_sim
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBS = {
+    "oracle": os.path.join(HERE, "_build", "libsphere_oracle.so"),
+    "ref": os.path.join(HERE, "_ref", "libsphere_ref.so"),
+}
+ENTRY = {"oracle": "or_step", "ref": "ref_step"}
+
+_dp = C.POINTER(C.c_double)
+_up = C.POINTER(C.c_uint32)
+_bp = C.POINTER(C.c_uint8)
+
+
+class OrState(C.Structure):
+    _fields_ = [
+        ("box", SphBox),
+        ("length_mode", C.c_int32), ("velocity_state", C.c_int32),
+        ("iter", C.c_uint64),
+        ("error_flags", C.c_int32), ("nthreads", C.c_int32),
+        ("x", _dp), ("xyzsum", _dp), ("vel", _dp), ("force", _dp), ("angpos", _dp),
+        ("angvel", _dp), ("torque", _dp), ("acc", _dp), ("angacc", _dp),
+        ("es_dot", _dp), ("es", _dp), ("ev_dot", _dp), ("ev", _dp), ("p", _dp),
+        ("contacts", _up), ("distmod", _dp), ("delta_t", _dp),
+        ("bonds", _up), ("bonds_delta", _dp), ("bonds_omega", _dp), ("bonds_broken", _bp),
+        ("walls_acc", C.c_double * 6),
+        ("cell_id", _up), ("perm", _up), ("cell_start", _up), ("cell_end", _up),
+        ("x_sorted", _dp), ("vel_sorted", _dp), ("angvel_sorted", _dp),
+        ("walls_force_pp", _dp), ("walls_force_partial", _dp),
+        ("tau_eff_x_pp", _dp), ("tau_eff_x_partial", _dp),
+    ]
+
+
+_loaded = {}
+
+
+def build():
+    """Compile the CPU oracles in place (make -C oracle)."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def available(which):
+    return os.path.exists(LIBS[which])
+
+
+def _lib(which):
+    if which not in _loaded:
+        if not os.path.exists(LIBS[which]):
+            build()
+        lib = C.CDLL(LIBS[which])
+        fn = getattr(lib, ENTRY[which])
+        fn.argtypes = [C.POINTER(OrState), C.c_uint64]
+        fn.restype = C.c_int
+        _loaded[which] = fn
+    return _loaded[which]
+
+
+def _f4(a3, w=None):
+    a3 = numpy.asarray(a3, dtype=numpy.float64).reshape(-1, 3)
+    out = numpy.zeros((a3.shape[0], 4))
+    out[:, :3] = a3
+    if w is not None:
+        out[:, 3] = w
+    return out
+
+
+class CpuRun(object):
+    """One simulation box stepped by a CPU oracle.  All arrays are numpy
+    arrays in the reference's device layouts and may be inspected after
+    each call to step()."""
+
+    def __init__(self, s, which="oracle", length_mode=0, nthreads=0):
+        self.which = which
+        self.fn = _lib(which)
+        n = int(s.np[0])
+        nb0 = int(s.nb0[0])
+        nw = int(s.nw[0])
+        self.n = n
+        self.x = _f4(s.x, s.radius)
+        self.xyzsum = _f4(s.xyzsum)
+        self.vel = _f4(s.vel, s.fixvel)
+        self.force = _f4(s.force)
+        self.angpos = _f4(s.angpos)
+        self.angvel = _f4(s.angvel)
+        self.torque = _f4(s.torque)
+        self.acc = numpy.zeros((n, 4))
+        self.angacc = numpy.zeros((n, 4))
+        self.es_dot = numpy.array(s.es_dot, dtype=numpy.float64)
+        self.es = numpy.array(s.es, dtype=numpy.float64)
+        self.ev_dot = numpy.array(s.ev_dot, dtype=numpy.float64)
+        self.ev = numpy.array(s.ev, dtype=numpy.float64)
+        self.p = numpy.array(s.p, dtype=numpy.float64)
+        self.contacts = numpy.full(n * NC, n, dtype=numpy.uint32)
+        self.distmod = numpy.zeros((n * NC, 4))
+        self.delta_t = numpy.zeros((n * NC, 4))
+        self.bonds = numpy.array(numpy.asarray(s.bonds).reshape(-1, 2)[:nb0], dtype=numpy.uint32)
+        self.bonds_delta = numpy.zeros((max(nb0, 1), 4))
+        self.bonds_omega = numpy.zeros((max(nb0, 1), 4))
+        if nb0:
+            self.bonds_delta[:nb0, :3] = numpy.asarray(s.bonds_delta_t).reshape(-1, 3)[:nb0]
+            self.bonds_delta[:nb0, 3] = numpy.asarray(s.bonds_delta_n).reshape(-1)[:nb0]
+            self.bonds_omega[:nb0, :3] = numpy.asarray(s.bonds_omega_t).reshape(-1, 3)[:nb0]
+            self.bonds_omega[:nb0, 3] = numpy.asarray(s.bonds_omega_n).reshape(-1)[:nb0]
+        if self.bonds.size == 0:
+            self.bonds = numpy.zeros((1, 2), dtype=numpy.uint32)
+        self.bonds_broken = numpy.zeros(max(nb0, 1), dtype=numpy.uint8)
+        ncells = int(s.num[0]) * int(s.num[1]) * int(s.num[2])
+        self.cell_id = numpy.zeros(max(n, 1), dtype=numpy.uint32)
+        self.perm = numpy.zeros(max(n, 1), dtype=numpy.uint32)
+        self.cell_start = numpy.full(ncells, 0xffffffff, dtype=numpy.uint32)
+        self.cell_end = numpy.zeros(ncells, dtype=numpy.uint32)
+        self.x_sorted = numpy.zeros((max(n, 1), 4))
+        self.vel_sorted = numpy.zeros((max(n, 1), 4))
+        self.angvel_sorted = numpy.zeros((max(n, 1), 4))
+        blocks = max((n + 255) // 256, 1)
+        self.walls_force_pp = numpy.zeros(max(nw * n, 1))
+        self.walls_force_partial = numpy.zeros(blocks)
+        self.tau_eff_x_pp = numpy.zeros(max(n, 1))
+        self.tau_eff_x_partial = numpy.zeros(blocks)
+        st = OrState()
+        st.box = box_from_sim(s)
+        st.length_mode = int(length_mode)
+        st.velocity_state = 1
+        st.iter = 0
+        st.error_flags = 0
+        st.nthreads = int(nthreads)
+        for name, _t in OrState._fields_:
+            if name in ("box", "length_mode", "velocity_state", "iter", "error_flags",
+                        "nthreads", "walls_acc"):
+                continue
+            a = getattr(self, name)
+            ct = dict(OrState._fields_)[name]
+            setattr(st, name, a.ctypes.data_as(ct))
+        self.state = st
+
+    def step(self, nsteps=1):
+        """Run nsteps steps; returns the accumulated error-flag bits."""
+        return self.fn(C.byref(self.state), int(nsteps))
+
+    @property
+    def box(self):
+        return self.state.box
+
+    def contact_rows(self):
+        return self.contacts.reshape(self.n, NC)
+
+    def to_sim(self, s):
+        """Copy the state back into a sim object (as a .bin output would)."""
+        s.x = self.x[:, :3].copy()
+        s.radius = self.x[:, 3].copy()
+        s.xyzsum = self.xyzsum[:, :3].copy()
+        s.vel = self.vel[:, :3].copy()
+        s.fixvel = self.vel[:, 3].copy()
+        s.force = self.force[:, :3].copy()
+        s.angpos = self.angpos[:, :3].copy()
+        s.angvel = self.angvel[:, :3].copy()
+        s.torque = self.torque[:, :3].copy()
+        for name in ("es_dot", "es", "ev_dot", "ev", "p"):
+            setattr(s, name, getattr(self, name).copy())
+        nb0 = int(s.nb0[0])
+        if nb0:
+            s.bonds = self.bonds[:nb0].copy()
+            s.bonds_delta_t = self.bonds_delta[:nb0, :3].copy()
+            s.bonds_delta_n = self.bonds_delta[:nb0, 3].copy()
+            s.bonds_omega_t = self.bonds_omega[:nb0, :3].copy()
+            s.bonds_omega_n = self.bonds_omega[:nb0, 3].copy()
+        b = self.state.box
+        s.L[2] = b.grid.L[2]
+        for i in range(int(b.walls.nw)):
+            s.w_x[i] = b.walls.nx[i][3]
+            s.w_vel[i] = b.walls.mvfd[i][1]
+            s.w_force[i] = b.walls.mvfd[i][2]
+        s.time_current[0] = b.t_current
+        return s

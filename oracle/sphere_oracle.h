@@ -1,0 +1,60 @@
+/*
+ * sphere_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * State layout shared by the two CPU oracles used by the tests and by the
+ * cpu_baseline leg of bench.py:
+ *   - oracle/sphere_oracle.c: a plain-C FP64 restatement of the reference's
+ *     DEM step (libsphere_oracle.so);
+ *   - oracle/ref_emu/ref_harness.cpp: the reference's own kernels compiled
+ *     for the CPU (oracle/_ref/libsphere_ref.so).
+ * The product library (sphere_b200) never links or calls either.
+ *
+ * Arrays use the reference's device layouts (src/datatypes.h:16-37):
+ * Float4 = 4 doubles per particle, contact rows of NC slots per particle
+ * indexed by the original particle index (src/device.cu:428-432).
+ */
+#ifndef SPHERE_ORACLE_H_
+#define SPHERE_ORACLE_H_
+
+#include <stdint.h>
+#include "../include/sphere_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OrState {
+    SphBox box;            /* grid, params, walls, dt, t_current, np, nb0 */
+    int32_t length_mode;   /* SphLengthMode */
+    int32_t velocity_state;/* src/device.cu:994, starts at 1 */
+    uint64_t iter;         /* TY3 step counter of this run (src/device.cu:919) */
+    int32_t error_flags;   /* bit (1 << SphStatus) for each condition seen */
+    int32_t nthreads;      /* OpenMP threads (0: default) */
+    /* particle state, [np][4] doubles unless noted */
+    double *x, *xyzsum, *vel, *force, *angpos, *angvel, *torque, *acc, *angacc;
+    double *es_dot, *es, *ev_dot, *ev, *p;          /* [np] */
+    /* contact bookkeeping, [np*NC] and [np*NC][4] */
+    uint32_t *contacts;
+    double *distmod, *delta_t;
+    /* bonds: pairs [nb0][2], delta/omega [nb0][4] (xyz tangential, w normal) */
+    uint32_t *bonds;
+    double *bonds_delta, *bonds_omega;
+    uint8_t *bonds_broken;  /* [nb0] bonds broken during this run */
+    double walls_acc[SPH_MAXWALLS];
+    /* products of the last step / scratch */
+    uint32_t *cell_id, *perm, *cell_start, *cell_end;   /* [np],[np],[ncells],[ncells] */
+    double *x_sorted, *vel_sorted, *angvel_sorted;      /* [np][4] */
+    double *walls_force_pp;                             /* [nw*np] */
+    double *walls_force_partial;                        /* [ceil(np/256)] */
+    double *tau_eff_x_pp, *tau_eff_x_partial;           /* [np], [ceil(np/256)] */
+} OrState;
+
+/* Run nsteps iterations of the fluid == 0 step loop.  Returns the OR of the
+ * error flags raised (0 = clean). */
+int or_step(OrState *s, uint64_t nsteps);
+int ref_step(OrState *s, uint64_t nsteps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

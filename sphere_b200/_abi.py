@@ -1,0 +1,206 @@
+"""ctypes mirror of include/sphere_b200.h and loader of the CUDA library.
+
+The structures below must match the C header field for field; tests check
+their sizes against the library (``sph_struct_sizes``).
+"""
+import ctypes as C
+import os
+
+NC = 32
+MAXWALLS = 6
+BIN_VERSION = 2.15
+
+SPH_OK = 0
+SPH_ERR_INPUT = 1
+SPH_ERR_CUDA = 2
+SPH_ERR_NC_OVERFLOW = 3
+SPH_ERR_OUT_OF_GRID = 4
+SPH_ERR_NAN = 5
+SPH_ERR_NOMEM = 6
+SPH_ERR_STATE = 7
+SPH_ERR_UNSUPPORTED = 8
+
+STATUS_NAMES = {
+    0: "SPH_OK", 1: "SPH_ERR_INPUT", 2: "SPH_ERR_CUDA", 3: "SPH_ERR_NC_OVERFLOW",
+    4: "SPH_ERR_OUT_OF_GRID", 5: "SPH_ERR_NAN", 6: "SPH_ERR_NOMEM",
+    7: "SPH_ERR_STATE", 8: "SPH_ERR_UNSUPPORTED",
+}
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+LEN_REFERENCE = 0
+LEN_FP64 = 1
+
+
+class SphParams(C.Structure):
+    _fields_ = [
+        ("g", C.c_double * 3),
+        ("k_n", C.c_double), ("k_t", C.c_double), ("k_r", C.c_double), ("E", C.c_double),
+        ("gamma_n", C.c_double), ("gamma_t", C.c_double), ("gamma_r", C.c_double),
+        ("mu_s", C.c_double), ("mu_d", C.c_double), ("mu_r", C.c_double),
+        ("gamma_wn", C.c_double), ("gamma_wt", C.c_double),
+        ("mu_ws", C.c_double), ("mu_wd", C.c_double),
+        ("rho", C.c_double),
+        ("contactmodel", C.c_uint32), ("pad0", C.c_uint32),
+        ("kappa", C.c_double), ("db", C.c_double), ("V_b", C.c_double),
+        ("lambda_bar", C.c_double), ("sigma_b", C.c_double), ("tau_b", C.c_double),
+        ("sigma0_A", C.c_double), ("sigma0_f", C.c_double),
+    ]
+
+
+class SphGrid(C.Structure):
+    _fields_ = [
+        ("origo", C.c_double * 3), ("L", C.c_double * 3), ("num", C.c_uint32 * 3),
+        ("periodic", C.c_int32), ("adaptive", C.c_int32), ("pad0", C.c_int32),
+    ]
+
+
+class SphWalls(C.Structure):
+    _fields_ = [
+        ("nw", C.c_uint32), ("wmode", C.c_int32 * MAXWALLS), ("pad0", C.c_uint32),
+        ("nx", (C.c_double * 4) * MAXWALLS), ("mvfd", (C.c_double * 4) * MAXWALLS),
+        ("tau_x", C.c_double),
+    ]
+
+
+class SphBox(C.Structure):
+    _fields_ = [
+        ("grid", SphGrid), ("params", SphParams), ("walls", SphWalls),
+        ("dt", C.c_double), ("t_current", C.c_double),
+        ("np", C.c_uint32), ("nb0", C.c_uint32),
+    ]
+
+
+_dp = C.POINTER(C.c_double)
+_up = C.POINTER(C.c_uint32)
+
+
+class SphParticles(C.Structure):
+    _fields_ = [(n, _dp) for n in ("x", "xyzsum", "vel", "force", "angpos", "angvel", "torque",
+                                  "es_dot", "es", "ev_dot", "ev", "p")]
+
+
+class SphBonds(C.Structure):
+    _fields_ = [("pairs", _up), ("delta_n", _dp), ("delta_t", _dp),
+                ("omega_n", _dp), ("omega_t", _dp)]
+
+
+def dptr(a):
+    """ctypes double* of a C-contiguous float64 numpy array (or NULL)."""
+    if a is None:
+        return C.cast(None, _dp)
+    assert a.dtype.name == "float64" and a.flags["C_CONTIGUOUS"], (a.dtype, a.flags)
+    return a.ctypes.data_as(_dp)
+
+
+def uptr(a):
+    if a is None:
+        return C.cast(None, _up)
+    assert a.dtype.name == "uint32" and a.flags["C_CONTIGUOUS"], (a.dtype, a.flags)
+    return a.ctypes.data_as(_up)
+
+
+def box_from_sim(s):
+    """Build an SphBox from a sim object (python/sphere.py attribute names)."""
+    b = SphBox()
+    g = b.grid
+    for d in range(3):
+        g.origo[d] = float(s.origo[d])
+        g.L[d] = float(s.L[d])
+        g.num[d] = int(s.num[d])
+    g.periodic = int(s.periodic[0])
+    g.adaptive = int(s.adaptive[0])
+    p = b.params
+    for d in range(3):
+        p.g[d] = float(s.g[d])
+    for name in ("k_n", "k_t", "k_r", "E", "gamma_n", "gamma_t", "gamma_r", "mu_s", "mu_d",
+                 "mu_r", "gamma_wn", "gamma_wt", "mu_ws", "mu_wd", "rho", "kappa", "db",
+                 "V_b", "lambda_bar", "sigma_b", "tau_b"):
+        setattr(p, name, float(getattr(s, name)[0]))
+    p.contactmodel = int(s.contactmodel[0])
+    p.sigma0_A = float(s.w_sigma0_A[0])
+    p.sigma0_f = float(s.w_sigma0_f[0])
+    w = b.walls
+    nw = int(s.nw[0])
+    if nw > MAXWALLS:
+        raise ValueError("nw = %d exceeds MAXWALLS = %d" % (nw, MAXWALLS))
+    w.nw = nw
+    for i in range(nw):
+        w.wmode[i] = int(s.wmode[i])
+        for d in range(3):
+            w.nx[i][d] = float(s.w_n[i, d])
+        w.nx[i][3] = float(s.w_x[i])
+        w.mvfd[i][0] = float(s.w_m[i])
+        w.mvfd[i][1] = float(s.w_vel[i])
+        w.mvfd[i][2] = float(s.w_force[i])
+        w.mvfd[i][3] = float(s.w_sigma0[i])
+    w.tau_x = float(s.w_tau_x[0])
+    b.dt = float(s.time_dt[0])
+    b.t_current = float(s.time_current[0])
+    b.np = int(s.np[0])
+    b.nb0 = int(s.nb0[0])
+    return b
+
+
+def sim_from_box(s, b):
+    """Copy the time-dependent box state (walls, adaptive L[2], time) to sim."""
+    s.L[2] = b.grid.L[2]
+    nw = int(b.walls.nw)
+    for i in range(nw):
+        s.w_x[i] = b.walls.nx[i][3]
+        s.w_m[i] = b.walls.mvfd[i][0]
+        s.w_vel[i] = b.walls.mvfd[i][1]
+        s.w_force[i] = b.walls.mvfd[i][2]
+        s.w_sigma0[i] = b.walls.mvfd[i][3]
+    s.time_current[0] = b.t_current
+
+
+_LIB = None
+LIB_NAME = "libsphere_b200.so"
+
+
+def lib_path():
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+
+
+def load_library():
+    """Load the in-tree CUDA library.  Raises if it is missing: there is no
+    CPU fallback for the step."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = lib_path()
+    if not os.path.exists(path):
+        raise RuntimeError(
+            "sphere_b200: CUDA library %s is missing; build it with "
+            "`python -m sphere_b200.build` (nvcc, sm_100a)" % path)
+    lib = C.CDLL(path)
+    H = C.c_void_p
+    lib.sph_create.argtypes = [C.POINTER(SphBox), C.c_uint32, C.c_int, C.c_int, C.c_int,
+                               C.POINTER(H)]
+    lib.sph_upload.argtypes = [H, C.POINTER(SphParticles), C.POINTER(SphBonds)]
+    lib.sph_step.argtypes = [H, C.c_uint64]
+    lib.sph_advance.argtypes = [H, C.c_double, C.c_double, C.POINTER(C.c_double),
+                                C.POINTER(C.c_double), C.c_uint64, C.POINTER(C.c_uint64)]
+    lib.sph_download.argtypes = [H, C.POINTER(SphParticles), C.POINTER(SphBonds)]
+    lib.sph_get_boxes.argtypes = [H, C.POINTER(SphBox)]
+    lib.sph_get_contacts.argtypes = [H, _up, _dp, _dp]
+    lib.sph_get_sort.argtypes = [H, _up, _up, _up, _up]
+    lib.sph_total_cells.argtypes = [H]
+    lib.sph_total_cells.restype = C.c_uint64
+    lib.sph_count_contacts.argtypes = [H, C.POINTER(C.c_uint64)]
+    lib.sph_kernel_launches.argtypes = [H]
+    lib.sph_kernel_launches.restype = C.c_uint64
+    lib.sph_last_error.argtypes = [H, C.c_char_p, C.c_size_t]
+    lib.sph_status_string.argtypes = [C.c_int]
+    lib.sph_status_string.restype = C.c_char_p
+    lib.sph_destroy.argtypes = [H]
+    lib.sph_destroy.restype = None
+    lib.sph_struct_sizes.argtypes = [C.POINTER(C.c_uint64)]
+    lib.sph_struct_sizes.restype = C.c_int
+    for name in ("sph_create", "sph_upload", "sph_step", "sph_advance", "sph_download",
+                 "sph_get_boxes", "sph_get_contacts", "sph_get_sort", "sph_count_contacts",
+                 "sph_last_error"):
+        getattr(lib, name).restype = C.c_int
+    _LIB = lib
+    return lib

@@ -1,0 +1,221 @@
+"""Reader and writer of sphere's binary input/output format (.bin).
+
+Layout: python/sphere.py:1355-1553 (writebin) and :965-1353 (readbin),
+src/file_io.cpp:30-731 (C++ readbin/writebin).  Files are little-endian;
+every block below is written in the order the reference writes it.  The
+writer produces files byte-identical to python/sphere.py:writebin for
+simulations without a fluid; the reader accepts versions >= 2.1 (older
+optional fields default as in python/sphere.py:readbin).  Fluid blocks
+(the Navier-Stokes / Darcy coupling) are outside this package's scope.
+"""
+import numpy
+
+VERSION = 2.15
+
+
+class _Reader(object):
+    def __init__(self, buf):
+        self.buf = memoryview(buf)
+        self.pos = 0
+
+    def take(self, dtype, count):
+        dtype = numpy.dtype(dtype)
+        n = dtype.itemsize * int(count)
+        if self.pos + n > len(self.buf):
+            raise ValueError("truncated .bin file: need %d bytes at offset %d, have %d"
+                             % (n, self.pos, len(self.buf) - self.pos))
+        a = numpy.frombuffer(self.buf[self.pos:self.pos + n], dtype=dtype).copy()
+        self.pos += n
+        return a
+
+
+def read_bin(target, sim, verbose=False, fluid=False):
+    """Read a sphere .bin file into the attributes of `sim`
+    (python/sphere.py:965 readbin)."""
+    if fluid:
+        raise NotImplementedError("fluid (Navier-Stokes/Darcy) blocks are not supported")
+    if verbose:
+        print("Input file: {0}".format(target))
+    with open(target, "rb") as fh:
+        r = _Reader(fh.read())
+    s = sim
+    s.version = r.take(numpy.float64, 1)
+    s.nd = r.take(numpy.int32, 1)
+    s.np = r.take(numpy.uint32, 1)
+    nd = int(s.nd[0])
+    n = int(s.np[0])
+    if nd != 3:
+        raise ValueError("only 3-D files are supported (nd = %d)" % nd)
+    s.time_dt = r.take(numpy.float64, 1)
+    s.time_current = r.take(numpy.float64, 1)
+    s.time_total = r.take(numpy.float64, 1)
+    s.time_file_dt = r.take(numpy.float64, 1)
+    s.time_step_count = r.take(numpy.uint32, 1)
+    s.origo = r.take(numpy.float64, nd)
+    s.L = r.take(numpy.float64, nd)
+    s.num = r.take(numpy.uint32, nd)
+    s.periodic = r.take(numpy.int32, 1)
+    if s.version[0] >= 2.14:
+        s.adaptive = r.take(numpy.int32, 1)
+    else:
+        s.adaptive = numpy.zeros(1, dtype=numpy.float64)
+    xr = r.take(numpy.float64, n * (nd + 1)).reshape(n, nd + 1)
+    s.x = numpy.ascontiguousarray(xr[:, :nd])
+    s.radius = numpy.ascontiguousarray(xr[:, nd])
+    if s.version[0] >= 1.03:
+        s.xyzsum = r.take(numpy.float64, n * 3).reshape(n, 3)
+    else:
+        s.xyzsum = r.take(numpy.float64, n * 2).reshape(n, 2)
+    vr = r.take(numpy.float64, n * (nd + 1)).reshape(n, nd + 1)
+    s.vel = numpy.ascontiguousarray(vr[:, :nd])
+    s.fixvel = numpy.ascontiguousarray(vr[:, nd])
+    s.force = r.take(numpy.float64, n * nd).reshape(n, nd)
+    s.angpos = r.take(numpy.float64, n * nd).reshape(n, nd)
+    s.angvel = r.take(numpy.float64, n * nd).reshape(n, nd)
+    s.torque = r.take(numpy.float64, n * nd).reshape(n, nd)
+    s.es_dot = r.take(numpy.float64, n)
+    s.es = r.take(numpy.float64, n)
+    s.ev_dot = r.take(numpy.float64, n)
+    s.ev = r.take(numpy.float64, n)
+    s.p = r.take(numpy.float64, n)
+    s.g = r.take(numpy.float64, nd)
+    s.k_n = r.take(numpy.float64, 1)
+    s.k_t = r.take(numpy.float64, 1)
+    s.k_r = r.take(numpy.float64, 1)
+    if s.version[0] >= 2.13:
+        s.E = r.take(numpy.float64, 1)
+    else:
+        s.E = numpy.zeros(1, dtype=numpy.float64)
+    for name in ("gamma_n", "gamma_t", "gamma_r", "mu_s", "mu_d", "mu_r", "gamma_wn",
+                 "gamma_wt", "mu_ws", "mu_wd", "rho"):
+        setattr(s, name, r.take(numpy.float64, 1))
+    s.contactmodel = r.take(numpy.uint32, 1)
+    s.kappa = r.take(numpy.float64, 1)
+    s.db = r.take(numpy.float64, 1)
+    s.V_b = r.take(numpy.float64, 1)
+    s.nw = r.take(numpy.uint32, 1)
+    nw = int(s.nw[0])
+    s.wmode = r.take(numpy.int32, nw)
+    wn = r.take(numpy.float64, nw * (nd + 1)).reshape(nw, nd + 1)
+    s.w_n = numpy.ascontiguousarray(wn[:, :nd])
+    s.w_x = numpy.ascontiguousarray(wn[:, nd])
+    wm = r.take(numpy.float64, nw * 4).reshape(nw, 4)
+    s.w_m = numpy.ascontiguousarray(wm[:, 0])
+    s.w_vel = numpy.ascontiguousarray(wm[:, 1])
+    s.w_force = numpy.ascontiguousarray(wm[:, 2])
+    s.w_sigma0 = numpy.ascontiguousarray(wm[:, 3])
+    s.w_sigma0_A = r.take(numpy.float64, 1)
+    s.w_sigma0_f = r.take(numpy.float64, 1)
+    if s.version[0] >= 2.1:
+        s.w_tau_x = r.take(numpy.float64, 1)
+    else:
+        s.w_tau_x = numpy.zeros(1, dtype=numpy.float64)
+    s.lambda_bar = r.take(numpy.float64, 1)
+    s.nb0 = r.take(numpy.uint32, 1)
+    s.sigma_b = r.take(numpy.float64, 1)
+    s.tau_b = r.take(numpy.float64, 1)
+    nb0 = int(s.nb0[0])
+    s.bonds = r.take(numpy.uint32, nb0 * 2).reshape(nb0, 2)
+    s.bonds_delta_n = r.take(numpy.float64, nb0)
+    s.bonds_delta_t = r.take(numpy.float64, nb0 * nd).reshape(nb0, nd)
+    s.bonds_omega_n = r.take(numpy.float64, nb0)
+    s.bonds_omega_t = r.take(numpy.float64, nb0 * nd).reshape(nb0, nd)
+    if s.version[0] >= 1.02:
+        s.color = r.take(numpy.int32, n)
+    else:
+        s.color = numpy.zeros(n, dtype=numpy.int32)
+    s.version[0] = VERSION
+    return s
+
+
+def _f64(a):
+    return numpy.ascontiguousarray(numpy.asarray(a), dtype=numpy.float64).tobytes()
+
+
+def _u32(a):
+    return numpy.ascontiguousarray(numpy.asarray(a).astype(numpy.uint32)).tobytes()
+
+
+def _i32(a):
+    return numpy.ascontiguousarray(numpy.asarray(a).astype(numpy.int32)).tobytes()
+
+
+def encode_bin(sim):
+    """Bytes of `sim` in the .bin layout of python/sphere.py:1355 writebin."""
+    s = sim
+    if getattr(s, "fluid", False):
+        raise NotImplementedError("fluid (Navier-Stokes/Darcy) blocks are not supported")
+    n = int(s.np[0])
+    nd = int(s.nd[0])
+    out = []
+    w = out.append
+    w(_f64(s.version))
+    w(_i32(s.nd))
+    w(_u32(s.np))
+    w(_f64(s.time_dt))
+    w(_f64(s.time_current))
+    w(_f64(s.time_total))
+    w(_f64(s.time_file_dt))
+    w(_u32(s.time_step_count))
+    w(_f64(s.origo))
+    w(_f64(s.L))
+    w(_u32(s.num))
+    w(_u32(s.periodic))
+    w(_u32(s.adaptive))
+    xr = numpy.empty((n, nd + 1))
+    xr[:, :nd] = s.x
+    xr[:, nd] = s.radius
+    w(xr.tobytes())
+    if n > 0:
+        w(_f64(s.xyzsum))
+    vr = numpy.empty((n, nd + 1))
+    vr[:, :nd] = s.vel
+    vr[:, nd] = s.fixvel
+    w(vr.tobytes())
+    if n > 0:
+        for name in ("force", "angpos", "angvel", "torque", "es_dot", "es", "ev_dot", "ev", "p"):
+            w(_f64(getattr(s, name)))
+    w(_f64(s.g))
+    for name in ("k_n", "k_t", "k_r", "E", "gamma_n", "gamma_t", "gamma_r", "mu_s", "mu_d",
+                 "mu_r", "gamma_wn", "gamma_wt", "mu_ws", "mu_wd", "rho"):
+        w(_f64(getattr(s, name)))
+    w(_u32(s.contactmodel))
+    w(_f64(s.kappa))
+    w(_f64(s.db))
+    w(_f64(s.V_b))
+    nw = int(s.nw[0])
+    w(_u32(s.nw))
+    w(_i32(numpy.asarray(s.wmode)[:nw]))
+    wn = numpy.empty((nw, nd + 1))
+    wn[:, :nd] = numpy.asarray(s.w_n)[:nw]
+    wn[:, nd] = numpy.asarray(s.w_x)[:nw]
+    w(wn.tobytes())
+    wm = numpy.empty((nw, 4))
+    wm[:, 0] = numpy.asarray(s.w_m)[:nw]
+    wm[:, 1] = numpy.asarray(s.w_vel)[:nw]
+    wm[:, 2] = numpy.asarray(s.w_force)[:nw]
+    wm[:, 3] = numpy.asarray(s.w_sigma0)[:nw]
+    w(wm.tobytes())
+    w(_f64(s.w_sigma0_A))
+    w(_f64(s.w_sigma0_f))
+    w(_f64(s.w_tau_x))
+    w(_f64(s.lambda_bar))
+    nb0 = int(s.nb0[0])
+    w(_u32(s.nb0))
+    w(_f64(s.sigma_b))
+    w(_f64(s.tau_b))
+    w(_u32(numpy.asarray(s.bonds).reshape(-1, 2)[:nb0]))
+    w(_f64(numpy.asarray(s.bonds_delta_n).reshape(-1)[:nb0]))
+    w(_f64(numpy.asarray(s.bonds_delta_t).reshape(-1, 3)[:nb0]))
+    w(_f64(numpy.asarray(s.bonds_omega_n).reshape(-1)[:nb0]))
+    w(_f64(numpy.asarray(s.bonds_omega_t).reshape(-1, 3)[:nb0]))
+    w(_i32(s.color))
+    return b"".join(out)
+
+
+def write_bin(target, sim):
+    """Write `sim` to `target` (python/sphere.py:1355 writebin layout)."""
+    data = encode_bin(sim)
+    with open(target, "wb") as fh:
+        fh.write(data)
+    return len(data)

@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""DEM step throughput in particle-steps/s on the 1e6-sphere sheared dense
+pack (log-normal radii, porosity ~0.40, x-y periodic, 20 kPa top wall, top
+layer sheared at 0.01 m/s, k_n = k_t = 1.16e9, gamma_n = 1e3, mu = 0.5,
+NC = 32), one pack per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                    [--impl ours|reference] [--n SPHERES]
+
+Our arm: W untimed steps, then K steps timed with CUDA events on the stream
+the library launches on (torch's current stream, handed to the library with
+sph_set_stream), bracketed by a barrier and torch.cuda.synchronize(); the
+max over ranks is reported.  The working set (~2.5 GB at 1e6 spheres) is
+far larger than L2, so no L2 flush is needed.  Per-kernel durations come
+from CUDA events recorded inside the last 8 step graphs of the timed region
+(sph_profile).  Then: live-contact count for the byte count, the roofline
+of the dominant kernel, the end-to-end time through the C ABI with host
+buffers, and (rank 0, N = 1) the CPU baseline: the reference's own step
+kernels compiled for the CPU (oracle/_ref) on a bounded sample.
+
+--impl reference times that CPU reference alone (rank 0; other ranks exit).
+
+One JSON line is printed by rank 0.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s @1e6 spheres, FP32-mixed vs FP64 on B200; adjoint/forward cost"
+UNIT = "particle-steps/s"
+WORKLOAD = ("sheared dense pack, 1e6 spheres: log-normal radii median 0.01 m sigma_ln 0.2 "
+            "clipped [0.005, 0.02], porosity 0.40, x-y periodic 1:1:0.5, top wall 20 kPa, "
+            "top layer +x 0.01 m/s, k_n=k_t=1.16e9, gamma_n=1e3, mu=0.5, NC=32")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler(object):
+    """nvidia-smi clocks and throttle reasons, sampled during the timed
+    region (100 ms period)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def make_scene(n, seed, device, sweeps=3000):
+    from sphere_b200 import scenes
+    return scenes.sheared_dense_pack(n=n, seed=seed, device=device, sweeps=sweeps)
+
+
+def interact_bytes(n, c, precision):
+    """Algorithmic bytes of one launch of the fused interact+integrate
+    kernel: per sphere, the compulsory state read and written once
+    (S_r = 184 B: x+r, vel+fixvel, angvel, angpos, xyzsum, acc0, angacc0;
+    S_w = 168 B: the same seven 3-vectors), per live directed contact its
+    partner id (4 B) and tangential history read and written (2 x 24 B)."""
+    if precision == "mixed":
+        return 220 * n + 52 * c
+    return 352 * n + 52 * c
+
+
+def step_bytes(n, c, precision):
+    """Whole-step algorithmic bytes: interact bytes + the cell sort
+    (16 B x 3 radix-equivalent passes per sphere)."""
+    return interact_bytes(n, c, precision) + 48 * n
+
+
+def cpu_reference_rate(s, nsteps, budget_s=25.0):
+    """Time the reference's own kernels on the CPU (oracle/_ref) on a
+    bounded sample: whole steps of the same scene, up to nsteps or budget_s
+    seconds.  Returns (particle-steps/s, steps, seconds, threads, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    kind = "reference" if O.available("ref") else "port"
+    which = "ref" if kind == "reference" else "oracle"
+    threads = os.cpu_count() or 1
+    run = O.CpuRun(s, which, nthreads=threads)
+    n = int(s.np[0])
+    t0 = time.perf_counter()
+    run.step(1)
+    done = 1
+    while done < nsteps and time.perf_counter() - t0 < budget_s:
+        run.step(1)
+        done += 1
+    dt = time.perf_counter() - t0
+    return n * done / dt, done, dt, threads, kind
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1000000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pack-sweeps", type=int, default=3000)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        s = make_scene(args.n, 0, local, args.pack_sweeps)
+        rate, done, secs, threads, kind = cpu_reference_rate(s, args.steps + args.warmup, 120.0)
+        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
+                "n_gpus": args.gpus, "steps": done, "warmup": 0,
+                "ms_per_step": secs / done * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "spheres": args.n},
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                                 "sample": "%d whole steps of the %d-sphere pack" % (done, args.n)},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    from sphere_b200.runner import Stepper, HostParticles
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    s = make_scene(args.n, rank, local, args.pack_sweeps)
+    n = int(s.np[0])
+    st = Stepper([s], precision=args.precision, length="reference", device=local)
+    stream = torch.cuda.current_stream()
+    st.set_stream(stream.cuda_stream)
+    st.upload()
+    st.step(args.warmup)
+
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    launches0 = st.kernel_launches()
+    st.profile(True)
+    torch.cuda.nvtx.range_push("timed")
+    start.record(stream)
+    st.step_async(args.steps)
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.nvtx.range_pop()
+    code = st.sync(raise_on_error=False)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = st.kernel_launches() - launches0
+    ms = start.elapsed_time(end)
+    kernels = st.profile_read()
+    st.profile(False)
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * n * args.steps / (ms_max / 1e3)
+    contacts = st.count_contacts()
+
+    # roofline of the dominant kernel
+    hbm, peak_kind = peaks()
+    t_int = kernels.get("k_interact")
+    b_int = interact_bytes(n, contacts, args.precision)
+    achieved = b_int / (t_int / 1e3) / 1e9 if t_int else None
+    roofline = {"bound": "hbm", "kernel": "k_interact", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm if achieved else None,
+                "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": b_int,
+                "kernel_ms": t_int}
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            tr = json.load(fh)
+        roofline["traffic"] = tr["k_interact_bytes_per_sphere"] * n
+        roofline["traffic_source"] = tr.get("source")
+    except Exception:
+        pass
+    st.close()
+
+    # end to end through the C ABI with host buffers: upload from pinned
+    # host memory, K steps each followed by a read of the box state (wall
+    # force/position, time), download of the final state
+    e2e = None
+    if rank == 0 or world > 1:
+        st2 = Stepper([s], precision=args.precision, length="reference", device=local)
+        st2.set_stream(stream.cuda_stream)
+        hp = HostParticles.from_sims([s])
+        for name in ("x", "xyzsum", "vel", "force", "angpos", "angvel", "torque", "es_dot", "es",
+                     "ev_dot", "ev", "p"):
+            a = getattr(hp, name)
+            pin = torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy()
+            pin[...] = a
+            setattr(hp, name, pin)
+        st2.hp = hp
+        import ctypes as C
+        from sphere_b200 import _abi
+        h2d = sum(getattr(hp, k).nbytes for k in ("x", "xyzsum", "vel", "force", "angpos",
+                                                   "angvel", "torque", "es_dot", "es", "ev_dot",
+                                                   "ev", "p"))
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        ps = hp.struct()
+        st2._check(st2.lib.sph_upload(st2.h, C.byref(ps), None), "sph_upload")
+        boxbuf = (_abi.SphBox * 1)()
+        for _ in range(args.steps):
+            st2._check(st2.lib.sph_step(st2.h, 1), "sph_step")
+            st2._check(st2.lib.sph_get_boxes(st2.h, boxbuf), "sph_get_boxes")
+        out = HostParticles(n)
+        po = out.struct()
+        st2._check(st2.lib.sph_download(st2.h, C.byref(po), None), "sph_download")
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter() - t0
+        barrier()
+        if world > 1:
+            t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        d2h = h2d + C.sizeof(_abi.SphBox) * args.steps
+        e2e = {"value": world * n * args.steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "seconds": t_e2e,
+               "what": "sph_upload from pinned host arrays + K x (sph_step + sph_get_boxes) + "
+                       "sph_download"}
+        st2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, done, secs, threads, kind = cpu_reference_rate(s, 50, 25.0)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": "%d whole steps of the same %d-sphere pack (%.1f s)" % (done, n, secs)}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+        "data": "synthetic (seeded GPU-relaxed pack per rank)",
+        "config": {"workload": WORKLOAD, "spheres_per_gpu": n, "precision": args.precision,
+                   "length_mode": "reference", "l2": "working set > L2 (no flush needed)",
+                   "parallelism": "replicas only (one independent pack per GPU)"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "live_contacts": contacts,
+        "kernel_ms": kernels,
+        "step_gbs": step_bytes(n, contacts, args.precision) / (ms_max / args.steps / 1e3) / 1e9,
+        "device_status": code,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -152,6 +152,27 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b);
  * a step that overflowed a contact list is still completed. */
 int sph_step(SphHandle *h, uint64_t nsteps);
 
+/* As sph_step, without waiting: the steps are queued on the handle's stream
+ * and their device errors are reported by the next sph_sync or sph_step. */
+int sph_step_async(SphHandle *h, uint64_t nsteps);
+
+/* Wait for queued steps; returns the first device error they raised. */
+int sph_sync(SphHandle *h);
+
+/* Run the steps on `cuda_stream` (a cudaStream_t of the handle's device)
+ * instead of the handle's own stream; NULL restores the own stream. */
+int sph_set_stream(SphHandle *h, void *cuda_stream);
+
+/* Per-kernel timing, the counterpart of the reference's PROFILING
+ * breakdown (src/device.cu:947-987, 2711-2808).  While enabled, steps run
+ * from a ring of 8 captured step graphs that record CUDA events between
+ * kernels; sph_profile_read returns the mean milliseconds per kernel group
+ * over the (up to 8) most recent steps in ms[] and the groups' names as a
+ * comma-separated list in names. */
+int sph_profile(SphHandle *h, int enable);
+int sph_profile_read(SphHandle *h, char *names, size_t names_len, double *ms,
+                     int max_kernels, int *nkernels);
+
 /* Output-cadence driver for a single box, replacing the loop control of
  * src/device.cu:1031, 2536-2537 and 2569: runs steps while
  * *time_current <= time_total, adding dt to *time_current and *filetimeclock
@@ -195,12 +216,26 @@ int sph_count_contacts(SphHandle *h, uint64_t *ncontacts);
 /* Kernel launches issued by this handle since creation. */
 uint64_t sph_kernel_launches(const SphHandle *h);
 
+/* Scene preparation (no counterpart in the reference's step; it stands in
+ * for the long gravity-settling runs sphere's scripts use to make dense
+ * packs): `sweeps` Jacobi sweeps of geometric overlap removal on the
+ * uploaded positions -- each overlapping pair is pushed apart by alpha/2 of
+ * its overlap per sweep, spheres are kept between the floor and z_top.
+ * *max_overlap receives the largest overlap of the last sweep.  Velocities
+ * and contact lists are untouched; download the positions afterwards. */
+int sph_relax(SphHandle *h, uint32_t sweeps, double alpha, double z_top,
+              double *max_overlap);
+
 /* Message of the last error on this handle (or a static message for a NULL
  * handle).  Returns the number of characters written. */
 int sph_last_error(const SphHandle *h, char *buf, size_t n);
 const char *sph_status_string(int status);
 
 void sph_destroy(SphHandle *h);
+
+/* sizeof of SphParams, SphGrid, SphWalls, SphBox, SphParticles, SphBonds
+ * (6 entries), for binding checks. */
+int sph_struct_sizes(uint64_t *sizes);
 
 #ifdef __cplusplus
 }

@@ -121,6 +121,8 @@ static int find_dist_mod(const Ctx *c, int t[3], v3 *dm)
         if (t[1] < 0 || t[1] >= (int)c->num[1]) return -1;
     }
     if (t[2] < 0 || t[2] >= (int)c->num[2]) return -1;
+    /* a particle far outside the grid can still be outside after one wrap */
+    if (t[0] < 0 || t[0] >= (int)c->num[0] || t[1] < 0 || t[1] >= (int)c->num[1]) return -1;
     return 0;
 }
 

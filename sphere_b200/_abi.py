@@ -198,9 +198,17 @@ def load_library():
     lib.sph_destroy.restype = None
     lib.sph_struct_sizes.argtypes = [C.POINTER(C.c_uint64)]
     lib.sph_struct_sizes.restype = C.c_int
+    lib.sph_relax.argtypes = [H, C.c_uint32, C.c_double, C.c_double, _dp]
+    lib.sph_relax.restype = C.c_int
+    lib.sph_step_async.argtypes = [H, C.c_uint64]
+    lib.sph_sync.argtypes = [H]
+    lib.sph_set_stream.argtypes = [H, C.c_void_p]
+    lib.sph_profile.argtypes = [H, C.c_int]
+    lib.sph_profile_read.argtypes = [H, C.c_char_p, C.c_size_t, _dp, C.c_int, C.POINTER(C.c_int)]
     for name in ("sph_create", "sph_upload", "sph_step", "sph_advance", "sph_download",
                  "sph_get_boxes", "sph_get_contacts", "sph_get_sort", "sph_count_contacts",
-                 "sph_last_error"):
+                 "sph_last_error", "sph_step_async", "sph_sync", "sph_set_stream",
+                 "sph_profile", "sph_profile_read"):
         getattr(lib, name).restype = C.c_int
     _LIB = lib
     return lib

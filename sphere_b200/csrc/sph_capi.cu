@@ -1,0 +1,844 @@
+// sph_capi.cu -- C ABI of include/sphere_b200.h: handle, device memory,
+// host<->device transfers and the CUDA-graph step driver.
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sph_device.cuh"
+#include "sph_internal.h"
+
+using sph::DevBox;
+using sph::StepArgs;
+using sph::StepConfig;
+
+namespace sph {
+int count_live_slots(const StepArgs &A, cudaStream_t st, unsigned long long *d_count,
+                     uint64_t *launches);
+int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
+                      uint64_t *launches, Prof *prof);
+int relax_sweep(const StepArgs &A, cudaStream_t st, double alpha, double z_top,
+                unsigned long long *d_max, uint64_t *launches);
+}
+
+struct SphHandle {
+    int device = 0;
+    cudaStream_t stream = nullptr;   // stream the steps run on (own or caller's)
+    cudaStream_t own = nullptr;      // stream created by the handle (graph capture)
+    int precision = SPH_PREC_FP64;
+    int lenmode = SPH_LEN_REFERENCE;
+    std::vector<SphBox> boxes;       // as created
+    std::vector<DevBox> dbox;        // host image of the device box table
+    std::vector<double> t_host;      // host mirror of each box's time.current
+    uint32_t nbox = 0;
+    uint64_t ntot = 0, ncells = 0, nbonds = 0, npartials = 0;
+    StepArgs A{};
+    StepConfig cfg{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    uint64_t launches_per_step = 0;
+    uint64_t launches = 0;
+    // profiling: a ring of captured step graphs with event-record nodes
+    static constexpr int PR = 8;
+    bool prof_on = false;
+    cudaGraph_t pgraph[PR] = {};
+    cudaGraphExec_t pexec[PR] = {};
+    sph::Prof prof[PR];
+    bool prof_events = false;
+    int pnext = 0;
+    uint64_t pcount = 0;
+    bool uploaded = false;
+    std::string err;
+    std::vector<void *> allocs;
+    unsigned long long *d_count = nullptr;
+};
+
+static int fail(SphHandle *h, int code, const std::string &msg)
+{
+    if (h) h->err = msg;
+    return code;
+}
+
+#define CUDA_TRY(h, call)                                                                   \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail((h), e_ == cudaErrorMemoryAllocation ? SPH_ERR_NOMEM : SPH_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                \
+    } while (0)
+
+template <typename T>
+static int dalloc(SphHandle *h, T **p, uint64_t count)
+{
+    if (count == 0) count = 1;
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, sizeof(T) * count);
+    if (e != cudaSuccess)
+        return fail(h, SPH_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    h->allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return SPH_OK;
+}
+
+// src/sphere.cpp:145-345 checkValues, parts that do not need particle data.
+static int check_box(SphHandle *h, const SphBox &b, uint32_t k)
+{
+    char buf[256];
+    const SphGrid &g = b.grid;
+    if (g.origo[0] < 0.0 || g.origo[1] < 0.0 || g.origo[2] < 0.0) {
+        snprintf(buf, sizeof buf, "box %u: negative values in grid.origo", k);
+        return fail(h, SPH_ERR_INPUT, buf);
+    }
+    if (!(g.L[0] > 0.0) || !(g.L[1] > 0.0) || !(g.L[2] > 0.0)) {
+        snprintf(buf, sizeof buf, "box %u: grid.L must be positive", k);
+        return fail(h, SPH_ERR_INPUT, buf);
+    }
+    if (g.num[0] == 0 || g.num[1] == 0 || g.num[2] == 0) {
+        snprintf(buf, sizeof buf, "box %u: grid.num must be positive", k);
+        return fail(h, SPH_ERR_INPUT, buf);
+    }
+    if (g.periodic == 2 && g.num[0] < 3) {
+        snprintf(buf, sizeof buf, "box %u: periodic x needs at least 3 cells along x", k);
+        return fail(h, SPH_ERR_INPUT, buf);
+    }
+    if (g.periodic == 1 && (g.num[0] < 3 || g.num[1] < 3)) {
+        snprintf(buf, sizeof buf, "box %u: periodic x/y needs at least 3 cells along x and y", k);
+        return fail(h, SPH_ERR_INPUT, buf);
+    }
+    if (!(b.params.k_n > 0.0)) return fail(h, SPH_ERR_INPUT, "k_n must be positive");
+    if (b.params.E < 0.0) return fail(h, SPH_ERR_INPUT, "E must not be negative");
+    if (!(b.params.rho > 0.0)) return fail(h, SPH_ERR_INPUT, "rho must be positive");
+    if (b.params.contactmodel < 1 || b.params.contactmodel > 3)
+        return fail(h, SPH_ERR_INPUT, "contact model must be 1, 2 or 3");
+    if (b.walls.nw > SPH_MAXWALLS) return fail(h, SPH_ERR_INPUT, "nw exceeds MAXWALLS (6)");
+    if (!(b.dt > 0.0)) return fail(h, SPH_ERR_INPUT, "time.dt must be positive");
+    return SPH_OK;
+}
+
+static void init_dev_box(DevBox &d, const SphBox &b)
+{
+    memset(&d, 0, sizeof d);
+    d.P = b.params;
+    for (int k = 0; k < 3; ++k) {
+        d.origo[k] = b.grid.origo[k];
+        d.L[k] = b.grid.L[k];
+        d.num[k] = b.grid.num[k];
+    }
+    d.periodic = b.grid.periodic;
+    d.adaptive = b.grid.adaptive;
+    d.np = b.np;
+    d.nb0 = b.nb0;
+    d.nblocks = (b.np + 255) / 256;
+    d.nw = b.walls.nw;
+    for (uint32_t w = 0; w < SPH_MAXWALLS; ++w) {
+        d.wmode[w] = b.walls.wmode[w];
+        for (int k = 0; k < 4; ++k) {
+            d.wnx[w][k] = b.walls.nx[w][k];
+            d.wmvfd[w][k] = b.walls.mvfd[w][k];
+        }
+        d.wacc[w] = 0.0;
+    }
+    d.tau_x = b.walls.tau_x;
+    d.tau_eff_x = 0.0;
+    d.dt = b.dt;
+    d.t_current = b.t_current;
+    d.iter = 0;
+    // device.cu:994 and 2455-2462: velocity-step state of the first step
+    d.velocity_state = 1;
+    d.change_velocity_state = 0;
+    if (d.t_current >= 10.0 && d.t_current < 15.0) {
+        d.change_velocity_state = 1;
+        d.velocity_state = 2;
+    }
+    // device.cu:1050-1052: adaptive grid height of the first step
+    d.L2_out = d.L[2];
+    if (d.adaptive == 1 && d.nw > 0) d.L[2] = d.wnx[0][3];
+}
+
+extern "C" {
+
+int sph_struct_sizes(uint64_t *sizes)
+{
+    if (!sizes) return SPH_ERR_INPUT;
+    sizes[0] = sizeof(SphParams);
+    sizes[1] = sizeof(SphGrid);
+    sizes[2] = sizeof(SphWalls);
+    sizes[3] = sizeof(SphBox);
+    sizes[4] = sizeof(SphParticles);
+    sizes[5] = sizeof(SphBonds);
+    return SPH_OK;
+}
+
+const char *sph_status_string(int status)
+{
+    switch (status) {
+    case SPH_OK: return "ok";
+    case SPH_ERR_INPUT: return "invalid input";
+    case SPH_ERR_CUDA: return "CUDA error";
+    case SPH_ERR_NC_OVERFLOW: return "a particle had more contacts than the contact list holds (NC = 32)";
+    case SPH_ERR_OUT_OF_GRID: return "a particle left the computational grid";
+    case SPH_ERR_NAN: return "a particle position is not finite";
+    case SPH_ERR_NOMEM: return "out of memory";
+    case SPH_ERR_STATE: return "call out of order";
+    case SPH_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+    }
+}
+
+int sph_last_error(const SphHandle *h, char *buf, size_t n)
+{
+    const char *m = h ? h->err.c_str() : "no handle";
+    if (!buf || n == 0) return 0;
+    size_t k = strlen(m);
+    if (k >= n) k = n - 1;
+    memcpy(buf, m, k);
+    buf[k] = 0;
+    return (int)k;
+}
+
+void sph_destroy(SphHandle *h)
+{
+    if (!h) return;
+    if (h->device >= 0) cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    for (int r = 0; r < SphHandle::PR; ++r) {
+        if (h->pexec[r]) cudaGraphExecDestroy(h->pexec[r]);
+        if (h->pgraph[r]) cudaGraphDestroy(h->pgraph[r]);
+        if (h->prof_events)
+            for (int k = 0; k <= sph::Prof::MAX; ++k) cudaEventDestroy(h->prof[r].ev[k]);
+    }
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->own) cudaStreamDestroy(h->own);
+    delete h;
+}
+
+int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_mode, int device,
+               SphHandle **out)
+{
+    if (!out) return SPH_ERR_INPUT;
+    *out = nullptr;
+    SphHandle *h = new SphHandle();
+    int st = SPH_OK;
+    auto bail = [&](int code) {
+        sph_destroy(h);
+        return code;
+    };
+    if (!boxes || nboxes == 0) return bail(SPH_ERR_INPUT);
+    if (precision != SPH_PREC_FP64 && precision != SPH_PREC_MIXED) return bail(SPH_ERR_INPUT);
+    if (precision == SPH_PREC_MIXED &&
+        sph::launch_step_mixed(StepArgs{}, StepConfig{}, nullptr, nullptr, nullptr) == SPH_ERR_UNSUPPORTED)
+        return bail(SPH_ERR_UNSUPPORTED);
+    if (length_mode != SPH_LEN_REFERENCE && length_mode != SPH_LEN_FP64) return bail(SPH_ERR_INPUT);
+    h->precision = precision;
+    h->lenmode = length_mode;
+    h->nbox = nboxes;
+    h->boxes.assign(boxes, boxes + nboxes);
+    h->dbox.resize(nboxes);
+    h->t_host.resize(nboxes);
+    bool any_walls = false, unfused = false;
+    uint64_t pb = 0, cb = 0, bb = 0, qb = 0;
+    for (uint32_t k = 0; k < nboxes; ++k) {
+        if ((st = check_box(h, boxes[k], k)) != SPH_OK) {
+            fprintf(stderr, "sphere_b200: %s\n", h->err.c_str());
+            return bail(st);
+        }
+        DevBox &d = h->dbox[k];
+        init_dev_box(d, boxes[k]);
+        d.p_base = (uint32_t)pb;
+        d.cell_base = (uint32_t)cb;
+        d.b_base = (uint32_t)bb;
+        d.part_base = (uint32_t)qb;
+        pb += boxes[k].np;
+        cb += (uint64_t)boxes[k].grid.num[0] * boxes[k].grid.num[1] * boxes[k].grid.num[2];
+        bb += boxes[k].nb0;
+        qb += d.nblocks;
+        if (boxes[k].walls.nw > 0) any_walls = true;
+        if (boxes[k].walls.nw > 0 && boxes[k].walls.wmode[0] == 3) unfused = true;
+        h->t_host[k] = boxes[k].t_current;
+    }
+    h->ntot = pb;
+    h->ncells = cb;
+    h->nbonds = bb;
+    h->npartials = qb;
+    if (pb >= sph::ID_MASK) return bail(SPH_ERR_UNSUPPORTED);
+    if (cb >= 0xffffffffull || cb > 4096ull * 4096ull) return bail(SPH_ERR_UNSUPPORTED);
+    h->cfg.lenmode = length_mode;
+    h->cfg.unfused = unfused;
+    h->cfg.any_walls = any_walls;
+
+    if (device >= 0) {
+        if (cudaSetDevice(device) != cudaSuccess) return bail(SPH_ERR_CUDA);
+        h->device = device;
+    } else {
+        cudaGetDevice(&h->device);
+    }
+    if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(SPH_ERR_CUDA);
+    h->stream = h->own;
+
+    StepArgs &A = h->A;
+    A.nboxes = nboxes;
+    A.ntot = (uint32_t)h->ntot;
+    A.ncells = h->ncells;
+    A.nbonds = (uint32_t)h->nbonds;
+    A.npartials = (uint32_t)h->npartials;
+    const uint64_t n = h->ntot, nb = h->nbonds;
+    uint32_t *box_of = nullptr, *part_owner = nullptr, *bond_box = nullptr, *bcsr_off = nullptr,
+             *bcsr_ent = nullptr;
+    const uint32_t scan_blocks = (uint32_t)((h->ncells + 4095) / 4096);
+    if ((st = dalloc(h, &A.boxes, nboxes)) || (st = dalloc(h, &A.x, n)) ||
+        (st = dalloc(h, &A.vel, n)) || (st = dalloc(h, &A.angvel, n)) ||
+        (st = dalloc(h, &A.angpos, n)) || (st = dalloc(h, &A.xyzsum, n)) ||
+        (st = dalloc(h, &A.acc, n)) || (st = dalloc(h, &A.angacc, n)) ||
+        (st = dalloc(h, &A.force, n)) || (st = dalloc(h, &A.torque, n)) ||
+        (st = dalloc(h, &A.es_dot, n)) || (st = dalloc(h, &A.es, n)) ||
+        (st = dalloc(h, &A.ev_dot, n)) || (st = dalloc(h, &A.ev, n)) ||
+        (st = dalloc(h, &A.p, n)) || (st = dalloc(h, &box_of, n)) ||
+        (st = dalloc(h, &A.cell_id, n)) || (st = dalloc(h, &A.local_off, n)) ||
+        (st = dalloc(h, &A.cell_count, h->ncells)) || (st = dalloc(h, &A.cell_off, h->ncells + 1)) ||
+        (st = dalloc(h, &A.scan_tmp, scan_blocks + 1)) || (st = dalloc(h, &A.perm, n)) ||
+        (st = dalloc(h, &A.rank, n)) || (st = dalloc(h, &A.xs, n)) || (st = dalloc(h, &A.vs, n)) ||
+        (st = dalloc(h, &A.ws, n)) || (st = dalloc(h, &A.slots, n * sph::NC)) ||
+        (st = dalloc(h, &A.hist, n * sph::NC)) || (st = dalloc(h, &A.wf_pp, n)) ||
+        (st = dalloc(h, &A.wall_partial, h->npartials)) || (st = dalloc(h, &A.tau_pp, n)) ||
+        (st = dalloc(h, &A.tau_partial, h->npartials)) ||
+        (st = dalloc(h, &part_owner, h->npartials)) || (st = dalloc(h, &A.bonds, nb)) ||
+        (st = dalloc(h, &A.bdelta, nb)) || (st = dalloc(h, &A.bomega, nb)) ||
+        (st = dalloc(h, &A.bf, nb)) || (st = dalloc(h, &A.bt, nb)) ||
+        (st = dalloc(h, &A.bbroken, nb)) || (st = dalloc(h, &bond_box, nb)) ||
+        (st = dalloc(h, &bcsr_off, n + 1)) || (st = dalloc(h, &bcsr_ent, 2 * nb)) ||
+        (st = dalloc(h, &A.err, 1)) || (st = dalloc(h, &h->d_count, 1))) {
+        fprintf(stderr, "sphere_b200: %s\n", h->err.c_str());
+        return bail(st);
+    }
+    A.box_of = box_of;
+    A.part_owner = part_owner;
+    A.bond_box = bond_box;
+    A.bcsr_off = bcsr_off;
+    A.bcsr_ent = bcsr_ent;
+
+    std::vector<uint32_t> hb(n ? n : 1), hp(h->npartials ? h->npartials : 1), hbb(nb ? nb : 1);
+    for (uint32_t k = 0; k < nboxes; ++k) {
+        const DevBox &d = h->dbox[k];
+        for (uint32_t j = 0; j < d.np; ++j) hb[d.p_base + j] = k;
+        for (uint32_t j = 0; j < d.nblocks; ++j) hp[d.part_base + j] = k;
+        for (uint32_t j = 0; j < d.nb0; ++j) hbb[d.b_base + j] = k;
+    }
+    if (cudaMemcpy(box_of, hb.data(), sizeof(uint32_t) * (n ? n : 1), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(part_owner, hp.data(), sizeof(uint32_t) * hp.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(bond_box, hbb.data(), sizeof(uint32_t) * hbb.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(A.boxes, h->dbox.data(), sizeof(DevBox) * nboxes, cudaMemcpyHostToDevice) ||
+        cudaMemset(A.err, 0, sizeof(uint32_t)))
+        return bail(SPH_ERR_CUDA);
+    *out = h;
+    return SPH_OK;
+}
+
+static int check_particles(SphHandle *h, const SphParticles *p)
+{
+    char buf[256];
+    for (uint32_t k = 0; k < h->nbox; ++k) {
+        const DevBox &d = h->dbox[k];
+        const SphBox &b = h->boxes[k];
+        double zmax = 0.0;
+        for (uint32_t j = 0; j < d.np; ++j) {
+            const double *x = p->x + 4 * (size_t)(d.p_base + j);
+            const double *v = p->vel + 4 * (size_t)(d.p_base + j);
+            if (!(x[3] > 0.0)) {
+                snprintf(buf, sizeof buf, "box %u particle %u has a radius of %g m", k, j, x[3]);
+                return fail(h, SPH_ERR_INPUT, buf);
+            }
+            for (int c = 0; c < 4; ++c)
+                if (x[c] != x[c] || v[c] != v[c]) {
+                    snprintf(buf, sizeof buf, "box %u particle %u has NaN values", k, j);
+                    return fail(h, SPH_ERR_INPUT, buf);
+                }
+            if (x[0] < b.grid.origo[0] || x[1] < b.grid.origo[1] || x[2] < b.grid.origo[2] ||
+                x[0] > b.grid.L[0] || x[1] > b.grid.L[1] || x[2] > b.grid.L[2]) {
+                snprintf(buf, sizeof buf, "box %u particle %u is outside of the computational grid",
+                         k, j);
+                return fail(h, SPH_ERR_INPUT, buf);
+            }
+            if (x[2] > zmax) zmax = x[2];
+        }
+        if (b.walls.nw > 0 && b.walls.nx[0][3] < zmax) {
+            snprintf(buf, sizeof buf,
+                     "box %u: one or more particles have centres above the upper, dynamic wall", k);
+            return fail(h, SPH_ERR_INPUT, buf);
+        }
+    }
+    return SPH_OK;
+}
+
+static int put3(SphHandle *h, double4 *dst, const double *src, uint64_t n)
+{
+    std::vector<double4> tmp(n ? n : 1);
+    for (uint64_t i = 0; i < n; ++i)
+        tmp[i] = src ? make_double4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0)
+                     : make_double4(0.0, 0.0, 0.0, 0.0);
+    CUDA_TRY(h, cudaMemcpy(dst, tmp.data(), sizeof(double4) * (n ? n : 1), cudaMemcpyHostToDevice));
+    return SPH_OK;
+}
+
+static int get3(SphHandle *h, double *dst, const double4 *src, uint64_t n)
+{
+    if (!dst) return SPH_OK;
+    std::vector<double4> tmp(n ? n : 1);
+    CUDA_TRY(h, cudaMemcpy(tmp.data(), src, sizeof(double4) * (n ? n : 1), cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < n; ++i) {
+        dst[3 * i] = tmp[i].x;
+        dst[3 * i + 1] = tmp[i].y;
+        dst[3 * i + 2] = tmp[i].z;
+    }
+    return SPH_OK;
+}
+
+static int put1(SphHandle *h, double *dst, const double *src, uint64_t n)
+{
+    if (src) CUDA_TRY(h, cudaMemcpy(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice));
+    else CUDA_TRY(h, cudaMemset(dst, 0, sizeof(double) * (n ? n : 1)));
+    return SPH_OK;
+}
+
+int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
+{
+    if (!h || !p) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    const uint64_t n = h->ntot, nb = h->nbonds;
+    if (n > 0 && (!p->x || !p->vel)) return fail(h, SPH_ERR_INPUT, "x and vel are required");
+    if (nb > 0 && (!b || !b->pairs)) return fail(h, SPH_ERR_INPUT, "bond pairs are required");
+    int st;
+    if ((st = check_particles(h, p)) != SPH_OK) return st;
+    StepArgs &A = h->A;
+    cudaStreamSynchronize(h->stream);
+    if (n > 0) {
+        CUDA_TRY(h, cudaMemcpy(A.x, p->x, sizeof(double4) * n, cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(A.vel, p->vel, sizeof(double4) * n, cudaMemcpyHostToDevice));
+    }
+    if ((st = put3(h, A.xyzsum, p->xyzsum, n)) || (st = put3(h, A.force, p->force, n)) ||
+        (st = put3(h, A.angpos, p->angpos, n)) || (st = put3(h, A.angvel, p->angvel, n)) ||
+        (st = put3(h, A.torque, p->torque, n)) || (st = put1(h, A.es_dot, p->es_dot, n)) ||
+        (st = put1(h, A.es, p->es, n)) || (st = put1(h, A.ev_dot, p->ev_dot, n)) ||
+        (st = put1(h, A.ev, p->ev, n)) || (st = put1(h, A.p, p->p, n)))
+        return st;
+    CUDA_TRY(h, cudaMemset(A.acc, 0, sizeof(double4) * (n ? n : 1)));
+    CUDA_TRY(h, cudaMemset(A.angacc, 0, sizeof(double4) * (n ? n : 1)));
+    CUDA_TRY(h, cudaMemset(A.wf_pp, 0, sizeof(double) * (n ? n : 1)));
+    CUDA_TRY(h, cudaMemset(A.tau_pp, 0, sizeof(double) * (n ? n : 1)));
+    // src/device.cu:458-464: empty contact lists; histories start at zero
+    CUDA_TRY(h, cudaMemset(A.slots, 0xff, sizeof(uint32_t) * (n ? n : 1) * sph::NC));
+    CUDA_TRY(h, cudaMemset(A.hist, 0, sizeof(double4) * (n ? n : 1) * sph::NC));
+
+    // bonds (local indexes) and the per-particle list of bond endpoints in
+    // ascending bond order
+    std::vector<uint32_t> cnt(n + 1, 0);
+    if (nb > 0) {
+        std::vector<uint2> pairs(nb);
+        std::vector<double4> dl(nb), om(nb);
+        for (uint32_t k = 0; k < h->nbox; ++k) {
+            const DevBox &d = h->dbox[k];
+            for (uint32_t j = 0; j < d.nb0; ++j) {
+                const uint64_t q = d.b_base + j;
+                pairs[q] = make_uint2(b->pairs[2 * q], b->pairs[2 * q + 1]);
+                dl[q] = make_double4(b->delta_t ? b->delta_t[3 * q] : 0.0,
+                                     b->delta_t ? b->delta_t[3 * q + 1] : 0.0,
+                                     b->delta_t ? b->delta_t[3 * q + 2] : 0.0,
+                                     b->delta_n ? b->delta_n[q] : 0.0);
+                om[q] = make_double4(b->omega_t ? b->omega_t[3 * q] : 0.0,
+                                     b->omega_t ? b->omega_t[3 * q + 1] : 0.0,
+                                     b->omega_t ? b->omega_t[3 * q + 2] : 0.0,
+                                     b->omega_n ? b->omega_n[q] : 0.0);
+                if (pairs[q].x < d.np && pairs[q].y < d.np) {
+                    cnt[d.p_base + pairs[q].x + 1]++;
+                    cnt[d.p_base + pairs[q].y + 1]++;
+                }
+            }
+        }
+        for (uint64_t i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
+        std::vector<uint32_t> ent(cnt[n] ? cnt[n] : 1), fill(cnt.begin(), cnt.end() - 1);
+        for (uint32_t k = 0; k < h->nbox; ++k) {
+            const DevBox &d = h->dbox[k];
+            for (uint32_t j = 0; j < d.nb0; ++j) {
+                const uint32_t q = d.b_base + j;
+                if (pairs[q].x < d.np && pairs[q].y < d.np) {
+                    ent[fill[d.p_base + pairs[q].x]++] = (q << 1) | 0u;
+                    ent[fill[d.p_base + pairs[q].y]++] = (q << 1) | 1u;
+                }
+            }
+        }
+        CUDA_TRY(h, cudaMemcpy(A.bonds, pairs.data(), sizeof(uint2) * nb, cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(A.bdelta, dl.data(), sizeof(double4) * nb, cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(A.bomega, om.data(), sizeof(double4) * nb, cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemset(A.bbroken, 0, nb));
+        CUDA_TRY(h, cudaMemset(A.bf, 0, sizeof(double4) * nb));
+        CUDA_TRY(h, cudaMemset(A.bt, 0, sizeof(double4) * nb));
+        CUDA_TRY(h, cudaMemcpy((void *)A.bcsr_ent, ent.data(), sizeof(uint32_t) * ent.size(),
+                               cudaMemcpyHostToDevice));
+    }
+    CUDA_TRY(h, cudaMemcpy((void *)A.bcsr_off, cnt.data(), sizeof(uint32_t) * (n + 1),
+                           cudaMemcpyHostToDevice));
+    // a new run: time state from the boxes, TY3 iteration counter at zero
+    for (uint32_t k = 0; k < h->nbox; ++k) {
+        init_dev_box(h->dbox[k], h->boxes[k]);
+        h->dbox[k].p_base = 0;
+    }
+    {
+        uint64_t pb = 0, cb = 0, bb = 0, qb = 0;
+        for (uint32_t k = 0; k < h->nbox; ++k) {
+            DevBox &d = h->dbox[k];
+            d.p_base = (uint32_t)pb;
+            d.cell_base = (uint32_t)cb;
+            d.b_base = (uint32_t)bb;
+            d.part_base = (uint32_t)qb;
+            pb += d.np;
+            cb += (uint64_t)d.num[0] * d.num[1] * d.num[2];
+            bb += d.nb0;
+            qb += d.nblocks;
+            h->t_host[k] = h->boxes[k].t_current;
+        }
+    }
+    CUDA_TRY(h, cudaMemcpy(A.boxes, h->dbox.data(), sizeof(DevBox) * h->nbox, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemset(A.err, 0, sizeof(uint32_t)));
+    h->uploaded = true;
+    return SPH_OK;
+}
+
+// Capture one step (optionally with event-record nodes between kernels)
+// into a CUDA graph.
+static int capture_step(SphHandle *h, sph::Prof *prof, cudaGraph_t *g, cudaGraphExec_t *ge,
+                        uint64_t *nl)
+{
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    CUDA_TRY(h, cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
+    int st = h->precision == SPH_PREC_MIXED
+                 ? sph::launch_step_mixed(h->A, h->cfg, h->own, nl, prof)
+                 : sph::launch_step(h->A, h->cfg, h->own, nl, prof);
+    cudaError_t e = cudaStreamEndCapture(h->own, g);
+    if (st != SPH_OK) return fail(h, st, "step launch failed during graph capture");
+    if (e != cudaSuccess) return fail(h, SPH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    CUDA_TRY(h, cudaGraphInstantiate(ge, *g, 0));
+    return SPH_OK;
+}
+
+static int build_graph(SphHandle *h)
+{
+    if (h->gexec) return SPH_OK;
+    uint64_t nl = 0;
+    int st = capture_step(h, nullptr, &h->graph, &h->gexec, &nl);
+    if (st != SPH_OK) return st;
+    h->launches_per_step = nl;
+    return SPH_OK;
+}
+
+static int build_prof_graphs(SphHandle *h)
+{
+    if (h->pexec[0]) return SPH_OK;
+    if (!h->prof_events) {
+        for (int r = 0; r < SphHandle::PR; ++r)
+            for (int k = 0; k <= sph::Prof::MAX; ++k) CUDA_TRY(h, cudaEventCreate(&h->prof[r].ev[k]));
+        h->prof_events = true;
+    }
+    for (int r = 0; r < SphHandle::PR; ++r) {
+        uint64_t nl = 0;
+        int st = capture_step(h, &h->prof[r], &h->pgraph[r], &h->pexec[r], &nl);
+        if (st != SPH_OK) return st;
+    }
+    return SPH_OK;
+}
+
+// Launch one step graph on the active stream (a profiled one when profiling).
+static int launch_one(SphHandle *h)
+{
+    if (h->prof_on) {
+        CUDA_TRY(h, cudaGraphLaunch(h->pexec[h->pnext], h->stream));
+        h->pnext = (h->pnext + 1) % SphHandle::PR;
+        h->pcount++;
+    } else {
+        CUDA_TRY(h, cudaGraphLaunch(h->gexec, h->stream));
+    }
+    for (uint32_t k = 0; k < h->nbox; ++k) h->t_host[k] += h->boxes[k].dt;
+    return SPH_OK;
+}
+
+static int collect_errors(SphHandle *h)
+{
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    uint32_t bits = 0;
+    CUDA_TRY(h, cudaMemcpy(&bits, h->A.err, sizeof bits, cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemset(h->A.err, 0, sizeof(uint32_t)));
+    if (!bits) return SPH_OK;
+    static const int order[] = {SPH_ERR_NAN, SPH_ERR_OUT_OF_GRID, SPH_ERR_INPUT, SPH_ERR_NC_OVERFLOW};
+    for (int code : order)
+        if (bits & (1u << code)) return fail(h, code, sph_status_string(code));
+    return fail(h, SPH_ERR_CUDA, "unknown device error bits");
+}
+
+int sph_step(SphHandle *h, uint64_t nsteps)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_step before sph_upload");
+    int st = sph_step_async(h, nsteps);
+    if (st != SPH_OK) return st;
+    return collect_errors(h);
+}
+
+int sph_step_async(SphHandle *h, uint64_t nsteps)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_step_async before sph_upload");
+    cudaSetDevice(h->device);
+    int st;
+    if ((st = build_graph(h)) != SPH_OK) return st;
+    for (uint64_t s = 0; s < nsteps; ++s)
+        if ((st = launch_one(h)) != SPH_OK) return st;
+    h->launches += nsteps * h->launches_per_step;
+    return SPH_OK;
+}
+
+int sph_profile(SphHandle *h, int enable)
+{
+    if (!h) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    if (enable) {
+        int st;
+        if ((st = build_graph(h)) != SPH_OK || (st = build_prof_graphs(h)) != SPH_OK) return st;
+        h->pnext = 0;
+        h->pcount = 0;
+    }
+    h->prof_on = enable != 0;
+    return SPH_OK;
+}
+
+int sph_profile_read(SphHandle *h, char *names, size_t names_len, double *ms, int max_kernels,
+                     int *nkernels)
+{
+    if (!h || !ms || !nkernels) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const int nr = (int)(h->pcount < (uint64_t)SphHandle::PR ? h->pcount : SphHandle::PR);
+    if (nr == 0) return fail(h, SPH_ERR_STATE, "no profiled steps ran");
+    const int n = h->prof[0].n;
+    std::string all;
+    for (int k = 0; k < n && k < max_kernels; ++k) {
+        double acc = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            float t = 0.f;
+            CUDA_TRY(h, cudaEventElapsedTime(&t, h->prof[r].ev[k], h->prof[r].ev[k + 1]));
+            acc += t;
+        }
+        ms[k] = acc / nr;
+        if (k) all += ",";
+        all += h->prof[0].name[k];
+    }
+    *nkernels = n < max_kernels ? n : max_kernels;
+    if (names && names_len) {
+        size_t m = all.size() < names_len - 1 ? all.size() : names_len - 1;
+        memcpy(names, all.data(), m);
+        names[m] = 0;
+    }
+    return SPH_OK;
+}
+
+int sph_sync(SphHandle *h)
+{
+    if (!h) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    return collect_errors(h);
+}
+
+int sph_set_stream(SphHandle *h, void *stream)
+{
+    if (!h) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own;
+    return SPH_OK;
+}
+
+int sph_advance(SphHandle *h, double time_total, double file_dt, double *time_current,
+                double *filetimeclock, uint64_t max_steps, uint64_t *steps_done)
+{
+    if (!h || !time_current || !filetimeclock) return SPH_ERR_INPUT;
+    if (h->nbox != 1) return fail(h, SPH_ERR_UNSUPPORTED, "sph_advance drives a single box");
+    if (*time_current != h->t_host[0])
+        return fail(h, SPH_ERR_STATE, "time_current differs from the handle's time");
+    const double dt = h->boxes[0].dt;
+    double cur = *time_current, ftc = *filetimeclock;
+    uint64_t k = 0;
+    // device.cu:1031 loop condition, :2536-2537 increments, :2569 output test
+    while (cur <= time_total && k < max_steps) {
+        cur += dt;
+        ftc += dt;
+        ++k;
+        if (ftc >= file_dt) break;
+    }
+    int st = sph_step(h, k);
+    *time_current = cur;
+    *filetimeclock = ftc;
+    if (steps_done) *steps_done = k;
+    return st;
+}
+
+int sph_download(SphHandle *h, SphParticles *p, SphBonds *b)
+{
+    if (!h) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const uint64_t n = h->ntot, nb = h->nbonds;
+    const StepArgs &A = h->A;
+    int st;
+    if (p) {
+        if (p->x && n) CUDA_TRY(h, cudaMemcpy(p->x, A.x, sizeof(double4) * n, cudaMemcpyDeviceToHost));
+        if (p->vel && n)
+            CUDA_TRY(h, cudaMemcpy(p->vel, A.vel, sizeof(double4) * n, cudaMemcpyDeviceToHost));
+        if ((st = get3(h, p->xyzsum, A.xyzsum, n)) || (st = get3(h, p->force, A.force, n)) ||
+            (st = get3(h, p->angpos, A.angpos, n)) || (st = get3(h, p->angvel, A.angvel, n)) ||
+            (st = get3(h, p->torque, A.torque, n)))
+            return st;
+        double *dst[5] = {p->es_dot, p->es, p->ev_dot, p->ev, p->p};
+        double *src[5] = {A.es_dot, A.es, A.ev_dot, A.ev, A.p};
+        for (int k = 0; k < 5; ++k)
+            if (dst[k] && n)
+                CUDA_TRY(h, cudaMemcpy(dst[k], src[k], sizeof(double) * n, cudaMemcpyDeviceToHost));
+    }
+    if (b && nb) {
+        std::vector<uint2> pairs(nb);
+        std::vector<double4> dl(nb), om(nb);
+        CUDA_TRY(h, cudaMemcpy(pairs.data(), A.bonds, sizeof(uint2) * nb, cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, cudaMemcpy(dl.data(), A.bdelta, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, cudaMemcpy(om.data(), A.bomega, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
+        for (uint64_t q = 0; q < nb; ++q) {
+            if (b->pairs) { b->pairs[2 * q] = pairs[q].x; b->pairs[2 * q + 1] = pairs[q].y; }
+            if (b->delta_n) b->delta_n[q] = dl[q].w;
+            if (b->delta_t) { b->delta_t[3 * q] = dl[q].x; b->delta_t[3 * q + 1] = dl[q].y; b->delta_t[3 * q + 2] = dl[q].z; }
+            if (b->omega_n) b->omega_n[q] = om[q].w;
+            if (b->omega_t) { b->omega_t[3 * q] = om[q].x; b->omega_t[3 * q + 1] = om[q].y; b->omega_t[3 * q + 2] = om[q].z; }
+        }
+    }
+    return SPH_OK;
+}
+
+int sph_get_boxes(SphHandle *h, SphBox *boxes)
+{
+    if (!h || !boxes) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    std::vector<DevBox> d(h->nbox);
+    CUDA_TRY(h, cudaMemcpy(d.data(), h->A.boxes, sizeof(DevBox) * h->nbox, cudaMemcpyDeviceToHost));
+    for (uint32_t k = 0; k < h->nbox; ++k) {
+        SphBox b = h->boxes[k];
+        for (int c = 0; c < 2; ++c) b.grid.L[c] = d[k].L[c];
+        b.grid.L[2] = d[k].L2_out;
+        for (uint32_t w = 0; w < SPH_MAXWALLS; ++w)
+            for (int c = 0; c < 4; ++c) {
+                b.walls.nx[w][c] = d[k].wnx[w][c];
+                b.walls.mvfd[w][c] = d[k].wmvfd[w][c];
+            }
+        b.t_current = d[k].t_current;
+        boxes[k] = b;
+    }
+    return SPH_OK;
+}
+
+int sph_get_contacts(SphHandle *h, uint32_t *contacts, double *delta_t, double *distmod)
+{
+    if (!h) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const uint64_t n = h->ntot, ns = n * sph::NC;
+    if (n == 0) return SPH_OK;
+    std::vector<uint32_t> w(ns);
+    std::vector<double4> x(n);
+    CUDA_TRY(h, cudaMemcpy(w.data(), h->A.slots, sizeof(uint32_t) * ns, cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(x.data(), h->A.x, sizeof(double4) * n, cudaMemcpyDeviceToHost));
+    if (delta_t)
+        CUDA_TRY(h, cudaMemcpy(delta_t, h->A.hist, sizeof(double4) * ns, cudaMemcpyDeviceToHost));
+    for (uint32_t k = 0; k < h->nbox; ++k) {
+        const DevBox &d = h->dbox[k];
+        for (uint64_t i = d.p_base; i < (uint64_t)d.p_base + d.np; ++i)
+            for (int s = 0; s < sph::NC; ++s) {
+                const uint64_t q = i * sph::NC + s;
+                const uint32_t v = w[q];
+                double dm[4] = {0.0, 0.0, 0.0, 0.0};
+                uint32_t partner = d.np;
+                if (v != sph::EMPTY) {
+                    const uint32_t g = v & sph::ID_MASK;
+                    partner = g - d.p_base;
+                    int sx = (int)((v >> sph::CODE_SHIFT) & 3u), sy = (int)((v >> (sph::CODE_SHIFT + 2)) & 3u);
+                    if (sx == 3) sx = -1;
+                    if (sy == 3) sy = -1;
+                    dm[0] = sx == 0 ? 0.0 : (sx > 0 ? d.L[0] : -d.L[0]);
+                    dm[1] = sy == 0 ? 0.0 : (sy > 0 ? d.L[1] : -d.L[1]);
+                    dm[3] = x[g].w;
+                }
+                if (contacts) contacts[q] = partner;
+                if (distmod)
+                    for (int c = 0; c < 4; ++c) distmod[4 * q + c] = dm[c];
+            }
+    }
+    return SPH_OK;
+}
+
+uint64_t sph_total_cells(const SphHandle *h) { return h ? h->ncells : 0; }
+
+int sph_get_sort(SphHandle *h, uint32_t *cell_id, uint32_t *perm, uint32_t *cell_start,
+                 uint32_t *cell_end)
+{
+    if (!h) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const uint64_t n = h->ntot, nc = h->ncells;
+    if (cell_id && n) CUDA_TRY(h, cudaMemcpy(cell_id, h->A.cell_id, 4 * n, cudaMemcpyDeviceToHost));
+    if (perm && n) CUDA_TRY(h, cudaMemcpy(perm, h->A.perm, 4 * n, cudaMemcpyDeviceToHost));
+    if (cell_start || cell_end) {
+        std::vector<uint32_t> off(nc + 1);
+        CUDA_TRY(h, cudaMemcpy(off.data(), h->A.cell_off, 4 * (nc + 1), cudaMemcpyDeviceToHost));
+        for (uint64_t c = 0; c < nc; ++c) {
+            const bool empty = off[c + 1] == off[c];
+            if (cell_start) cell_start[c] = empty ? 0xffffffffu : off[c];
+            if (cell_end) cell_end[c] = empty ? 0xffffffffu : off[c + 1];
+        }
+    }
+    return SPH_OK;
+}
+
+int sph_count_contacts(SphHandle *h, uint64_t *ncontacts)
+{
+    if (!h || !ncontacts) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    uint64_t nl = 0;
+    int st = sph::count_live_slots(h->A, h->stream, h->d_count, &nl);
+    h->launches += nl;
+    if (st != SPH_OK) return fail(h, st, "count_live_slots failed");
+    unsigned long long c = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&c, h->d_count, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    *ncontacts = c;
+    return SPH_OK;
+}
+
+uint64_t sph_kernel_launches(const SphHandle *h) { return h ? h->launches : 0; }
+
+int sph_relax(SphHandle *h, uint32_t sweeps, double alpha, double z_top, double *max_overlap)
+{
+    if (!h || !(alpha > 0.0) || !(alpha <= 1.0)) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_relax before sph_upload");
+    cudaSetDevice(h->device);
+    uint64_t nl = 0;
+    for (uint32_t k = 0; k < sweeps; ++k) {
+        int st = sph::relax_sweep(h->A, h->stream, alpha, z_top, h->d_count, &nl);
+        if (st != SPH_OK) return fail(h, st, "relax sweep launch failed");
+    }
+    h->launches += nl;
+    unsigned long long bits = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&bits, h->d_count, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (max_overlap) memcpy(max_overlap, &bits, sizeof(double));
+    CUDA_TRY(h, cudaMemset(h->A.force, 0, sizeof(double4) * (h->ntot ? h->ntot : 1)));
+    return collect_errors(h);
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+// sph_internal.h -- kernel argument block shared by the step kernels and the
+// C-ABI host code.  Not part of the public interface.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sphere_b200.h"
+
+namespace sph {
+
+struct DevBox;
+
+// Device pointers of one handle, passed by value to every step kernel.
+struct StepArgs {
+    DevBox *boxes;
+    uint32_t nboxes;
+    uint32_t ntot;        // particles over all boxes
+    uint64_t ncells;      // cells over all boxes
+    uint32_t nbonds;      // bonds over all boxes
+    uint32_t npartials;   // per-256-particle partial sums over all boxes
+    // particle state, original order
+    double4 *x, *vel, *angvel, *angpos, *xyzsum, *acc, *angacc, *force, *torque;
+    double *es_dot, *es, *ev_dot, *ev, *p;
+    const uint32_t *box_of;
+    // cell sort
+    uint32_t *cell_id, *local_off, *cell_count, *cell_off, *scan_tmp, *perm, *rank;
+    double4 *xs, *vs, *ws;     // sorted copies
+    // contact rows: slot word = partner | image code << 28, EMPTY when free
+    uint32_t *slots;
+    double4 *hist;             // tangential displacement per slot (w unused)
+    // walls and shear stress
+    double *wf_pp, *wall_partial, *tau_pp, *tau_partial;
+    const uint32_t *part_owner;
+    // bonds
+    uint2 *bonds;
+    double4 *bdelta, *bomega, *bf, *bt;
+    uint8_t *bbroken;
+    const uint32_t *bond_box;
+    const uint32_t *bcsr_off, *bcsr_ent;
+    uint32_t *err;
+};
+
+struct StepConfig {
+    int lenmode;
+    bool unfused;     // some box has a shear-stress (wmode 3) top wall
+    bool any_walls;   // some box has nw > 0
+};
+
+// Per-kernel timing of an un-graphed step (the counterpart of the
+// reference's PROFILING breakdown, src/device.cu:947-987 and 2711-2808):
+// an event is recorded on the stream after each kernel.
+struct Prof {
+    static constexpr int MAX = 32;
+    cudaEvent_t ev[MAX + 1];
+    const char *name[MAX];
+    int n = 0;
+};
+
+// Enqueue one step on `st`; adds the number of kernel launches to
+// *launches.  Capturable in a CUDA graph (prof must then be null).
+int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
+                Prof *prof = nullptr);
+
+}  // namespace sph

@@ -1,0 +1,388 @@
+"""Host driver of the CUDA step: handle wrapper and the run() loop.
+
+``Stepper`` owns one C-ABI handle (include/sphere_b200.h) for one or more
+simulation boxes.  ``run_sim`` replaces the ``sphere`` executable that
+python/sphere.py:4482 (sim.run) launches: it applies the reference's input
+checks (src/sphere.cpp:145-345), then follows DEM::startTime
+(src/device.cu:826-2677) for fluid == 0 -- output file 0, status.dat, steps
+until time.total with an output file every time.file_dt.
+"""
+import copy
+import ctypes as C
+import os
+
+import numpy
+
+from . import _abi, binio
+from ._abi import NC
+
+PRECISIONS = {"fp64": _abi.PREC_FP64, "mixed": _abi.PREC_MIXED}
+LENGTHS = {"reference": _abi.LEN_REFERENCE, "fp64": _abi.LEN_FP64}
+
+
+class SphereError(RuntimeError):
+    def __init__(self, status, message):
+        RuntimeError.__init__(self, "%s (%s): %s" % (_abi.STATUS_NAMES.get(status, status),
+                                                      status, message))
+        self.status = status
+
+
+def _f(a, shape):
+    return numpy.ascontiguousarray(numpy.asarray(a, dtype=numpy.float64).reshape(shape))
+
+
+class HostParticles(object):
+    """Host arrays of all boxes in the .bin block layouts of the C ABI."""
+
+    def __init__(self, n):
+        self.x = numpy.zeros((n, 4))
+        self.xyzsum = numpy.zeros((n, 3))
+        self.vel = numpy.zeros((n, 4))
+        self.force = numpy.zeros((n, 3))
+        self.angpos = numpy.zeros((n, 3))
+        self.angvel = numpy.zeros((n, 3))
+        self.torque = numpy.zeros((n, 3))
+        for name in ("es_dot", "es", "ev_dot", "ev", "p"):
+            setattr(self, name, numpy.zeros(n))
+
+    def struct(self):
+        s = _abi.SphParticles()
+        for name, _ in _abi.SphParticles._fields_:
+            setattr(s, name, _abi.dptr(getattr(self, name)))
+        return s
+
+    @classmethod
+    def from_sims(cls, sims):
+        n = sum(int(s.np[0]) for s in sims)
+        h = cls(n)
+        o = 0
+        for s in sims:
+            k = int(s.np[0])
+            h.x[o:o + k, :3] = s.x
+            h.x[o:o + k, 3] = s.radius
+            h.xyzsum[o:o + k] = _f(s.xyzsum, (k, 3))
+            h.vel[o:o + k, :3] = s.vel
+            h.vel[o:o + k, 3] = s.fixvel
+            for name in ("force", "angpos", "angvel", "torque"):
+                getattr(h, name)[o:o + k] = _f(getattr(s, name), (k, 3))
+            for name in ("es_dot", "es", "ev_dot", "ev", "p"):
+                getattr(h, name)[o:o + k] = _f(getattr(s, name), (k,))
+            o += k
+        return h
+
+
+class HostBonds(object):
+    def __init__(self, nb):
+        self.pairs = numpy.zeros((nb, 2), dtype=numpy.uint32)
+        self.delta_n = numpy.zeros(nb)
+        self.delta_t = numpy.zeros((nb, 3))
+        self.omega_n = numpy.zeros(nb)
+        self.omega_t = numpy.zeros((nb, 3))
+
+    def struct(self):
+        b = _abi.SphBonds()
+        b.pairs = _abi.uptr(self.pairs)
+        for name in ("delta_n", "delta_t", "omega_n", "omega_t"):
+            setattr(b, name, _abi.dptr(getattr(self, name)))
+        return b
+
+    @classmethod
+    def from_sims(cls, sims):
+        nb = sum(int(s.nb0[0]) for s in sims)
+        h = cls(nb)
+        o = 0
+        for s in sims:
+            k = int(s.nb0[0])
+            if k:
+                h.pairs[o:o + k] = numpy.asarray(s.bonds).reshape(-1, 2)[:k]
+                h.delta_n[o:o + k] = numpy.asarray(s.bonds_delta_n, dtype=numpy.float64).reshape(-1)[:k]
+                h.delta_t[o:o + k] = numpy.asarray(s.bonds_delta_t, dtype=numpy.float64).reshape(-1, 3)[:k]
+                h.omega_n[o:o + k] = numpy.asarray(s.bonds_omega_n, dtype=numpy.float64).reshape(-1)[:k]
+                h.omega_t[o:o + k] = numpy.asarray(s.bonds_omega_t, dtype=numpy.float64).reshape(-1, 3)[:k]
+            o += k
+        return h
+
+
+class Stepper(object):
+    """One C-ABI handle stepping one or more independent boxes on a GPU."""
+
+    def __init__(self, sims, precision="fp64", length="reference", device=-1):
+        if not isinstance(sims, (list, tuple)):
+            sims = [sims]
+        self.lib = _abi.load_library()
+        self.sims = list(sims)
+        self.np = [int(s.np[0]) for s in sims]
+        self.nb = [int(s.nb0[0]) for s in sims]
+        self.ntot = sum(self.np)
+        self.nbonds = sum(self.nb)
+        boxes = (_abi.SphBox * len(sims))(*[_abi.box_from_sim(s) for s in sims])
+        self._boxes = boxes
+        h = C.c_void_p()
+        st = self.lib.sph_create(boxes, len(sims), PRECISIONS[precision], LENGTHS[length],
+                                 int(device), C.byref(h))
+        if st != 0:
+            raise SphereError(st, self._msg(None))
+        self.h = h
+
+    def _msg(self, h):
+        buf = C.create_string_buffer(512)
+        self.lib.sph_last_error(h, buf, 512)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, st, what):
+        if st != 0:
+            raise SphereError(st, "%s: %s" % (what, self._msg(self.h)))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.sph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self):
+        self.hp = HostParticles.from_sims(self.sims)
+        self.hb = HostBonds.from_sims(self.sims)
+        ps = self.hp.struct()
+        bs = self.hb.struct()
+        self._check(self.lib.sph_upload(self.h, C.byref(ps), C.byref(bs) if self.nbonds else None),
+                    "sph_upload")
+
+    def step(self, nsteps=1, raise_on_error=True):
+        st = self.lib.sph_step(self.h, int(nsteps))
+        if raise_on_error:
+            self._check(st, "sph_step")
+        return st
+
+    def step_async(self, nsteps=1):
+        self._check(self.lib.sph_step_async(self.h, int(nsteps)), "sph_step_async")
+
+    def sync(self, raise_on_error=True):
+        st = self.lib.sph_sync(self.h)
+        if raise_on_error:
+            self._check(st, "sph_sync")
+        return st
+
+    def set_stream(self, cuda_stream):
+        """Run on a caller's cudaStream_t (an int handle, e.g. a torch
+        stream's .cuda_stream); 0/None restores the handle's own stream."""
+        self._check(self.lib.sph_set_stream(self.h, C.c_void_p(cuda_stream or None)),
+                    "sph_set_stream")
+
+    def profile(self, enable=True):
+        """Run subsequent steps from the profiled graph ring (sph_profile)."""
+        self._check(self.lib.sph_profile(self.h, int(bool(enable))), "sph_profile")
+
+    def profile_read(self):
+        """Mean milliseconds per kernel group over the most recent (up to 8)
+        profiled steps."""
+        names = C.create_string_buffer(1024)
+        ms = numpy.zeros(32)
+        nk = C.c_int(0)
+        self._check(self.lib.sph_profile_read(self.h, names, 1024, _abi.dptr(ms), 32, C.byref(nk)),
+                    "sph_profile_read")
+        keys = names.value.decode().split(",")
+        return dict(zip(keys, ms[:nk.value].tolist()))
+
+    def relax(self, sweeps, alpha=0.6, z_top=1e300):
+        """Geometric overlap removal on the device (sph_relax); returns the
+        largest overlap of the last sweep."""
+        mo = C.c_double(0.0)
+        self._check(self.lib.sph_relax(self.h, int(sweeps), float(alpha), float(z_top),
+                                       C.byref(mo)), "sph_relax")
+        return mo.value
+
+    def advance(self, total, file_dt, current, ftc, max_steps=2 ** 62):
+        cur = C.c_double(current)
+        f = C.c_double(ftc)
+        done = C.c_uint64(0)
+        st = self.lib.sph_advance(self.h, float(total), float(file_dt), C.byref(cur), C.byref(f),
+                                  int(max_steps), C.byref(done))
+        return st, cur.value, f.value, done.value
+
+    def download(self):
+        hp = HostParticles(self.ntot)
+        hb = HostBonds(self.nbonds)
+        ps = hp.struct()
+        bs = hb.struct()
+        self._check(self.lib.sph_download(self.h, C.byref(ps), C.byref(bs) if self.nbonds else None),
+                    "sph_download")
+        return hp, hb
+
+    def boxes(self):
+        out = (_abi.SphBox * len(self.sims))()
+        self._check(self.lib.sph_get_boxes(self.h, out), "sph_get_boxes")
+        return list(out)
+
+    def contacts(self):
+        n = self.ntot
+        c = numpy.zeros(n * NC, dtype=numpy.uint32)
+        dt = numpy.zeros((n * NC, 4))
+        dm = numpy.zeros((n * NC, 4))
+        self._check(self.lib.sph_get_contacts(self.h, _abi.uptr(c), _abi.dptr(dt), _abi.dptr(dm)),
+                    "sph_get_contacts")
+        return c, dt, dm
+
+    def sort_products(self):
+        n = self.ntot
+        nc = int(self.lib.sph_total_cells(self.h))
+        cid = numpy.zeros(max(n, 1), dtype=numpy.uint32)
+        perm = numpy.zeros(max(n, 1), dtype=numpy.uint32)
+        cs = numpy.zeros(nc, dtype=numpy.uint32)
+        ce = numpy.zeros(nc, dtype=numpy.uint32)
+        self._check(self.lib.sph_get_sort(self.h, _abi.uptr(cid), _abi.uptr(perm), _abi.uptr(cs),
+                                          _abi.uptr(ce)), "sph_get_sort")
+        return cid[:n], perm[:n], cs, ce
+
+    def count_contacts(self):
+        c = C.c_uint64(0)
+        self._check(self.lib.sph_count_contacts(self.h, C.byref(c)), "sph_count_contacts")
+        return c.value
+
+    def kernel_launches(self):
+        return int(self.lib.sph_kernel_launches(self.h))
+
+    def to_sims(self):
+        """Copy device state into the sim objects (as an output file would)."""
+        hp, hb = self.download()
+        boxes = self.boxes()
+        o = ob = 0
+        for s, b, k, kb in zip(self.sims, boxes, self.np, self.nb):
+            s.x = hp.x[o:o + k, :3].copy()
+            s.radius = hp.x[o:o + k, 3].copy()
+            s.xyzsum = hp.xyzsum[o:o + k].copy()
+            s.vel = hp.vel[o:o + k, :3].copy()
+            s.fixvel = hp.vel[o:o + k, 3].copy()
+            for name in ("force", "angpos", "angvel", "torque", "es_dot", "es", "ev_dot", "ev", "p"):
+                setattr(s, name, getattr(hp, name)[o:o + k].copy())
+            if kb:
+                s.bonds = hb.pairs[ob:ob + kb].copy()
+                s.bonds_delta_n = hb.delta_n[ob:ob + kb].copy()
+                s.bonds_delta_t = hb.delta_t[ob:ob + kb].copy()
+                s.bonds_omega_n = hb.omega_n[ob:ob + kb].copy()
+                s.bonds_omega_t = hb.omega_t[ob:ob + kb].copy()
+            _abi.sim_from_box(s, b)
+            o += k
+            ob += kb
+        return self.sims
+
+
+# src/sphere.cpp:145-345 checkValues (host side, before any device work)
+def check_values(s):
+    if int(s.nd[0]) != 3:
+        return "Error: nd = %d, ND = 3" % int(s.nd[0])
+    if s.time_current[0] > s.time_total[0] or s.time_current[0] < 0.0:
+        return "Error: time.current = %g s, time.total = %g s" % (s.time_current[0], s.time_total[0])
+    if (numpy.asarray(s.origo) < 0.0).any():
+        return "Error: Negative values in grid.origo are known to cause problems."
+    if (numpy.asarray(s.L) <= 0.0).any():
+        return "Error: grid.L must be positive"
+    if (numpy.asarray(s.num) <= 0).any():
+        return "Error: grid.num must be positive"
+    if s.periodic[0] == 2 and s.num[0] < 3:
+        return "Error: When 1st dimension boundaries are periodic, there must be at least 3 cells in that dimension."
+    if s.periodic[0] == 1 and (s.num[0] < 3 or s.num[1] < 3):
+        return ("Error: When 1st and 2nd dimension boundaries are periodic, there must be at "
+                "least 3 cells in each of those dimensions.")
+    n = int(s.np[0])
+    if n:
+        if (s.radius <= 0.0).any():
+            return "Error: Particle %d has a radius of %g m." % (int(numpy.argmax(s.radius <= 0.0)),
+                                                                  float(s.radius.min()))
+        if numpy.isnan(s.x).any() or numpy.isnan(s.vel).any() or numpy.isnan(s.fixvel).any():
+            return "Error: NaN particle position or velocity"
+        out = (s.x < numpy.asarray(s.origo)).any(axis=1) | (s.x > numpy.asarray(s.L)).any(axis=1)
+        if out.any():
+            return "Error: Particle %d is outside of the computational grid" % int(numpy.argmax(out))
+        if s.nw[0] > 0 and s.w_x[0] < max(0.0, float(s.x[:, 2].max())):
+            return "Error: One or more particles have centres above the upper, dynamic wall"
+    if s.k_n[0] <= 0.0:
+        return "Error: k_n = %g N/m" % s.k_n[0]
+    if s.E[0] < 0.0:
+        return "Error: E = %g N/m^3" % s.E[0]
+    if s.rho[0] <= 0.0:
+        return "Error: rho = %g kg/m3" % s.rho[0]
+    return None
+
+
+def report_values(s):
+    """The `--dry` report of src/sphere.cpp:349-466."""
+    print("  - Number of dimensions: nd = %d" % s.nd[0])
+    print("  - Number of particles:  np = %d" % s.np[0])
+    print("  - Compiled for double precision")
+    print("  - Timestep length:      time.dt         = %g s" % s.time_dt[0])
+    print("  - Start at time:        time.current    = %g s" % s.time_current[0])
+    print("  - Total sim. time:      time.total      = %g s" % s.time_total[0])
+    print("  - File output interval: time.file_dt    = %g s" % s.time_file_dt[0])
+    print("  - Start at step count:  time.step_count = %d" % s.time_step_count[0])
+    cm = int(s.contactmodel[0])
+    names = {1: "Linear-elastic-viscous (n), visco-frictional (t)",
+             2: "Linear-elastic-visco-frictional", 3: "Nonlinear-elastic-visco-frictional"}
+    print("  - Contact model: " + names.get(cm, "unknown (%d)" % cm))
+    print("  - Using Young's modulus for contact stiffness" if s.E[0] > 0.01 else
+          "  - Using global value for contact stiffness")
+    print("  - Number of dynamic walls: %d" % s.nw[0])
+    print("  - Grid: %d * %d * %d cells" % tuple(int(v) for v in s.num))
+    print("  - Domain size: %g * %g * %g m" % tuple(float(v) for v in s.L))
+    print("  - No. of particle bonds: %d" % s.nb0[0])
+
+
+def _write_status(path, s):
+    with open(path, "w") as fh:
+        cur = float(s.time_current[0])
+        tot = float(s.time_total[0])
+        fh.write("%2.4e %2.4e %d\n" % (cur, 100.0 * cur / tot if tot else 0.0,
+                                       int(s.time_step_count[0])))
+
+
+def run_sim(s, root="..", verbose=True, device=-1, precision="fp64", length="reference"):
+    """Run `s` to time_total, writing the reference's output files.  Returns
+    0 or the SphStatus of the first failure (as the binary's exit status)."""
+    msg = check_values(s)
+    if msg:
+        print(msg)
+        return 1
+    # the caller's object keeps its input state, as with the reference binary
+    s = copy.deepcopy(s)
+    outdir = os.path.join(root, "output")
+    os.makedirs(outdir, exist_ok=True)
+    status_path = os.path.join(outdir, s.sid + ".status.dat")
+    # device.cu:840-842: output file 0 before the first step
+    if int(s.time_step_count[0]) == 0:
+        binio.write_bin(os.path.join(outdir, s.sid + ".output00000.bin"), s)
+    st = Stepper([s], precision=precision, length=length, device=device)
+    try:
+        st.upload()
+        _write_status(status_path, s)
+        cur = float(s.time_current[0])
+        total = float(s.time_total[0])
+        file_dt = float(s.time_file_dt[0])
+        ftc = 0.0
+        status = 0
+        while cur <= total:
+            code, cur, ftc, done = st.advance(total, file_dt, cur, ftc)
+            if code != 0:
+                status = code
+                if verbose:
+                    print("sphere_b200: " + st._msg(st.h))
+                if code in (_abi.SPH_ERR_NAN, _abi.SPH_ERR_OUT_OF_GRID, _abi.SPH_ERR_CUDA):
+                    break
+            if ftc >= file_dt:
+                st.to_sims()
+                s.time_current[0] = cur
+                s.time_step_count[0] += 1
+                binio.write_bin(os.path.join(outdir, "%s.output%05d.bin" %
+                                             (s.sid, int(s.time_step_count[0]))), s)
+                _write_status(status_path, s)
+                ftc = 0.0
+        st.to_sims()
+        s.time_current[0] = cur
+        if verbose:
+            print("  - Last output file number: %d" % int(s.time_step_count[0]))
+        return status
+    finally:
+        st.close()

@@ -1,0 +1,230 @@
+"""Seeded synthetic scenes: small parity cases and the benchmark workloads.
+
+All generators return ``sim`` objects (sphere_b200.sim) built from a numpy
+Generator seed, so every run of a test or benchmark sees the same inputs.
+"""
+import math
+
+import numpy
+
+from .sim import sim, V_sphere
+
+
+def lattice_pack(n, seed=0, r_min=0.009, r_max=0.011, spacing=None, jitter=None, periodic=1,
+                 contactmodel=2, nw=1, wmode=1, sigma0=1.0e4, wvel=0.0, k_n=1.16e9, gamma_n=1.0e2,
+                 gamma_t=5.0e1, mu=0.5, E=0.0, g=(0.0, 0.0, -9.81), vel_sigma=0.05,
+                 angvel_sigma=1.0, aspect=(1.0, 1.0), margin_cells=0, fixvel_layers=False,
+                 dt_scale=0.17, sid="lattice"):
+    """A jittered cubic lattice of n spheres, packed so that neighbours
+    overlap slightly (many contacts from the first step), random velocities
+    and spins, a top wall (nw=1) and periodic or wall sides."""
+    rng = numpy.random.default_rng(seed)
+    s = sim(np=n, nw=0, sid=sid)
+    s.radius[:] = rng.uniform(r_min, r_max, n)
+    if spacing is None:
+        spacing = 1.96 * (0.5 * (r_min + r_max))
+    if jitter is None:
+        jitter = 0.03 * spacing
+    ax, ay = aspect
+    side = max(int(math.ceil((n / (ax * ay)) ** (1.0 / 3.0))), 1)
+    nx_ = max(int(round(side * ax)), 1)
+    ny_ = max(int(round(side * ay)), 1)
+    nz_ = int(math.ceil(n / float(nx_ * ny_)))
+    i = numpy.arange(n)
+    gp = numpy.stack([i % nx_, (i // nx_) % ny_, i // (nx_ * ny_)], 1).astype(float)
+    cell = 2.1 * r_max
+    if periodic:
+        Lx, Ly = nx_ * spacing, ny_ * spacing
+        base = numpy.array([0.5 * spacing, 0.5 * spacing, r_max * 1.5])
+    else:
+        Lx, Ly = nx_ * spacing + 2 * r_max, ny_ * spacing + 2 * r_max
+        base = numpy.array([r_max + 0.5 * spacing, r_max + 0.5 * spacing, r_max * 1.5])
+    s.x[:] = gp * spacing + base + rng.uniform(-jitter, jitter, (n, 3))
+    if periodic:
+        s.x[:, 0] = numpy.mod(s.x[:, 0], Lx)
+        s.x[:, 1] = numpy.mod(s.x[:, 1], Ly)
+    s.x[:, 2] = numpy.maximum(s.x[:, 2], s.radius * 0.999)
+    s.vel[:] = rng.normal(0.0, vel_sigma, (n, 3))
+    s.angvel[:] = rng.normal(0.0, angvel_sigma, (n, 3))
+    s.g[:] = g
+    s.k_n[0] = k_n
+    s.k_t[0] = k_n
+    s.gamma_n[0] = gamma_n
+    s.gamma_t[0] = gamma_t
+    s.mu_s[0] = mu
+    s.mu_d[0] = mu
+    s.E[0] = E
+    s.contactmodel[0] = contactmodel
+    s.periodic[0] = periodic
+    ztop = float(numpy.max(s.x[:, 2] + s.radius))
+    Lz = ztop + (3 + margin_cells) * cell
+    nxc = max(int(Lx / cell), 3)
+    nyc = max(int(Ly / cell), 3)
+    nzc = max(int(Lz / cell), 3)
+    s.origo[:] = 0.0
+    s.L[:] = [Lx, Ly, Lz]
+    s.num[:] = [nxc, nyc, nzc]
+    if nw:
+        s.nw = numpy.ones(1, dtype=numpy.uint32)
+        s.wmode = numpy.array([wmode], dtype=numpy.int32)
+        s.w_n = numpy.array([[0.0, 0.0, -1.0]])
+        s.w_x = numpy.array([ztop - 0.2 * r_min])
+        s.w_m = numpy.array([s.totalMass()])
+        s.w_vel = numpy.array([wvel])
+        s.w_force = numpy.zeros(1)
+        s.w_sigma0 = numpy.array([sigma0])
+    if fixvel_layers:
+        zlo = s.x[:, 2] < s.x[:, 2].min() + 1.5 * r_max
+        zhi = s.x[:, 2] > s.x[:, 2].max() - 1.5 * r_max
+        s.fixvel[zlo | zhi] = 1.0
+        s.vel[zlo | zhi, :2] = 0.0
+        s.vel[zhi, 0] = 0.01
+        s.angvel[zlo | zhi] = 0.0
+    m_min = s.rho[0] * V_sphere(r_min)
+    k = k_n if E <= 0.001 else math.pi / 2.0 * E * r_max
+    s.time_dt[0] = dt_scale * math.sqrt(m_min / k)
+    s.time_total[0] = 1.0
+    s.time_file_dt[0] = 1.0
+    return s
+
+
+def two_particles(radii=(1.0, 1.0), x0=(5.0, 5.0, 2.0), x1=(5.0, 5.0, 4.05), vel0=(0.0, 0.0, 1.0),
+                  total=0.1, file_dt=0.01, sid="contactmodeltest"):
+    """The two-sphere impact of the reference's tests/contactmodel.py."""
+    s = sim(np=2, sid=sid)
+    s.radius[:] = radii
+    s.x[0, :] = x0
+    s.x[1, :] = x1
+    s.vel[0, :] = vel0
+    s.defineWorldBoundaries(L=[10, 10, 10])
+    s.initTemporal(total=total, file_dt=file_dt)
+    return s
+
+
+def gravity_settling(n=10000, seed=0, steps=1000):
+    """Plain FP64 gravity settling of n spheres: radii U[0.010, 0.012] m,
+    rho 2600, jittered cubic lattice (spacing 2.5*r_max, jitter +-0.2*r_max)
+    in a 0.5 x 0.5 m box, zero velocity, linear contacts k_n = k_t = 1.16e9,
+    no damping, mu 0.5, fixed bottom, wall sides, dt = 0.17*sqrt(m_min/k_n).
+    The lattice is 16 x 16 per layer, so 40 layers reach z ~ 1.2 m; the box
+    height is 1.25 m instead of 1.0 m to hold them."""
+    rng = numpy.random.default_rng(seed)
+    r_min, r_max = 0.010, 0.012
+    s = sim(np=n, nw=0, sid="settle")
+    s.radius[:] = rng.uniform(r_min, r_max, n)
+    sp = 2.5 * r_max
+    per = int(0.5 / sp)
+    i = numpy.arange(n)
+    gp = numpy.stack([i % per, (i // per) % per, i // (per * per)], 1).astype(float)
+    s.x[:] = gp * sp + sp * 0.5 + rng.uniform(-0.2 * r_max, 0.2 * r_max, (n, 3))
+    s.g[:] = [0.0, 0.0, -9.81]
+    s.k_n[0] = s.k_t[0] = 1.16e9
+    s.gamma_n[0] = s.gamma_t[0] = 0.0
+    s.mu_s[0] = s.mu_d[0] = 0.5
+    s.periodic[0] = 0
+    s.defineWorldBoundaries(L=[0.5, 0.5, 1.25])
+    m_min = s.rho[0] * V_sphere(r_min)
+    s.time_dt[0] = 0.17 * math.sqrt(m_min / s.k_n[0])
+    s.time_total[0] = (steps - 0.5) * s.time_dt[0]
+    s.time_file_dt[0] = s.time_total[0]
+    return s
+
+
+def _fcc_sites(nxc, nyc, nzc, a):
+    """FCC lattice sites (4 per cube of side a), layer by layer in z."""
+    base = numpy.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]])
+    iz, iy, ix = numpy.meshgrid(numpy.arange(nzc), numpy.arange(nyc), numpy.arange(nxc),
+                                indexing="ij")
+    cubes = numpy.stack([ix.ravel(), iy.ravel(), iz.ravel()], 1).astype(float)
+    sites = (cubes[:, None, :] + base[None, :, :]).reshape(-1, 3)
+    order = numpy.lexsort((sites[:, 0], sites[:, 1], sites[:, 2]))
+    return sites[order] * a
+
+
+def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.005, 0.02),
+               aspect_z=0.5, sweeps=3000, alpha=0.6, inflate=2.0e-7, device=-1, sid="dense"):
+    """A dense x-y periodic pack of n log-normal spheres at the given
+    porosity, made on the GPU: FCC lattice start in a box of aspect
+    1 : 1 : aspect_z sized for the porosity, then geometric overlap removal
+    (sph_relax) between the floor and the box top, then radii grown by the
+    factor (1 + inflate) so that touching spheres overlap by ~inflate * r
+    and form contacts.  Returns the sim (no walls yet) and the largest
+    residual overlap of the relaxation."""
+    from .runner import Stepper
+    rng = numpy.random.default_rng(seed)
+    r = numpy.clip(numpy.exp(rng.normal(math.log(median), sigma_ln, n)), *r_clip)
+    v_solid = float(numpy.sum(4.0 / 3.0 * math.pi * r ** 3))
+    v_box = v_solid / (1.0 - porosity)
+    L = (v_box / aspect_z) ** (1.0 / 3.0)
+    H = aspect_z * L
+    a0 = (4.0 * L * L * H / n) ** (1.0 / 3.0)   # FCC cube side for n sites in the box
+    nxc = max(int(round(L / a0)), 3)
+    a = L / nxc
+    nzc = int(math.ceil(n / (4.0 * nxc * nxc)))
+    sites = _fcc_sites(nxc, nxc, nzc, a)[:n]
+    sites[:, 2] *= (H - 2.0 * median) / max(sites[:, 2].max(), 1e-12)
+    s = sim(np=n, nw=0, sid=sid)
+    s.radius[:] = r
+    s.x[:] = sites + numpy.array([0.25 * a, 0.25 * a, median]) + \
+        rng.uniform(-0.05 * a, 0.05 * a, (n, 3))
+    s.x[:, 0] = numpy.mod(s.x[:, 0], L)
+    s.x[:, 1] = numpy.mod(s.x[:, 1], L)
+    s.x[:, 2] = numpy.clip(s.x[:, 2], r, H - r)
+    r_max = float(r.max())
+    cell = 2.1 * r_max
+    ncx = max(int(L / cell), 3)
+    s.periodic[0] = 1
+    s.origo[:] = 0.0
+    Lz = H + 4.0 * cell
+    s.L[:] = [L, L, Lz]
+    s.num[:] = [ncx, ncx, max(int(Lz / cell), 3)]
+    s.time_dt[0] = 1e-7
+    s.time_total[0] = 1.0
+    st = Stepper([s], device=device)
+    st.upload()
+    worst = st.relax(sweeps, alpha=alpha, z_top=H)
+    st.to_sims()
+    st.close()
+    s.radius *= 1.0 + inflate
+    s.time_current[0] = 0.0
+    return s, worst
+
+
+def sheared_dense_pack(n=1000000, seed=0, device=-1, sweeps=3000):
+    """The 1e6-sphere sheared dense pack: log-normal radii (median 0.01 m,
+    sigma_ln 0.2, clipped to [0.005, 0.02]) packed to porosity ~0.40 in an
+    x-y periodic box of aspect 1:1:0.5 (dense_pack, on the GPU), a top wall
+    at 20 kPa normal stress (wmode 1, mass = total particle mass as in
+    sim.consolidate), the top layer moving at +x 0.01 m/s and the bottom
+    layer held (fixvel, as in sim.shear), linear contacts
+    k_n = k_t = 1.16e9 N/m, gamma_n = 1e3, mu = 0.5, NC = 32 slots,
+    dt = 0.17 * sqrt(m_min / k_n), 5,000 steps."""
+    s, _worst = dense_pack(n, seed=seed, device=device, sweeps=sweeps, sid="shear1e6")
+    s.g[:] = [0.0, 0.0, -9.81]
+    s.k_n[0] = s.k_t[0] = 1.16e9
+    s.gamma_n[0] = 1.0e3
+    s.gamma_t[0] = 0.0
+    s.mu_s[0] = s.mu_d[0] = 0.5
+    rr = s.radius
+    r_max = float(rr.max())
+    ztop = float((s.x[:, 2] + rr).max())
+    zmin = float((s.x[:, 2] - rr).min())
+    s.nw = numpy.ones(1, dtype=numpy.uint32)
+    s.wmode = numpy.array([1], dtype=numpy.int32)
+    s.w_n = numpy.array([[0.0, 0.0, -1.0]])
+    s.w_x = numpy.array([ztop])
+    s.w_m = numpy.array([s.totalMass()])
+    s.w_vel = numpy.zeros(1)
+    s.w_force = numpy.zeros(1)
+    s.w_sigma0 = numpy.array([2.0e4])
+    top = s.x[:, 2] > ztop - 2.0 * r_max
+    bot = s.x[:, 2] < zmin + 2.0 * r_max
+    s.fixvel[top | bot] = 1.0
+    s.vel[:] = 0.0
+    s.vel[top, 0] = 0.01
+    m_min = s.rho[0] * V_sphere(float(rr.min()))
+    s.time_dt[0] = 0.17 * math.sqrt(m_min / s.k_n[0])
+    s.time_current[0] = 0.0
+    s.time_total[0] = 5000 * s.time_dt[0]
+    s.time_file_dt[0] = s.time_total[0]
+    return s

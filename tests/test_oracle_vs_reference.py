@@ -1,0 +1,50 @@
+"""The C oracle against the reference's own kernels run on the CPU.
+
+oracle/_ref/libsphere_ref.so is the reference's src/*.cuh step kernels
+compiled for the CPU (oracle/ref_emu); oracle/_build/libsphere_oracle.so is
+this project's restatement.  On every parity case they must agree bit for
+bit: positions, velocities, forces, torques, energies, contact lists,
+tangential histories, the sorted permutation and the walls.
+"""
+import numpy
+import pytest
+
+import cases
+import oracle as O
+
+FIELDS = ["x", "vel", "angvel", "angpos", "xyzsum", "force", "torque", "es", "ev", "es_dot",
+          "ev_dot", "p", "contacts", "delta_t", "perm", "cell_id", "bonds", "bonds_delta",
+          "bonds_omega"]
+
+needs_ref = pytest.mark.skipif(not O.available("ref") and not __import__("os").path.isdir(
+    "/root/reference/src"), reason="reference sources unavailable to build oracle/_ref")
+
+
+def _same(a, b):
+    return numpy.array_equal(a, b) or (a.dtype.kind == "f" and numpy.array_equal(a, b, equal_nan=True))
+
+
+@needs_ref
+@pytest.mark.parametrize("name", [c for c in cases.CASES if cases.make(c)[1]])
+def test_oracle_matches_reference_kernels(name):
+    if not O.available("ref"):
+        O.build()
+    s, ref_ok, steps = cases.make(name)
+    a = O.CpuRun(s, "oracle")
+    b = O.CpuRun(s, "ref")
+    for chunk in range(2):
+        a.step(steps // 2)
+        b.step(steps // 2)
+        for f in FIELDS:
+            A, B = getattr(a, f), getattr(b, f)
+            assert _same(A, B), "%s differs after %d steps (max %g)" % (
+                f, (chunk + 1) * steps // 2,
+                float(numpy.nanmax(numpy.abs(A.astype(float) - B.astype(float)))))
+        live = a.contacts != s.np[0]
+        assert numpy.array_equal(a.distmod[live], b.distmod[live])
+        for w in range(int(s.nw[0])):
+            assert list(a.box.walls.nx[w]) == list(b.box.walls.nx[w])
+            assert list(a.box.walls.mvfd[w]) == list(b.box.walls.mvfd[w])
+        assert a.box.grid.L[2] == b.box.grid.L[2]
+        assert a.box.t_current == b.box.t_current
+    assert int((a.contacts != s.np[0]).sum()) > 0 or s.contactmodel[0] == 1

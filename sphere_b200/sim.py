@@ -540,9 +540,9 @@ class sim(object):
                       "particles may produce instabilities.")
         elif self.np[0] > 0:
             r_min = numpy.min(self.radius)
-            m_min = self.rho * 4.0 / 3.0 * numpy.pi * r_min ** 3
-            if self.E > 0.001:
-                k_max = numpy.max(numpy.pi / 2.0 * self.E * self.radius)
+            m_min = self.rho[0] * 4.0 / 3.0 * numpy.pi * r_min ** 3
+            if self.E[0] > 0.001:
+                k_max = numpy.max(numpy.pi / 2.0 * self.E[0] * self.radius)
             else:
                 k_max = numpy.max([self.k_n[:], self.k_t[:]])
             self.time_dt[0] = epsilon / (numpy.sqrt(k_max / m_min))

@@ -228,9 +228,6 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_m
     };
     if (!boxes || nboxes == 0) return bail(SPH_ERR_INPUT);
     if (precision != SPH_PREC_FP64 && precision != SPH_PREC_MIXED) return bail(SPH_ERR_INPUT);
-    if (precision == SPH_PREC_MIXED &&
-        sph::launch_step_mixed(StepArgs{}, StepConfig{}, nullptr, nullptr, nullptr) == SPH_ERR_UNSUPPORTED)
-        return bail(SPH_ERR_UNSUPPORTED);
     if (length_mode != SPH_LEN_REFERENCE && length_mode != SPH_LEN_FP64) return bail(SPH_ERR_INPUT);
     h->precision = precision;
     h->lenmode = length_mode;
@@ -301,7 +298,8 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_m
         (st = dalloc(h, &A.cell_count, h->ncells)) || (st = dalloc(h, &A.cell_off, h->ncells + 1)) ||
         (st = dalloc(h, &A.scan_tmp, scan_blocks + 1)) || (st = dalloc(h, &A.perm, n)) ||
         (st = dalloc(h, &A.rank, n)) || (st = dalloc(h, &A.xs, n)) || (st = dalloc(h, &A.vs, n)) ||
-        (st = dalloc(h, &A.ws, n)) || (st = dalloc(h, &A.slots, n * sph::NC)) ||
+        (st = dalloc(h, &A.ws, n)) || (st = dalloc(h, &A.xf, n)) ||
+        (st = dalloc(h, &A.slots, n * sph::NC)) ||
         (st = dalloc(h, &A.hist, n * sph::NC)) || (st = dalloc(h, &A.wf_pp, n)) ||
         (st = dalloc(h, &A.wall_partial, h->npartials)) || (st = dalloc(h, &A.tau_pp, n)) ||
         (st = dalloc(h, &A.tau_partial, h->npartials)) ||
@@ -498,6 +496,13 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
             bb += d.nb0;
             qb += d.nblocks;
             h->t_host[k] = h->boxes[k].t_current;
+            // FP32 prefilter margin: bounds the rounding of FP32 coordinates
+            // (|x| <= 2 max L), their differences and periodic shifts, and
+            // of the reference's FP32-rounded lengths, with room to spare.
+            double rmax = 0.0, lmax = 0.0;
+            for (uint32_t j = 0; j < d.np; ++j) rmax = fmax(rmax, p->x[4 * (size_t)(d.p_base + j) + 3]);
+            for (int c = 0; c < 3; ++c) lmax = fmax(lmax, fabs(d.L[c]) + fabs(d.origo[c]));
+            d.pre_margin = (float)(ldexp(2.0 * lmax + 2.0 * rmax, -19));
         }
     }
     CUDA_TRY(h, cudaMemcpy(A.boxes, h->dbox.data(), sizeof(DevBox) * h->nbox, cudaMemcpyHostToDevice));

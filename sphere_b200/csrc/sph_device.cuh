@@ -48,6 +48,8 @@ struct DevBox {
     double tau_eff_x;          // sum of shear-stress partials (wmode 3)
     double dt, t_current;
     double L2_out;             // grid.L[2] of the last step (what an output file holds)
+    float pre_margin;          // FP32 candidate prefilter margin (see k_interact)
+    float pad_f;
     uint64_t iter;
     int32_t velocity_state;
     int32_t change_velocity_state;

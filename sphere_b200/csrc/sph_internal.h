@@ -26,6 +26,7 @@ struct StepArgs {
     // cell sort
     uint32_t *cell_id, *local_off, *cell_count, *cell_off, *scan_tmp, *perm, *rank;
     double4 *xs, *vs, *ws;     // sorted copies
+    float4 *xf;                // sorted FP32 copy of x+r for the candidate prefilter
     // contact rows: slot word = partner | image code << 28, EMPTY when free
     uint32_t *slots;
     double4 *hist;             // tangential displacement per slot (w unused)
@@ -58,8 +59,16 @@ struct Prof {
 };
 
 // Enqueue one step on `st`; adds the number of kernel launches to
-// *launches.  Capturable in a CUDA graph (prof must then be null).
+// *launches.  Capturable in a CUDA graph (events in prof become event-record
+// nodes).  launch_step runs the FP64 form; launch_step_with takes the
+// launcher of the fused interact kernel (FP64 or FP32-mixed variant).
+typedef void (*InteractLauncher)(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused,
+                                 int lenmode);
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
                 Prof *prof = nullptr);
+int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
+                     uint64_t *launches, Prof *prof, InteractLauncher interact);
+int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
+                      uint64_t *launches, Prof *prof);
 
 }  // namespace sph

@@ -27,6 +27,7 @@
 
 #include "sph_device.cuh"
 #include "sph_internal.h"
+#include "sph_step.cuh"
 
 namespace sph {
 
@@ -187,7 +188,9 @@ __global__ void k_reorder(StepArgs A)
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= A.ntot) return;
     const uint32_t i = A.perm[j];
-    A.xs[j] = A.x[i];
+    const double4 x = A.x[i];
+    A.xs[j] = x;
+    A.xf[j] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
     A.vs[j] = A.vel[i];
     A.ws[j] = A.angvel[i];
     A.rank[i] = j;
@@ -261,348 +264,6 @@ __global__ void k_bonds(StepArgs A)
     A.bomega[k] = make_double4(omega_t.x, omega_t.y, omega_t.z, omega_n);
     A.bf[k] = make_double4(f.x, f.y, f.z, 1.0);
     A.bt[k] = make_double4(t_j.x, t_j.y, t_j.z, 0.0);
-}
-
-// ---------------------------------------------------------------- integrate
-
-// integration.cuh:14-305 integrate (TY3) for one particle.
-__device__ __forceinline__ void integrate_particle(const StepArgs &A, const DevBox &B,
-                                                   uint32_t i, double4 x, double4 vel,
-                                                   double4 angvel, d3 F, d3 T)
-{
-    const SphParams &P = B.P;
-    const double dt = B.dt;
-    const double4 angpos = A.angpos[i];
-    double4 xyzsum = A.xyzsum[i];
-    int wall0mode = 0;
-    double wall0mass = 0.0;
-    if (B.nw > 0) {
-        wall0mode = B.wmode[0];
-        wall0mass = B.wmvfd[0][0];
-    }
-    double4 acc0 = make_double4(0.0, 0.0, 0.0, 0.0), angacc0 = acc0;
-    if (B.iter != 0) {
-        acc0 = A.acc[i];
-        angacc0 = A.angacc[i];
-    }
-    const double radius = x.w;
-    const double m = 4.0 / 3.0 * PI * radius * radius * radius * P.rho;
-    double acc[3], angacc[3];
-    acc[0] = F.x / m + P.g[0];
-    acc[1] = F.y / m + P.g[1];
-    acc[2] = F.z / m + P.g[2];
-    angacc[0] = T.x * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    angacc[1] = T.y * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    angacc[2] = T.z * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    double angacc_w = 0.0;
-    if (wall0mode == 3 && vel.w > 0.0001 && x.z > B.L[2] * 0.5) {
-        const double f_tau_x = (B.tau_x + B.tau_eff_x) * B.L[0] * B.L[1];
-        acc[0] = f_tau_x / wall0mass;
-        acc[1] = 0.0;
-        acc[2] -= P.g[2];
-        angacc[0] = angacc[1] = angacc[2] = 0.0;
-        angacc_w = 0.0;
-    } else if (vel.w > 0.0001 && vel.w < 10.0) {
-        acc[0] = 0.0;
-        acc[1] = 0.0;
-        acc[2] -= P.g[2];
-        angacc[0] = angacc[1] = angacc[2] = 0.0;
-    }
-    if (vel.w >= 10.0) {
-        acc[1] = 0.0;
-        angacc[0] = 0.0;
-        angacc[2] = 0.0;
-    }
-    if (vel.w < -0.0001) {
-        acc[0] = acc[1] = acc[2] = 0.0;
-        angacc[0] = angacc[1] = angacc[2] = 0.0;
-    }
-    const double a0[3] = {acc0.x, acc0.y, acc0.z};
-    const double w0[3] = {angacc0.x, angacc0.y, angacc0.z};
-    const double xv[3] = {x.x, x.y, x.z};
-    const double vv[3] = {vel.x, vel.y, vel.z};
-    const double pv[3] = {angpos.x, angpos.y, angpos.z};
-    const double wv[3] = {angvel.x, angvel.y, angvel.z};
-    double sv[3] = {xyzsum.x, xyzsum.y, xyzsum.z};
-    double xn[3], vn[3], pn[3], wn[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const double dacc = (acc[d] - a0[d]) / dt;
-        const double dangacc = (angacc[d] - w0[d]) / dt;
-        xn[d] = xv[d] + vv[d] * dt + 0.5 * acc[d] * dt * dt + 1.0 / 6.0 * dacc * dt * dt * dt;
-        vn[d] = vv[d] + acc[d] * dt + 0.5 * dacc * dt * dt;
-        pn[d] = pv[d] + wv[d] * dt + 0.5 * angacc[d] * dt * dt + 1.0 / 6.0 * dangacc * dt * dt * dt;
-        wn[d] = wv[d] + angacc[d] * dt + 0.5 * dangacc * dt * dt;
-        sv[d] += vv[d] * dt + 0.5 * acc[d] * dt * dt + 1.0 / 6.0 * dacc * dt * dt * dt;
-    }
-    if (B.periodic == 1) {
-        if (xn[0] < B.origo[0]) xn[0] += B.L[0];
-        if (xn[0] > B.L[0]) xn[0] -= B.L[0];
-        if (xn[1] < B.origo[1]) xn[1] += B.L[1];
-        if (xn[1] > B.L[1]) xn[1] -= B.L[1];
-    } else if (B.periodic == 2) {
-        if (xn[0] < B.origo[0]) xn[0] += B.L[0];
-        if (xn[0] > B.L[0]) xn[0] -= B.L[0];
-    }
-    if (vel.w > 5.0 && vel.w < 10.0) {
-        if (B.change_velocity_state == 1) vn[0] *= 10.0;
-        else if (B.change_velocity_state == -1) vn[0] /= 10.0;
-    }
-    xyzsum.x = sv[0];
-    xyzsum.y = sv[1];
-    xyzsum.z = sv[2];
-    A.xyzsum[i] = xyzsum;
-    A.acc[i] = make_double4(acc[0], acc[1], acc[2], 0.0);
-    A.angacc[i] = make_double4(angacc[0], angacc[1], angacc[2], angacc_w);
-    A.angvel[i] = make_double4(wn[0], wn[1], wn[2], angvel.w);
-    A.vel[i] = make_double4(vn[0], vn[1], vn[2], vel.w);
-    A.angpos[i] = make_double4(pn[0], pn[1], pn[2], angpos.w);
-    A.x[i] = make_double4(xn[0], xn[1], xn[2], x.w);
-}
-
-// ------------------------------------------------------------------ interact
-
-constexpr int INTERACT_THREADS = 128;
-
-// Fused topology + interact + walls + bond gather (+ integrate when FUSED)
-// for the particle at sorted position a.  Neighbour data is read from the
-// sorted copies only, so writing the particle's new state in place is safe.
-// The particle's contact row is staged in shared memory (slot-major, one
-// column per thread); only live slots are processed, empty slots keep a
-// zero tangential history by construction.
-template <int LM, bool FUSED>
-__global__ void __launch_bounds__(INTERACT_THREADS) k_interact(StepArgs A)
-{
-    __shared__ uint32_t s_row[NC * INTERACT_THREADS];
-    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A.ntot) return;
-    uint32_t *row = s_row + threadIdx.x;
-    const int RS = INTERACT_THREADS;
-    const uint32_t i = A.perm[a];
-    const DevBox &B = A.boxes[A.box_of[i]];
-    const SphParams &P = B.P;
-    const double dt = B.dt;
-    const double4 xa = A.xs[a];
-    const double radius_a = xa.w;
-    const double4 va4 = A.vs[a];
-    const double4 wa4 = A.ws[a];
-    const d3 vel_a = xyz(va4);
-    const d3 angvel_a = xyz(wa4);
-    const uint32_t cm = P.contactmodel;
-
-    const uint4 *grow = reinterpret_cast<const uint4 *>(A.slots + (size_t)i * NC);
-#pragma unroll
-    for (int q = 0; q < NC / 4; ++q) {
-        const uint4 w = grow[q];
-        row[(4 * q + 0) * RS] = w.x;
-        row[(4 * q + 1) * RS] = w.y;
-        row[(4 * q + 2) * RS] = w.z;
-        row[(4 * q + 3) * RS] = w.w;
-    }
-    bool dirty = false;
-
-    Acc acc;
-    acc.F = mk(0.0, 0.0, 0.0);
-    acc.T = mk(0.0, 0.0, 0.0);
-    acc.es_dot = 0.0;
-    acc.ev_dot = 0.0;
-    acc.p = 0.0;
-
-    const int nx = (int)B.num[0], ny = (int)B.num[1];
-    int g[3];
-    if (cm != 0) {
-        g[0] = (int)floor((xa.x - B.origo[0]) / (B.L[0] / B.num[0]));
-        g[1] = (int)floor((xa.y - B.origo[1]) / (B.L[1] / B.num[1]));
-        g[2] = (int)floor((xa.z - B.origo[2]) / (B.L[2] / B.num[2]));
-    }
-
-    if (cm == 2 || cm == 3) {
-        // ---- topology: contactsearch.cuh:329-371 and :194-322
-        int nc = 0;
-        for (int dz = -1; dz < 2; ++dz)
-            for (int dy = -1; dy < 2; ++dy)
-                for (int dx = -1; dx < 2; ++dx) {
-                    int tx = g[0] + dx, ty = g[1] + dy, sx, sy;
-                    const int tz = g[2] + dz;
-                    if (!image_cell(B, tx, ty, tz, sx, sy)) continue;
-                    const d3 dm = shift_vec(B, sx, sy);
-                    const uint32_t cell = B.cell_base + (uint32_t)(tx + ty * nx + (nx * ny) * tz);
-                    const uint32_t start = A.cell_off[cell], end = A.cell_off[cell + 1];
-                    for (uint32_t b = start; b < end; ++b) {
-                        if (b == a) continue;
-                        const double4 xb = A.xs[b];
-                        d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
-                        x_ab = vadd(x_ab, dm);
-                        const double len = vlen<LM>(x_ab);
-                        const double delta = len - (radius_a + xb.w);
-                        if (delta < 0.0) {
-                            const uint32_t b_orig = A.perm[b];
-                            int cpos = nc;
-                            for (int s = 0; s < NC; ++s) {
-                                const uint32_t w = row[s * RS];
-                                if (w == EMPTY) cpos = s;
-                                else if ((w & ID_MASK) == b_orig) { cpos = s; break; }
-                            }
-                            if (cpos < NC) {
-                                row[cpos * RS] = b_orig | (shift_code(sx, sy) << CODE_SHIFT);
-                                dirty = true;
-                            } else {
-                                raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-                            }
-                            ++nc;
-                            if (nc > NC) {
-                                raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-                                break;
-                            }
-                        }
-                    }
-                }
-
-        // ---- interact over the contact row: contactsearch.cuh:484-559
-        double4 *hist = A.hist + (size_t)i * NC;
-        for (int s = 0; s < NC; ++s) {
-            const uint32_t w = row[s * RS];
-            if (w == EMPTY) continue;
-            const uint32_t b_orig = w & ID_MASK;
-            int sx, sy;
-            decode_shift(w >> CODE_SHIFT, sx, sy);
-            const d3 dm = shift_vec(B, sx, sy);
-            const uint32_t bs = A.rank[b_orig];
-            const double4 xb = A.xs[bs];
-            const d3 x_ab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
-            const double x_ab_length = vlen<LM>(x_ab);
-            const double delta_n = x_ab_length - (radius_a + xb.w);
-            if (delta_n < 0.0) {
-                const d3 vel_b = xyz(A.vs[bs]);
-                const d3 angvel_b = xyz(A.ws[bs]);
-                const d3 h0 = xyz(hist[s]);
-                d3 nd;
-                if (cm == 2)
-                    nd = contact_linear<LM>(P, dt, acc, vel_a, vel_b, angvel_a, angvel_b, radius_a,
-                                            xb.w, x_ab, x_ab_length, delta_n, h0);
-                else
-                    nd = contact_hertz<LM>(P, dt, acc, vel_a, vel_b, angvel_a, angvel_b, radius_a,
-                                           xb.w, x_ab, x_ab_length, delta_n, h0);
-                hist[s] = make_double4(nd.x, nd.y, nd.z, 0.0);
-            } else {
-                row[s * RS] = EMPTY;
-                dirty = true;
-                hist[s] = make_double4(0.0, 0.0, 0.0, 0.0);
-            }
-        }
-    } else if (cm == 1) {
-        // ---- contact model 1: contactsearch.cuh:564-598 and :91-186
-        for (int dz = -1; dz < 2; ++dz)
-            for (int dy = -1; dy < 2; ++dy)
-                for (int dx = -1; dx < 2; ++dx) {
-                    int tx = g[0] + dx, ty = g[1] + dy, sx, sy;
-                    const int tz = g[2] + dz;
-                    if (!image_cell(B, tx, ty, tz, sx, sy)) continue;
-                    const d3 dm = shift_vec(B, sx, sy);
-                    const uint32_t cell = B.cell_base + (uint32_t)(tx + ty * nx + (nx * ny) * tz);
-                    const uint32_t start = A.cell_off[cell], end = A.cell_off[cell + 1];
-                    for (uint32_t b = start; b < end; ++b) {
-                        if (b == a) continue;
-                        const double4 xb = A.xs[b];
-                        const double kappa = P.kappa;
-                        d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
-                        x_ab = vadd(x_ab, dm);
-                        const double x_ab_length = vlen<LM>(x_ab);
-                        const double delta_ab = x_ab_length - (radius_a + xb.w);
-                        if (delta_ab < 0.0) {
-                            contact_linear_viscous<LM>(P, acc, vel_a, xyz(A.vs[b]), angvel_a,
-                                                       xyz(A.ws[b]), radius_a, xb.w, x_ab,
-                                                       x_ab_length, delta_ab, kappa);
-                        } else if (delta_ab < P.db) {
-                            capillary_cohesion_exp(P, acc, radius_a, xb.w, delta_ab, x_ab,
-                                                   x_ab_length, kappa);
-                        }
-                    }
-                }
-    }
-
-    // ---- walls: contactsearch.cuh:428-465 and :602-701
-    double wnx[5][4] = {{0.0, 0.0, -1.0, B.L[2]}, {-1.0, 0.0, 0.0, B.L[0]}, {1.0, 0.0, 0.0, 0.0},
-                        {0.0, -1.0, 0.0, B.L[1]}, {0.0, 1.0, 0.0, 0.0}};
-    double wvel[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const uint32_t nw = B.nw;
-    for (uint32_t w = 0; w < 5 && w < nw; ++w) {
-        wnx[w][0] = B.wnx[w][0];
-        wnx[w][1] = B.wnx[w][1];
-        wnx[w][2] = B.wnx[w][2];
-        wnx[w][3] = B.wnx[w][3];
-        wvel[w] = B.wmvfd[w][1];
-    }
-    double w0_force = 0.0;
-    {
-        double delta_w = wnx[0][3] - (xa.z + radius_a);
-        if (delta_w < 0.0)
-            w0_force = contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                               mk(wnx[0][0], wnx[0][1], wnx[0][2]), delta_w, wvel[0]);
-        delta_w = xa.z - radius_a - B.origo[2];
-        if (delta_w < 0.0)
-            (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a, mk(0.0, 0.0, 1.0),
-                                          delta_w, 0.0);
-        if (B.periodic == 0) {
-            delta_w = wnx[1][3] - (xa.x + radius_a);
-            if (delta_w < 0.0)
-                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                              mk(wnx[1][0], wnx[1][1], wnx[1][2]), delta_w, wvel[1]);
-            delta_w = xa.x - radius_a - wnx[2][3];
-            if (delta_w < 0.0)
-                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                              mk(wnx[2][0], wnx[2][1], wnx[2][2]), delta_w, wvel[2]);
-        }
-        if (B.periodic == 0 || B.periodic == 2) {
-            delta_w = wnx[3][3] - (xa.y + radius_a);
-            if (delta_w < 0.0)
-                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                              mk(wnx[3][0], wnx[3][1], wnx[3][2]), delta_w, wvel[3]);
-            delta_w = xa.y - radius_a - wnx[4][3];
-            if (delta_w < 0.0)
-                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                              mk(wnx[4][0], wnx[4][1], wnx[4][2]), delta_w, wvel[4]);
-        }
-    }
-
-    // ---- bond forces in ascending bond order: cohesion.cuh:220-226
-    if (A.nbonds) {
-        const uint32_t e0 = A.bcsr_off[i], e1 = A.bcsr_off[i + 1];
-        for (uint32_t e = e0; e < e1; ++e) {
-            const uint32_t ent = A.bcsr_ent[e];
-            const uint32_t k = ent >> 1;
-            const double4 f = A.bf[k];
-            if (f.w == 0.0) continue;
-            const double4 t = A.bt[k];
-            if ((ent & 1u) == 0) {
-                acc.F = vadd(acc.F, xyz(f));
-                acc.T = vsub(acc.T, xyz(t));
-            } else {
-                acc.F = vsub(acc.F, xyz(f));
-                acc.T = vadd(acc.T, xyz(t));
-            }
-        }
-    }
-
-    if (dirty) {
-        uint4 *wrow = reinterpret_cast<uint4 *>(A.slots + (size_t)i * NC);
-#pragma unroll
-        for (int q = 0; q < NC / 4; ++q)
-            wrow[q] = make_uint4(row[(4 * q) * RS], row[(4 * q + 1) * RS], row[(4 * q + 2) * RS],
-                                 row[(4 * q + 3) * RS]);
-    }
-
-    // ---- contactsearch.cuh:707-724
-    A.force[i] = make_double4(acc.F.x, acc.F.y, acc.F.z, 0.0);
-    A.torque[i] = make_double4(acc.T.x, acc.T.y, acc.T.z, 0.0);
-    A.es_dot[i] = acc.es_dot;
-    A.ev_dot[i] = acc.ev_dot;
-    A.es[i] += acc.es_dot * dt;
-    A.ev[i] += acc.ev_dot * dt;
-    A.p[i] = acc.p;
-    if (nw > 0) A.wf_pp[i] = w0_force;
-
-    if (FUSED) integrate_particle(A, B, i, xa, va4, wa4, acc.F, acc.T);
 }
 
 // Unfused integrate (boxes with a shear-stress wall).
@@ -834,8 +495,26 @@ static inline void mark(Prof *prof, cudaStream_t st, const char *name)
     prof->n++;
 }
 
+// FP64 interact launcher (bit-exact form).
+static void interact_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused, int lm)
+{
+    if (fused) {
+        if (lm == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, true, false><<<grid, INTERACT_THREADS, 0, st>>>(A);
+        else k_interact<SPH_LEN_REFERENCE, true, false><<<grid, INTERACT_THREADS, 0, st>>>(A);
+    } else {
+        if (lm == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, false, false><<<grid, INTERACT_THREADS, 0, st>>>(A);
+        else k_interact<SPH_LEN_REFERENCE, false, false><<<grid, INTERACT_THREADS, 0, st>>>(A);
+    }
+}
+
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
                 Prof *prof)
+{
+    return launch_step_with(A, cfg, st, launches, prof, interact_fp64);
+}
+
+int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
+                     uint64_t *launches, Prof *prof, InteractLauncher interact)
 {
     uint64_t nl = 0;
     if (prof) {
@@ -866,13 +545,11 @@ int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint6
         }
         const unsigned gi = blocks_for(A.ntot, INTERACT_THREADS);
         if (!cfg.unfused) {
-            if (cfg.lenmode == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, true><<<gi, INTERACT_THREADS, 0, st>>>(A);
-            else k_interact<SPH_LEN_REFERENCE, true><<<gi, INTERACT_THREADS, 0, st>>>(A);
+            interact(A, st, gi, true, cfg.lenmode);
             mark(prof, st, "k_interact");
             nl += 1;
         } else {
-            if (cfg.lenmode == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, false><<<gi, INTERACT_THREADS, 0, st>>>(A);
-            else k_interact<SPH_LEN_REFERENCE, false><<<gi, INTERACT_THREADS, 0, st>>>(A);
+            interact(A, st, gi, false, cfg.lenmode);
             mark(prof, st, "k_interact");
             k_shear_stress<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
             k_block_sums<<<A.npartials, 256, 0, st>>>(A, A.tau_pp, A.tau_partial, 1);

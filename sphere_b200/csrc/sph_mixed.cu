@@ -1,12 +1,31 @@
 // sph_mixed.cu -- FP32-mixed step (SPH_PREC_MIXED).
+//
+// Same step as the FP64 form (sort, contact search with the exact FP64
+// overlap test, so the contact lists are identical; walls; bonds; FP64 TY3
+// integration) with the contact-law arithmetic in FP32
+// (sph_mixed_laws.cuh).  Compiled with FMA contraction.
 #include "sph_device.cuh"
 #include "sph_internal.h"
+#include "sph_step.cuh"
 
 namespace sph {
 
-int launch_step_mixed(const StepArgs &, const StepConfig &, cudaStream_t, uint64_t *, Prof *)
+static void interact_mixed(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused, int lm)
 {
-    return SPH_ERR_UNSUPPORTED;
+    if (fused) {
+        if (lm == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, true, true><<<grid, INTERACT_THREADS, 0, st>>>(A);
+        else k_interact<SPH_LEN_REFERENCE, true, true><<<grid, INTERACT_THREADS, 0, st>>>(A);
+    } else {
+        if (lm == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, false, true><<<grid, INTERACT_THREADS, 0, st>>>(A);
+        else k_interact<SPH_LEN_REFERENCE, false, true><<<grid, INTERACT_THREADS, 0, st>>>(A);
+    }
+}
+
+int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
+                      uint64_t *launches, Prof *prof)
+{
+    if (!st && !launches) return SPH_OK;  // capability probe from sph_create
+    return launch_step_with(A, cfg, st, launches, prof, interact_mixed);
 }
 
 }  // namespace sph

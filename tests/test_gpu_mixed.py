@@ -1,0 +1,59 @@
+"""The FP32-mixed step against the FP64 step.
+
+The mixed form keeps the overlap test in FP64, so its contact lists must be
+identical to the FP64 form's; its forces, computed with FP32 contact-law
+arithmetic, must agree per step within 1e-5 relative L2 (the tolerance of
+the precision target), torques within 1e-4, and positions after 100 steps
+within 1e-9 relative to the box size."""
+import numpy
+import pytest
+
+import cases
+from sphere_b200.runner import Stepper
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5
+TORQUE_TOL = 1e-4
+
+
+def rel_l2(a, b):
+    return float(numpy.linalg.norm(a - b) / max(numpy.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("name", ["periodic_xy_wall_stress", "walls_all_sides", "contact_model_1",
+                                  "youngs_modulus", "bonds", "contact_model_3_hertz",
+                                  "shear_stress_wall"])
+def test_mixed_step_error(name):
+    s = cases.make(name)[0]
+    a = Stepper([s], precision="fp64")
+    b = Stepper([s], precision="mixed")
+    a.upload()
+    b.upload()
+    a.step(1)
+    b.step(1)
+    pa, _ = a.download()
+    pb, _ = b.download()
+    assert rel_l2(pb.force, pa.force) < FORCE_TOL
+    assert rel_l2(pb.torque, pa.torque) < TORQUE_TOL
+    ca = a.contacts()[0]
+    cb = b.contacts()[0]
+    assert numpy.array_equal(ca, cb)
+    a.close()
+    b.close()
+
+
+def test_mixed_positions_after_100_steps():
+    s = cases.make("periodic_xy_wall_stress")[0]
+    a = Stepper([s], precision="fp64")
+    b = Stepper([s], precision="mixed")
+    a.upload()
+    b.upload()
+    a.step(100)
+    b.step(100)
+    pa, _ = a.download()
+    pb, _ = b.download()
+    L = float(max(s.L))
+    assert float(numpy.max(numpy.abs(pa.x[:, :3] - pb.x[:, :3]))) / L < 1e-9
+    a.close()
+    b.close()

@@ -5,18 +5,19 @@ layer sheared at 0.01 m/s, k_n = k_t = 1.16e9, gamma_n = 1e3, mu = 0.5,
 NC = 32), one pack per GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-                    [--impl ours|reference] [--n SPHERES]
+                    [--impl ours|reference] [--n SPHERES] [--no-adjoint]
 
 Our arm: W untimed steps, then K steps timed with CUDA events on the stream
 the library launches on (torch's current stream, handed to the library with
 sph_set_stream), bracketed by a barrier and torch.cuda.synchronize(); the
 max over ranks is reported.  The working set (~2.5 GB at 1e6 spheres) is
 far larger than L2, so no L2 flush is needed.  Per-kernel durations come
-from CUDA events recorded inside the last 8 step graphs of the timed region
+from CUDA events recorded inside 8 step graphs run after the timed region
 (sph_profile).  Then: live-contact count for the byte count, the roofline
 of the dominant kernel, the end-to-end time through the C ABI with host
 buffers, and (rank 0, N = 1) the CPU baseline: the reference's own step
-kernels compiled for the CPU (oracle/_ref) on a bounded sample.
+kernels compiled for the CPU (oracle/_ref) on a bounded sample.  Rank 0
+also reports the cost of the adjoint (time_adjoint) under "adjoint".
 
 --impl reference times that CPU reference alone (rank 0; other ranks exit).
 
@@ -35,6 +36,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s @1e6 spheres, FP32-mixed vs FP64 on B200; adjoint/forward cost"
 UNIT = "particle-steps/s"
+PROFILE_RING = 8  # step graphs with event-record nodes held by the C ABI (SphHandle::PR)
 WORKLOAD = ("sheared dense pack, 1e6 spheres: log-normal radii median 0.01 m sigma_ln 0.2 "
             "clipped [0.005, 0.02], porosity 0.40, x-y periodic 1:1:0.5, top wall 20 kPa, "
             "top layer +x 0.01 m/s, k_n=k_t=1.16e9, gamma_n=1e3, mu=0.5, NC=32")
@@ -141,16 +143,65 @@ def cpu_reference_rate(s, nsteps, budget_s=25.0):
     return n * done / dt, done, dt, threads, kind
 
 
+def time_adjoint(device, stream, n=50000, steps=2000, ckpt=100):
+    """Cost of the adjoint on the differentiable settling/impact scene
+    (50,000 spheres, radii U[0.009, 0.011] m, loose pack porosity 0.5,
+    v0 ~ N(0, 0.1) m/s, k_n = 1.5e8, gamma_n = 20, mu = 0.5, 2,000 steps,
+    checkpoint every 100 steps): device time of the plain forward (graph
+    steps), of the checkpointed forward and of the backward pass
+    (recompute + reverse) for loss = mean |x_T - x_target|^2, the target
+    being the same scene run with k_n = 1e8, gamma_n = 50, mu = 0.4."""
+    import numpy
+    import torch
+    from sphere_b200 import scenes
+    from sphere_b200.runner import Stepper
+    s = scenes.loose_pack(n, seed=0, device=device)
+    st = Stepper([s], precision="fp64", length="fp64", device=device)
+    st.set_stream(stream.cuda_stream)
+    st.upload()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    st.step(3)          # graph build and first launches, untimed
+    st.upload()
+    start.record(stream)
+    st.step_async(steps)
+    end.record(stream)
+    end.synchronize()
+    st.sync()
+    plain_ms = start.elapsed_time(end)
+    st.upload()
+    fwd_ms = st.adjoint_forward(steps, ckpt)
+    hp, _ = st.download()
+    tgt = Stepper([scenes.reparam(s, k_n=1e8, gamma_n=50.0, mu=0.4)], precision="fp64",
+                  length="fp64", device=device)
+    tgt.upload()
+    tgt.step(steps)
+    ht, _ = tgt.download()
+    tgt.close()
+    dx = 2.0 * (hp.x[:, :3] - ht.x[:, :3]) / n      # d/dx_T of mean |x_T - x_target|^2
+    g, gv, adj_ms = st.adjoint_backward(dx)
+    st.close()
+    return {"workload": "differentiable settling/impact, 50,000 spheres U[0.009, 0.011] m, "
+                        "loose pack porosity 0.5, v0 ~ N(0, 0.1) m/s, linear contacts "
+                        "k_n=1.5e8 gamma_n=20 mu=0.5, FP64, 2,000 steps, checkpoint every 100",
+            "forward_ms": plain_ms, "forward_checkpointed_ms": fwd_ms, "backward_ms": adj_ms,
+            "backward_over_forward": adj_ms / plain_ms,
+            "forward_and_backward_over_forward": (fwd_ms + adj_ms) / plain_ms,
+            "grad_params": [g["k_n"], g["gamma_n"], g["mu"]],
+            "grad_v0_norm": float(numpy.linalg.norm(gv))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1000000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pack-sweeps", type=int, default=3000)
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -191,68 +242,90 @@ def main():
 
     s = make_scene(args.n, rank, local, args.pack_sweeps)
     n = int(s.np[0])
-    st = Stepper([s], precision=args.precision, length="reference", device=local)
     stream = torch.cuda.current_stream()
-    st.set_stream(stream.cuda_stream)
-    st.upload()
-    st.step(args.warmup)
-
-    clocks = ClockSampler(local)
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    time.sleep(0.3)
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    launches0 = st.kernel_launches()
-    st.profile(True)
-    torch.cuda.nvtx.range_push("timed")
-    start.record(stream)
-    st.step_async(args.steps)
-    end.record(stream)
-    end.synchronize()
-    torch.cuda.nvtx.range_pop()
-    code = st.sync(raise_on_error=False)
-    torch.cuda.synchronize()
-    barrier()
-    clk = clocks.stop()
-    launches = st.kernel_launches() - launches0
-    ms = start.elapsed_time(end)
-    kernels = st.profile_read()
-    st.profile(False)
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * n * args.steps / (ms_max / 1e3)
-    contacts = st.count_contacts()
-
-    # roofline of the dominant kernel
     hbm, peak_kind = peaks()
-    t_int = kernels.get("k_interact")
-    b_int = interact_bytes(n, contacts, args.precision)
-    achieved = b_int / (t_int / 1e3) / 1e9 if t_int else None
-    roofline = {"bound": "hbm", "kernel": "k_interact", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm if achieved else None,
-                "peak_source": peak_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": b_int,
-                "kernel_ms": t_int}
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
-            tr = json.load(fh)
-        roofline["traffic"] = tr["k_interact_bytes_per_sphere"] * n
-        roofline["traffic_source"] = tr.get("source")
-    except Exception:
-        pass
-    st.close()
+
+    def max_over_ranks(v):
+        if world > 1:
+            t = torch.tensor([v], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return v
+
+    def time_form(precision):
+        """W warm-up steps, then K steps timed with CUDA events on the
+        launching stream; per-kernel times from the last 8 step graphs."""
+        st = Stepper([s], precision=precision, length="reference", device=local)
+        st.set_stream(stream.cuda_stream)
+        st.upload()
+        st.step(args.warmup)
+        clocks = ClockSampler(local)
+        barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        time.sleep(0.3)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        launches0 = st.kernel_launches()
+        torch.cuda.nvtx.range_push("timed")
+        start.record(stream)
+        st.step_async(args.steps)
+        end.record(stream)
+        end.synchronize()
+        torch.cuda.nvtx.range_pop()
+        code = st.sync(raise_on_error=False)
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop()
+        launches = st.kernel_launches() - launches0
+        ms_max = max_over_ranks(start.elapsed_time(end))
+        # per-kernel breakdown, after the timed region: the ring of step
+        # graphs with event-record nodes; every ring graph runs once untimed
+        # before the steps whose events are read
+        try:
+            st.profile(True)
+            st.step_async(PROFILE_RING)
+            st.sync(raise_on_error=False)
+            st.step_async(PROFILE_RING)
+            st.sync(raise_on_error=False)
+            kernels = st.profile_read()
+        except Exception as e:  # the timing above stands without the breakdown
+            kernels = {"error": str(e)}
+        st.profile(False)
+        contacts = st.count_contacts()
+        t_int = kernels.get("k_interact")
+        t_int = t_int if isinstance(t_int, float) else None
+        b_int = interact_bytes(n, contacts, precision)
+        achieved = b_int / (t_int / 1e3) / 1e9 if t_int else None
+        roofline = {"bound": "hbm", "kernel": "k_interact", "achieved": achieved, "peak": hbm,
+                    "unit": "GB/s", "frac": achieved / hbm if achieved else None,
+                    "peak_source": peak_kind, "traffic": None,
+                    "algorithmic_bytes_per_launch": b_int, "kernel_ms": t_int}
+        try:
+            with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+                tr = json.load(fh)
+            roofline["traffic"] = tr[precision]["k_interact_bytes_per_sphere"] * n
+            roofline["traffic_source"] = tr.get("source")
+        except Exception:
+            pass
+        st.close()
+        ms_step = ms_max / args.steps
+        return {"value": world * n * args.steps / (ms_max / 1e3), "ms_per_step": ms_step,
+                "roofline": roofline, "kernel_ms": kernels, "live_contacts": contacts,
+                "gpu_launches": launches, "clocks": clk, "device_status": code,
+                "step_gbs": step_bytes(n, contacts, precision) / (ms_step / 1e3) / 1e9}
+
+    forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    res = {f: time_form(f) for f in forms}
+    head = "mixed" if "mixed" in res else forms[0]
+    H = res[head]
 
     # end to end through the C ABI with host buffers: upload from pinned
     # host memory, K steps each followed by a read of the box state (wall
     # force/position, time), download of the final state
     e2e = None
     if rank == 0 or world > 1:
-        st2 = Stepper([s], precision=args.precision, length="reference", device=local)
+        st2 = Stepper([s], precision=head, length="reference", device=local)
         st2.set_stream(stream.cuda_stream)
         hp = HostParticles.from_sims([s])
         for name in ("x", "xyzsum", "vel", "force", "angpos", "angvel", "torque", "es_dot", "es",
@@ -294,6 +367,10 @@ def main():
                        "sph_download"}
         st2.close()
 
+    adj = None
+    if rank == 0 and not args.no_adjoint:
+        adj = time_adjoint(local, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, done, secs, threads, kind = cpu_reference_rate(s, 50, 25.0)
@@ -305,24 +382,30 @@ def main():
     if rank != 0:
         return 0
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+        "metric": METRIC, "value": H["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": H["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if head == "fp64" else "f64+f32",
         "data": "synthetic (seeded GPU-relaxed pack per rank)",
-        "config": {"workload": WORKLOAD, "spheres_per_gpu": n, "precision": args.precision,
-                   "length_mode": "reference", "l2": "working set > L2 (no flush needed)",
+        "config": {"workload": WORKLOAD, "spheres_per_gpu": n, "precision": head,
+                   "forms_timed": forms, "length_mode": "reference",
+                   "l2": "working set > L2 (no flush needed)",
                    "parallelism": "replicas only (one independent pack per GPU)"},
-        "roofline": roofline,
+        "roofline": H["roofline"],
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": launches,
-        "clocks": clk,
-        "live_contacts": contacts,
-        "kernel_ms": kernels,
-        "step_gbs": step_bytes(n, contacts, args.precision) / (ms_max / args.steps / 1e3) / 1e9,
-        "device_status": code,
+        "gpu_launches": H["gpu_launches"],
+        "clocks": H["clocks"],
+        "live_contacts": H["live_contacts"],
+        "kernel_ms": H["kernel_ms"],
+        "step_gbs": H["step_gbs"],
+        "device_status": H["device_status"],
+        "forms": res,
     }
+    if "fp64" in res and "mixed" in res:
+        line["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    if adj is not None:
+        line["adjoint"] = adj
     print(json.dumps(line))
     return 0
 

@@ -226,6 +226,31 @@ uint64_t sph_kernel_launches(const SphHandle *h);
 int sph_relax(SphHandle *h, uint32_t sweeps, double alpha, double z_top,
               double *max_overlap);
 
+/* Differentiable steps (no counterpart in the reference).
+ *
+ * sph_adjoint_forward runs `nsteps` steps as sph_step does and keeps a
+ * device checkpoint of the full state at the start of every `ckpt` steps
+ * and at the end (held by the handle until the backward pass or
+ * sph_destroy).  forward_ms (may be NULL) gets the device time.
+ *
+ * sph_adjoint_backward takes dx_final [np][3] = dLoss/d(final positions)
+ * and returns grad_params[3] = dLoss/dk_n, dLoss/dgamma_n, dLoss/dmu (mu_s
+ * and mu_d tied; k_t held fixed) and grad_v0 [np][3] = dLoss/d(velocities
+ * at the start of the forward); either may be NULL.  Each segment is
+ * recomputed from its checkpoint while a tape of the contact rows and
+ * tangential histories is recorded, then its steps are reversed with the
+ * contact set of each step frozen and each contact law differentiated on
+ * the branch it took (normal force on/off, stick/slip).  adjoint_ms gets
+ * the device time of recompute + reverse.  Afterwards the handle holds the
+ * forward's final state and the checkpoints are released.
+ *
+ * Scope: one box, SPH_PREC_FP64 with SPH_LEN_FP64, contact model 2, E = 0,
+ * kappa = 0, no bonds, no dynamic walls, fixed grid (adaptive 0),
+ * gamma_wt = 0 (SPH_ERR_UNSUPPORTED otherwise). */
+int sph_adjoint_forward(SphHandle *h, uint64_t nsteps, uint32_t ckpt, double *forward_ms);
+int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_params,
+                         double *grad_v0, double *adjoint_ms);
+
 /* Message of the last error on this handle (or a static message for a NULL
  * handle).  Returns the number of characters written. */
 int sph_last_error(const SphHandle *h, char *buf, size_t n);

@@ -201,6 +201,10 @@ def load_library():
     lib.sph_relax.argtypes = [H, C.c_uint32, C.c_double, C.c_double, _dp]
     lib.sph_relax.restype = C.c_int
     lib.sph_step_async.argtypes = [H, C.c_uint64]
+    lib.sph_adjoint_forward.argtypes = [H, C.c_uint64, C.c_uint32, _dp]
+    lib.sph_adjoint_forward.restype = C.c_int
+    lib.sph_adjoint_backward.argtypes = [H, _dp, _dp, _dp, _dp]
+    lib.sph_adjoint_backward.restype = C.c_int
     lib.sph_sync.argtypes = [H]
     lib.sph_set_stream.argtypes = [H, C.c_void_p]
     lib.sph_profile.argtypes = [H, C.c_int]

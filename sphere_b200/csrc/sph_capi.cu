@@ -2,6 +2,7 @@
 // host<->device transfers and the CUDA-graph step driver.
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -20,6 +21,10 @@ int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                       uint64_t *launches, Prof *prof);
 int relax_sweep(const StepArgs &A, cudaStream_t st, double alpha, double z_top,
                 unsigned long long *d_max, uint64_t *launches);
+int adjoint_step(const DevBox *box, uint32_t n, uint64_t iter, const double4 *x,
+                 const double4 *vel, const double4 *angvel, const uint32_t *rows_pre,
+                 const uint32_t *rows_post, const double4 *hist, const double4 *const lnext[5],
+                 double4 *const lcur[5], double4 *lH, double *gparam, cudaStream_t st);
 }
 
 struct SphHandle {
@@ -52,6 +57,10 @@ struct SphHandle {
     std::string err;
     std::vector<void *> allocs;
     unsigned long long *d_count = nullptr;
+    // adjoint: checkpoints of the last sph_adjoint_forward (null when none)
+    char *adj_snaps = nullptr;
+    uint64_t adj_nsteps = 0, adj_iter0 = 0;
+    uint32_t adj_ckpt = 0;
 };
 
 static int fail(SphHandle *h, int code, const std::string &msg)
@@ -210,6 +219,7 @@ void sph_destroy(SphHandle *h)
         if (h->prof_events)
             for (int k = 0; k <= sph::Prof::MAX; ++k) cudaEventDestroy(h->prof[r].ev[k]);
     }
+    if (h->adj_snaps) cudaFree(h->adj_snaps);
     for (void *p : h->allocs) cudaFree(p);
     if (h->own) cudaStreamDestroy(h->own);
     delete h;
@@ -826,6 +836,211 @@ int sph_count_contacts(SphHandle *h, uint64_t *ncontacts)
 }
 
 uint64_t sph_kernel_launches(const SphHandle *h) { return h ? h->launches : 0; }
+
+// ------------------------------------------------------------- adjoint
+
+namespace {
+
+struct StateRef {
+    void *ptr;
+    size_t bytes;
+};
+
+// Every device array a step mutates; a checkpoint is a copy of all of them.
+std::vector<StateRef> mutable_state(SphHandle *h)
+{
+    const size_t n = h->ntot ? h->ntot : 1;
+    const StepArgs &A = h->A;
+    return {{A.x, 32 * n},       {A.vel, 32 * n},      {A.angvel, 32 * n},   {A.angpos, 32 * n},
+            {A.xyzsum, 32 * n},  {A.acc, 32 * n},      {A.angacc, 32 * n},   {A.force, 32 * n},
+            {A.torque, 32 * n},  {A.es_dot, 8 * n},    {A.es, 8 * n},        {A.ev_dot, 8 * n},
+            {A.ev, 8 * n},       {A.p, 8 * n},         {A.slots, 4 * n * sph::NC},
+            {A.hist, 32 * n * sph::NC},                {A.boxes, sizeof(DevBox) * h->nbox}};
+}
+
+size_t state_bytes(SphHandle *h)
+{
+    size_t b = 0;
+    for (const auto &p : mutable_state(h)) b += p.bytes;
+    return b;
+}
+
+void copy_state(SphHandle *h, char *snaps, uint64_t k, bool save)
+{
+    const size_t sb = state_bytes(h);
+    char *c = snaps + sb * k;
+    for (const auto &p : mutable_state(h)) {
+        if (save) cudaMemcpyAsync(c, p.ptr, p.bytes, cudaMemcpyDeviceToDevice, h->stream);
+        else cudaMemcpyAsync(p.ptr, c, p.bytes, cudaMemcpyDeviceToDevice, h->stream);
+        c += p.bytes;
+    }
+}
+
+void free_adjoint(SphHandle *h)
+{
+    if (h->adj_snaps) cudaFree(h->adj_snaps);
+    h->adj_snaps = nullptr;
+    h->adj_nsteps = 0;
+}
+
+}  // namespace
+
+int sph_adjoint_forward(SphHandle *h, uint64_t nsteps, uint32_t ckpt, double *forward_ms)
+{
+    if (!h || nsteps == 0 || ckpt == 0) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_adjoint_forward before sph_upload");
+    const SphBox &b0 = h->boxes[0];
+    if (h->nbox != 1 || h->precision != SPH_PREC_FP64 || h->lenmode != SPH_LEN_FP64 ||
+        b0.params.contactmodel != 2 || b0.params.E > 0.001 || b0.params.kappa != 0.0 ||
+        b0.nb0 != 0 || b0.walls.nw != 0 || b0.grid.adaptive != 0 || b0.params.gamma_wt != 0.0)
+        return fail(h, SPH_ERR_UNSUPPORTED,
+                    "the adjoint covers one box, FP64 with FP64 lengths, contact model 2, E = 0, "
+                    "kappa = 0, no bonds, no dynamic walls, fixed grid, gamma_wt = 0");
+    cudaSetDevice(h->device);
+    int st;
+    if ((st = build_graph(h)) != SPH_OK) return st;
+    free_adjoint(h);
+    const uint64_t nseg = (nsteps + ckpt - 1) / ckpt;
+    const size_t sb = state_bytes(h);
+    void *q = nullptr;
+    if (cudaMalloc(&q, sb * (nseg + 1)) != cudaSuccess)
+        return fail(h, SPH_ERR_NOMEM, "adjoint checkpoints do not fit in device memory");
+    h->adj_snaps = (char *)q;
+    DevBox box0;
+    CUDA_TRY(h, cudaMemcpy(&box0, h->A.boxes, sizeof box0, cudaMemcpyDeviceToHost));
+    h->adj_iter0 = box0.iter;
+    h->adj_nsteps = nsteps;
+    h->adj_ckpt = ckpt;
+    cudaEvent_t ev[2];
+    for (auto &e : ev) cudaEventCreate(&e);
+    cudaEventRecord(ev[0], h->stream);
+    for (uint64_t sgm = 0; sgm < nseg; ++sgm) {
+        copy_state(h, h->adj_snaps, sgm, true);
+        const uint64_t ns = std::min<uint64_t>(ckpt, nsteps - sgm * ckpt);
+        for (uint64_t k = 0; k < ns; ++k)
+            if ((st = launch_one(h)) != SPH_OK) break;
+        if (st != SPH_OK) break;
+    }
+    copy_state(h, h->adj_snaps, nseg, true);
+    cudaEventRecord(ev[1], h->stream);
+    h->launches += nsteps * h->launches_per_step;
+    st = st == SPH_OK ? collect_errors(h) : st;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (forward_ms) *forward_ms = ms;
+    if (st != SPH_OK) free_adjoint(h);
+    return st;
+}
+
+int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_params,
+                         double *grad_v0, double *adjoint_ms)
+{
+    if (!h || !dx_final) return SPH_ERR_INPUT;
+    if (!h->adj_snaps) return fail(h, SPH_ERR_STATE, "sph_adjoint_backward without a forward");
+    cudaSetDevice(h->device);
+    const uint32_t n = (uint32_t)h->ntot;
+    const uint64_t nsteps = h->adj_nsteps, ckpt = h->adj_ckpt;
+    const uint64_t nseg = (nsteps + ckpt - 1) / ckpt;
+    const size_t n4 = sizeof(double4) * (n ? n : 1);
+    const size_t step_tape = 3 * n4 + 2 * sizeof(uint32_t) * n * sph::NC + n4 * sph::NC;
+    std::vector<void *> mine;
+    auto get = [&](size_t bytes) -> void * {
+        void *q = nullptr;
+        if (cudaMalloc(&q, bytes) != cudaSuccess) return nullptr;
+        mine.push_back(q);
+        return q;
+    };
+    auto release = [&]() {
+        for (void *q : mine) cudaFree(q);
+        mine.clear();
+    };
+    char *tape = (char *)get(step_tape * ckpt);
+    double4 *lbuf = (double4 *)get(10 * n4);
+    double4 *lH = (double4 *)get(n4 * sph::NC);
+    double *dscal = (double *)get(sizeof(double) * 3);
+    if (!tape || !lbuf || !lH || !dscal) {
+        release();
+        return fail(h, SPH_ERR_NOMEM, "adjoint buffers do not fit in device memory");
+    }
+    double4 *lnext[5], *lcur[5];
+    for (int k = 0; k < 5; ++k) {
+        lnext[k] = lbuf + (size_t)k * n;
+        lcur[k] = lbuf + (size_t)(5 + k) * n;
+    }
+    std::vector<double4> seed(n ? n : 1);
+    for (uint32_t i = 0; i < n; ++i)
+        seed[i] = make_double4(dx_final[3 * i], dx_final[3 * i + 1], dx_final[3 * i + 2], 0.0);
+    cudaEvent_t ev[2];
+    for (auto &e : ev) cudaEventCreate(&e);
+    int st = SPH_OK;
+    cudaError_t e = cudaMemsetAsync(lbuf, 0, 10 * n4, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(lH, 0, n4 * sph::NC, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dscal, 0, sizeof(double) * 3, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(lnext[0], seed.data(), n4, cudaMemcpyHostToDevice, h->stream);
+    cudaEventRecord(ev[0], h->stream);
+    for (uint64_t sgm = nseg; e == cudaSuccess && sgm-- > 0;) {
+        // recompute the segment from its checkpoint, recording the tape
+        copy_state(h, h->adj_snaps, sgm, false);
+        const uint64_t ns = std::min<uint64_t>(ckpt, nsteps - sgm * ckpt);
+        for (uint64_t k = 0; k < ns; ++k) {
+            char *t = tape + step_tape * k;
+            cudaMemcpyAsync(t, h->A.x, n4, cudaMemcpyDeviceToDevice, h->stream);
+            cudaMemcpyAsync(t + n4, h->A.vel, n4, cudaMemcpyDeviceToDevice, h->stream);
+            cudaMemcpyAsync(t + 2 * n4, h->A.angvel, n4, cudaMemcpyDeviceToDevice, h->stream);
+            StepArgs Ar = h->A;
+            Ar.tape_rows_pre = (uint32_t *)(t + 3 * n4);
+            Ar.tape_rows_post = Ar.tape_rows_pre + (size_t)n * sph::NC;
+            Ar.tape_hist = (double4 *)(Ar.tape_rows_post + (size_t)n * sph::NC);
+            uint64_t nl = 0;
+            if ((st = sph::launch_step(Ar, h->cfg, h->stream, &nl)) != SPH_OK) break;
+            h->launches += nl;
+        }
+        if (st != SPH_OK) break;
+        // reverse the segment's steps
+        for (uint64_t k = ns; k-- > 0;) {
+            const char *t = tape + step_tape * k;
+            const double4 *tx = (const double4 *)t, *tv = tx + n, *tw = tv + n;
+            const uint32_t *rpre = (const uint32_t *)(t + 3 * n4);
+            const uint32_t *rpost = rpre + (size_t)n * sph::NC;
+            const double4 *th = (const double4 *)(rpost + (size_t)n * sph::NC);
+            st = sph::adjoint_step(h->A.boxes, n, h->adj_iter0 + sgm * ckpt + k, tx, tv, tw, rpre,
+                                   rpost, th, lnext, lcur, lH, dscal, h->stream);
+            h->launches += 2;
+            if (st != SPH_OK) break;
+            for (int q = 0; q < 5; ++q) std::swap(lnext[q], lcur[q]);
+        }
+        if (st != SPH_OK) break;
+    }
+    cudaEventRecord(ev[1], h->stream);
+    // leave the handle at the forward's final state
+    copy_state(h, h->adj_snaps, nseg, false);
+    double scal[3] = {0, 0, 0};
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(scal, dscal, sizeof scal, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && grad_v0)
+        e = cudaMemcpyAsync(seed.data(), lnext[1], n4, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    for (auto &x : ev) cudaEventDestroy(x);
+    release();
+    free_adjoint(h);
+    if (st != SPH_OK) return fail(h, st, "adjoint launch failed");
+    if (e != cudaSuccess)
+        return fail(h, SPH_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
+    if (grad_params)
+        for (int k = 0; k < 3; ++k) grad_params[k] = scal[k];
+    if (grad_v0)
+        for (uint32_t i = 0; i < n; ++i) {
+            grad_v0[3 * i] = seed[i].x;
+            grad_v0[3 * i + 1] = seed[i].y;
+            grad_v0[3 * i + 2] = seed[i].z;
+        }
+    if (adjoint_ms) *adjoint_ms = ms;
+    return collect_errors(h);
+}
 
 int sph_relax(SphHandle *h, uint32_t sweeps, double alpha, double z_top, double *max_overlap)
 {

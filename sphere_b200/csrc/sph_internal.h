@@ -40,6 +40,11 @@ struct StepArgs {
     const uint32_t *bond_box;
     const uint32_t *bcsr_off, *bcsr_ent;
     uint32_t *err;
+    // adjoint tape of the current step (null outside a recorded segment):
+    // contact rows at kernel entry and after the contact search, and the
+    // tangential histories the interact pass reads
+    uint32_t *tape_rows_pre, *tape_rows_post;
+    double4 *tape_hist;
 };
 
 struct StepConfig {

@@ -417,6 +417,16 @@ __global__ void k_relax(StepArgs A, double alpha, double z_top, unsigned long lo
     if (below > 0.0) { dz += below; worst = fmax(worst, below); }
     const double above = xa.z + xa.w - z_top;
     if (above > 0.0) { dz -= above; worst = fmax(worst, above); }
+    if (B.periodic == 0) {   // side walls along x
+        const double lo = (B.origo[0] + xa.w) - xa.x, hi = xa.x + xa.w - B.L[0];
+        if (lo > 0.0) { dx += lo; worst = fmax(worst, lo); }
+        if (hi > 0.0) { dx -= hi; worst = fmax(worst, hi); }
+    }
+    if (B.periodic != 1) {   // side walls along y
+        const double lo = (B.origo[1] + xa.w) - xa.y, hi = xa.y + xa.w - B.L[1];
+        if (lo > 0.0) { dy += lo; worst = fmax(worst, lo); }
+        if (hi > 0.0) { dy -= hi; worst = fmax(worst, hi); }
+    }
     A.force[i] = make_double4(dx, dy, dz, 0.0);
     atomicMax(max_ov, (unsigned long long)__double_as_longlong(worst));
 }
@@ -487,11 +497,21 @@ int count_live_slots(const StepArgs &A, cudaStream_t st, unsigned long long *d_c
 
 // ------------------------------------------------------------------ launch
 
+// Record a profiling event on st.  Under stream capture the record must be
+// external, or it only orders the capture and is never timed.
+static inline void record(cudaEvent_t ev, cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal);
+    else cudaEventRecord(ev, st);
+}
+
 static inline void mark(Prof *prof, cudaStream_t st, const char *name)
 {
     if (!prof || prof->n >= Prof::MAX) return;
     prof->name[prof->n] = name;
-    cudaEventRecord(prof->ev[prof->n + 1], st);
+    record(prof->ev[prof->n + 1], st);
     prof->n++;
 }
 
@@ -519,7 +539,7 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
     uint64_t nl = 0;
     if (prof) {
         prof->n = 0;
-        cudaEventRecord(prof->ev[0], st);
+        record(prof->ev[0], st);
     }
     if (A.ntot > 0) {
         cudaMemsetAsync(A.cell_count, 0, sizeof(uint32_t) * A.ncells, st);

@@ -162,6 +162,11 @@ __global__ void __launch_bounds__(INTERACT_THREADS) k_interact(StepArgs A)
         row[(4 * q + 3) * RS] = w.w;
     }
     bool dirty = false;
+    if (A.tape_rows_pre) {
+        uint4 *t = reinterpret_cast<uint4 *>(A.tape_rows_pre + (size_t)i * NC);
+#pragma unroll
+        for (int q = 0; q < NC / 4; ++q) t[q] = grow[q];
+    }
 
     Acc acc;
     acc.F = mk(0.0, 0.0, 0.0);
@@ -228,6 +233,13 @@ __global__ void __launch_bounds__(INTERACT_THREADS) k_interact(StepArgs A)
 
         // ---- interact over the contact row: contactsearch.cuh:484-559
         double4 *hist = A.hist + (size_t)i * NC;
+        if (A.tape_rows_post) {
+            for (int s = 0; s < NC; ++s) {
+                const uint32_t w = row[s * RS];
+                A.tape_rows_post[(size_t)i * NC + s] = w;
+                if (w != EMPTY) A.tape_hist[(size_t)i * NC + s] = hist[s];
+            }
+        }
         for (int s = 0; s < NC; ++s) {
             const uint32_t w = row[s * RS];
             if (w == EMPTY) continue;

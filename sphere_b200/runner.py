@@ -196,6 +196,27 @@ class Stepper(object):
                                        C.byref(mo)), "sph_relax")
         return mo.value
 
+    def adjoint_forward(self, nsteps, ckpt=100):
+        """nsteps steps with a checkpoint every ckpt steps kept for
+        adjoint_backward (sph_adjoint_forward); returns the device ms."""
+        ms = C.c_double(0.0)
+        self._check(self.lib.sph_adjoint_forward(self.h, int(nsteps), int(ckpt), C.byref(ms)),
+                    "sph_adjoint_forward")
+        return ms.value
+
+    def adjoint_backward(self, dx_final):
+        """Reverse pass for dLoss/d(final positions) dx_final [np, 3]
+        (sph_adjoint_backward).  Returns ({"k_n", "gamma_n", "mu"} gradients,
+        dLoss/dv0 [np, 3], device ms)."""
+        dx = numpy.ascontiguousarray(dx_final, dtype=numpy.float64).reshape(-1, 3)
+        gp = numpy.zeros(3)
+        gv = numpy.zeros((dx.shape[0], 3))
+        ms = C.c_double(0.0)
+        self._check(self.lib.sph_adjoint_backward(self.h, _abi.dptr(dx), _abi.dptr(gp),
+                                                  _abi.dptr(gv), C.byref(ms)),
+                    "sph_adjoint_backward")
+        return {"k_n": gp[0], "gamma_n": gp[1], "mu": gp[2]}, gv, ms.value
+
     def advance(self, total, file_dt, current, ftc, max_steps=2 ** 62):
         cur = C.c_double(current)
         f = C.c_double(ftc)

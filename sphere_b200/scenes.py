@@ -228,3 +228,94 @@ def sheared_dense_pack(n=1000000, seed=0, device=-1, sweeps=3000):
     s.time_total[0] = 5000 * s.time_dt[0]
     s.time_file_dt[0] = s.time_total[0]
     return s
+
+
+def _relax_cpu(x, r, lo, hi, iters=4000, tol=1e-12):
+    """Overlap removal on the host: Jacobi sweeps that push every
+    overlapping pair apart by half its overlap each, positions clamped to
+    [lo + r, hi - r].  Stops when the largest overlap is below tol * r."""
+    from scipy.spatial import cKDTree
+    rmax = float(r.max())
+    for _ in range(iters):
+        pairs = cKDTree(x).query_pairs(2.0 * rmax, output_type="ndarray")
+        if len(pairs) == 0:
+            break
+        i, j = pairs[:, 0], pairs[:, 1]
+        d = x[i] - x[j]
+        dist = numpy.sqrt((d * d).sum(1))
+        ov = r[i] + r[j] - dist
+        hit = ov > 0.0
+        if not hit.any() or ov[hit].max() < tol * rmax:
+            break
+        i, j, d, dist, ov = i[hit], j[hit], d[hit], dist[hit], ov[hit]
+        u = d / numpy.maximum(dist, 1e-30)[:, None]
+        push = (0.75 * ov)[:, None] * u
+        dx = numpy.zeros_like(x)
+        numpy.add.at(dx, i, push)
+        numpy.add.at(dx, j, -push)
+        x += dx
+        x[:] = numpy.clip(x, lo + r[:, None], hi - r[:, None])
+    return x
+
+
+def loose_pack(n=50000, seed=0, porosity=0.5, r_range=(0.009, 0.011), vel_sigma=0.1,
+               k_n=1.5e8, gamma_n=20.0, mu=0.5, g=(0.0, 0.0, -9.81), nsteps=2000, device=None,
+               sweeps=4000, sid="loose"):
+    """The differentiable settling/impact scene: n spheres, radii
+    U[r_range], random loose pack at the given porosity in a cube with fixed
+    walls on all sides (uniform random positions, then overlap removal: on
+    the host, or with sph_relax on GPU `device` when one is given),
+    initial velocities N(0, vel_sigma) per component, no spin, linear
+    contacts with k_t = k_n, gamma_t = 0, mu_s = mu_d = mu, wall damping
+    gamma_wn = gamma_n, dt = 0.17 * sqrt(m_min / k_n), nsteps steps."""
+    rng = numpy.random.default_rng(seed)
+    s = sim(np=n, nw=0, sid=sid)
+    r = rng.uniform(r_range[0], r_range[1], n)
+    s.radius[:] = r
+    side = (float(numpy.sum(4.0 / 3.0 * math.pi * r ** 3)) / (1.0 - porosity)) ** (1.0 / 3.0)
+    x = rng.uniform(0.0, side, (n, 3))
+    x = numpy.clip(x, r[:, None], side - r[:, None])
+    s.periodic[0] = 0
+    s.defineWorldBoundaries(L=[side, side, side])
+    if device is None:
+        s.x[:] = _relax_cpu(x, r, 0.0, side)
+    else:
+        from .runner import Stepper
+        s.x[:] = x
+        s.time_dt[0] = 1e-7
+        s.time_total[0] = 1.0
+        st = Stepper([s], device=device)
+        st.upload()
+        st.relax(sweeps, alpha=1.5, z_top=side)
+        st.to_sims()
+        st.close()
+        s.radius[:] = r
+    s.vel[:] = rng.normal(0.0, vel_sigma, (n, 3))
+    s.g[:] = g
+    s.k_n[0] = s.k_t[0] = k_n
+    s.gamma_n[0] = gamma_n
+    s.gamma_t[0] = 0.0
+    s.gamma_wn[0] = gamma_n
+    s.gamma_wt[0] = 0.0
+    s.mu_s[0] = s.mu_d[0] = mu
+    m_min = s.rho[0] * V_sphere(r_range[0])
+    s.time_dt[0] = 0.17 * math.sqrt(m_min / k_n)
+    s.time_current[0] = 0.0
+    s.time_total[0] = nsteps * s.time_dt[0]
+    s.time_file_dt[0] = s.time_total[0]
+    return s
+
+
+def reparam(s, k_n=None, gamma_n=None, mu=None):
+    """A copy of sim s with the contact parameters the adjoint
+    differentiates replaced (mu sets mu_s and mu_d); k_t, the wall damping
+    and the time step are kept."""
+    import copy
+    q = copy.deepcopy(s)
+    if k_n is not None:
+        q.k_n[0] = k_n
+    if gamma_n is not None:
+        q.gamma_n[0] = gamma_n
+    if mu is not None:
+        q.mu_s[0] = q.mu_d[0] = mu
+    return q

@@ -10,7 +10,8 @@ import pytest
 
 import oracle as O
 import physics_cases as P
-from sphere_b200 import binio, sim as simmod
+import sphere_b200 as simmod
+from sphere_b200 import binio
 
 pytestmark = pytest.mark.gpu
 

@@ -8,8 +8,8 @@ NC = 32), one pack per GPU.
                     [--impl ours|reference] [--n SPHERES] [--no-adjoint]
 
 Our arm: W untimed steps, then K steps timed with CUDA events on the stream
-the library launches on (torch's current stream, handed to the library with
-sph_set_stream), bracketed by a barrier and torch.cuda.synchronize(); the
+the library launches on (a torch stream made current and handed to the
+library with sph_set_stream), bracketed by a barrier and torch.cuda.synchronize(); the
 max over ranks is reported.  The working set (~2.5 GB at 1e6 spheres) is
 far larger than L2, so no L2 flush is needed.  Per-kernel durations come
 from CUDA events recorded inside 8 step graphs run after the timed region
@@ -242,7 +242,12 @@ def main():
 
     s = make_scene(args.n, rank, local, args.pack_sweeps)
     n = int(s.np[0])
-    stream = torch.cuda.current_stream()
+    # a stream of our own (never the legacy default stream, whose handle is
+    # 0 and would send the library to its internal stream): the library
+    # launches on it (sph_set_stream) and the timing events are recorded on it
+    stream = torch.cuda.Stream(device=local)
+    assert stream.cuda_stream != 0
+    torch.cuda.set_stream(stream)
     hbm, peak_kind = peaks()
 
     def max_over_ranks(v):
@@ -254,7 +259,7 @@ def main():
 
     def time_form(precision):
         """W warm-up steps, then K steps timed with CUDA events on the
-        launching stream; per-kernel times from the last 8 step graphs."""
+        launching stream; per-kernel times from the profiled step graphs."""
         st = Stepper([s], precision=precision, length="reference", device=local)
         st.set_stream(stream.cuda_stream)
         st.upload()

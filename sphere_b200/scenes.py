@@ -286,7 +286,7 @@ def loose_pack(n=50000, seed=0, porosity=0.5, r_range=(0.009, 0.011), vel_sigma=
         s.time_total[0] = 1.0
         st = Stepper([s], device=device)
         st.upload()
-        st.relax(sweeps, alpha=1.5, z_top=side)
+        st.relax(sweeps, alpha=1.0, z_top=side)
         st.to_sims()
         st.close()
         s.radius[:] = r

@@ -55,7 +55,7 @@ def test_adjoint_matches_torch_autograd_n2000():
     gp_t = numpy.array([q.grad.item() for q in p])
     gv_t = v0.grad.cpu().numpy()
     # same forward up to the order of the force sums
-    assert numpy.abs(x.detach().cpu().numpy() - x_a.numpy()).max() < 1e-13
+    assert numpy.abs(x.detach().cpu().numpy() - x_a.detach().numpy()).max() < 1e-13
     assert abs(loss.item() - loss_a) <= 1e-9 * loss_a
     rel = numpy.abs(gp_a - gp_t) / numpy.abs(gp_t)
     print("param gradients adjoint", gp_a, "autograd", gp_t, "rel", rel)

@@ -38,7 +38,17 @@ def test_run_writes_reference_files_and_matches_oracle(tmp_path):
     assert s.run(verbose=False, root=root) == 0
     assert numpy.array_equal(s.x, x0), "run() must not change the caller's object"
     last = simmod.status(s.sid, root=root)
-    assert last == int(round(0.02 / 0.005))
+    # the reference's output cadence (src/device.cu:1031, 2536-2537, 2569,
+    # 2672): step while time <= total, write when the file clock reaches
+    # file_dt, then restart the file clock at zero
+    dt, cur, ftc, files = float(s.time_dt[0]), float(s.time_current[0]), 0.0, 0
+    while cur <= 0.02:
+        cur += dt
+        ftc += dt
+        if ftc >= 0.005:
+            files += 1
+            ftc = 0.0
+    assert last == files
     for k in range(last + 1):
         assert os.path.exists(os.path.join(root, "output", "%s.output%05d.bin" % (s.sid, k)))
     # output 0 is the input state; the input file is the writebin of the sim

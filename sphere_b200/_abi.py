@@ -202,6 +202,8 @@ def load_library():
     lib.sph_relax.restype = C.c_int
     lib.sph_step_async.argtypes = [H, C.c_uint64]
     lib.sph_adjoint_forward.argtypes = [H, C.c_uint64, C.c_uint32, _dp]
+    lib.sph_cell_offsets_static.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    lib.sph_cell_offsets_static.restype = C.c_int
     lib.sph_adjoint_forward.restype = C.c_int
     lib.sph_adjoint_backward.argtypes = [H, _dp, _dp, _dp, _dp]
     lib.sph_adjoint_backward.restype = C.c_int

@@ -27,6 +27,7 @@ SOURCES = [
     ("sph_capi.cu", ["-fmad=false"]),
     ("sph_mixed.cu", ["-fmad=true"]),
     ("sph_adjoint.cu", ["-fmad=false"]),
+    ("sph_noalloc.cu", []),
 ]
 
 

@@ -263,6 +263,9 @@ def main():
         st = Stepper([s], precision=precision, length="reference", device=local)
         st.set_stream(stream.cuda_stream)
         st.upload()
+        # launch variant of the interact kernel picked on this scene (the
+        # state is put back afterwards), then the warm-up steps
+        variant, variant_ms = st.autotune(steps=20)
         st.step(args.warmup)
         clocks = ClockSampler(local)
         barrier()
@@ -316,6 +319,7 @@ def main():
         st.close()
         ms_step = ms_max / args.steps
         return {"value": world * n * args.steps / (ms_max / 1e3), "ms_per_step": ms_step,
+                "variant": variant, "variant_ms_per_step": variant_ms,
                 "roofline": roofline, "kernel_ms": kernels, "live_contacts": contacts,
                 "gpu_launches": launches, "clocks": clk, "device_status": code,
                 "step_gbs": step_bytes(n, contacts, precision) / (ms_step / 1e3) / 1e9}
@@ -332,6 +336,7 @@ def main():
     if rank == 0 or world > 1:
         st2 = Stepper([s], precision=head, length="reference", device=local)
         st2.set_stream(stream.cuda_stream)
+        st2.set_variant(H["variant"])
         hp = HostParticles.from_sims([s])
         for name in ("x", "xyzsum", "vel", "force", "angpos", "angvel", "torque", "es_dot", "es",
                      "ev_dot", "ev", "p"):
@@ -403,6 +408,7 @@ def main():
         "clocks": H["clocks"],
         "live_contacts": H["live_contacts"],
         "kernel_ms": H["kernel_ms"],
+        "interact_variant": H["variant"],
         "step_gbs": H["step_gbs"],
         "device_status": H["device_status"],
         "forms": res,

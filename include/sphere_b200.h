@@ -251,6 +251,27 @@ int sph_adjoint_forward(SphHandle *h, uint64_t nsteps, uint32_t ckpt, double *fo
 int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_params,
                          double *grad_v0, double *adjoint_ms);
 
+/* Neighbour lists of the contact search (contact models 2 and 3; no
+ * counterpart in the reference, whose search scans the 27 neighbour cells
+ * every step): each sphere keeps the ids of the spheres within
+ * r_a + r_b + 0.1 r_min, rebuilt when a sphere has moved half that skin;
+ * the contacts found, and their order, are those of the cell search.
+ * capacity = list entries per sphere (1..48, default 48; a sphere with
+ * more neighbours uses the cell search), 0 = lists off (cell search for
+ * all).  Takes effect at the next step. */
+int sph_set_neighbor_lists(SphHandle *h, uint32_t capacity);
+
+/* Launch variants of the fused interact kernel (no counterpart in the
+ * reference): the same arithmetic compiled for different register budgets
+ * (variant 0: up to 255 registers per thread, 1: 128, 2: 80), so different
+ * occupancy.  sph_autotune times `steps` steps with each variant from the
+ * current state, keeps the fastest for this handle and puts the state back
+ * as it was (ms_per_step[SPH_TUNE_VARIANTS] may be NULL).  sph_set_variant
+ * picks one directly.  Default 1. */
+#define SPH_TUNE_VARIANTS 3
+int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen);
+int sph_set_variant(SphHandle *h, int variant);
+
 /* Message of the last error on this handle (or a static message for a NULL
  * handle).  Returns the number of characters written. */
 int sph_last_error(const SphHandle *h, char *buf, size_t n);

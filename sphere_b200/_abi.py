@@ -201,6 +201,12 @@ def load_library():
     lib.sph_relax.argtypes = [H, C.c_uint32, C.c_double, C.c_double, _dp]
     lib.sph_relax.restype = C.c_int
     lib.sph_step_async.argtypes = [H, C.c_uint64]
+    lib.sph_set_neighbor_lists.argtypes = [H, C.c_uint32]
+    lib.sph_autotune.argtypes = [H, C.c_uint32, _dp, C.POINTER(C.c_int)]
+    lib.sph_autotune.restype = C.c_int
+    lib.sph_set_variant.argtypes = [H, C.c_int]
+    lib.sph_set_variant.restype = C.c_int
+    lib.sph_set_neighbor_lists.restype = C.c_int
     lib.sph_adjoint_forward.argtypes = [H, C.c_uint64, C.c_uint32, _dp]
     lib.sph_cell_offsets_static.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.sph_cell_offsets_static.restype = C.c_int

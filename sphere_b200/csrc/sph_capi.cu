@@ -57,6 +57,7 @@ struct SphHandle {
     std::string err;
     std::vector<void *> allocs;
     unsigned long long *d_count = nullptr;
+    uint32_t *vlist_mem = nullptr;   // neighbour-list storage (A.vlist is null when off)
     // adjoint: checkpoints of the last sph_adjoint_forward (null when none)
     char *adj_snaps = nullptr;
     uint64_t adj_nsteps = 0, adj_iter0 = 0;
@@ -318,10 +319,15 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_m
         (st = dalloc(h, &A.bf, nb)) || (st = dalloc(h, &A.bt, nb)) ||
         (st = dalloc(h, &A.bbroken, nb)) || (st = dalloc(h, &bond_box, nb)) ||
         (st = dalloc(h, &bcsr_off, n + 1)) || (st = dalloc(h, &bcsr_ent, 2 * nb)) ||
-        (st = dalloc(h, &A.err, 1)) || (st = dalloc(h, &h->d_count, 1))) {
+        (st = dalloc(h, &A.err, 1)) || (st = dalloc(h, &h->d_count, 1)) ||
+        (st = dalloc(h, &A.vlist, n * sph::VL_MAX)) || (st = dalloc(h, &A.vcount, n)) ||
+        (st = dalloc(h, &A.vflag, 2)) || (st = dalloc(h, &A.xref, n)) ||
+        (st = dalloc(h, &A.cellc, n))) {
         fprintf(stderr, "sphere_b200: %s\n", h->err.c_str());
         return bail(st);
     }
+    A.vcap = sph::VL_MAX;
+    h->vlist_mem = A.vlist;
     A.box_of = box_of;
     A.part_owner = part_owner;
     A.bond_box = bond_box;
@@ -513,10 +519,26 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
             for (uint32_t j = 0; j < d.np; ++j) rmax = fmax(rmax, p->x[4 * (size_t)(d.p_base + j) + 3]);
             for (int c = 0; c < 3; ++c) lmax = fmax(lmax, fabs(d.L[c]) + fabs(d.origo[c]));
             d.pre_margin = (float)(ldexp(2.0 * lmax + 2.0 * rmax, -19));
+            // neighbour lists: skin 0.1 r_min; the list is rebuilt once a
+            // sphere has moved half the skin less the rounding allowance;
+            // the build searches the cells that can hold a sphere within
+            // 2 r_max + skin (up to +-3 cells, else lists are off)
+            double rmin = rmax;
+            for (uint32_t j = 0; j < d.np; ++j) rmin = fmin(rmin, p->x[4 * (size_t)(d.p_base + j) + 3]);
+            const double skin = 0.1 * rmin;
+            const double cmin = fmin(d.L[0] / d.num[0], fmin(d.L[1] / d.num[1], d.L[2] / d.num[2]));
+            const double half = 0.5 * skin - 4.0 * (double)d.pre_margin;
+            const double reach = 2.0 * rmax + skin + 2.0 * (double)d.pre_margin;
+            const int R = cmin > 0.0 ? (int)ceil(reach / cmin) : 99;
+            d.vskin = (float)skin;
+            d.vdisp2 = half > 0.0 ? (float)(half * half) : -1.0f;
+            d.vrange = (half > 0.0 && R >= 1 && R <= 3) ? R : 0;
         }
     }
     CUDA_TRY(h, cudaMemcpy(A.boxes, h->dbox.data(), sizeof(DevBox) * h->nbox, cudaMemcpyHostToDevice));
     CUDA_TRY(h, cudaMemset(A.err, 0, sizeof(uint32_t)));
+    CUDA_TRY(h, cudaMemset(A.vflag, 0, 2 * sizeof(uint32_t)));
+    CUDA_TRY(h, cudaMemset(A.vflag, 1, 1));   // build the lists in the first step
     h->uploaded = true;
     return SPH_OK;
 }
@@ -874,6 +896,8 @@ void copy_state(SphHandle *h, char *snaps, uint64_t k, bool save)
         else cudaMemcpyAsync(p.ptr, c, p.bytes, cudaMemcpyDeviceToDevice, h->stream);
         c += p.bytes;
     }
+    // restored positions may lie outside the current neighbour lists
+    if (!save) cudaMemsetAsync(h->A.vflag, 1, 1, h->stream);
 }
 
 void free_adjoint(SphHandle *h)
@@ -1042,6 +1066,100 @@ int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_para
     return collect_errors(h);
 }
 
+// Drop the captured step graphs (they hold the kernel arguments and launch
+// shapes); the next step captures them again.
+static int drop_graphs(SphHandle *h)
+{
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->gexec = nullptr;
+    h->graph = nullptr;
+    for (int r = 0; r < SphHandle::PR; ++r) {
+        if (h->pexec[r]) cudaGraphExecDestroy(h->pexec[r]);
+        if (h->pgraph[r]) cudaGraphDestroy(h->pgraph[r]);
+        h->pexec[r] = nullptr;
+        h->pgraph[r] = nullptr;
+    }
+    if (h->prof_on) return build_prof_graphs(h);
+    return SPH_OK;
+}
+
+int sph_set_variant(SphHandle *h, int variant)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (variant < 0 || variant >= sph::INTERACT_VARIANTS)
+        return fail(h, SPH_ERR_INPUT, "variant out of range");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->cfg.variant = variant;
+    return drop_graphs(h);
+}
+
+int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
+{
+    if (!h || steps == 0) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_autotune before sph_upload");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const size_t sb = state_bytes(h);
+    char *snap = nullptr;
+    if (cudaMalloc((void **)&snap, sb) != cudaSuccess)
+        return fail(h, SPH_ERR_NOMEM, "no device memory for the autotune snapshot");
+    const std::vector<double> t_saved = h->t_host;
+    const uint64_t launches_saved = h->launches;
+    copy_state(h, snap, 0, true);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = h->cfg.variant, st = SPH_OK;
+    double best_ms = 1e300;
+    for (int v = 0; v < sph::INTERACT_VARIANTS && st == SPH_OK; ++v) {
+        h->cfg.variant = v;
+        if ((st = drop_graphs(h)) != SPH_OK || (st = build_graph(h)) != SPH_OK) break;
+        copy_state(h, snap, 0, false);
+        // one untimed step (graph upload, list build), then the timed ones
+        if ((st = launch_one(h)) != SPH_OK) break;
+        cudaEventRecord(e0, h->stream);
+        for (uint32_t k = 0; k < steps && st == SPH_OK; ++k) st = launch_one(h);
+        cudaEventRecord(e1, h->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = SPH_ERR_CUDA;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double per = (double)ms / steps;
+        if (ms_per_step) ms_per_step[v] = per;
+        if (per < best_ms) {
+            best_ms = per;
+            best = v;
+        }
+    }
+    copy_state(h, snap, 0, false);
+    cudaStreamSynchronize(h->stream);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(snap);
+    h->t_host = t_saved;
+    h->launches = launches_saved;
+    cudaMemset(h->A.err, 0, sizeof(uint32_t));
+    h->cfg.variant = best;
+    const int st2 = drop_graphs(h);
+    if (st != SPH_OK) return fail(h, st, "autotune step failed");
+    if (chosen) *chosen = best;
+    return st2;
+}
+
+int sph_set_neighbor_lists(SphHandle *h, uint32_t capacity)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (capacity > (uint32_t)sph::VL_MAX)
+        return fail(h, SPH_ERR_INPUT, "neighbour-list capacity above " + std::to_string(sph::VL_MAX));
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->A.vlist = capacity ? h->vlist_mem : nullptr;
+    h->A.vcap = capacity;
+    CUDA_TRY(h, cudaMemset(h->A.vflag, 1, 1));
+    return drop_graphs(h);
+}
+
 int sph_relax(SphHandle *h, uint32_t sweeps, double alpha, double z_top, double *max_overlap)
 {
     if (!h || !(alpha > 0.0) || !(alpha <= 1.0)) return SPH_ERR_INPUT;
@@ -1058,6 +1176,7 @@ int sph_relax(SphHandle *h, uint32_t sweeps, double alpha, double z_top, double 
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     if (max_overlap) memcpy(max_overlap, &bits, sizeof(double));
     CUDA_TRY(h, cudaMemset(h->A.force, 0, sizeof(double4) * (h->ntot ? h->ntot : 1)));
+    CUDA_TRY(h, cudaMemset(h->A.vflag, 1, 1));
     return collect_errors(h);
 }
 

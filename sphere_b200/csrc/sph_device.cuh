@@ -49,7 +49,13 @@ struct DevBox {
     double dt, t_current;
     double L2_out;             // grid.L[2] of the last step (what an output file holds)
     float pre_margin;          // FP32 candidate prefilter margin (see k_interact)
-    float pad_f;
+    // neighbour lists (k_vlist_build): pairs closer than ra + rb + vskin
+    // at the last build; rebuilt once a sphere has moved more than
+    // sqrt(vdisp2) (< vskin / 2) since; candidates searched over
+    // +-vrange cells
+    float vskin;
+    float vdisp2;
+    int32_t vrange;
     uint64_t iter;
     int32_t velocity_state;
     int32_t change_velocity_state;
@@ -120,6 +126,48 @@ __device__ __forceinline__ bool image_cell(const DevBox &B, int &tx, int &ty, in
     // k_hash) can still be outside after one periodic wrap; never index
     // outside the box's cells.
     if (tx < 0 || tx >= nx || ty < 0 || ty >= ny) return false;
+    return true;
+}
+
+// Cell coordinates packed 21 bits each (k_hash writes them per sphere).
+__device__ __forceinline__ uint64_t pack_cell(uint32_t x, uint32_t y, uint32_t z)
+{
+    return (uint64_t)x | ((uint64_t)y << 21) | ((uint64_t)z << 42);
+}
+__device__ __forceinline__ void unpack_cell(uint64_t c, int &x, int &y, int &z)
+{
+    x = (int)(c & 0x1fffffu);
+    y = (int)((c >> 21) & 0x1fffffu);
+    z = (int)((c >> 42) & 0x1fffffu);
+}
+
+// The neighbour-cell offset (dx, dy, dz in -1..1) and image shift (sx, sy)
+// under which the cell search around cell g visits a sphere in cell b,
+// i.e. the inverse of image_cell; false when the search never visits b's
+// cell.  Needs num >= 3 along periodic axes (checked at sph_create), which
+// makes the offset unique.
+__device__ __forceinline__ bool relative_cell(const DevBox &B, const int g[3], int bx, int by,
+                                              int bz, int &dx, int &dy, int &dz, int &sx, int &sy)
+{
+    dz = bz - g[2];
+    if (dz < -1 || dz > 1) return false;
+    const int nx = (int)B.num[0], ny = (int)B.num[1];
+    sx = 0;
+    sy = 0;
+    dx = bx - g[0];
+    if (dx < -1 || dx > 1) {
+        if (B.periodic != 1 && B.periodic != 2) return false;
+        if (dx == nx - 1 && g[0] == 0) { dx = -1; sx = 1; }
+        else if (dx == 1 - nx && g[0] == nx - 1) { dx = 1; sx = -1; }
+        else return false;
+    }
+    dy = by - g[1];
+    if (dy < -1 || dy > 1) {
+        if (B.periodic != 1) return false;
+        if (dy == ny - 1 && g[1] == 0) { dy = -1; sy = 1; }
+        else if (dy == 1 - ny && g[1] == ny - 1) { dy = 1; sy = -1; }
+        else return false;
+    }
     return true;
 }
 

@@ -40,6 +40,16 @@ struct StepArgs {
     const uint32_t *bond_box;
     const uint32_t *bcsr_off, *bcsr_ent;
     uint32_t *err;
+    // neighbour lists (contact models 2 and 3; vlist null = off): per
+    // sphere (original order) up to vcap partner ids in ascending order,
+    // vcount = their number (VL_MAX + 1 when the list overflowed: that
+    // sphere uses the cell search), xref = position at the list build; cellc = packed cell
+    // coordinates of the current step (k_hash); vflag[0] != 0 requests a
+    // rebuild before the next contact search, vflag[1] counts rebuilds
+    uint32_t *vlist, *vcount, *vflag;
+    float4 *xref;
+    uint64_t *cellc;
+    uint32_t vcap;             // list capacity in use (<= VL_MAX)
     // adjoint tape of the current step (null outside a recorded segment):
     // contact rows at kernel entry and after the contact search, and the
     // tangential histories the interact pass reads
@@ -47,10 +57,14 @@ struct StepArgs {
     double4 *tape_hist;
 };
 
+constexpr int VL_MAX = 48;   // neighbour-list capacity per sphere
+constexpr int INTERACT_VARIANTS = 3;   // launch variants of k_interact (sph_autotune)
+
 struct StepConfig {
     int lenmode;
     bool unfused;     // some box has a shear-stress (wmode 3) top wall
     bool any_walls;   // some box has nw > 0
+    int variant = 1;  // k_interact launch variant (sph_autotune)
 };
 
 // Per-kernel timing of an un-graphed step (the counterpart of the
@@ -68,7 +82,7 @@ struct Prof {
 // nodes).  launch_step runs the FP64 form; launch_step_with takes the
 // launcher of the fused interact kernel (FP64 or FP32-mixed variant).
 typedef void (*InteractLauncher)(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused,
-                                 int lenmode);
+                                 int lenmode, int variant);
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
                 Prof *prof = nullptr);
 int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,

@@ -57,6 +57,7 @@ __global__ void k_hash(StepArgs A)
         raise_flag(A.err, SPH_ERR_OUT_OF_GRID);
     const uint32_t cell = B.cell_base + (c[2] * B.num[1]) * B.num[0] + c[1] * B.num[0] + c[0];
     A.cell_id[i] = cell;
+    if (A.cellc) A.cellc[i] = pack_cell(c[0], c[1], c[2]);
     A.local_off[i] = atomicAdd(&A.cell_count[cell], 1u);
 }
 
@@ -196,6 +197,87 @@ __global__ void k_reorder(StepArgs A)
     A.rank[i] = j;
 }
 
+// --------------------------------------------------------- neighbour lists
+
+constexpr int VLIST_THREADS = 128;
+
+// Neighbour lists for the contact search of contact models 2 and 3: for the
+// sphere at sorted position a, the ids of all spheres within
+// ra + rb + vskin among the +-vrange cells around it (FP32 test widened by
+// the prefilter margin, so the list may hold a few more), ascending and
+// without repeats.  A sphere that moves less than vskin / 2 (checked in the
+// integration against xref) keeps every sphere it can touch in its list.
+// Runs only when vflag[0] is set; a list that overflows vcap (<= VL_MAX) is
+// marked VL_MAX + 1 and that sphere uses the cell search.
+__global__ void __launch_bounds__(VLIST_THREADS) k_vlist_build(StepArgs A)
+{
+    if (A.vflag[0] == 0u) return;
+    __shared__ uint32_t s_list[VL_MAX * VLIST_THREADS];
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A.ntot) return;
+    const int RS = VLIST_THREADS;
+    uint32_t *lst = s_list + threadIdx.x;
+    const uint32_t i = A.perm[a];
+    const DevBox &B = A.boxes[A.box_of[i]];
+    const float4 xaf = A.xf[a];
+    A.xref[i] = xaf;
+    const int R = B.vrange;
+    const uint32_t cm = B.P.contactmodel;
+    if (R < 1 || (cm != 2 && cm != 3)) {
+        A.vcount[i] = VL_MAX + 1;
+        return;
+    }
+    int g0, g1, g2;
+    unpack_cell(A.cellc[i], g0, g1, g2);
+    const int nx = (int)B.num[0], ny = (int)B.num[1];
+    const float reach = B.pre_margin + B.vskin;
+    const float Lf0 = (float)B.L[0], Lf1 = (float)B.L[1];
+    int n = 0;
+    bool over = false;
+    for (int dz = -R; dz <= R && !over; ++dz)
+        for (int dy = -R; dy <= R && !over; ++dy)
+            for (int dx = -R; dx <= R && !over; ++dx) {
+                int tx = g0 + dx, ty = g1 + dy, sx, sy;
+                const int tz = g2 + dz;
+                if (!image_cell(B, tx, ty, tz, sx, sy)) continue;
+                const float fsx = sx == 0 ? 0.f : (sx > 0 ? Lf0 : -Lf0);
+                const float fsy = sy == 0 ? 0.f : (sy > 0 ? Lf1 : -Lf1);
+                const uint32_t cell = B.cell_base + (uint32_t)(tx + ty * nx + (nx * ny) * tz);
+                const uint32_t start = A.cell_off[cell], end = A.cell_off[cell + 1];
+                for (uint32_t b = start; b < end; ++b) {
+                    if (b == a) continue;
+                    if (!maybe_touching(xaf, A.xf[b], fsx, fsy, reach)) continue;
+                    const uint32_t bo = A.perm[b];
+                    int q = n;
+                    while (q > 0 && lst[(q - 1) * RS] > bo) --q;
+                    if (q > 0 && lst[(q - 1) * RS] == bo) continue;   // another image
+                    if (n == (int)A.vcap) {
+                        over = true;
+                        break;
+                    }
+                    for (int k = n; k > q; --k) lst[k * RS] = lst[(k - 1) * RS];
+                    lst[q * RS] = bo;
+                    ++n;
+                }
+            }
+    if (over) {
+        A.vcount[i] = VL_MAX + 1;
+        return;
+    }
+    uint32_t *out = A.vlist + (size_t)i * VL_MAX;
+    for (int k = 0; k < n; ++k) out[k] = lst[k * RS];
+    A.vcount[i] = (uint32_t)n;
+}
+
+// After the (possible) build: clear the request, count builds.
+__global__ void k_vlist_done(StepArgs A)
+{
+    if (A.vflag[0] != 0u) {
+        A.vflag[0] = 0u;
+        A.vflag[1] += 1u;
+    }
+}
+
 // -------------------------------------------------------------------- bonds
 
 // cohesion.cuh:8-233 bondsLinear.  Forces go to per-bond buffers (w = 1
@@ -329,19 +411,40 @@ __global__ void k_tau_final(StepArgs A)
 // integration.cuh:344-450 integrateWalls, then the loop bookkeeping of
 // device.cu:2536-2538, the adaptive grid of device.cu:1050 and the
 // velocity-step state of device.cu:2455-2462 for the next step.
-__global__ void k_box_step(StepArgs A)
+constexpr int BOX_THREADS = 256;
+constexpr int BOX_STAGE = 2048;
+
+// One block per box.  The wall-force total is the sequential sum of the
+// per-block partials in block order (as the reference's integrateWalls
+// loop); the block stages the partials in shared memory with coalesced
+// loads and thread 0 adds them in order.
+__global__ void __launch_bounds__(BOX_THREADS) k_box_step(StepArgs A)
 {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double s_part[BOX_STAGE];
+    const uint32_t b = blockIdx.x;
     if (b >= A.nboxes) return;
     DevBox &B = A.boxes[b];
+    bool any = false;
+    for (uint32_t w = 0; w < B.nw; ++w) any = any || B.wmode[w] != 0;
+    double fsum = 0.0;
+    if (B.np > 0 && any) {
+        for (uint32_t base = 0; base < B.nblocks; base += BOX_STAGE) {
+            const uint32_t cnt = min((uint32_t)BOX_STAGE, B.nblocks - base);
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x)
+                s_part[k] = A.wall_partial[B.part_base + base + k];
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (uint32_t k = 0; k < cnt; ++k) fsum += s_part[k];
+        }
+    }
+    if (threadIdx.x != 0) return;
     const double dt = B.dt;
     if (B.np > 0) {
         for (uint32_t w = 0; w < B.nw; ++w) {
             const int wmode = B.wmode[w];
             if (wmode == 0) continue;
             const double acc0 = B.iter == 0 ? 0.0 : B.wacc[w];
-            double fsum = 0.0;
-            for (uint32_t k = 0; k < B.nblocks; ++k) fsum += A.wall_partial[B.part_base + k];
             B.wmvfd[w][2] = fsum;
             const double sigma_0 =
                 B.wmvfd[w][3] + B.P.sigma0_A * sin(2.0 * PI * B.P.sigma0_f * B.t_current);
@@ -516,15 +619,10 @@ static inline void mark(Prof *prof, cudaStream_t st, const char *name)
 }
 
 // FP64 interact launcher (bit-exact form).
-static void interact_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused, int lm)
+static void interact_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused, int lm,
+                          int variant)
 {
-    if (fused) {
-        if (lm == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, true, false><<<grid, INTERACT_THREADS, 0, st>>>(A);
-        else k_interact<SPH_LEN_REFERENCE, true, false><<<grid, INTERACT_THREADS, 0, st>>>(A);
-    } else {
-        if (lm == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, false, false><<<grid, INTERACT_THREADS, 0, st>>>(A);
-        else k_interact<SPH_LEN_REFERENCE, false, false><<<grid, INTERACT_THREADS, 0, st>>>(A);
-    }
+    launch_interact<false>(A, st, grid, fused, lm, variant);
 }
 
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
@@ -557,6 +655,12 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         k_reorder<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
         mark(prof, st, "k_reorder");
         nl += 8;
+        if (A.vlist) {
+            k_vlist_build<<<blocks_for(A.ntot, VLIST_THREADS), VLIST_THREADS, 0, st>>>(A);
+            k_vlist_done<<<1, 1, 0, st>>>(A);
+            mark(prof, st, "k_vlist");
+            nl += 2;
+        }
         if (A.nbonds) {
             if (cfg.lenmode == SPH_LEN_FP64) k_bonds<SPH_LEN_FP64><<<blocks_for(A.nbonds, 128), 128, 0, st>>>(A);
             else k_bonds<SPH_LEN_REFERENCE><<<blocks_for(A.nbonds, 128), 128, 0, st>>>(A);
@@ -565,11 +669,11 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         }
         const unsigned gi = blocks_for(A.ntot, INTERACT_THREADS);
         if (!cfg.unfused) {
-            interact(A, st, gi, true, cfg.lenmode);
+            interact(A, st, gi, true, cfg.lenmode, cfg.variant);
             mark(prof, st, "k_interact");
             nl += 1;
         } else {
-            interact(A, st, gi, false, cfg.lenmode);
+            interact(A, st, gi, false, cfg.lenmode, cfg.variant);
             mark(prof, st, "k_interact");
             k_shear_stress<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
             k_block_sums<<<A.npartials, 256, 0, st>>>(A, A.tau_pp, A.tau_partial, 1);
@@ -585,7 +689,7 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             nl += 1;
         }
     }
-    k_box_step<<<blocks_for(A.nboxes, 128), 128, 0, st>>>(A);
+    k_box_step<<<A.nboxes, BOX_THREADS, 0, st>>>(A);
     mark(prof, st, "k_box_step");
     nl += 1;
     if (launches) *launches += nl;

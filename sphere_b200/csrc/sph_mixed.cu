@@ -10,15 +10,10 @@
 
 namespace sph {
 
-static void interact_mixed(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused, int lm)
+static void interact_mixed(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused, int lm,
+                           int variant)
 {
-    if (fused) {
-        if (lm == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, true, true><<<grid, INTERACT_THREADS, 0, st>>>(A);
-        else k_interact<SPH_LEN_REFERENCE, true, true><<<grid, INTERACT_THREADS, 0, st>>>(A);
-    } else {
-        if (lm == SPH_LEN_FP64) k_interact<SPH_LEN_FP64, false, true><<<grid, INTERACT_THREADS, 0, st>>>(A);
-        else k_interact<SPH_LEN_REFERENCE, false, true><<<grid, INTERACT_THREADS, 0, st>>>(A);
-    }
+    launch_interact<true>(A, st, grid, fused, lm, variant);
 }
 
 int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,

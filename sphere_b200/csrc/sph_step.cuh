@@ -106,6 +106,24 @@ __device__ __forceinline__ void integrate_particle(const StepArgs &A, const DevB
         if (xn[0] < B.origo[0]) xn[0] += B.L[0];
         if (xn[0] > B.L[0]) xn[0] -= B.L[0];
     }
+    if (A.xref) {
+        // neighbour-list validity: displacement since the list build
+        // (nearest periodic image), FP32
+        const float4 r = A.xref[i];
+        float ex = (float)xn[0] - r.x, ey = (float)xn[1] - r.y;
+        const float ez = (float)xn[2] - r.z;
+        if (B.periodic == 1 || B.periodic == 2) {
+            const float lx = (float)B.L[0];
+            if (ex > 0.5f * lx) ex -= lx;
+            else if (ex < -0.5f * lx) ex += lx;
+        }
+        if (B.periodic == 1) {
+            const float ly = (float)B.L[1];
+            if (ey > 0.5f * ly) ey -= ly;
+            else if (ey < -0.5f * ly) ey += ly;
+        }
+        if (!(ex * ex + ey * ey + ez * ez <= B.vdisp2)) A.vflag[0] = 1u;
+    }
     if (vel.w > 5.0 && vel.w < 10.0) {
         if (B.change_velocity_state == 1) vn[0] *= 10.0;
         else if (B.change_velocity_state == -1) vn[0] /= 10.0;
@@ -132,10 +150,11 @@ constexpr int INTERACT_THREADS = 128;
 // The particle's contact row is staged in shared memory (slot-major, one
 // column per thread); only live slots are processed, empty slots keep a
 // zero tangential history by construction.
-template <int LM, bool FUSED, bool MIXED>
-__global__ void __launch_bounds__(INTERACT_THREADS) k_interact(StepArgs A)
+template <int LM, bool FUSED, bool MIXED, int MINB>
+__global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
 {
     __shared__ uint32_t s_row[NC * INTERACT_THREADS];
+    __shared__ uint16_t s_keys[VL_MAX * INTERACT_THREADS];
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= A.ntot) return;
     uint32_t *row = s_row + threadIdx.x;
@@ -189,6 +208,70 @@ __global__ void __launch_bounds__(INTERACT_THREADS) k_interact(StepArgs A)
         // ---- topology: contactsearch.cuh:329-371 and :194-322
         int nc = 0;
         const float margin = B.pre_margin;
+        const uint32_t vc = A.vlist ? A.vcount[i] : (uint32_t)VL_MAX + 1u;
+        if (vc <= (uint32_t)VL_MAX) {
+            // Same contacts, same order: the cell search visits the 27
+            // neighbour cells in (dz, dy, dx) order and, within a cell, the
+            // spheres in ascending original index (the stable sort).  Every
+            // sphere that can touch is in the neighbour list (ascending
+            // index), so the touching ones are found there, keyed by
+            // (cell ordinal, list position) and inserted in key order.
+            uint16_t *keys = s_keys + threadIdx.x;
+            const uint32_t *lst = A.vlist + (size_t)i * VL_MAX;
+            int nk = 0;
+            for (uint32_t k = 0; k < vc; ++k) {
+                const uint32_t bo = lst[k];
+                int bx, by, bz, dx, dy, dz, sx, sy;
+                unpack_cell(A.cellc[bo], bx, by, bz);
+                if (!relative_cell(B, g, bx, by, bz, dx, dy, dz, sx, sy)) continue;
+                const double4 xb = A.xs[A.rank[bo]];
+                const d3 dm = shift_vec(B, sx, sy);
+                d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
+                x_ab = vadd(x_ab, dm);
+                const double len = vlen<LM>(x_ab);
+                if (len - (radius_a + xb.w) < 0.0) {
+                    const int ord = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+                    const uint16_t key =
+                        (uint16_t)((ord << 10) | (shift_code(sx, sy) << 6) | (int)k);
+                    int q = nk;
+                    while (q > 0 && keys[(q - 1) * RS] > key) {
+                        keys[q * RS] = keys[(q - 1) * RS];
+                        --q;
+                    }
+                    keys[q * RS] = key;
+                    ++nk;
+                }
+            }
+            int cur_ord = -1;
+            bool full = false;
+            for (int q = 0; q < nk; ++q) {
+                const uint32_t key = keys[q * RS];
+                const int ord = (int)(key >> 10);
+                if (ord != cur_ord) {   // the cell search leaves a cell on overflow
+                    cur_ord = ord;
+                    full = false;
+                }
+                if (full) continue;
+                const uint32_t b_orig = lst[key & 63u];
+                int cpos = nc;
+                for (int s = 0; s < NC; ++s) {
+                    const uint32_t w = row[s * RS];
+                    if (w == EMPTY) cpos = s;
+                    else if ((w & ID_MASK) == b_orig) { cpos = s; break; }
+                }
+                if (cpos < NC) {
+                    row[cpos * RS] = b_orig | (((key >> 6) & 15u) << CODE_SHIFT);
+                    dirty = true;
+                } else {
+                    raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+                }
+                ++nc;
+                if (nc > NC) {
+                    raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+                    full = true;
+                }
+            }
+        } else
         for (int dz = -1; dz < 2; ++dz)
             for (int dy = -1; dy < 2; ++dy)
                 for (int dx = -1; dx < 2; ++dx) {
@@ -240,9 +323,16 @@ __global__ void __launch_bounds__(INTERACT_THREADS) k_interact(StepArgs A)
                 if (w != EMPTY) A.tape_hist[(size_t)i * NC + s] = hist[s];
             }
         }
-        for (int s = 0; s < NC; ++s) {
+        // live slots in ascending order, so that the threads of a warp work
+        // on their q-th contact together (the forces still add up in slot
+        // order)
+        uint16_t *live = s_keys + threadIdx.x;
+        int nlive = 0;
+        for (int s = 0; s < NC; ++s)
+            if (row[s * RS] != EMPTY) live[(nlive++) * RS] = (uint16_t)s;
+        for (int q = 0; q < nlive; ++q) {
+            const int s = live[q * RS];
             const uint32_t w = row[s * RS];
-            if (w == EMPTY) continue;
             const uint32_t b_orig = w & ID_MASK;
             int sx, sy;
             decode_shift(w >> CODE_SHIFT, sx, sy);
@@ -401,6 +491,32 @@ __global__ void __launch_bounds__(INTERACT_THREADS) k_interact(StepArgs A)
     if (nw > 0) A.wf_pp[i] = w0_force;
 
     if (FUSED) integrate_particle(A, B, i, xa, va4, wa4, acc.F, acc.T);
+}
+
+// Launch variants of k_interact (INTERACT_VARIANTS): the minimum resident
+// blocks per SM given to the compiler (register budget 255, 128 and 80 per
+// thread), chosen per handle by sph_autotune.  The arithmetic is the same
+// in every variant.
+
+template <bool MIXED, int LM, bool FUSED>
+inline void launch_interact_lm(const StepArgs &A, cudaStream_t st, unsigned grid, int variant)
+{
+    if (variant == 0) k_interact<LM, FUSED, MIXED, 1><<<grid, INTERACT_THREADS, 0, st>>>(A);
+    else if (variant == 2) k_interact<LM, FUSED, MIXED, 6><<<grid, INTERACT_THREADS, 0, st>>>(A);
+    else k_interact<LM, FUSED, MIXED, 4><<<grid, INTERACT_THREADS, 0, st>>>(A);
+}
+
+template <bool MIXED>
+inline void launch_interact(const StepArgs &A, cudaStream_t st, unsigned grid, bool fused, int lm,
+                            int variant)
+{
+    if (fused) {
+        if (lm == SPH_LEN_FP64) launch_interact_lm<MIXED, SPH_LEN_FP64, true>(A, st, grid, variant);
+        else launch_interact_lm<MIXED, SPH_LEN_REFERENCE, true>(A, st, grid, variant);
+    } else {
+        if (lm == SPH_LEN_FP64) launch_interact_lm<MIXED, SPH_LEN_FP64, false>(A, st, grid, variant);
+        else launch_interact_lm<MIXED, SPH_LEN_REFERENCE, false>(A, st, grid, variant);
+    }
 }
 
 }  // namespace sph

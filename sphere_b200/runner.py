@@ -196,6 +196,25 @@ class Stepper(object):
                                        C.byref(mo)), "sph_relax")
         return mo.value
 
+    def set_neighbor_lists(self, capacity):
+        """Neighbour-list capacity per sphere (0 = off, cell search only;
+        default 48), sph_set_neighbor_lists."""
+        self._check(self.lib.sph_set_neighbor_lists(self.h, int(capacity)),
+                    "sph_set_neighbor_lists")
+
+    def autotune(self, steps=20):
+        """Time each launch variant of the interact kernel for `steps` steps
+        from the current state, keep the fastest, restore the state
+        (sph_autotune).  Returns (chosen, [ms per step of each variant])."""
+        ms = numpy.zeros(3)
+        ch = C.c_int(-1)
+        self._check(self.lib.sph_autotune(self.h, int(steps), _abi.dptr(ms), C.byref(ch)),
+                    "sph_autotune")
+        return ch.value, ms.tolist()
+
+    def set_variant(self, variant):
+        self._check(self.lib.sph_set_variant(self.h, int(variant)), "sph_set_variant")
+
     def adjoint_forward(self, nsteps, ckpt=100):
         """nsteps steps with a checkpoint every ckpt steps kept for
         adjoint_backward (sph_adjoint_forward); returns the device ms."""

@@ -84,12 +84,19 @@ def make(name):
         s.w_sigma0_A[0] = 2.0e3
         s.w_sigma0_f[0] = 50.0
         return s, True, 10
+    if name == "fast_spheres":
+        # fast enough that spheres cross cells and periodic boundaries and
+        # the neighbour lists are rebuilt several times
+        s = scenes.lattice_pack(500, seed=13, periodic=1, nw=1, wmode=1, vel_sigma=60.0,
+                                angvel_sigma=100.0)
+        return s, True, 40
     raise KeyError(name)
 
 
 CASES = ["periodic_xy_wall_stress", "walls_all_sides", "periodic_x_wall_velocity",
          "contact_model_1", "contact_model_3_hertz", "youngs_modulus", "bonds", "bonds_breaking",
-         "fixvel_modes", "shear_stress_wall", "adaptive_grid", "sinusoidal_stress"]
+         "fixvel_modes", "shear_stress_wall", "adaptive_grid", "sinusoidal_stress",
+         "fast_spheres"]
 
 # Cases whose results go through a transcendental function (sin) that CUDA
 # and the C library round differently in the last bit.

@@ -65,12 +65,17 @@ def check_same(st, cpu, s, approx=False):
     assert b.t_current == cpu.box.t_current
 
 
+@pytest.mark.parametrize("lists", [48, 0, 3])
 @pytest.mark.parametrize("length", ["reference", "fp64"])
 @pytest.mark.parametrize("name", cases.CASES)
-def test_gpu_matches_oracle(name, length):
+def test_gpu_matches_oracle(name, length, lists):
+    """lists: neighbour-list capacity (48 = default, 0 = cell search only,
+    3 = most spheres overflow their list and fall back to the cell search
+    while others use theirs, in the same step)."""
     s, _ref_ok, steps = cases.make(name)
     cpu = O.CpuRun(s, "oracle", length_mode=0 if length == "reference" else 1)
     st = Stepper([s], precision="fp64", length=length)
+    st.set_neighbor_lists(lists)
     st.upload()
     done = 0
     for chunk in (1, steps // 2 - 1, steps - steps // 2):
@@ -95,3 +100,45 @@ def test_gpu_deterministic():
         st.close()
     for a, b in zip(out[0], out[1]):
         assert numpy.array_equal(a, b)
+
+
+@pytest.mark.parametrize("variant", [0, 2])
+@pytest.mark.parametrize("name", ["periodic_xy_wall_stress", "walls_all_sides", "fast_spheres",
+                                  "shear_stress_wall"])
+def test_launch_variants_match_oracle(name, variant):
+    """Every launch variant of the interact kernel (register budgets 255 and
+    80; 128 is the default above) gives the same bits."""
+    s, _ref_ok, steps = cases.make(name)
+    cpu = O.CpuRun(s, "oracle")
+    st = Stepper([s], precision="fp64")
+    st.set_variant(variant)
+    st.upload()
+    st.step(steps)
+    cpu.step(steps)
+    check_same(st, cpu, s, approx=name in cases.APPROX)
+    st.close()
+
+
+def test_autotune_keeps_the_state_and_the_bits():
+    s, _, steps = cases.make("fast_spheres")
+    a = Stepper([s], precision="fp64")
+    a.upload()
+    a.step(3)
+    before, _ = a.download()
+    c_before = a.contacts()[0].copy()
+    chosen, ms = a.autotune(steps=5)
+    assert chosen in (0, 1, 2) and all(m > 0.0 for m in ms)
+    after, _ = a.download()
+    assert numpy.array_equal(before.x, after.x) and numpy.array_equal(before.vel, after.vel)
+    assert numpy.array_equal(c_before, a.contacts()[0])
+    b = Stepper([s], precision="fp64")
+    b.upload()
+    b.step(3)
+    a.step(steps)
+    b.step(steps)
+    ha, _ = a.download()
+    hb, _ = b.download()
+    assert numpy.array_equal(ha.x, hb.x) and numpy.array_equal(ha.force, hb.force)
+    assert a.boxes()[0].t_current == b.boxes()[0].t_current
+    a.close()
+    b.close()

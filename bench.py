@@ -301,6 +301,7 @@ def main():
             kernels = {"error": str(e)}
         st.profile(False)
         contacts = st.count_contacts()
+        nstats = st.neighbor_stats()
         t_int = kernels.get("k_interact")
         t_int = t_int if isinstance(t_int, float) else None
         b_int = interact_bytes(n, contacts, precision)
@@ -320,6 +321,7 @@ def main():
         ms_step = ms_max / args.steps
         return {"value": world * n * args.steps / (ms_max / 1e3), "ms_per_step": ms_step,
                 "variant": variant, "variant_ms_per_step": variant_ms,
+                "neighbor_lists": nstats,
                 "roofline": roofline, "kernel_ms": kernels, "live_contacts": contacts,
                 "gpu_launches": launches, "clocks": clk, "device_status": code,
                 "step_gbs": step_bytes(n, contacts, precision) / (ms_step / 1e3) / 1e9}

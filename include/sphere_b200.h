@@ -160,7 +160,9 @@ int sph_step_async(SphHandle *h, uint64_t nsteps);
 int sph_sync(SphHandle *h);
 
 /* Run the steps on `cuda_stream` (a cudaStream_t of the handle's device)
- * instead of the handle's own stream; NULL restores the own stream. */
+ * instead of the handle's own stream; NULL restores the own stream.  The
+ * legacy default stream has the handle value NULL too, so a caller that
+ * wants ordering with its own work passes a stream it created. */
 int sph_set_stream(SphHandle *h, void *cuda_stream);
 
 /* Per-kernel timing, the counterpart of the reference's PROFILING
@@ -260,6 +262,10 @@ int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_para
  * more neighbours uses the cell search), 0 = lists off (cell search for
  * all).  Takes effect at the next step. */
 int sph_set_neighbor_lists(SphHandle *h, uint32_t capacity);
+/* stats[5] as of the last step: spheres using their list, spheres whose
+ * list overflowed (they use the cell search), list entries in use, longest
+ * list, list builds so far. */
+int sph_neighbor_stats(SphHandle *h, uint64_t *stats);
 
 /* Launch variants of the fused interact kernel (no counterpart in the
  * reference): the same arithmetic compiled for different register budgets

@@ -202,6 +202,8 @@ def load_library():
     lib.sph_relax.restype = C.c_int
     lib.sph_step_async.argtypes = [H, C.c_uint64]
     lib.sph_set_neighbor_lists.argtypes = [H, C.c_uint32]
+    lib.sph_neighbor_stats.argtypes = [H, C.POINTER(C.c_uint64)]
+    lib.sph_neighbor_stats.restype = C.c_int
     lib.sph_autotune.argtypes = [H, C.c_uint32, _dp, C.POINTER(C.c_int)]
     lib.sph_autotune.restype = C.c_int
     lib.sph_set_variant.argtypes = [H, C.c_int]

@@ -857,6 +857,34 @@ int sph_count_contacts(SphHandle *h, uint64_t *ncontacts)
     return SPH_OK;
 }
 
+int sph_neighbor_stats(SphHandle *h, uint64_t *stats)
+{
+    if (!h || !stats) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const uint64_t n = h->ntot;
+    std::vector<uint32_t> vc(n ? n : 1);
+    uint32_t flag[2] = {0, 0};
+    if (n) CUDA_TRY(h, cudaMemcpy(vc.data(), h->A.vcount, 4 * n, cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(flag, h->A.vflag, sizeof flag, cudaMemcpyDeviceToHost));
+    uint64_t with = 0, over = 0, sum = 0, mx = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (vc[i] > (uint32_t)sph::VL_MAX) {
+            ++over;
+        } else {
+            ++with;
+            sum += vc[i];
+            mx = vc[i] > mx ? vc[i] : mx;
+        }
+    }
+    stats[0] = with;
+    stats[1] = over;
+    stats[2] = sum;
+    stats[3] = mx;
+    stats[4] = flag[1];
+    return SPH_OK;
+}
+
 uint64_t sph_kernel_launches(const SphHandle *h) { return h ? h->launches : 0; }
 
 // ------------------------------------------------------------- adjoint

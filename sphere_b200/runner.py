@@ -202,6 +202,14 @@ class Stepper(object):
         self._check(self.lib.sph_set_neighbor_lists(self.h, int(capacity)),
                     "sph_set_neighbor_lists")
 
+    def neighbor_stats(self):
+        """(spheres with a list, spheres whose list overflowed, entries,
+        longest list, builds so far): sph_neighbor_stats."""
+        out = (C.c_uint64 * 5)()
+        self._check(self.lib.sph_neighbor_stats(self.h, out), "sph_neighbor_stats")
+        return dict(zip(("with_list", "overflowed", "entries", "longest", "builds"),
+                        [int(v) for v in out]))
+
     def autotune(self, steps=20):
         """Time each launch variant of the interact kernel for `steps` steps
         from the current state, keep the fastest, restore the state

@@ -267,14 +267,18 @@ int sph_set_neighbor_lists(SphHandle *h, uint32_t capacity);
  * list, list builds so far. */
 int sph_neighbor_stats(SphHandle *h, uint64_t *stats);
 
-/* Launch variants of the fused interact kernel (no counterpart in the
- * reference): the same arithmetic compiled for different register budgets
- * (variant 0: up to 255 registers per thread, 1: 128, 2: 80), so different
- * occupancy.  sph_autotune times `steps` steps with each variant from the
- * current state, keeps the fastest for this handle and puts the state back
- * as it was (ms_per_step[SPH_TUNE_VARIANTS] may be NULL).  sph_set_variant
- * picks one directly.  Default 1. */
-#define SPH_TUNE_VARIANTS 3
+/* Launch variants of the interact stage (no counterpart in the
+ * reference), all with the same arithmetic and results: 0, 1, 2 = the
+ * fused kernel compiled for up to 255, 128 and 80 registers per thread
+ * (different occupancy); 3 = the split step (contact search, one thread
+ * per contact for the contact laws, one thread per sphere for the sums and
+ * integration), for contact models 2 and 3 with neighbour lists on, which
+ * allocates 32 x 88 B + 36 B per sphere when first chosen.  sph_autotune times
+ * `steps` steps with each applicable variant from the current state, keeps
+ * the fastest for this handle and puts the state back as it was
+ * (ms_per_step[SPH_TUNE_VARIANTS] may be NULL; -1 for a variant not
+ * tried).  sph_set_variant picks one directly.  Default 1. */
+#define SPH_TUNE_VARIANTS 4
 int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen);
 int sph_set_variant(SphHandle *h, int variant);
 

@@ -276,6 +276,10 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_m
     h->cfg.lenmode = length_mode;
     h->cfg.unfused = unfused;
     h->cfg.any_walls = any_walls;
+    h->cfg.all_cm23 = true;
+    for (uint32_t k = 0; k < nboxes; ++k)
+        if (boxes[k].params.contactmodel != 2 && boxes[k].params.contactmodel != 3)
+            h->cfg.all_cm23 = false;
 
     if (device >= 0) {
         if (cudaSetDevice(device) != cudaSuccess) return bail(SPH_ERR_CUDA);
@@ -1112,6 +1116,24 @@ static int drop_graphs(SphHandle *h)
     return SPH_OK;
 }
 
+// Buffers of the split step, allocated when that variant is first chosen.
+static int ensure_split(SphHandle *h)
+{
+    if (h->A.crec) return SPH_OK;
+    const uint64_t n = h->ntot;
+    uint8_t *live = nullptr;
+    uint32_t *nlive = nullptr;
+    sph::ContactRec *crec = nullptr;
+    int st;
+    if ((st = dalloc(h, &live, n * sph::NC)) || (st = dalloc(h, &nlive, n)) ||
+        (st = dalloc(h, &crec, n * sph::NC)))
+        return st;
+    h->A.live = live;
+    h->A.nlive = nlive;
+    h->A.crec = crec;
+    return SPH_OK;
+}
+
 int sph_set_variant(SphHandle *h, int variant)
 {
     if (!h) return SPH_ERR_INPUT;
@@ -1119,6 +1141,10 @@ int sph_set_variant(SphHandle *h, int variant)
         return fail(h, SPH_ERR_INPUT, "variant out of range");
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (variant == sph::SPLIT_VARIANT) {
+        int st = ensure_split(h);
+        if (st != SPH_OK) return st;
+    }
     h->cfg.variant = variant;
     return drop_graphs(h);
 }
@@ -1142,6 +1168,12 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
     int best = h->cfg.variant, st = SPH_OK;
     double best_ms = 1e300;
     for (int v = 0; v < sph::INTERACT_VARIANTS && st == SPH_OK; ++v) {
+        if (ms_per_step) ms_per_step[v] = -1.0;
+        // the split step needs contact models 2/3, fused integration,
+        // neighbour lists and its buffers; otherwise it is not a candidate
+        if (v == sph::SPLIT_VARIANT &&
+            (!h->cfg.all_cm23 || h->cfg.unfused || !h->A.vlist || ensure_split(h) != SPH_OK))
+            continue;
         h->cfg.variant = v;
         if ((st = drop_graphs(h)) != SPH_OK || (st = build_graph(h)) != SPH_OK) break;
         copy_state(h, snap, 0, false);

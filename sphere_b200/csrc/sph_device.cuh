@@ -94,10 +94,42 @@ __device__ __forceinline__ double fsqrtf_d(double d)
     return (double)__fsqrt_rn(__double2float_rn(d));
 }
 
+// Per-sphere sums of a step; the contact laws add to them through these
+// members, in a fixed order per field.
 struct Acc {
     d3 F, T;
     double es_dot, ev_dot, p;
+    __device__ __forceinline__ void addF(d3 v) { F = vadd(F, v); }
+    __device__ __forceinline__ void addT(d3 v) { T = vadd(T, v); }
+    __device__ __forceinline__ void addEs(double v) { es_dot += v; }
+    __device__ __forceinline__ void addEv(double v) { ev_dot += v; }
+    __device__ __forceinline__ void addP(double v) { p += v; }
 };
+
+// The additions one contact law call makes, recorded instead of applied
+// (contact laws add F, T and p once, es_dot at most once and ev_dot at
+// most twice), so that another thread can replay them into the sphere's
+// sums in slot order with the same rounding.  nev < 0 marks a slot whose
+// contact ended this step (nothing to add).
+struct ContactRec {
+    d3 F, T;
+    double ev[2], es, p;
+    int32_t nev, nes;
+    __device__ __forceinline__ void addF(d3 v) { F = v; }
+    __device__ __forceinline__ void addT(d3 v) { T = v; }
+    __device__ __forceinline__ void addEs(double v) { es = v; nes = 1; }
+    __device__ __forceinline__ void addEv(double v) { ev[nev++] = v; }
+    __device__ __forceinline__ void addP(double v) { p = v; }
+};
+
+__device__ __forceinline__ void replay(Acc &a, const ContactRec &r)
+{
+    a.addF(r.F);
+    a.addT(r.T);
+    for (int k = 0; k < r.nev; ++k) a.addEv(r.ev[k]);
+    if (r.nes) a.addEs(r.es);
+    a.addP(r.p);
+}
 
 // Periodic image of a neighbour cell: src/contactsearch.cuh:12-83
 // (findDistMod).  Returns false when the cell lies outside the grid; sx, sy
@@ -192,8 +224,8 @@ __device__ __forceinline__ void decode_shift(uint32_t code, int &sx, int &sy)
 }
 
 // contactmodels.cuh:10-117 contactLinear_wall
-template <int LM>
-__device__ __forceinline__ double contact_linear_wall(const SphParams &P, double dt, Acc &a,
+template <int LM, class AccT>
+__device__ __forceinline__ double contact_linear_wall(const SphParams &P, double dt, AccT &a,
                                                       d3 vel_linear, d3 angvel, double radius_a,
                                                       d3 n, double delta, double wvel)
 {
@@ -205,7 +237,7 @@ __device__ __forceinline__ double contact_linear_wall(const SphParams &P, double
     if (P.E > .001) k_n = 3.141592654 / 2.0 * P.E * radius_a;
     d3 f_n = smul(fmax(0.0, -k_n * delta - P.gamma_wn * vel_n), n);
     double f_n_length = vlen<LM>(f_n);
-    a.ev_dot += P.gamma_wn * vel_n * vel_n;
+    a.addEv(P.gamma_wn * vel_n * vel_n);
     d3 f_t = mk(0.0, 0.0, 0.0);
     if (vel_t_length > 0.0 && P.gamma_wt > 0.0) {
         d3 f_t_visc = smul(P.gamma_wt, vel_t);
@@ -217,18 +249,18 @@ __device__ __forceinline__ double contact_linear_wall(const SphParams &P, double
             f_t = smul(-1.0, f_t_visc);
         } else {
             f_t = divs(smul(-f_t_limit, vel_t), vel_t_length);
-            a.es_dot += vlen<LM>(muls(smul(vlen<LM>(f_t), vel_t), dt)) / dt;
+            a.addEs(vlen<LM>(muls(smul(vlen<LM>(f_t), vel_t), dt)) / dt);
         }
     }
-    a.F = vadd(a.F, vadd(f_n, f_t));
-    a.T = vadd(a.T, cross(smul(-(radius_a + delta * 0.5), n), f_t));
-    a.p += f_n_length / (4.0 * PI * radius_a * radius_a);
+    a.addF(vadd(f_n, f_t));
+    a.addT(cross(smul(-(radius_a + delta * 0.5), n), f_t));
+    a.addP(f_n_length / (4.0 * PI * radius_a * radius_a));
     return dot(f_n, n);
 }
 
 // contactmodels.cuh:122-240 contactLinearViscous (contact model 1)
-template <int LM>
-__device__ __forceinline__ void contact_linear_viscous(const SphParams &P, Acc &a, d3 vel_a,
+template <int LM, class AccT>
+__device__ __forceinline__ void contact_linear_viscous(const SphParams &P, AccT &a, d3 vel_a,
                                                        d3 vel_b, d3 angvel_a, d3 angvel_b,
                                                        double radius_a, double radius_b,
                                                        d3 x_ab, double x_ab_length,
@@ -256,16 +288,16 @@ __device__ __forceinline__ void contact_linear_viscous(const SphParams &P, Acc &
         if (f_t_visc < f_t_limit) f_t = divs(smul(-f_t_visc, vel_t_ab), vel_t_ab_length);
         else f_t = divs(smul(-f_t_limit, vel_t_ab), vel_t_ab_length);
     }
-    a.F = vadd(a.F, vadd(vadd(f_n, f_t), f_c));
-    a.T = vadd(a.T, smul(-(radius_a + delta_ab / 2.0), cross(n_ab, f_t)));
-    a.p += f_n_length / (4.0 * PI * radius_a * radius_a);
+    a.addF(vadd(vadd(f_n, f_t), f_c));
+    a.addT(smul(-(radius_a + delta_ab / 2.0), cross(n_ab, f_t)));
+    a.addP(f_n_length / (4.0 * PI * radius_a * radius_a));
 }
 
 // contactmodels.cuh:244-411 contactLinear (contact model 2); returns the new
 // tangential displacement.  Where the reference leaves it uninitialised
 // (both lengths zero) it is zero.
-template <int LM>
-__device__ __forceinline__ d3 contact_linear(const SphParams &P, double dt, Acc &a, d3 vel_a,
+template <int LM, class AccT>
+__device__ __forceinline__ d3 contact_linear(const SphParams &P, double dt, AccT &a, d3 vel_a,
                                              d3 vel_b, d3 angvel_a, d3 angvel_b, double radius_a,
                                              double radius_b, d3 x, double x_length,
                                              double delta, d3 delta_t0_uncor)
@@ -287,7 +319,7 @@ __device__ __forceinline__ d3 contact_linear(const SphParams &P, double dt, Acc 
     }
     d3 f_n = smul(fmax(0.0, -k_n * delta + P.gamma_n * vel_n), n);
     double f_n_length = vlen<LM>(f_n);
-    a.ev_dot += 0.5 * P.gamma_n * vel_n * vel_n;
+    a.addEv(0.5 * P.gamma_n * vel_n * vel_n);
     d3 f_c = smul(-P.kappa * fsqrtf_d(radius_a * radius_b), n);
     d3 f_t = mk(0.0, 0.0, 0.0);
     if (delta_t0_length > 0.0 || vel_t_length > 0.0) {
@@ -297,18 +329,18 @@ __device__ __forceinline__ d3 contact_linear(const SphParams &P, double dt, Acc 
         f_t = vadd(f_t_elast, f_t_visc);
         double f_t_length = vlen<LM>(f_t);
         double f_t_limit = P.mu_s * vlen<LM>(vsub(f_n, f_c));
-        a.ev_dot += 0.5 * P.gamma_t * vel_t_length * vel_t_length;
+        a.addEv(0.5 * P.gamma_t * vel_t_length * vel_t_length);
         if (f_t_length > f_t_limit) {
             d3 t = divs(f_t, vlen<LM>(f_t));
             f_t = smul(f_t_limit, t);
             delta_t = smul(-1.0 / k_t, vadd(smul(P.mu_d * vlen<LM>(vsub(f_n, f_c)), t),
                                             smul(P.gamma_t, vel_t)));
-            a.es_dot += 0.5 * vlen<LM>(muls(smul(vlen<LM>(f_t), vel_t), dt)) / dt;
+            a.addEs(0.5 * vlen<LM>(muls(smul(vlen<LM>(f_t), vel_t), dt)) / dt);
         }
     }
-    a.F = vadd(a.F, vadd(vadd(f_n, f_t), f_c));
-    a.T = vadd(a.T, cross(smul(-(radius_a + delta * 0.5), n), f_t));
-    a.p += f_n_length / (4.0 * PI * radius_a * radius_a);
+    a.addF(vadd(vadd(f_n, f_t), f_c));
+    a.addT(cross(smul(-(radius_a + delta * 0.5), n), f_t));
+    a.addP(f_n_length / (4.0 * PI * radius_a * radius_a));
     return delta_t;
 }
 
@@ -316,8 +348,8 @@ __device__ __forceinline__ d3 contact_linear(const SphParams &P, double dt, Acc 
 // raises the negative overlap to fractional powers (NaN); here
 // delta^(3/2) = delta*sqrt(|delta|) and delta^(1/4), delta^(1/2) act on
 // |delta|.
-template <int LM>
-__device__ __forceinline__ d3 contact_hertz(const SphParams &P, double dt, Acc &a, d3 vel_a,
+template <int LM, class AccT>
+__device__ __forceinline__ d3 contact_hertz(const SphParams &P, double dt, AccT &a, d3 vel_a,
                                             d3 vel_b, d3 angvel_a, d3 angvel_b, double radius_a,
                                             double radius_b, d3 x_ab, double x_ab_length,
                                             double delta_ab, d3 delta_t0_uncor)
@@ -344,7 +376,7 @@ __device__ __forceinline__ d3 contact_hertz(const SphParams &P, double dt, Acc &
         k_t = k_n;
     }
     d3 f_n = smul(-k_n * d32 - P.gamma_n * d14 * vel_n_ab, n_ab);
-    a.ev_dot += P.gamma_n * vel_n_ab * vel_n_ab;
+    a.addEv(P.gamma_n * vel_n_ab * vel_n_ab);
     if (dot(f_n, n_ab) < 0.0) f_n = mk(0.0, 0.0, 0.0);
     double f_n_length = vlen<LM>(f_n);
     d3 f_c = smul(-P.kappa * fsqrtf_d(radius_a * radius_b), n_ab);
@@ -361,7 +393,7 @@ __device__ __forceinline__ d3 contact_hertz(const SphParams &P, double dt, Acc &
         if (f_t_length > f_t_limit) {
             f_t = muls(f_t, f_t_limit / f_t_length);
             delta_t = divs(vadd(f_t, smul(P.gamma_t * d14, vel_t_ab)), -k_t * d12);
-            a.es_dot += vlen<LM>(vsub(delta_t0, delta_t)) * k_t / dt;
+            a.addEs(vlen<LM>(vsub(delta_t0, delta_t)) * k_t / dt);
         } else {
             delta_t = vadd(delta_t0, muls(vel_t_ab, dt));
         }
@@ -372,9 +404,9 @@ __device__ __forceinline__ d3 contact_hertz(const SphParams &P, double dt, Acc &
                           angvel_ab),
                      angvel_ab_length);
     }
-    a.F = vadd(a.F, vadd(vadd(f_n, f_t), f_c));
-    a.T = vadd(a.T, vadd(smul(-(radius_a + delta_ab / 2.0), cross(n_ab, f_t)), T_res));
-    a.p += f_n_length / (4.0 * PI * radius_a * radius_a);
+    a.addF(vadd(vadd(f_n, f_t), f_c));
+    a.addT(vadd(smul(-(radius_a + delta_ab / 2.0), cross(n_ab, f_t)), T_res));
+    a.addP(f_n_length / (4.0 * PI * radius_a * radius_a));
     return delta_t;
 }
 
@@ -393,7 +425,7 @@ __device__ __forceinline__ void capillary_cohesion_exp(const SphParams &P, Acc &
     double R_geo = fsqrtf_d(radius_a * radius_b);
     double lambda = (double)0.9f * h * fsqrtf_d(P.V_b / R_har);
     d3 f_c = smul(-kappa * R_geo * (double)expf(__double2float_rn(-delta_ab / lambda)), n_ab);
-    a.F = vadd(a.F, f_c);
+    a.addF(f_c);
 }
 
 }  // namespace sph

@@ -10,6 +10,7 @@
 namespace sph {
 
 struct DevBox;
+struct ContactRec;
 
 // Device pointers of one handle, passed by value to every step kernel.
 struct StepArgs {
@@ -50,6 +51,12 @@ struct StepArgs {
     float4 *xref;
     uint64_t *cellc;
     uint32_t vcap;             // list capacity in use (<= VL_MAX)
+    // split step (k_search / k_contacts / k_finish): per sphere the live
+    // slots in ascending order and their number, and per live contact the
+    // additions its law made (null until the split step is first used)
+    uint8_t *live;
+    uint32_t *nlive;
+    ContactRec *crec;
     // adjoint tape of the current step (null outside a recorded segment):
     // contact rows at kernel entry and after the contact search, and the
     // tangential histories the interact pass reads
@@ -58,13 +65,15 @@ struct StepArgs {
 };
 
 constexpr int VL_MAX = 48;   // neighbour-list capacity per sphere
-constexpr int INTERACT_VARIANTS = 3;   // launch variants of k_interact (sph_autotune)
+constexpr int INTERACT_VARIANTS = 4;   // launch variants of the interact stage (sph_autotune)
+constexpr int SPLIT_VARIANT = 3;       // the split step (k_search / k_contacts / k_finish)
 
 struct StepConfig {
     int lenmode;
     bool unfused;     // some box has a shear-stress (wmode 3) top wall
     bool any_walls;   // some box has nw > 0
-    int variant = 1;  // k_interact launch variant (sph_autotune)
+    int variant = 1;  // interact launch variant (sph_autotune)
+    bool all_cm23 = false;   // every box uses contact model 2 or 3
 };
 
 // Per-kernel timing of an un-graphed step (the counterpart of the
@@ -85,8 +94,10 @@ typedef void (*InteractLauncher)(const StepArgs &A, cudaStream_t st, unsigned gr
                                  int lenmode, int variant);
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
                 Prof *prof = nullptr);
+typedef void (*ContactLauncher)(const StepArgs &A, cudaStream_t st, unsigned grid, int lenmode);
 int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
-                     uint64_t *launches, Prof *prof, InteractLauncher interact);
+                     uint64_t *launches, Prof *prof, InteractLauncher interact,
+                     ContactLauncher contact);
 int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                       uint64_t *launches, Prof *prof);
 

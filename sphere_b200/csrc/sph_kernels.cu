@@ -625,14 +625,20 @@ static void interact_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, boo
     launch_interact<false>(A, st, grid, fused, lm, variant);
 }
 
+static void contacts_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, int lm)
+{
+    launch_contacts<false>(A, st, grid, lm);
+}
+
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
                 Prof *prof)
 {
-    return launch_step_with(A, cfg, st, launches, prof, interact_fp64);
+    return launch_step_with(A, cfg, st, launches, prof, interact_fp64, contacts_fp64);
 }
 
 int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
-                     uint64_t *launches, Prof *prof, InteractLauncher interact)
+                     uint64_t *launches, Prof *prof, InteractLauncher interact,
+                     ContactLauncher contact)
 {
     uint64_t nl = 0;
     if (prof) {
@@ -668,12 +674,31 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             nl += 1;
         }
         const unsigned gi = blocks_for(A.ntot, INTERACT_THREADS);
-        if (!cfg.unfused) {
-            interact(A, st, gi, true, cfg.lenmode, cfg.variant);
+        const bool split = cfg.variant == SPLIT_VARIANT && !cfg.unfused && cfg.all_cm23 &&
+                           A.vlist && A.crec;
+        if (split) {
+            if (cfg.lenmode == SPH_LEN_FP64)
+                k_search<SPH_LEN_FP64><<<blocks_for(A.ntot, SEARCH_THREADS), SEARCH_THREADS, 0, st>>>(A);
+            else
+                k_search<SPH_LEN_REFERENCE><<<blocks_for(A.ntot, SEARCH_THREADS), SEARCH_THREADS, 0, st>>>(A);
+            mark(prof, st, "k_search");
+            contact(A, st, blocks_for((uint64_t)A.ntot * CONTACT_LANES, CONTACT_THREADS),
+                    cfg.lenmode);
+            mark(prof, st, "k_contacts");
+            if (cfg.lenmode == SPH_LEN_FP64)
+                k_finish<SPH_LEN_FP64><<<blocks_for(A.ntot, FINISH_THREADS), FINISH_THREADS, 0, st>>>(A);
+            else
+                k_finish<SPH_LEN_REFERENCE><<<blocks_for(A.ntot, FINISH_THREADS), FINISH_THREADS, 0, st>>>(A);
+            mark(prof, st, "k_finish");
+            nl += 3;
+        } else if (!cfg.unfused) {
+            interact(A, st, gi, true, cfg.lenmode,
+                     cfg.variant == SPLIT_VARIANT ? 1 : cfg.variant);
             mark(prof, st, "k_interact");
             nl += 1;
         } else {
-            interact(A, st, gi, false, cfg.lenmode, cfg.variant);
+            interact(A, st, gi, false, cfg.lenmode,
+                     cfg.variant == SPLIT_VARIANT ? 1 : cfg.variant);
             mark(prof, st, "k_interact");
             k_shear_stress<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
             k_block_sums<<<A.npartials, 256, 0, st>>>(A, A.tau_pp, A.tau_partial, 1);

@@ -16,11 +16,16 @@ static void interact_mixed(const StepArgs &A, cudaStream_t st, unsigned grid, bo
     launch_interact<true>(A, st, grid, fused, lm, variant);
 }
 
+static void contacts_mixed(const StepArgs &A, cudaStream_t st, unsigned grid, int lm)
+{
+    launch_contacts<true>(A, st, grid, lm);
+}
+
 int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                       uint64_t *launches, Prof *prof)
 {
     if (!st && !launches) return SPH_OK;  // capability probe from sph_create
-    return launch_step_with(A, cfg, st, launches, prof, interact_mixed);
+    return launch_step_with(A, cfg, st, launches, prof, interact_mixed, contacts_mixed);
 }
 
 }  // namespace sph

@@ -67,7 +67,8 @@ __device__ __forceinline__ void mixed_stiffness(const SphParams &P, float ra, fl
 }
 
 // contactLinear (contact model 2), contactmodels.cuh:244-411
-__device__ __forceinline__ d3 contact_linear_mixed(const SphParams &P, double dt, Acc &a,
+template <class AccT>
+__device__ __forceinline__ d3 contact_linear_mixed(const SphParams &P, double dt, AccT &a,
                                                    const MixedPair &q, d3 delta_t0_uncor)
 {
     const f3 n = q.n;
@@ -86,7 +87,7 @@ __device__ __forceinline__ d3 contact_linear_mixed(const SphParams &P, double dt
     const float fnm = fmaxf(0.0f, -k_n * delta + gn * vel_n);
     const f3 f_n = fmul(fnm, n);
     const float f_n_length = fabsf(fnm);
-    a.ev_dot += (double)(0.5f * gn * vel_n * vel_n);
+    a.addEv((double)(0.5f * gn * vel_n * vel_n));
     const f3 f_c = fmul(-(float)P.kappa * sqrtf(q.ra * q.rb), n);
     f3 f_t = fk(0.f, 0.f, 0.f);
     d3 delta_t = mk(0.0, 0.0, 0.0);
@@ -96,23 +97,24 @@ __device__ __forceinline__ d3 contact_linear_mixed(const SphParams &P, double dt
         const float f_t_length = flen(f_t);
         const float fnc = flen(fsub(f_n, f_c));
         const float f_t_limit = (float)P.mu_s * fnc;
-        a.ev_dot += (double)(0.5f * gt * vel_t_length * vel_t_length);
+        a.addEv((double)(0.5f * gt * vel_t_length * vel_t_length));
         if (f_t_length > f_t_limit) {
             const f3 t = fmul(1.0f / f_t_length, f_t);
             f_t = fmul(f_t_limit, t);
             delta_t = tod(fmul(-1.0f / k_t, fadd(fmul((float)P.mu_d * fnc, t), fmul(gt, vel_t))));
-            a.es_dot += (double)(0.5f * flen(fmul((float)dt * f_t_limit, vel_t)) / (float)dt);
+            a.addEs((double)(0.5f * flen(fmul((float)dt * f_t_limit, vel_t)) / (float)dt));
         }
     }
-    a.F = vadd(a.F, tod(fadd(fadd(f_n, f_t), f_c)));
-    a.T = vadd(a.T, tod(fcross(fmul(-(q.ra + delta * 0.5f), n), f_t)));
-    a.p += (double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra));
+    a.addF(tod(fadd(fadd(f_n, f_t), f_c)));
+    a.addT(tod(fcross(fmul(-(q.ra + delta * 0.5f), n), f_t)));
+    a.addP((double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra)));
     return delta_t;
 }
 
 // contactHertz (contact model 3) with the overlap-magnitude powers of the
 // FP64 form, contactmodels.cuh:417-600
-__device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt, Acc &a,
+template <class AccT>
+__device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt, AccT &a,
                                                   const MixedPair &q, d3 delta_t0_uncor)
 {
     const f3 n = q.n;
@@ -132,7 +134,7 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
     mixed_stiffness(P, q.ra, q.rb, k_n, k_t);
     const float gn = (float)P.gamma_n, gt = (float)P.gamma_t;
     f3 f_n = fmul(-k_n * d32 - gn * d14 * vel_n_ab, n);
-    a.ev_dot += (double)(gn * vel_n_ab * vel_n_ab);
+    a.addEv((double)(gn * vel_n_ab * vel_n_ab));
     if (fdot(f_n, n) < 0.0f) f_n = fk(0.f, 0.f, 0.f);
     const float f_n_length = flen(f_n);
     const f3 f_c = fmul(-(float)P.kappa * sqrtf(q.ra * q.rb), n);
@@ -149,7 +151,7 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
         if (f_t_length > f_t_limit) {
             f_t = fmul(f_t_limit / f_t_length, f_t);
             delta_t = tod(fmul(1.0f / (-k_t * d12), fadd(f_t, fmul(gt * d14, vel_t_ab))));
-            a.es_dot += sqrt(dot(vsub(delta_t0, delta_t), vsub(delta_t0, delta_t))) * (double)k_t / dt;
+            a.addEs(sqrt(dot(vsub(delta_t0, delta_t), vsub(delta_t0, delta_t))) * (double)k_t / dt);
         } else {
             delta_t = vadd(delta_t0, muls(tod(vel_t_ab), dt));
         }
@@ -158,14 +160,15 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
         T_res = fmul(-fminf((float)P.gamma_r * q.ra * angvel_ab_length,
                             (float)P.mu_r * q.ra * f_n_length) / angvel_ab_length,
                      angvel_ab);
-    a.F = vadd(a.F, tod(fadd(fadd(f_n, f_t), f_c)));
-    a.T = vadd(a.T, tod(fadd(fmul(-(q.ra + delta * 0.5f), fcross(n, f_t)), T_res)));
-    a.p += (double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra));
+    a.addF(tod(fadd(fadd(f_n, f_t), f_c)));
+    a.addT(tod(fadd(fmul(-(q.ra + delta * 0.5f), fcross(n, f_t)), T_res)));
+    a.addP((double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra)));
     return delta_t;
 }
 
 // contactLinearViscous (contact model 1), contactmodels.cuh:122-240
-__device__ __forceinline__ void contact_linear_viscous_mixed(const SphParams &P, Acc &a,
+template <class AccT>
+__device__ __forceinline__ void contact_linear_viscous_mixed(const SphParams &P, AccT &a,
                                                              const MixedPair &q, float kappa)
 {
     const f3 n = q.n;
@@ -189,9 +192,9 @@ __device__ __forceinline__ void contact_linear_viscous_mixed(const SphParams &P,
         const float mag = f_t_visc < f_t_limit ? f_t_visc : f_t_limit;
         f_t = fmul(-mag / vel_t_ab_length, vel_t_ab);
     }
-    a.F = vadd(a.F, tod(fadd(fadd(f_n, f_t), f_c)));
-    a.T = vadd(a.T, tod(fmul(-(q.ra + delta * 0.5f), fcross(n, f_t))));
-    a.p += (double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra));
+    a.addF(tod(fadd(fadd(f_n, f_t), f_c)));
+    a.addT(tod(fmul(-(q.ra + delta * 0.5f), fcross(n, f_t))));
+    a.addP((double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra)));
 }
 
 }  // namespace sph

@@ -142,6 +142,221 @@ __device__ __forceinline__ void integrate_particle(const StepArgs &A, const DevB
 
 // ------------------------------------------------------------------ interact
 
+// The contact search of one sphere (contact models 2 and 3) on its slot row
+// staged in shared memory (row[s * RS]): new contacts inserted with the
+// reference's rule, from the neighbour list when the sphere has one, else
+// from the 27 neighbour cells.  keys: shared scratch of VL_MAX entries at
+// stride RS.  Returns whether the row changed.
+template <int LM>
+__device__ __forceinline__ bool search_contacts(const StepArgs &A, const DevBox &B, uint32_t a,
+                                                uint32_t i, double4 xa, const int g[3],
+                                                float4 xaf, uint32_t *row, uint16_t *keys,
+                                                int RS)
+{
+    const double radius_a = xa.w;
+    const int nx = (int)B.num[0], ny = (int)B.num[1];
+    const float Lf0 = (float)B.L[0], Lf1 = (float)B.L[1];
+    bool dirty = false;
+    int nc = 0;
+    const float margin = B.pre_margin;
+    const uint32_t vc = A.vlist ? A.vcount[i] : (uint32_t)VL_MAX + 1u;
+    if (vc <= (uint32_t)VL_MAX) {
+        // Same contacts, same order: the cell search visits the 27
+        // neighbour cells in (dz, dy, dx) order and, within a cell, the
+        // spheres in ascending original index (the stable sort).  Every
+        // sphere that can touch is in the neighbour list (ascending
+        // index), so the touching ones are found there, keyed by
+        // (cell ordinal, list position) and inserted in key order.
+        const uint32_t *lst = A.vlist + (size_t)i * VL_MAX;
+        int nk = 0;
+        for (uint32_t k = 0; k < vc; ++k) {
+            const uint32_t bo = lst[k];
+            int bx, by, bz, dx, dy, dz, sx, sy;
+            unpack_cell(A.cellc[bo], bx, by, bz);
+            if (!relative_cell(B, g, bx, by, bz, dx, dy, dz, sx, sy)) continue;
+            const double4 xb = A.xs[A.rank[bo]];
+            const d3 dm = shift_vec(B, sx, sy);
+            d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
+            x_ab = vadd(x_ab, dm);
+            const double len = vlen<LM>(x_ab);
+            if (len - (radius_a + xb.w) < 0.0) {
+                const int ord = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+                const uint16_t key =
+                    (uint16_t)((ord << 10) | (shift_code(sx, sy) << 6) | (int)k);
+                int q = nk;
+                while (q > 0 && keys[(q - 1) * RS] > key) {
+                    keys[q * RS] = keys[(q - 1) * RS];
+                    --q;
+                }
+                keys[q * RS] = key;
+                ++nk;
+            }
+        }
+        int cur_ord = -1;
+        bool full = false;
+        for (int q = 0; q < nk; ++q) {
+            const uint32_t key = keys[q * RS];
+            const int ord = (int)(key >> 10);
+            if (ord != cur_ord) {   // the cell search leaves a cell on overflow
+                cur_ord = ord;
+                full = false;
+            }
+            if (full) continue;
+            const uint32_t b_orig = lst[key & 63u];
+            int cpos = nc;
+            for (int s = 0; s < NC; ++s) {
+                const uint32_t w = row[s * RS];
+                if (w == EMPTY) cpos = s;
+                else if ((w & ID_MASK) == b_orig) { cpos = s; break; }
+            }
+            if (cpos < NC) {
+                row[cpos * RS] = b_orig | (((key >> 6) & 15u) << CODE_SHIFT);
+                dirty = true;
+            } else {
+                raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+            }
+            ++nc;
+            if (nc > NC) {
+                raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+                full = true;
+            }
+        }
+    } else
+    for (int dz = -1; dz < 2; ++dz)
+        for (int dy = -1; dy < 2; ++dy)
+            for (int dx = -1; dx < 2; ++dx) {
+                int tx = g[0] + dx, ty = g[1] + dy, sx, sy;
+                const int tz = g[2] + dz;
+                if (!image_cell(B, tx, ty, tz, sx, sy)) continue;
+                const d3 dm = shift_vec(B, sx, sy);
+                const float fsx = sx == 0 ? 0.f : (sx > 0 ? Lf0 : -Lf0);
+                const float fsy = sy == 0 ? 0.f : (sy > 0 ? Lf1 : -Lf1);
+                const uint32_t cell = B.cell_base + (uint32_t)(tx + ty * nx + (nx * ny) * tz);
+                const uint32_t start = A.cell_off[cell], end = A.cell_off[cell + 1];
+                for (uint32_t b = start; b < end; ++b) {
+                    if (b == a) continue;
+                    if (!maybe_touching(xaf, A.xf[b], fsx, fsy, margin)) continue;
+                    const double4 xb = A.xs[b];
+                    d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
+                    x_ab = vadd(x_ab, dm);
+                    const double len = vlen<LM>(x_ab);
+                    const double delta = len - (radius_a + xb.w);
+                    if (delta < 0.0) {
+                        const uint32_t b_orig = A.perm[b];
+                        int cpos = nc;
+                        for (int s = 0; s < NC; ++s) {
+                            const uint32_t w = row[s * RS];
+                            if (w == EMPTY) cpos = s;
+                            else if ((w & ID_MASK) == b_orig) { cpos = s; break; }
+                        }
+                        if (cpos < NC) {
+                            row[cpos * RS] = b_orig | (shift_code(sx, sy) << CODE_SHIFT);
+                            dirty = true;
+                        } else {
+                            raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+                        }
+                        ++nc;
+                        if (nc > NC) {
+                            raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+                            break;
+                        }
+                    }
+                }
+            }
+    return dirty;
+}
+
+// Static and dynamic walls (contactsearch.cuh:428-465 and :602-701) and the
+// bond forces in ascending bond order (cohesion.cuh:220-226), added to acc
+// after the contacts.  Returns the normal force on wall 0.
+template <int LM>
+__device__ __forceinline__ double walls_and_bonds(const StepArgs &A, const DevBox &B, uint32_t i,
+                                                  double4 xa, d3 vel_a, d3 angvel_a, Acc &acc)
+{
+    const SphParams &P = B.P;
+    const double dt = B.dt;
+    const double radius_a = xa.w;
+    double wnx[5][4] = {{0.0, 0.0, -1.0, B.L[2]}, {-1.0, 0.0, 0.0, B.L[0]}, {1.0, 0.0, 0.0, 0.0},
+                        {0.0, -1.0, 0.0, B.L[1]}, {0.0, 1.0, 0.0, 0.0}};
+    double wvel[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const uint32_t nw = B.nw;
+    for (uint32_t w = 0; w < 5 && w < nw; ++w) {
+        wnx[w][0] = B.wnx[w][0];
+        wnx[w][1] = B.wnx[w][1];
+        wnx[w][2] = B.wnx[w][2];
+        wnx[w][3] = B.wnx[w][3];
+        wvel[w] = B.wmvfd[w][1];
+    }
+    double w0_force = 0.0;
+    {
+        double delta_w = wnx[0][3] - (xa.z + radius_a);
+        if (delta_w < 0.0)
+            w0_force = contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
+                                               mk(wnx[0][0], wnx[0][1], wnx[0][2]), delta_w, wvel[0]);
+        delta_w = xa.z - radius_a - B.origo[2];
+        if (delta_w < 0.0)
+            (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a, mk(0.0, 0.0, 1.0),
+                                          delta_w, 0.0);
+        if (B.periodic == 0) {
+            delta_w = wnx[1][3] - (xa.x + radius_a);
+            if (delta_w < 0.0)
+                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
+                                              mk(wnx[1][0], wnx[1][1], wnx[1][2]), delta_w, wvel[1]);
+            delta_w = xa.x - radius_a - wnx[2][3];
+            if (delta_w < 0.0)
+                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
+                                              mk(wnx[2][0], wnx[2][1], wnx[2][2]), delta_w, wvel[2]);
+        }
+        if (B.periodic == 0 || B.periodic == 2) {
+            delta_w = wnx[3][3] - (xa.y + radius_a);
+            if (delta_w < 0.0)
+                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
+                                              mk(wnx[3][0], wnx[3][1], wnx[3][2]), delta_w, wvel[3]);
+            delta_w = xa.y - radius_a - wnx[4][3];
+            if (delta_w < 0.0)
+                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
+                                              mk(wnx[4][0], wnx[4][1], wnx[4][2]), delta_w, wvel[4]);
+        }
+    }
+
+    // ---- bond forces in ascending bond order: cohesion.cuh:220-226
+    if (A.nbonds) {
+        const uint32_t e0 = A.bcsr_off[i], e1 = A.bcsr_off[i + 1];
+        for (uint32_t e = e0; e < e1; ++e) {
+            const uint32_t ent = A.bcsr_ent[e];
+            const uint32_t k = ent >> 1;
+            const double4 f = A.bf[k];
+            if (f.w == 0.0) continue;
+            const double4 t = A.bt[k];
+            if ((ent & 1u) == 0) {
+                acc.F = vadd(acc.F, xyz(f));
+                acc.T = vsub(acc.T, xyz(t));
+            } else {
+                acc.F = vsub(acc.F, xyz(f));
+                acc.T = vadd(acc.T, xyz(t));
+            }
+        }
+    }
+
+    return w0_force;
+}
+
+// The per-sphere sums of the step (contactsearch.cuh:707-724).
+__device__ __forceinline__ void store_sums(const StepArgs &A, const DevBox &B, uint32_t i,
+                                           const Acc &acc, double w0_force)
+{
+    const double dt = B.dt;
+    A.force[i] = make_double4(acc.F.x, acc.F.y, acc.F.z, 0.0);
+    A.torque[i] = make_double4(acc.T.x, acc.T.y, acc.T.z, 0.0);
+    A.es_dot[i] = acc.es_dot;
+    A.ev_dot[i] = acc.ev_dot;
+    A.es[i] += acc.es_dot * dt;
+    A.ev[i] += acc.ev_dot * dt;
+    A.p[i] = acc.p;
+    if (B.nw > 0) A.wf_pp[i] = w0_force;
+
+}
+
 constexpr int INTERACT_THREADS = 128;
 
 // Fused topology + interact + walls + bond gather (+ integrate when FUSED)
@@ -206,113 +421,7 @@ __global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
     const float Lf0 = (float)B.L[0], Lf1 = (float)B.L[1];
     if (cm == 2 || cm == 3) {
         // ---- topology: contactsearch.cuh:329-371 and :194-322
-        int nc = 0;
-        const float margin = B.pre_margin;
-        const uint32_t vc = A.vlist ? A.vcount[i] : (uint32_t)VL_MAX + 1u;
-        if (vc <= (uint32_t)VL_MAX) {
-            // Same contacts, same order: the cell search visits the 27
-            // neighbour cells in (dz, dy, dx) order and, within a cell, the
-            // spheres in ascending original index (the stable sort).  Every
-            // sphere that can touch is in the neighbour list (ascending
-            // index), so the touching ones are found there, keyed by
-            // (cell ordinal, list position) and inserted in key order.
-            uint16_t *keys = s_keys + threadIdx.x;
-            const uint32_t *lst = A.vlist + (size_t)i * VL_MAX;
-            int nk = 0;
-            for (uint32_t k = 0; k < vc; ++k) {
-                const uint32_t bo = lst[k];
-                int bx, by, bz, dx, dy, dz, sx, sy;
-                unpack_cell(A.cellc[bo], bx, by, bz);
-                if (!relative_cell(B, g, bx, by, bz, dx, dy, dz, sx, sy)) continue;
-                const double4 xb = A.xs[A.rank[bo]];
-                const d3 dm = shift_vec(B, sx, sy);
-                d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
-                x_ab = vadd(x_ab, dm);
-                const double len = vlen<LM>(x_ab);
-                if (len - (radius_a + xb.w) < 0.0) {
-                    const int ord = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
-                    const uint16_t key =
-                        (uint16_t)((ord << 10) | (shift_code(sx, sy) << 6) | (int)k);
-                    int q = nk;
-                    while (q > 0 && keys[(q - 1) * RS] > key) {
-                        keys[q * RS] = keys[(q - 1) * RS];
-                        --q;
-                    }
-                    keys[q * RS] = key;
-                    ++nk;
-                }
-            }
-            int cur_ord = -1;
-            bool full = false;
-            for (int q = 0; q < nk; ++q) {
-                const uint32_t key = keys[q * RS];
-                const int ord = (int)(key >> 10);
-                if (ord != cur_ord) {   // the cell search leaves a cell on overflow
-                    cur_ord = ord;
-                    full = false;
-                }
-                if (full) continue;
-                const uint32_t b_orig = lst[key & 63u];
-                int cpos = nc;
-                for (int s = 0; s < NC; ++s) {
-                    const uint32_t w = row[s * RS];
-                    if (w == EMPTY) cpos = s;
-                    else if ((w & ID_MASK) == b_orig) { cpos = s; break; }
-                }
-                if (cpos < NC) {
-                    row[cpos * RS] = b_orig | (((key >> 6) & 15u) << CODE_SHIFT);
-                    dirty = true;
-                } else {
-                    raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-                }
-                ++nc;
-                if (nc > NC) {
-                    raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-                    full = true;
-                }
-            }
-        } else
-        for (int dz = -1; dz < 2; ++dz)
-            for (int dy = -1; dy < 2; ++dy)
-                for (int dx = -1; dx < 2; ++dx) {
-                    int tx = g[0] + dx, ty = g[1] + dy, sx, sy;
-                    const int tz = g[2] + dz;
-                    if (!image_cell(B, tx, ty, tz, sx, sy)) continue;
-                    const d3 dm = shift_vec(B, sx, sy);
-                    const float fsx = sx == 0 ? 0.f : (sx > 0 ? Lf0 : -Lf0);
-                    const float fsy = sy == 0 ? 0.f : (sy > 0 ? Lf1 : -Lf1);
-                    const uint32_t cell = B.cell_base + (uint32_t)(tx + ty * nx + (nx * ny) * tz);
-                    const uint32_t start = A.cell_off[cell], end = A.cell_off[cell + 1];
-                    for (uint32_t b = start; b < end; ++b) {
-                        if (b == a) continue;
-                        if (!maybe_touching(xaf, A.xf[b], fsx, fsy, margin)) continue;
-                        const double4 xb = A.xs[b];
-                        d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
-                        x_ab = vadd(x_ab, dm);
-                        const double len = vlen<LM>(x_ab);
-                        const double delta = len - (radius_a + xb.w);
-                        if (delta < 0.0) {
-                            const uint32_t b_orig = A.perm[b];
-                            int cpos = nc;
-                            for (int s = 0; s < NC; ++s) {
-                                const uint32_t w = row[s * RS];
-                                if (w == EMPTY) cpos = s;
-                                else if ((w & ID_MASK) == b_orig) { cpos = s; break; }
-                            }
-                            if (cpos < NC) {
-                                row[cpos * RS] = b_orig | (shift_code(sx, sy) << CODE_SHIFT);
-                                dirty = true;
-                            } else {
-                                raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-                            }
-                            ++nc;
-                            if (nc > NC) {
-                                raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-                                break;
-                            }
-                        }
-                    }
-                }
+        if (search_contacts<LM>(A, B, a, i, xa, g, xaf, row, s_keys + threadIdx.x, RS)) dirty = true;
 
         // ---- interact over the contact row: contactsearch.cuh:484-559
         double4 *hist = A.hist + (size_t)i * NC;
@@ -409,68 +518,7 @@ __global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
                 }
     }
 
-    // ---- walls: contactsearch.cuh:428-465 and :602-701
-    double wnx[5][4] = {{0.0, 0.0, -1.0, B.L[2]}, {-1.0, 0.0, 0.0, B.L[0]}, {1.0, 0.0, 0.0, 0.0},
-                        {0.0, -1.0, 0.0, B.L[1]}, {0.0, 1.0, 0.0, 0.0}};
-    double wvel[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const uint32_t nw = B.nw;
-    for (uint32_t w = 0; w < 5 && w < nw; ++w) {
-        wnx[w][0] = B.wnx[w][0];
-        wnx[w][1] = B.wnx[w][1];
-        wnx[w][2] = B.wnx[w][2];
-        wnx[w][3] = B.wnx[w][3];
-        wvel[w] = B.wmvfd[w][1];
-    }
-    double w0_force = 0.0;
-    {
-        double delta_w = wnx[0][3] - (xa.z + radius_a);
-        if (delta_w < 0.0)
-            w0_force = contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                               mk(wnx[0][0], wnx[0][1], wnx[0][2]), delta_w, wvel[0]);
-        delta_w = xa.z - radius_a - B.origo[2];
-        if (delta_w < 0.0)
-            (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a, mk(0.0, 0.0, 1.0),
-                                          delta_w, 0.0);
-        if (B.periodic == 0) {
-            delta_w = wnx[1][3] - (xa.x + radius_a);
-            if (delta_w < 0.0)
-                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                              mk(wnx[1][0], wnx[1][1], wnx[1][2]), delta_w, wvel[1]);
-            delta_w = xa.x - radius_a - wnx[2][3];
-            if (delta_w < 0.0)
-                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                              mk(wnx[2][0], wnx[2][1], wnx[2][2]), delta_w, wvel[2]);
-        }
-        if (B.periodic == 0 || B.periodic == 2) {
-            delta_w = wnx[3][3] - (xa.y + radius_a);
-            if (delta_w < 0.0)
-                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                              mk(wnx[3][0], wnx[3][1], wnx[3][2]), delta_w, wvel[3]);
-            delta_w = xa.y - radius_a - wnx[4][3];
-            if (delta_w < 0.0)
-                (void)contact_linear_wall<LM>(P, dt, acc, vel_a, angvel_a, radius_a,
-                                              mk(wnx[4][0], wnx[4][1], wnx[4][2]), delta_w, wvel[4]);
-        }
-    }
-
-    // ---- bond forces in ascending bond order: cohesion.cuh:220-226
-    if (A.nbonds) {
-        const uint32_t e0 = A.bcsr_off[i], e1 = A.bcsr_off[i + 1];
-        for (uint32_t e = e0; e < e1; ++e) {
-            const uint32_t ent = A.bcsr_ent[e];
-            const uint32_t k = ent >> 1;
-            const double4 f = A.bf[k];
-            if (f.w == 0.0) continue;
-            const double4 t = A.bt[k];
-            if ((ent & 1u) == 0) {
-                acc.F = vadd(acc.F, xyz(f));
-                acc.T = vsub(acc.T, xyz(t));
-            } else {
-                acc.F = vsub(acc.F, xyz(f));
-                acc.T = vadd(acc.T, xyz(t));
-            }
-        }
-    }
+    const double w0_force = walls_and_bonds<LM>(A, B, i, xa, vel_a, angvel_a, acc);
 
     if (dirty) {
         uint4 *wrow = reinterpret_cast<uint4 *>(A.slots + (size_t)i * NC);
@@ -480,17 +528,172 @@ __global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
                                  row[(4 * q + 3) * RS]);
     }
 
-    // ---- contactsearch.cuh:707-724
-    A.force[i] = make_double4(acc.F.x, acc.F.y, acc.F.z, 0.0);
-    A.torque[i] = make_double4(acc.T.x, acc.T.y, acc.T.z, 0.0);
-    A.es_dot[i] = acc.es_dot;
-    A.ev_dot[i] = acc.ev_dot;
-    A.es[i] += acc.es_dot * dt;
-    A.ev[i] += acc.ev_dot * dt;
-    A.p[i] = acc.p;
-    if (nw > 0) A.wf_pp[i] = w0_force;
+    store_sums(A, B, i, acc, w0_force);
 
     if (FUSED) integrate_particle(A, B, i, xa, va4, wa4, acc.F, acc.T);
+}
+
+// ------------------------------------------------------------ split step
+//
+// The step of k_interact for contact models 2 and 3 with fused integration,
+// in three launches that keep more memory requests in flight:
+//   k_search   one thread per sphere: contact search on the slot row, the
+//              list of live slots (ascending);
+//   k_contacts CONTACT_LANES threads per sphere, one live contact each: the
+//              contact law, its additions recorded (ContactRec), the new
+//              history written, ended contacts removed from the row;
+//   k_finish   one thread per sphere: the recorded additions replayed in
+//              slot order, walls, bonds, sums, integration.
+// Each contact's arithmetic and the order of every sum are those of
+// k_interact, so the results are bit-identical.
+constexpr int SEARCH_THREADS = 128;
+constexpr int CONTACT_LANES = 4;
+constexpr int CONTACT_THREADS = 128;
+constexpr int FINISH_THREADS = 128;
+
+template <int LM>
+__global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
+{
+    __shared__ uint32_t s_row[NC * SEARCH_THREADS];
+    __shared__ uint16_t s_keys[VL_MAX * SEARCH_THREADS];
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A.ntot) return;
+    const int RS = SEARCH_THREADS;
+    uint32_t *row = s_row + threadIdx.x;
+    const uint32_t i = A.perm[a];
+    const DevBox &B = A.boxes[A.box_of[i]];
+    const double4 xa = A.xs[a];
+    const uint4 *grow = reinterpret_cast<const uint4 *>(A.slots + (size_t)i * NC);
+#pragma unroll
+    for (int q = 0; q < NC / 4; ++q) {
+        const uint4 w = grow[q];
+        row[(4 * q + 0) * RS] = w.x;
+        row[(4 * q + 1) * RS] = w.y;
+        row[(4 * q + 2) * RS] = w.z;
+        row[(4 * q + 3) * RS] = w.w;
+    }
+    if (A.tape_rows_pre) {
+        uint4 *t = reinterpret_cast<uint4 *>(A.tape_rows_pre + (size_t)i * NC);
+#pragma unroll
+        for (int q = 0; q < NC / 4; ++q) t[q] = grow[q];
+    }
+    int g[3];
+    g[0] = (int)floor((xa.x - B.origo[0]) / (B.L[0] / B.num[0]));
+    g[1] = (int)floor((xa.y - B.origo[1]) / (B.L[1] / B.num[1]));
+    g[2] = (int)floor((xa.z - B.origo[2]) / (B.L[2] / B.num[2]));
+    const bool dirty =
+        search_contacts<LM>(A, B, a, i, xa, g, A.xf[a], row, s_keys + threadIdx.x, RS);
+    if (A.tape_rows_post) {
+        const double4 *hist = A.hist + (size_t)i * NC;
+        for (int s = 0; s < NC; ++s) {
+            const uint32_t w = row[s * RS];
+            A.tape_rows_post[(size_t)i * NC + s] = w;
+            if (w != EMPTY) A.tape_hist[(size_t)i * NC + s] = hist[s];
+        }
+    }
+    uint8_t *live = A.live + (size_t)i * NC;
+    uint32_t nl = 0;
+    for (int s = 0; s < NC; ++s)
+        if (row[s * RS] != EMPTY) live[nl++] = (uint8_t)s;
+    A.nlive[i] = nl;
+    if (dirty) {
+        uint4 *wrow = reinterpret_cast<uint4 *>(A.slots + (size_t)i * NC);
+#pragma unroll
+        for (int q = 0; q < NC / 4; ++q)
+            wrow[q] = make_uint4(row[(4 * q) * RS], row[(4 * q + 1) * RS], row[(4 * q + 2) * RS],
+                                 row[(4 * q + 3) * RS]);
+    }
+}
+
+template <int LM, bool MIXED>
+__global__ void __launch_bounds__(CONTACT_THREADS) k_contacts(StepArgs A)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t a = t / CONTACT_LANES, lane = t % CONTACT_LANES;
+    if (a >= A.ntot) return;
+    const uint32_t i = A.perm[a];
+    const uint32_t nl = A.nlive[i];
+    if (lane >= nl) return;
+    const DevBox &B = A.boxes[A.box_of[i]];
+    const SphParams &P = B.P;
+    const double dt = B.dt;
+    const uint32_t cm = P.contactmodel;
+    const double4 xa = A.xs[a];
+    const double radius_a = xa.w;
+    const d3 vel_a = xyz(A.vs[a]);
+    const d3 angvel_a = xyz(A.ws[a]);
+    const uint8_t *live = A.live + (size_t)i * NC;
+    uint32_t *slots = A.slots + (size_t)i * NC;
+    double4 *hist = A.hist + (size_t)i * NC;
+    ContactRec *rec = A.crec + (size_t)i * NC;
+    for (uint32_t q = lane; q < nl; q += CONTACT_LANES) {
+        const int s = live[q];
+        const uint32_t w = slots[s];
+        const uint32_t b_orig = w & ID_MASK;
+        int sx, sy;
+        decode_shift(w >> CODE_SHIFT, sx, sy);
+        const d3 dm = shift_vec(B, sx, sy);
+        const uint32_t bs = A.rank[b_orig];
+        const double4 xb = A.xs[bs];
+        const d3 x_ab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
+        const double x_ab_length = vlen<LM>(x_ab);
+        const double delta_n = x_ab_length - (radius_a + xb.w);
+        ContactRec r;
+        r.nev = 0;
+        r.nes = 0;
+        if (delta_n < 0.0) {
+            const d3 vel_b = xyz(A.vs[bs]);
+            const d3 h0 = xyz(hist[s]);
+            d3 nd;
+            if (MIXED) {
+                const MixedPair mp = mixed_pair(x_ab, x_ab_length, delta_n, vel_a, vel_b,
+                                                tof(angvel_a), xyzf(A.ws[bs]), radius_a, xb.w);
+                if (cm == 2) nd = contact_linear_mixed(P, dt, r, mp, h0);
+                else nd = contact_hertz_mixed(P, dt, r, mp, h0);
+            } else {
+                const d3 angvel_b = xyz(A.ws[bs]);
+                if (cm == 2)
+                    nd = contact_linear<LM>(P, dt, r, vel_a, vel_b, angvel_a, angvel_b, radius_a,
+                                            xb.w, x_ab, x_ab_length, delta_n, h0);
+                else
+                    nd = contact_hertz<LM>(P, dt, r, vel_a, vel_b, angvel_a, angvel_b, radius_a,
+                                           xb.w, x_ab, x_ab_length, delta_n, h0);
+            }
+            hist[s] = make_double4(nd.x, nd.y, nd.z, 0.0);
+        } else {
+            slots[s] = EMPTY;
+            hist[s] = make_double4(0.0, 0.0, 0.0, 0.0);
+            r.nev = -1;
+        }
+        rec[q] = r;
+    }
+}
+
+template <int LM>
+__global__ void __launch_bounds__(FINISH_THREADS) k_finish(StepArgs A)
+{
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A.ntot) return;
+    const uint32_t i = A.perm[a];
+    const DevBox &B = A.boxes[A.box_of[i]];
+    const double4 xa = A.xs[a];
+    const double4 va4 = A.vs[a];
+    const double4 wa4 = A.ws[a];
+    Acc acc;
+    acc.F = mk(0.0, 0.0, 0.0);
+    acc.T = mk(0.0, 0.0, 0.0);
+    acc.es_dot = 0.0;
+    acc.ev_dot = 0.0;
+    acc.p = 0.0;
+    const uint32_t nl = A.nlive[i];
+    const ContactRec *rec = A.crec + (size_t)i * NC;
+    for (uint32_t q = 0; q < nl; ++q) {
+        const ContactRec r = rec[q];
+        if (r.nev >= 0) replay(acc, r);
+    }
+    const double w0_force = walls_and_bonds<LM>(A, B, i, xa, xyz(va4), xyz(wa4), acc);
+    store_sums(A, B, i, acc, w0_force);
+    integrate_particle(A, B, i, xa, va4, wa4, acc.F, acc.T);
 }
 
 // Launch variants of k_interact (INTERACT_VARIANTS): the minimum resident
@@ -504,6 +707,13 @@ inline void launch_interact_lm(const StepArgs &A, cudaStream_t st, unsigned grid
     if (variant == 0) k_interact<LM, FUSED, MIXED, 1><<<grid, INTERACT_THREADS, 0, st>>>(A);
     else if (variant == 2) k_interact<LM, FUSED, MIXED, 6><<<grid, INTERACT_THREADS, 0, st>>>(A);
     else k_interact<LM, FUSED, MIXED, 4><<<grid, INTERACT_THREADS, 0, st>>>(A);
+}
+
+template <bool MIXED>
+inline void launch_contacts(const StepArgs &A, cudaStream_t st, unsigned grid, int lm)
+{
+    if (lm == SPH_LEN_FP64) k_contacts<SPH_LEN_FP64, MIXED><<<grid, CONTACT_THREADS, 0, st>>>(A);
+    else k_contacts<SPH_LEN_REFERENCE, MIXED><<<grid, CONTACT_THREADS, 0, st>>>(A);
 }
 
 template <bool MIXED>

@@ -214,7 +214,7 @@ class Stepper(object):
         """Time each launch variant of the interact kernel for `steps` steps
         from the current state, keep the fastest, restore the state
         (sph_autotune).  Returns (chosen, [ms per step of each variant])."""
-        ms = numpy.zeros(3)
+        ms = numpy.zeros(4)
         ch = C.c_int(-1)
         self._check(self.lib.sph_autotune(self.h, int(steps), _abi.dptr(ms), C.byref(ch)),
                     "sph_autotune")

@@ -21,13 +21,16 @@ def rel_l2(a, b):
     return float(numpy.linalg.norm(a - b) / max(numpy.linalg.norm(b), 1e-300))
 
 
+@pytest.mark.parametrize("variant", [1, 3])
 @pytest.mark.parametrize("name", ["periodic_xy_wall_stress", "walls_all_sides", "contact_model_1",
                                   "youngs_modulus", "bonds", "contact_model_3_hertz",
                                   "shear_stress_wall"])
-def test_mixed_step_error(name):
+def test_mixed_step_error(name, variant):
+    """variant 1: fused kernel; 3: split step (where it applies)."""
     s = cases.make(name)[0]
     a = Stepper([s], precision="fp64")
     b = Stepper([s], precision="mixed")
+    b.set_variant(variant)
     a.upload()
     b.upload()
     a.step(1)

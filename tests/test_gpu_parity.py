@@ -102,15 +102,19 @@ def test_gpu_deterministic():
         assert numpy.array_equal(a, b)
 
 
-@pytest.mark.parametrize("variant", [0, 2])
+@pytest.mark.parametrize("length", ["reference", "fp64"])
+@pytest.mark.parametrize("variant", [0, 2, 3])
 @pytest.mark.parametrize("name", ["periodic_xy_wall_stress", "walls_all_sides", "fast_spheres",
-                                  "shear_stress_wall"])
-def test_launch_variants_match_oracle(name, variant):
-    """Every launch variant of the interact kernel (register budgets 255 and
-    80; 128 is the default above) gives the same bits."""
+                                  "shear_stress_wall", "contact_model_3_hertz", "youngs_modulus",
+                                  "bonds_breaking", "adaptive_grid", "fixvel_modes"])
+def test_launch_variants_match_oracle(name, variant, length):
+    """Every launch variant of the interact stage gives the same bits: the
+    fused kernel for register budgets 255 and 80 (128 is the default above)
+    and the split step (variant 3; cases it does not cover, such as the
+    shear-stress wall, fall back to the fused kernel)."""
     s, _ref_ok, steps = cases.make(name)
-    cpu = O.CpuRun(s, "oracle")
-    st = Stepper([s], precision="fp64")
+    cpu = O.CpuRun(s, "oracle", length_mode=0 if length == "reference" else 1)
+    st = Stepper([s], precision="fp64", length=length)
     st.set_variant(variant)
     st.upload()
     st.step(steps)
@@ -127,7 +131,7 @@ def test_autotune_keeps_the_state_and_the_bits():
     before, _ = a.download()
     c_before = a.contacts()[0].copy()
     chosen, ms = a.autotune(steps=5)
-    assert chosen in (0, 1, 2) and all(m > 0.0 for m in ms)
+    assert chosen in (0, 1, 2, 3) and all(m > 0.0 for m in ms)
     after, _ = a.download()
     assert numpy.array_equal(before.x, after.x) and numpy.array_equal(before.vel, after.vel)
     assert numpy.array_equal(c_before, a.contacts()[0])

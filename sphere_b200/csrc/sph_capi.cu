@@ -1119,18 +1119,18 @@ static int drop_graphs(SphHandle *h)
 // Buffers of the split step, allocated when that variant is first chosen.
 static int ensure_split(SphHandle *h)
 {
-    if (h->A.crec) return SPH_OK;
+    if (h->A.csum) return SPH_OK;
     const uint64_t n = h->ntot;
     uint8_t *live = nullptr;
     uint32_t *nlive = nullptr;
-    sph::ContactRec *crec = nullptr;
+    sph::Acc *csum = nullptr;
     int st;
     if ((st = dalloc(h, &live, n * sph::NC)) || (st = dalloc(h, &nlive, n)) ||
-        (st = dalloc(h, &crec, n * sph::NC)))
+        (st = dalloc(h, &csum, n)))
         return st;
     h->A.live = live;
     h->A.nlive = nlive;
-    h->A.crec = crec;
+    h->A.csum = csum;
     return SPH_OK;
 }
 

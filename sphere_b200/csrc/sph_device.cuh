@@ -113,12 +113,17 @@ struct Acc {
 // contact ended this step (nothing to add).
 struct ContactRec {
     d3 F, T;
-    double ev[2], es, p;
+    double ev0, ev1, es, p;
     int32_t nev, nes;
     __device__ __forceinline__ void addF(d3 v) { F = v; }
     __device__ __forceinline__ void addT(d3 v) { T = v; }
     __device__ __forceinline__ void addEs(double v) { es = v; nes = 1; }
-    __device__ __forceinline__ void addEv(double v) { ev[nev++] = v; }
+    __device__ __forceinline__ void addEv(double v)
+    {
+        if (nev == 0) ev0 = v;
+        else ev1 = v;
+        ++nev;
+    }
     __device__ __forceinline__ void addP(double v) { p = v; }
 };
 
@@ -126,7 +131,8 @@ __device__ __forceinline__ void replay(Acc &a, const ContactRec &r)
 {
     a.addF(r.F);
     a.addT(r.T);
-    for (int k = 0; k < r.nev; ++k) a.addEv(r.ev[k]);
+    if (r.nev > 0) a.addEv(r.ev0);
+    if (r.nev > 1) a.addEv(r.ev1);
     if (r.nes) a.addEs(r.es);
     a.addP(r.p);
 }

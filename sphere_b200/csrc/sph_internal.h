@@ -10,7 +10,7 @@
 namespace sph {
 
 struct DevBox;
-struct ContactRec;
+struct Acc;
 
 // Device pointers of one handle, passed by value to every step kernel.
 struct StepArgs {
@@ -52,11 +52,11 @@ struct StepArgs {
     uint64_t *cellc;
     uint32_t vcap;             // list capacity in use (<= VL_MAX)
     // split step (k_search / k_contacts / k_finish): per sphere the live
-    // slots in ascending order and their number, and per live contact the
-    // additions its law made (null until the split step is first used)
+    // slots in ascending order, their number, and the sums of its contacts
+    // (null until the split step is first used)
     uint8_t *live;
     uint32_t *nlive;
-    ContactRec *crec;
+    Acc *csum;
     // adjoint tape of the current step (null outside a recorded segment):
     // contact rows at kernel entry and after the contact search, and the
     // tangential histories the interact pass reads

@@ -675,7 +675,7 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         }
         const unsigned gi = blocks_for(A.ntot, INTERACT_THREADS);
         const bool split = cfg.variant == SPLIT_VARIANT && !cfg.unfused && cfg.all_cm23 &&
-                           A.vlist && A.crec;
+                           A.vlist && A.csum;
         if (split) {
             if (cfg.lenmode == SPH_LEN_FP64)
                 k_search<SPH_LEN_FP64><<<blocks_for(A.ntot, SEARCH_THREADS), SEARCH_THREADS, 0, st>>>(A);

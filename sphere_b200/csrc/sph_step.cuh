@@ -540,10 +540,11 @@ __global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
 //   k_search   one thread per sphere: contact search on the slot row, the
 //              list of live slots (ascending);
 //   k_contacts CONTACT_LANES threads per sphere, one live contact each: the
-//              contact law, its additions recorded (ContactRec), the new
-//              history written, ended contacts removed from the row;
-//   k_finish   one thread per sphere: the recorded additions replayed in
-//              slot order, walls, bonds, sums, integration.
+//              contact law with its additions recorded (ContactRec), the
+//              new history written, ended contacts removed from the row;
+//              the records go by warp shuffle to the sphere's first lane,
+//              which adds them in slot order and stores the sums;
+//   k_finish   one thread per sphere: walls, bonds, sums, integration.
 // Each contact's arithmetic and the order of every sum are those of
 // k_interact, so the results are bit-identical.
 constexpr int SEARCH_THREADS = 128;
@@ -605,72 +606,108 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
     }
 }
 
+// Shuffle a contact's record from lane src of the warp.
+__device__ __forceinline__ ContactRec shfl_rec(const ContactRec &r, int src)
+{
+    ContactRec o;
+    o.F = mk(__shfl_sync(0xffffffffu, r.F.x, src), __shfl_sync(0xffffffffu, r.F.y, src),
+             __shfl_sync(0xffffffffu, r.F.z, src));
+    o.T = mk(__shfl_sync(0xffffffffu, r.T.x, src), __shfl_sync(0xffffffffu, r.T.y, src),
+             __shfl_sync(0xffffffffu, r.T.z, src));
+    o.ev0 = __shfl_sync(0xffffffffu, r.ev0, src);
+    o.ev1 = __shfl_sync(0xffffffffu, r.ev1, src);
+    o.es = __shfl_sync(0xffffffffu, r.es, src);
+    o.p = __shfl_sync(0xffffffffu, r.p, src);
+    o.nev = __shfl_sync(0xffffffffu, r.nev, src);
+    o.nes = __shfl_sync(0xffffffffu, r.nes, src);
+    return o;
+}
+
 template <int LM, bool MIXED>
 __global__ void __launch_bounds__(CONTACT_THREADS) k_contacts(StepArgs A)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t a = t / CONTACT_LANES, lane = t % CONTACT_LANES;
-    if (a >= A.ntot) return;
-    const uint32_t i = A.perm[a];
-    const uint32_t nl = A.nlive[i];
-    if (lane >= nl) return;
-    const DevBox &B = A.boxes[A.box_of[i]];
-    const SphParams &P = B.P;
-    const double dt = B.dt;
-    const uint32_t cm = P.contactmodel;
-    const double4 xa = A.xs[a];
-    const double radius_a = xa.w;
-    const d3 vel_a = xyz(A.vs[a]);
-    const d3 angvel_a = xyz(A.ws[a]);
-    const uint8_t *live = A.live + (size_t)i * NC;
-    uint32_t *slots = A.slots + (size_t)i * NC;
-    double4 *hist = A.hist + (size_t)i * NC;
-    ContactRec *rec = A.crec + (size_t)i * NC;
-    for (uint32_t q = lane; q < nl; q += CONTACT_LANES) {
-        const int s = live[q];
-        const uint32_t w = slots[s];
-        const uint32_t b_orig = w & ID_MASK;
-        int sx, sy;
-        decode_shift(w >> CODE_SHIFT, sx, sy);
-        const d3 dm = shift_vec(B, sx, sy);
-        const uint32_t bs = A.rank[b_orig];
-        const double4 xb = A.xs[bs];
-        const d3 x_ab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
-        const double x_ab_length = vlen<LM>(x_ab);
-        const double delta_n = x_ab_length - (radius_a + xb.w);
+    const bool valid = a < A.ntot;
+    const uint32_t i = valid ? A.perm[a] : 0u;
+    const uint32_t nl = valid ? A.nlive[i] : 0u;
+    // the whole warp runs the same number of rounds (its shuffles need
+    // every lane); round r computes live contacts 4r .. 4r + 3 of each sphere
+    const uint32_t rounds =
+        __reduce_max_sync(0xffffffffu, (nl + CONTACT_LANES - 1) / CONTACT_LANES);
+    Acc acc;
+    acc.F = mk(0.0, 0.0, 0.0);
+    acc.T = mk(0.0, 0.0, 0.0);
+    acc.es_dot = 0.0;
+    acc.ev_dot = 0.0;
+    acc.p = 0.0;
+    const int base = (int)(threadIdx.x & 31u) & ~(CONTACT_LANES - 1);
+    for (uint32_t rd = 0; rd < rounds; ++rd) {
+        const uint32_t q = rd * CONTACT_LANES + lane;
         ContactRec r;
-        r.nev = 0;
+        r.F = mk(0.0, 0.0, 0.0);
+        r.T = mk(0.0, 0.0, 0.0);
+        r.ev0 = r.ev1 = r.es = r.p = 0.0;
+        r.nev = -1;   // nothing to add unless a live contact is computed
         r.nes = 0;
-        if (delta_n < 0.0) {
-            const d3 vel_b = xyz(A.vs[bs]);
-            const d3 h0 = xyz(hist[s]);
-            d3 nd;
-            if (MIXED) {
-                const MixedPair mp = mixed_pair(x_ab, x_ab_length, delta_n, vel_a, vel_b,
-                                                tof(angvel_a), xyzf(A.ws[bs]), radius_a, xb.w);
-                if (cm == 2) nd = contact_linear_mixed(P, dt, r, mp, h0);
-                else nd = contact_hertz_mixed(P, dt, r, mp, h0);
+        if (q < nl) {
+            const DevBox &B = A.boxes[A.box_of[i]];
+            const SphParams &P = B.P;
+            const double dt = B.dt;
+            const uint32_t cm = P.contactmodel;
+            const double4 xa = A.xs[a];
+            const double radius_a = xa.w;
+            const d3 vel_a = xyz(A.vs[a]);
+            const d3 angvel_a = xyz(A.ws[a]);
+            uint32_t *slots = A.slots + (size_t)i * NC;
+            double4 *hist = A.hist + (size_t)i * NC;
+            const int s = A.live[(size_t)i * NC + q];
+            const uint32_t w = slots[s];
+            const uint32_t b_orig = w & ID_MASK;
+            int sx, sy;
+            decode_shift(w >> CODE_SHIFT, sx, sy);
+            const d3 dm = shift_vec(B, sx, sy);
+            const uint32_t bs = A.rank[b_orig];
+            const double4 xb = A.xs[bs];
+            const d3 x_ab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
+            const double x_ab_length = vlen<LM>(x_ab);
+            const double delta_n = x_ab_length - (radius_a + xb.w);
+            if (delta_n < 0.0) {
+                r.nev = 0;
+                const d3 vel_b = xyz(A.vs[bs]);
+                const d3 h0 = xyz(hist[s]);
+                d3 nd;
+                if (MIXED) {
+                    const MixedPair mp = mixed_pair(x_ab, x_ab_length, delta_n, vel_a, vel_b,
+                                                    tof(angvel_a), xyzf(A.ws[bs]), radius_a, xb.w);
+                    if (cm == 2) nd = contact_linear_mixed(P, dt, r, mp, h0);
+                    else nd = contact_hertz_mixed(P, dt, r, mp, h0);
+                } else {
+                    const d3 angvel_b = xyz(A.ws[bs]);
+                    if (cm == 2)
+                        nd = contact_linear<LM>(P, dt, r, vel_a, vel_b, angvel_a, angvel_b,
+                                                radius_a, xb.w, x_ab, x_ab_length, delta_n, h0);
+                    else
+                        nd = contact_hertz<LM>(P, dt, r, vel_a, vel_b, angvel_a, angvel_b,
+                                               radius_a, xb.w, x_ab, x_ab_length, delta_n, h0);
+                }
+                hist[s] = make_double4(nd.x, nd.y, nd.z, 0.0);
             } else {
-                const d3 angvel_b = xyz(A.ws[bs]);
-                if (cm == 2)
-                    nd = contact_linear<LM>(P, dt, r, vel_a, vel_b, angvel_a, angvel_b, radius_a,
-                                            xb.w, x_ab, x_ab_length, delta_n, h0);
-                else
-                    nd = contact_hertz<LM>(P, dt, r, vel_a, vel_b, angvel_a, angvel_b, radius_a,
-                                           xb.w, x_ab, x_ab_length, delta_n, h0);
+                slots[s] = EMPTY;
+                hist[s] = make_double4(0.0, 0.0, 0.0, 0.0);
             }
-            hist[s] = make_double4(nd.x, nd.y, nd.z, 0.0);
-        } else {
-            slots[s] = EMPTY;
-            hist[s] = make_double4(0.0, 0.0, 0.0, 0.0);
-            r.nev = -1;
         }
-        rec[q] = r;
+        // lane 0 of the sphere adds the round's contacts in slot order
+        for (int j = 0; j < CONTACT_LANES; ++j) {
+            const ContactRec o = shfl_rec(r, base + j);
+            if (lane == 0 && o.nev >= 0) replay(acc, o);
+        }
     }
+    if (valid && lane == 0) A.csum[i] = acc;
 }
 
 template <int LM>
-__global__ void __launch_bounds__(FINISH_THREADS) k_finish(StepArgs A)
+__global__ void __launch_bounds__(FINISH_THREADS, 4) k_finish(StepArgs A)
 {
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= A.ntot) return;
@@ -685,12 +722,7 @@ __global__ void __launch_bounds__(FINISH_THREADS) k_finish(StepArgs A)
     acc.es_dot = 0.0;
     acc.ev_dot = 0.0;
     acc.p = 0.0;
-    const uint32_t nl = A.nlive[i];
-    const ContactRec *rec = A.crec + (size_t)i * NC;
-    for (uint32_t q = 0; q < nl; ++q) {
-        const ContactRec r = rec[q];
-        if (r.nev >= 0) replay(acc, r);
-    }
+    acc = A.csum[i];   // the contacts' sums, added in slot order by k_contacts
     const double w0_force = walls_and_bonds<LM>(A, B, i, xa, xyz(va4), xyz(wa4), acc);
     store_sums(A, B, i, acc, w0_force);
     integrate_particle(A, B, i, xa, va4, wa4, acc.F, acc.T);

@@ -17,7 +17,9 @@ from CUDA events recorded inside 8 step graphs run after the timed region
 of the dominant kernel, the end-to-end time through the C ABI with host
 buffers, and (rank 0, N = 1) the CPU baseline: the reference's own step
 kernels compiled for the CPU (oracle/_ref) on a bounded sample.  Rank 0
-also reports the cost of the adjoint (time_adjoint) under "adjoint".
+also reports the cost of the adjoint (time_adjoint) under "adjoint" and the
+batched-ensemble throughput and per-box error (time_ensemble) under
+"ensemble".
 
 --impl reference times that CPU reference alone (rank 0; other ranks exit).
 
@@ -191,6 +193,73 @@ def time_adjoint(device, stream, n=50000, steps=2000, ckpt=100):
             "grad_v0_norm": float(numpy.linalg.norm(gv))}
 
 
+def time_ensemble(device, stream, nboxes=256, steps=200, err_steps=100):
+    """The batched ensemble (256 independent x-y periodic shear boxes with
+    uniform particle counts in [500, 20000], radii U[0.009, 0.011] m,
+    per-box normal stress U[10, 80] kPa and mu U[0.3, 0.6]) stepped by one
+    handle: every step is one CUDA graph whose launches cover all boxes.
+    Reports the FP32-mixed ensemble throughput (launch variant picked by
+    sph_autotune) and, per box, the mixed form's error against the FP64
+    form: force relative L2 after one step and the largest position
+    difference after err_steps steps, relative to the mean radius."""
+    import numpy
+    import torch
+    from sphere_b200 import scenes
+    from sphere_b200.runner import Stepper
+    sims = scenes.shear_ensemble(nboxes=nboxes, seed=0, device=device)
+    counts = [int(q.np[0]) for q in sims]
+    n = sum(counts)
+    st = Stepper(sims, precision="mixed", length="reference", device=device)
+    st.set_stream(stream.cuda_stream)
+    st.upload()
+    variant, variant_ms = st.autotune(steps=10)
+    st.step(5)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    st.step_async(steps)
+    end.record(stream)
+    end.synchronize()
+    code = st.sync(raise_on_error=False)
+    ms = start.elapsed_time(end)
+    st.close()
+    # per-box error of the mixed form against the FP64 form
+    a = Stepper(sims, precision="fp64", length="reference", device=device)
+    b = Stepper(sims, precision="mixed", length="reference", device=device)
+    a.upload()
+    b.upload()
+    a.step(1)
+    b.step(1)
+    fa, _ = a.download()
+    fb, _ = b.download()
+    a.step(err_steps - 1)
+    b.step(err_steps - 1)
+    xa, _ = a.download()
+    xb, _ = b.download()
+    a.close()
+    b.close()
+    ferr, xerr = [], []
+    o = 0
+    for q, k in zip(sims, counts):
+        da = fa.force[o:o + k]
+        db = fb.force[o:o + k]
+        ferr.append(float(numpy.linalg.norm(db - da) / max(numpy.linalg.norm(da), 1e-300)))
+        xerr.append(float(numpy.max(numpy.abs(xa.x[o:o + k, :3] - xb.x[o:o + k, :3]))) /
+                    float(numpy.mean(q.radius)))
+        o += k
+    return {"workload": "%d independent x-y periodic shear boxes, %d..%d spheres each "
+                        "(%d in total), radii U[0.009, 0.011] m, porosity ~0.40, normal "
+                        "stress U[10, 80] kPa, mu U[0.3, 0.6], FP32-mixed, one handle"
+                        % (nboxes, min(counts), max(counts), n),
+            "value": n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "spheres": n, "variant": variant, "variant_ms_per_step": variant_ms,
+            "device_status": code,
+            "per_box_force_rel_l2_max": max(ferr), "per_box_force_rel_l2_median":
+                float(numpy.median(ferr)),
+            "per_box_dx_over_rmean_max_after_%d_steps" % err_steps: max(xerr)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -202,6 +271,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pack-sweeps", type=int, default=3000)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--variant", type=int, default=-1,
                     help="interact launch variant (0-3); default: picked by sph_autotune")
     args = ap.parse_args()
@@ -392,6 +462,9 @@ def main():
     adj = None
     if rank == 0 and not args.no_adjoint:
         adj = time_adjoint(local, stream)
+    ens = None
+    if rank == 0 and not args.no_ensemble:
+        ens = time_ensemble(local, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -429,6 +502,8 @@ def main():
         line["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
     if adj is not None:
         line["adjoint"] = adj
+    if ens is not None:
+        line["ensemble"] = ens
     print(json.dumps(line))
     return 0
 

@@ -1122,13 +1122,14 @@ static int ensure_split(SphHandle *h)
     if (h->A.csum) return SPH_OK;
     const uint64_t n = h->ntot;
     uint8_t *live = nullptr;
-    uint32_t *nlive = nullptr;
+    uint32_t *livew = nullptr, *nlive = nullptr;
     sph::Acc *csum = nullptr;
     int st;
-    if ((st = dalloc(h, &live, n * sph::NC)) || (st = dalloc(h, &nlive, n)) ||
-        (st = dalloc(h, &csum, n)))
+    if ((st = dalloc(h, &live, n * sph::NC)) || (st = dalloc(h, &livew, n * sph::NC)) ||
+        (st = dalloc(h, &nlive, n)) || (st = dalloc(h, &csum, n)))
         return st;
     h->A.live = live;
+    h->A.livew = livew;
     h->A.nlive = nlive;
     h->A.csum = csum;
     return SPH_OK;

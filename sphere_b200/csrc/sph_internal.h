@@ -51,10 +51,12 @@ struct StepArgs {
     float4 *xref;
     uint64_t *cellc;
     uint32_t vcap;             // list capacity in use (<= VL_MAX)
-    // split step (k_search / k_contacts / k_finish): per sphere the live
-    // slots in ascending order, their number, and the sums of its contacts
-    // (null until the split step is first used)
+    // split step (k_search / k_contacts / k_finish), indexed by sorted
+    // position: per sphere the live slots in ascending order (slot index
+    // and slot word), their number, and the sums of its contacts (null
+    // until the split step is first used)
     uint8_t *live;
+    uint32_t *livew;
     uint32_t *nlive;
     Acc *csum;
     // adjoint tape of the current step (null outside a recorded segment):

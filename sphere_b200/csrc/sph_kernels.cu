@@ -677,10 +677,11 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         const bool split = cfg.variant == SPLIT_VARIANT && !cfg.unfused && cfg.all_cm23 &&
                            A.vlist && A.csum;
         if (split) {
+            const unsigned gs = blocks_for(A.ntot, SEARCH_THREADS);
             if (cfg.lenmode == SPH_LEN_FP64)
-                k_search<SPH_LEN_FP64><<<blocks_for(A.ntot, SEARCH_THREADS), SEARCH_THREADS, 0, st>>>(A);
+                k_search<SPH_LEN_FP64><<<gs, SEARCH_THREADS, 0, st>>>(A);
             else
-                k_search<SPH_LEN_REFERENCE><<<blocks_for(A.ntot, SEARCH_THREADS), SEARCH_THREADS, 0, st>>>(A);
+                k_search<SPH_LEN_REFERENCE><<<gs, SEARCH_THREADS, 0, st>>>(A);
             mark(prof, st, "k_search");
             contact(A, st, blocks_for((uint64_t)A.ntot * CONTACT_LANES, CONTACT_THREADS),
                     cfg.lenmode);

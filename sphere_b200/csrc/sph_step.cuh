@@ -142,86 +142,98 @@ __device__ __forceinline__ void integrate_particle(const StepArgs &A, const DevB
 
 // ------------------------------------------------------------------ interact
 
-// The contact search of one sphere (contact models 2 and 3) on its slot row
-// staged in shared memory (row[s * RS]): new contacts inserted with the
-// reference's rule, from the neighbour list when the sphere has one, else
-// from the 27 neighbour cells.  keys: shared scratch of VL_MAX entries at
-// stride RS.  Returns whether the row changed.
+// Neighbour-list entry k of sphere a (partner id bo): the cell search visits
+// the partner's cell at ordinal (dz, dy, dx) of the 27-cell loop under image
+// (sx, sy), and the exact FP64 test says the pair touches.  Returns the
+// insertion key (ordinal << 10 | image code << 6 | k), or NO_KEY.
+constexpr uint16_t NO_KEY = 0xffffu;
+
 template <int LM>
-__device__ __forceinline__ bool search_contacts(const StepArgs &A, const DevBox &B, uint32_t a,
-                                                uint32_t i, double4 xa, const int g[3],
-                                                float4 xaf, uint32_t *row, uint16_t *keys,
-                                                int RS)
+__device__ __forceinline__ uint16_t list_key(const StepArgs &A, const DevBox &B, double4 xa,
+                                             const int g[3], uint32_t bo, uint32_t k)
+{
+    int bx, by, bz, dx, dy, dz, sx, sy;
+    unpack_cell(A.cellc[bo], bx, by, bz);
+    if (!relative_cell(B, g, bx, by, bz, dx, dy, dz, sx, sy)) return NO_KEY;
+    const double4 xb = A.xs[A.rank[bo]];
+    const d3 dm = shift_vec(B, sx, sy);
+    d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
+    x_ab = vadd(x_ab, dm);
+    const double len = vlen<LM>(x_ab);
+    if (!(len - (xa.w + xb.w) < 0.0)) return NO_KEY;
+    const int ord = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+    return (uint16_t)((ord << 10) | (shift_code(sx, sy) << 6) | (int)k);
+}
+
+// Insert the touching list entries, keys sorted ascending (keys[q * KS]),
+// into the slot row with the reference's rule: an existing contact keeps
+// its slot, a new one takes the last free slot (slot nc when none is free);
+// more than NC contacts raise SPH_ERR_NC_OVERFLOW and skip the rest of that
+// cell, as the cell search does.  occ: bit s set when slot s is in use
+// (updated).  Returns whether the row changed.
+__device__ __forceinline__ bool insert_keys(const StepArgs &A, const uint16_t *keys, int nk, int KS,
+                                            const uint32_t *lst, uint32_t *row, int RS,
+                                            uint32_t &occ)
+{
+    bool dirty = false;
+    int nc = 0, cur_ord = -1;
+    bool full = false;
+    for (int q = 0; q < nk; ++q) {
+        const uint32_t key = keys[q * KS];
+        const int ord = (int)(key >> 10);
+        if (ord != cur_ord) {
+            cur_ord = ord;
+            full = false;
+        }
+        if (full) continue;
+        const uint32_t b_orig = lst[key & 63u];
+        // the partner's slot if it is in the row, else the highest free slot
+        int cpos = -1;
+        for (uint32_t m = occ; m; m &= m - 1u) {
+            const int s = __ffs(m) - 1;
+            if ((row[s * RS] & ID_MASK) == b_orig) {
+                cpos = s;
+                break;
+            }
+        }
+        if (cpos < 0) cpos = ~occ ? 31 - __clz(~occ) : nc;
+        if (cpos < NC) {
+            row[cpos * RS] = b_orig | (((key >> 6) & 15u) << CODE_SHIFT);
+            occ |= 1u << cpos;
+            dirty = true;
+        } else {
+            raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+        }
+        ++nc;
+        if (nc > NC) {
+            raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+            full = true;
+        }
+    }
+    return dirty;
+}
+
+__device__ __forceinline__ uint32_t occupancy(const uint32_t *row, int RS)
+{
+    uint32_t occ = 0;
+#pragma unroll
+    for (int s = 0; s < NC; ++s) occ |= (row[s * RS] != EMPTY ? 1u : 0u) << s;
+    return occ;
+}
+
+// The 27-cell contact search (contactsearch.cuh:329-371 and :194-322) on
+// the slot row, for spheres without a usable neighbour list.
+template <int LM>
+__device__ __forceinline__ bool search_cells(const StepArgs &A, const DevBox &B, uint32_t a,
+                                             double4 xa, const int g[3], float4 xaf,
+                                             uint32_t *row, int RS)
 {
     const double radius_a = xa.w;
     const int nx = (int)B.num[0], ny = (int)B.num[1];
     const float Lf0 = (float)B.L[0], Lf1 = (float)B.L[1];
+    const float margin = B.pre_margin;
     bool dirty = false;
     int nc = 0;
-    const float margin = B.pre_margin;
-    const uint32_t vc = A.vlist ? A.vcount[i] : (uint32_t)VL_MAX + 1u;
-    if (vc <= (uint32_t)VL_MAX) {
-        // Same contacts, same order: the cell search visits the 27
-        // neighbour cells in (dz, dy, dx) order and, within a cell, the
-        // spheres in ascending original index (the stable sort).  Every
-        // sphere that can touch is in the neighbour list (ascending
-        // index), so the touching ones are found there, keyed by
-        // (cell ordinal, list position) and inserted in key order.
-        const uint32_t *lst = A.vlist + (size_t)i * VL_MAX;
-        int nk = 0;
-        for (uint32_t k = 0; k < vc; ++k) {
-            const uint32_t bo = lst[k];
-            int bx, by, bz, dx, dy, dz, sx, sy;
-            unpack_cell(A.cellc[bo], bx, by, bz);
-            if (!relative_cell(B, g, bx, by, bz, dx, dy, dz, sx, sy)) continue;
-            const double4 xb = A.xs[A.rank[bo]];
-            const d3 dm = shift_vec(B, sx, sy);
-            d3 x_ab = mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
-            x_ab = vadd(x_ab, dm);
-            const double len = vlen<LM>(x_ab);
-            if (len - (radius_a + xb.w) < 0.0) {
-                const int ord = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
-                const uint16_t key =
-                    (uint16_t)((ord << 10) | (shift_code(sx, sy) << 6) | (int)k);
-                int q = nk;
-                while (q > 0 && keys[(q - 1) * RS] > key) {
-                    keys[q * RS] = keys[(q - 1) * RS];
-                    --q;
-                }
-                keys[q * RS] = key;
-                ++nk;
-            }
-        }
-        int cur_ord = -1;
-        bool full = false;
-        for (int q = 0; q < nk; ++q) {
-            const uint32_t key = keys[q * RS];
-            const int ord = (int)(key >> 10);
-            if (ord != cur_ord) {   // the cell search leaves a cell on overflow
-                cur_ord = ord;
-                full = false;
-            }
-            if (full) continue;
-            const uint32_t b_orig = lst[key & 63u];
-            int cpos = nc;
-            for (int s = 0; s < NC; ++s) {
-                const uint32_t w = row[s * RS];
-                if (w == EMPTY) cpos = s;
-                else if ((w & ID_MASK) == b_orig) { cpos = s; break; }
-            }
-            if (cpos < NC) {
-                row[cpos * RS] = b_orig | (((key >> 6) & 15u) << CODE_SHIFT);
-                dirty = true;
-            } else {
-                raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-            }
-            ++nc;
-            if (nc > NC) {
-                raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-                full = true;
-            }
-        }
-    } else
     for (int dz = -1; dz < 2; ++dz)
         for (int dy = -1; dy < 2; ++dy)
             for (int dx = -1; dx < 2; ++dx) {
@@ -264,6 +276,37 @@ __device__ __forceinline__ bool search_contacts(const StepArgs &A, const DevBox 
                 }
             }
     return dirty;
+}
+
+// The contact search of one sphere (contact models 2 and 3) on its slot row
+// staged in shared memory (row[s * RS]), one thread: from the neighbour list
+// when the sphere has one (the touching entries keyed and inserted in the
+// order the cell search would find them), else the 27-cell search.  keys:
+// shared scratch of VL_MAX entries at stride RS.  Returns whether the row
+// changed.
+template <int LM>
+__device__ __forceinline__ bool search_contacts(const StepArgs &A, const DevBox &B, uint32_t a,
+                                                uint32_t i, double4 xa, const int g[3],
+                                                float4 xaf, uint32_t *row, uint16_t *keys,
+                                                int RS)
+{
+    const uint32_t vc = A.vlist ? A.vcount[i] : (uint32_t)VL_MAX + 1u;
+    if (vc > (uint32_t)VL_MAX) return search_cells<LM>(A, B, a, xa, g, xaf, row, RS);
+    const uint32_t *lst = A.vlist + (size_t)i * VL_MAX;
+    int nk = 0;
+    for (uint32_t k = 0; k < vc; ++k) {
+        const uint16_t key = list_key<LM>(A, B, xa, g, lst[k], k);
+        if (key == NO_KEY) continue;
+        int q = nk;
+        while (q > 0 && keys[(q - 1) * RS] > key) {
+            keys[q * RS] = keys[(q - 1) * RS];
+            --q;
+        }
+        keys[q * RS] = key;
+        ++nk;
+    }
+    uint32_t occ = occupancy(row, RS);
+    return insert_keys(A, keys, nk, RS, lst, row, RS, occ);
 }
 
 // Static and dynamic walls (contactsearch.cuh:428-465 and :602-701) and the
@@ -537,8 +580,9 @@ __global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
 //
 // The step of k_interact for contact models 2 and 3 with fused integration,
 // in three launches that keep more memory requests in flight:
-//   k_search   one thread per sphere: contact search on the slot row, the
-//              list of live slots (ascending);
+//   k_search   one thread per sphere: contact search on the slot row (kept
+//              with a bitmask of the slots in use), the list of live slots
+//              (ascending);
 //   k_contacts CONTACT_LANES threads per sphere, one live contact each: the
 //              contact law with its additions recorded (ContactRec), the
 //              new history written, ended contacts removed from the row;
@@ -561,10 +605,12 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
     if (a >= A.ntot) return;
     const int RS = SEARCH_THREADS;
     uint32_t *row = s_row + threadIdx.x;
+    uint16_t *keys = s_keys + threadIdx.x;
     const uint32_t i = A.perm[a];
     const DevBox &B = A.boxes[A.box_of[i]];
     const double4 xa = A.xs[a];
     const uint4 *grow = reinterpret_cast<const uint4 *>(A.slots + (size_t)i * NC);
+    uint32_t occ = 0;
 #pragma unroll
     for (int q = 0; q < NC / 4; ++q) {
         const uint4 w = grow[q];
@@ -572,18 +618,41 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
         row[(4 * q + 1) * RS] = w.y;
         row[(4 * q + 2) * RS] = w.z;
         row[(4 * q + 3) * RS] = w.w;
+        occ |= (w.x != EMPTY ? 1u : 0u) << (4 * q);
+        occ |= (w.y != EMPTY ? 1u : 0u) << (4 * q + 1);
+        occ |= (w.z != EMPTY ? 1u : 0u) << (4 * q + 2);
+        occ |= (w.w != EMPTY ? 1u : 0u) << (4 * q + 3);
     }
     if (A.tape_rows_pre) {
-        uint4 *t = reinterpret_cast<uint4 *>(A.tape_rows_pre + (size_t)i * NC);
+        uint4 *tp = reinterpret_cast<uint4 *>(A.tape_rows_pre + (size_t)i * NC);
 #pragma unroll
-        for (int q = 0; q < NC / 4; ++q) t[q] = grow[q];
+        for (int q = 0; q < NC / 4; ++q) tp[q] = grow[q];
     }
     int g[3];
     g[0] = (int)floor((xa.x - B.origo[0]) / (B.L[0] / B.num[0]));
     g[1] = (int)floor((xa.y - B.origo[1]) / (B.L[1] / B.num[1]));
     g[2] = (int)floor((xa.z - B.origo[2]) / (B.L[2] / B.num[2]));
-    const bool dirty =
-        search_contacts<LM>(A, B, a, i, xa, g, A.xf[a], row, s_keys + threadIdx.x, RS);
+    const uint32_t vc = A.vlist ? A.vcount[i] : (uint32_t)VL_MAX + 1u;
+    bool dirty;
+    if (vc <= (uint32_t)VL_MAX) {
+        const uint32_t *lst = A.vlist + (size_t)i * VL_MAX;
+        int nk = 0;
+        for (uint32_t k = 0; k < vc; ++k) {
+            const uint16_t key = list_key<LM>(A, B, xa, g, lst[k], k);
+            if (key == NO_KEY) continue;
+            int q = nk;
+            while (q > 0 && keys[(q - 1) * RS] > key) {
+                keys[q * RS] = keys[(q - 1) * RS];
+                --q;
+            }
+            keys[q * RS] = key;
+            ++nk;
+        }
+        dirty = insert_keys(A, keys, nk, RS, lst, row, RS, occ);
+    } else {
+        dirty = search_cells<LM>(A, B, a, xa, g, A.xf[a], row, RS);
+        occ = occupancy(row, RS);
+    }
     if (A.tape_rows_post) {
         const double4 *hist = A.hist + (size_t)i * NC;
         for (int s = 0; s < NC; ++s) {
@@ -592,11 +661,16 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
             if (w != EMPTY) A.tape_hist[(size_t)i * NC + s] = hist[s];
         }
     }
-    uint8_t *live = A.live + (size_t)i * NC;
+    uint8_t *live = A.live + (size_t)a * NC;
+    uint32_t *livew = A.livew + (size_t)a * NC;
     uint32_t nl = 0;
-    for (int s = 0; s < NC; ++s)
-        if (row[s * RS] != EMPTY) live[nl++] = (uint8_t)s;
-    A.nlive[i] = nl;
+    for (uint32_t m = occ; m; m &= m - 1u) {
+        const int s = __ffs(m) - 1;
+        live[nl] = (uint8_t)s;
+        livew[nl] = row[s * RS];
+        ++nl;
+    }
+    A.nlive[a] = nl;
     if (dirty) {
         uint4 *wrow = reinterpret_cast<uint4 *>(A.slots + (size_t)i * NC);
 #pragma unroll
@@ -630,7 +704,7 @@ __global__ void __launch_bounds__(CONTACT_THREADS) k_contacts(StepArgs A)
     const uint32_t a = t / CONTACT_LANES, lane = t % CONTACT_LANES;
     const bool valid = a < A.ntot;
     const uint32_t i = valid ? A.perm[a] : 0u;
-    const uint32_t nl = valid ? A.nlive[i] : 0u;
+    const uint32_t nl = valid ? A.nlive[a] : 0u;
     // the whole warp runs the same number of rounds (its shuffles need
     // every lane); round r computes live contacts 4r .. 4r + 3 of each sphere
     const uint32_t rounds =
@@ -661,8 +735,8 @@ __global__ void __launch_bounds__(CONTACT_THREADS) k_contacts(StepArgs A)
             const d3 angvel_a = xyz(A.ws[a]);
             uint32_t *slots = A.slots + (size_t)i * NC;
             double4 *hist = A.hist + (size_t)i * NC;
-            const int s = A.live[(size_t)i * NC + q];
-            const uint32_t w = slots[s];
+            const int s = A.live[(size_t)a * NC + q];
+            const uint32_t w = A.livew[(size_t)a * NC + q];
             const uint32_t b_orig = w & ID_MASK;
             int sx, sy;
             decode_shift(w >> CODE_SHIFT, sx, sy);
@@ -703,7 +777,7 @@ __global__ void __launch_bounds__(CONTACT_THREADS) k_contacts(StepArgs A)
             if (lane == 0 && o.nev >= 0) replay(acc, o);
         }
     }
-    if (valid && lane == 0) A.csum[i] = acc;
+    if (valid && lane == 0) A.csum[a] = acc;
 }
 
 template <int LM>
@@ -722,7 +796,7 @@ __global__ void __launch_bounds__(FINISH_THREADS, 4) k_finish(StepArgs A)
     acc.es_dot = 0.0;
     acc.ev_dot = 0.0;
     acc.p = 0.0;
-    acc = A.csum[i];   // the contacts' sums, added in slot order by k_contacts
+    acc = A.csum[a];   // the contacts' sums, added in slot order by k_contacts
     const double w0_force = walls_and_bonds<LM>(A, B, i, xa, xyz(va4), xyz(wa4), acc);
     store_sums(A, B, i, acc, w0_force);
     integrate_particle(A, B, i, xa, va4, wa4, acc.F, acc.T);

@@ -141,18 +141,11 @@ def _fcc_sites(nxc, nyc, nzc, a):
     return sites[order] * a
 
 
-def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.005, 0.02),
-               aspect_z=0.5, sweeps=3000, alpha=0.6, inflate=2.0e-7, device=-1, sid="dense"):
-    """A dense x-y periodic pack of n log-normal spheres at the given
-    porosity, made on the GPU: FCC lattice start in a box of aspect
-    1 : 1 : aspect_z sized for the porosity, then geometric overlap removal
-    (sph_relax) between the floor and the box top, then radii grown by the
-    factor (1 + inflate) so that touching spheres overlap by ~inflate * r
-    and form contacts.  Returns the sim (no walls yet) and the largest
-    residual overlap of the relaxation."""
-    from .runner import Stepper
-    rng = numpy.random.default_rng(seed)
-    r = numpy.clip(numpy.exp(rng.normal(math.log(median), sigma_ln, n)), *r_clip)
+def _fcc_start(n, rng, r, porosity, aspect_z, zlift, sid):
+    """Spheres of radii r on an FCC lattice (jittered) filling an x-y
+    periodic box of aspect 1 : 1 : aspect_z sized for the porosity, with a
+    sorting grid of cells 2.1 r_max wide and room above.  Returns the sim and
+    the packing height H."""
     v_solid = float(numpy.sum(4.0 / 3.0 * math.pi * r ** 3))
     v_box = v_solid / (1.0 - porosity)
     L = (v_box / aspect_z) ** (1.0 / 3.0)
@@ -162,10 +155,10 @@ def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.00
     a = L / nxc
     nzc = int(math.ceil(n / (4.0 * nxc * nxc)))
     sites = _fcc_sites(nxc, nxc, nzc, a)[:n]
-    sites[:, 2] *= (H - 2.0 * median) / max(sites[:, 2].max(), 1e-12)
+    sites[:, 2] *= (H - 2.0 * zlift) / max(sites[:, 2].max(), 1e-12)
     s = sim(np=n, nw=0, sid=sid)
     s.radius[:] = r
-    s.x[:] = sites + numpy.array([0.25 * a, 0.25 * a, median]) + \
+    s.x[:] = sites + numpy.array([0.25 * a, 0.25 * a, zlift]) + \
         rng.uniform(-0.05 * a, 0.05 * a, (n, 3))
     s.x[:, 0] = numpy.mod(s.x[:, 0], L)
     s.x[:, 1] = numpy.mod(s.x[:, 1], L)
@@ -180,6 +173,22 @@ def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.00
     s.num[:] = [ncx, ncx, max(int(Lz / cell), 3)]
     s.time_dt[0] = 1e-7
     s.time_total[0] = 1.0
+    return s, H
+
+
+def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.005, 0.02),
+               aspect_z=0.5, sweeps=3000, alpha=0.6, inflate=2.0e-7, device=-1, sid="dense"):
+    """A dense x-y periodic pack of n log-normal spheres at the given
+    porosity, made on the GPU: FCC lattice start in a box of aspect
+    1 : 1 : aspect_z sized for the porosity, then geometric overlap removal
+    (sph_relax) between the floor and the box top, then radii grown by the
+    factor (1 + inflate) so that touching spheres overlap by ~inflate * r
+    and form contacts.  Returns the sim (no walls yet) and the largest
+    residual overlap of the relaxation."""
+    from .runner import Stepper
+    rng = numpy.random.default_rng(seed)
+    r = numpy.clip(numpy.exp(rng.normal(math.log(median), sigma_ln, n)), *r_clip)
+    s, H = _fcc_start(n, rng, r, porosity, aspect_z, median, sid)
     st = Stepper([s], device=device)
     st.upload()
     worst = st.relax(sweeps, alpha=alpha, z_top=H)
@@ -188,6 +197,68 @@ def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.00
     s.radius *= 1.0 + inflate
     s.time_current[0] = 0.0
     return s, worst
+
+
+def _shear_setup(s, sigma0, mu, k_n=1.16e9, gamma_n=1.0e3, top_vel=0.01, steps=5000):
+    """Turn a relaxed pack into a shear box: gravity, linear contacts, a top
+    wall at normal stress sigma0 (wmode 1, mass = total particle mass as in
+    sim.consolidate), the top layer moving at +x top_vel and the bottom
+    layer held (fixvel, as in sim.shear), dt = 0.17 sqrt(m_min / k_n)."""
+    s.g[:] = [0.0, 0.0, -9.81]
+    s.k_n[0] = s.k_t[0] = k_n
+    s.gamma_n[0] = gamma_n
+    s.gamma_t[0] = 0.0
+    s.mu_s[0] = s.mu_d[0] = mu
+    rr = s.radius
+    r_max = float(rr.max())
+    ztop = float((s.x[:, 2] + rr).max())
+    zmin = float((s.x[:, 2] - rr).min())
+    s.nw = numpy.ones(1, dtype=numpy.uint32)
+    s.wmode = numpy.array([1], dtype=numpy.int32)
+    s.w_n = numpy.array([[0.0, 0.0, -1.0]])
+    s.w_x = numpy.array([ztop])
+    s.w_m = numpy.array([s.totalMass()])
+    s.w_vel = numpy.zeros(1)
+    s.w_force = numpy.zeros(1)
+    s.w_sigma0 = numpy.array([sigma0])
+    top = s.x[:, 2] > ztop - 2.0 * r_max
+    bot = s.x[:, 2] < zmin + 2.0 * r_max
+    s.fixvel[top | bot] = 1.0
+    s.vel[:] = 0.0
+    s.vel[top, 0] = top_vel
+    m_min = s.rho[0] * V_sphere(float(rr.min()))
+    s.time_dt[0] = 0.17 * math.sqrt(m_min / s.k_n[0])
+    s.time_current[0] = 0.0
+    s.time_total[0] = steps * s.time_dt[0]
+    s.time_file_dt[0] = s.time_total[0]
+    return s
+
+
+def shear_ensemble(nboxes=256, seed=0, device=-1, counts=(500, 20000), r_range=(0.009, 0.011),
+                   porosity=0.40, sweeps=2000, inflate=2.0e-7, steps=2000):
+    """The batched ensemble: nboxes independent x-y periodic shear boxes
+    with particle counts uniform in [counts], radii U[r_range], packed to
+    ~porosity on the GPU in one handle (FCC start, sph_relax of all boxes
+    at once, radii grown by 1 + inflate), each with its own normal stress
+    U[10, 80] kPa and friction mu U[0.3, 0.6] (_shear_setup)."""
+    from .runner import Stepper
+    rng = numpy.random.default_rng(seed)
+    sims = []
+    for b in range(nboxes):
+        n = int(rng.integers(counts[0], counts[1] + 1))
+        r = rng.uniform(r_range[0], r_range[1], n)
+        s, _H = _fcc_start(n, rng, r, porosity, 0.5, float(r.mean()), "box%03d" % b)
+        sims.append(s)
+    st = Stepper(sims, device=device)
+    st.upload()
+    st.relax(sweeps, alpha=0.6, z_top=1e300)
+    st.to_sims()
+    st.close()
+    for s in sims:
+        s.radius *= 1.0 + inflate
+        _shear_setup(s, sigma0=float(rng.uniform(1.0e4, 8.0e4)), mu=float(rng.uniform(0.3, 0.6)),
+                     steps=steps)
+    return sims
 
 
 def sheared_dense_pack(n=1000000, seed=0, device=-1, sweeps=3000):
@@ -200,34 +271,7 @@ def sheared_dense_pack(n=1000000, seed=0, device=-1, sweeps=3000):
     k_n = k_t = 1.16e9 N/m, gamma_n = 1e3, mu = 0.5, NC = 32 slots,
     dt = 0.17 * sqrt(m_min / k_n), 5,000 steps."""
     s, _worst = dense_pack(n, seed=seed, device=device, sweeps=sweeps, sid="shear1e6")
-    s.g[:] = [0.0, 0.0, -9.81]
-    s.k_n[0] = s.k_t[0] = 1.16e9
-    s.gamma_n[0] = 1.0e3
-    s.gamma_t[0] = 0.0
-    s.mu_s[0] = s.mu_d[0] = 0.5
-    rr = s.radius
-    r_max = float(rr.max())
-    ztop = float((s.x[:, 2] + rr).max())
-    zmin = float((s.x[:, 2] - rr).min())
-    s.nw = numpy.ones(1, dtype=numpy.uint32)
-    s.wmode = numpy.array([1], dtype=numpy.int32)
-    s.w_n = numpy.array([[0.0, 0.0, -1.0]])
-    s.w_x = numpy.array([ztop])
-    s.w_m = numpy.array([s.totalMass()])
-    s.w_vel = numpy.zeros(1)
-    s.w_force = numpy.zeros(1)
-    s.w_sigma0 = numpy.array([2.0e4])
-    top = s.x[:, 2] > ztop - 2.0 * r_max
-    bot = s.x[:, 2] < zmin + 2.0 * r_max
-    s.fixvel[top | bot] = 1.0
-    s.vel[:] = 0.0
-    s.vel[top, 0] = 0.01
-    m_min = s.rho[0] * V_sphere(float(rr.min()))
-    s.time_dt[0] = 0.17 * math.sqrt(m_min / s.k_n[0])
-    s.time_current[0] = 0.0
-    s.time_total[0] = 5000 * s.time_dt[0]
-    s.time_file_dt[0] = s.time_total[0]
-    return s
+    return _shear_setup(s, sigma0=2.0e4, mu=0.5, steps=5000)
 
 
 def _relax_cpu(x, r, lo, hi, iters=4000, tol=1e-12):

@@ -666,8 +666,9 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
     uint32_t nl = 0;
     for (uint32_t m = occ; m; m &= m - 1u) {
         const int s = __ffs(m) - 1;
+        const uint32_t w = row[s * RS];
         live[nl] = (uint8_t)s;
-        livew[nl] = row[s * RS];
+        livew[nl] = __ldg(A.rank + (w & ID_MASK)) | (w & ~ID_MASK);   // sorted position
         ++nl;
     }
     A.nlive[a] = nl;
@@ -737,27 +738,30 @@ __global__ void __launch_bounds__(CONTACT_THREADS) k_contacts(StepArgs A)
             double4 *hist = A.hist + (size_t)i * NC;
             const int s = A.live[(size_t)a * NC + q];
             const uint32_t w = A.livew[(size_t)a * NC + q];
-            const uint32_t b_orig = w & ID_MASK;
+            const uint32_t bs = w & ID_MASK;   // partner's sorted position
             int sx, sy;
             decode_shift(w >> CODE_SHIFT, sx, sy);
             const d3 dm = shift_vec(B, sx, sy);
-            const uint32_t bs = A.rank[b_orig];
+            // the partner's data and the history are loaded together
             const double4 xb = A.xs[bs];
+            const double4 vb4 = A.vs[bs];
+            const double4 wb4 = A.ws[bs];
+            const double4 h4 = hist[s];
             const d3 x_ab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
             const double x_ab_length = vlen<LM>(x_ab);
             const double delta_n = x_ab_length - (radius_a + xb.w);
             if (delta_n < 0.0) {
                 r.nev = 0;
-                const d3 vel_b = xyz(A.vs[bs]);
-                const d3 h0 = xyz(hist[s]);
+                const d3 vel_b = xyz(vb4);
+                const d3 h0 = xyz(h4);
                 d3 nd;
                 if (MIXED) {
                     const MixedPair mp = mixed_pair(x_ab, x_ab_length, delta_n, vel_a, vel_b,
-                                                    tof(angvel_a), xyzf(A.ws[bs]), radius_a, xb.w);
+                                                    tof(angvel_a), xyzf(wb4), radius_a, xb.w);
                     if (cm == 2) nd = contact_linear_mixed(P, dt, r, mp, h0);
                     else nd = contact_hertz_mixed(P, dt, r, mp, h0);
                 } else {
-                    const d3 angvel_b = xyz(A.ws[bs]);
+                    const d3 angvel_b = xyz(wb4);
                     if (cm == 2)
                         nd = contact_linear<LM>(P, dt, r, vel_a, vel_b, angvel_a, angvel_b,
                                                 radius_a, xb.w, x_ab, x_ab_length, delta_n, h0);

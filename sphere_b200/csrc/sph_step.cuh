@@ -165,6 +165,44 @@ __device__ __forceinline__ uint16_t list_key(const StepArgs &A, const DevBox &B,
     return (uint16_t)((ord << 10) | (shift_code(sx, sy) << 6) | (int)k);
 }
 
+// list_key for entries k0 .. k0 + KB - 1 (those below vc), their loads
+// issued together so that KB gathers are in flight at once.
+constexpr int KB = 4;
+
+template <int LM>
+__device__ __forceinline__ void list_keys_batch(const StepArgs &A, const DevBox &B, double4 xa,
+                                                const int g[3], const uint32_t *lst, uint32_t k0,
+                                                uint32_t vc, uint16_t out[KB])
+{
+    uint32_t bo[KB], rk[KB];
+    uint64_t cc[KB];
+    double4 xb[KB];
+#pragma unroll
+    for (int j = 0; j < KB; ++j) bo[j] = k0 + j < vc ? lst[k0 + j] : 0u;
+#pragma unroll
+    for (int j = 0; j < KB; ++j) {
+        cc[j] = k0 + j < vc ? A.cellc[bo[j]] : 0ull;
+        rk[j] = k0 + j < vc ? A.rank[bo[j]] : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < KB; ++j) xb[j] = k0 + j < vc ? A.xs[rk[j]] : make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < KB; ++j) {
+        out[j] = NO_KEY;
+        if (k0 + j >= vc) continue;
+        int bx, by, bz, dx, dy, dz, sx, sy;
+        unpack_cell(cc[j], bx, by, bz);
+        if (!relative_cell(B, g, bx, by, bz, dx, dy, dz, sx, sy)) continue;
+        const d3 dm = shift_vec(B, sx, sy);
+        d3 x_ab = mk(xa.x - xb[j].x, xa.y - xb[j].y, xa.z - xb[j].z);
+        x_ab = vadd(x_ab, dm);
+        const double len = vlen<LM>(x_ab);
+        if (!(len - (xa.w + xb[j].w) < 0.0)) continue;
+        const int ord = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+        out[j] = (uint16_t)((ord << 10) | (shift_code(sx, sy) << 6) | (int)(k0 + j));
+    }
+}
+
 // Insert the touching list entries, keys sorted ascending (keys[q * KS]),
 // into the slot row with the reference's rule: an existing contact keeps
 // its slot, a new one takes the last free slot (slot nc when none is free);
@@ -637,16 +675,21 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
     if (vc <= (uint32_t)VL_MAX) {
         const uint32_t *lst = A.vlist + (size_t)i * VL_MAX;
         int nk = 0;
-        for (uint32_t k = 0; k < vc; ++k) {
-            const uint16_t key = list_key<LM>(A, B, xa, g, lst[k], k);
-            if (key == NO_KEY) continue;
-            int q = nk;
-            while (q > 0 && keys[(q - 1) * RS] > key) {
-                keys[q * RS] = keys[(q - 1) * RS];
-                --q;
+        for (uint32_t k0 = 0; k0 < vc; k0 += KB) {
+            uint16_t kb[KB];
+            list_keys_batch<LM>(A, B, xa, g, lst, k0, vc, kb);
+#pragma unroll
+            for (int j = 0; j < KB; ++j) {
+                const uint16_t key = kb[j];
+                if (key == NO_KEY) continue;
+                int q = nk;
+                while (q > 0 && keys[(q - 1) * RS] > key) {
+                    keys[q * RS] = keys[(q - 1) * RS];
+                    --q;
+                }
+                keys[q * RS] = key;
+                ++nk;
             }
-            keys[q * RS] = key;
-            ++nk;
         }
         dirty = insert_keys(A, keys, nk, RS, lst, row, RS, occ);
     } else {

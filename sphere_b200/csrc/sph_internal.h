@@ -51,10 +51,11 @@ struct StepArgs {
     float4 *xref;
     uint64_t *cellc;
     uint32_t vcap;             // list capacity in use (<= VL_MAX)
-    // split step (k_search / k_contacts / k_finish), indexed by sorted
-    // position: per sphere the live slots in ascending order (slot index,
-    // and the partner's sorted position | image code << 28), their number,
-    // and the sums of its contacts (null until the split step is first used)
+    // split step (k_search / k_contacts / k_finish): per sphere, by sorted
+    // position, the live slots in ascending order (slot index, and the
+    // partner's sorted position | image code << 28) and their number; by
+    // original index, the sums of its contacts (null until the split step
+    // is first used)
     uint8_t *live;
     uint32_t *livew;
     uint32_t *nlive;

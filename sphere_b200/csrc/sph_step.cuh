@@ -626,7 +626,8 @@ __global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
 //              new history written, ended contacts removed from the row;
 //              the records go by warp shuffle to the sphere's first lane,
 //              which adds them in slot order and stores the sums;
-//   k_finish   one thread per sphere: walls, bonds, sums, integration.
+//   k_finish   one thread per sphere, original order: walls, bonds, sums,
+//              integration.
 // Each contact's arithmetic and the order of every sum are those of
 // k_interact, so the results are bit-identical.
 constexpr int SEARCH_THREADS = 128;
@@ -742,7 +743,7 @@ __device__ __forceinline__ ContactRec shfl_rec(const ContactRec &r, int src)
 }
 
 template <int LM, bool MIXED>
-__global__ void __launch_bounds__(CONTACT_THREADS) k_contacts(StepArgs A)
+__global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t a = t / CONTACT_LANES, lane = t % CONTACT_LANES;
@@ -824,26 +825,28 @@ __global__ void __launch_bounds__(CONTACT_THREADS) k_contacts(StepArgs A)
             if (lane == 0 && o.nev >= 0) replay(acc, o);
         }
     }
-    if (valid && lane == 0) A.csum[a] = acc;
+    if (valid && lane == 0) A.csum[i] = acc;
 }
 
 template <int LM>
 __global__ void __launch_bounds__(FINISH_THREADS, 4) k_finish(StepArgs A)
 {
-    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A.ntot) return;
-    const uint32_t i = A.perm[a];
+    // original order: every access of this kernel is to the sphere's own
+    // entries, so they are all coalesced (x, vel, angvel still hold the
+    // state at the start of the step: only this thread rewrites them)
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.ntot) return;
     const DevBox &B = A.boxes[A.box_of[i]];
-    const double4 xa = A.xs[a];
-    const double4 va4 = A.vs[a];
-    const double4 wa4 = A.ws[a];
+    const double4 xa = A.x[i];
+    const double4 va4 = A.vel[i];
+    const double4 wa4 = A.angvel[i];
     Acc acc;
     acc.F = mk(0.0, 0.0, 0.0);
     acc.T = mk(0.0, 0.0, 0.0);
     acc.es_dot = 0.0;
     acc.ev_dot = 0.0;
     acc.p = 0.0;
-    acc = A.csum[a];   // the contacts' sums, added in slot order by k_contacts
+    acc = A.csum[i];   // the contacts' sums, added in slot order by k_contacts
     const double w0_force = walls_and_bonds<LM>(A, B, i, xa, xyz(va4), xyz(wa4), acc);
     store_sums(A, B, i, acc, w0_force);
     integrate_particle(A, B, i, xa, va4, wa4, acc.F, acc.T);

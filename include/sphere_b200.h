@@ -282,6 +282,22 @@ int sph_neighbor_stats(SphHandle *h, uint64_t *stats);
 int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen);
 int sph_set_variant(SphHandle *h, int variant);
 
+/* Output snapshot, the output path of the reference's loop
+ * (transferFromGlobalDeviceMemory before each output file,
+ * src/device.cu:747-822 and 2569-2590) without stopping the steps:
+ * sph_snapshot enqueues on the handle's stream, after the steps already
+ * queued, a device copy of everything sph_download and sph_get_boxes
+ * return, and returns at once; steps queued later do not change it.
+ * sph_snapshot_read waits for that copy only (not for later steps) and
+ * fills p and b as sph_download and boxes[nboxes] as sph_get_boxes (each
+ * may be NULL); it returns the first device error raised by the steps
+ * before the snapshot and after the previous one.  One snapshot is held at
+ * a time; a new sph_snapshot replaces an unread one.  The copies take
+ * 272 B per sphere and 72 B per bond of device memory, allocated at the
+ * first call. */
+int sph_snapshot(SphHandle *h);
+int sph_snapshot_read(SphHandle *h, SphParticles *p, SphBonds *b, SphBox *boxes);
+
 /* Message of the last error on this handle (or a static message for a NULL
  * handle).  Returns the number of characters written. */
 int sph_last_error(const SphHandle *h, char *buf, size_t n);

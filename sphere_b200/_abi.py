@@ -202,6 +202,10 @@ def load_library():
     lib.sph_relax.restype = C.c_int
     lib.sph_step_async.argtypes = [H, C.c_uint64]
     lib.sph_set_neighbor_lists.argtypes = [H, C.c_uint32]
+    lib.sph_snapshot.argtypes = [H]
+    lib.sph_snapshot.restype = C.c_int
+    lib.sph_snapshot_read.argtypes = [H, C.POINTER(SphParticles), C.POINTER(SphBonds), C.POINTER(SphBox)]
+    lib.sph_snapshot_read.restype = C.c_int
     lib.sph_neighbor_stats.argtypes = [H, C.POINTER(C.c_uint64)]
     lib.sph_neighbor_stats.restype = C.c_int
     lib.sph_autotune.argtypes = [H, C.c_uint32, _dp, C.POINTER(C.c_int)]

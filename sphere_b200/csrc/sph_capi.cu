@@ -58,6 +58,13 @@ struct SphHandle {
     std::vector<void *> allocs;
     unsigned long long *d_count = nullptr;
     uint32_t *vlist_mem = nullptr;   // neighbour-list storage (A.vlist is null when off)
+    // output snapshot (sph_snapshot): device copies of what sph_download and
+    // sph_get_boxes return, the error word, an event after the copies and a
+    // stream for reading them back
+    StepArgs snap{};
+    bool snap_alloc = false, snap_pending = false;
+    cudaEvent_t snap_ev = nullptr;
+    cudaStream_t snap_stream = nullptr;
     // adjoint: checkpoints of the last sph_adjoint_forward (null when none)
     char *adj_snaps = nullptr;
     uint64_t adj_nsteps = 0, adj_iter0 = 0;
@@ -221,6 +228,8 @@ void sph_destroy(SphHandle *h)
             for (int k = 0; k <= sph::Prof::MAX; ++k) cudaEventDestroy(h->prof[r].ev[k]);
     }
     if (h->adj_snaps) cudaFree(h->adj_snaps);
+    if (h->snap_ev) cudaEventDestroy(h->snap_ev);
+    if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
     for (void *p : h->allocs) cudaFree(p);
     if (h->own) cudaStreamDestroy(h->own);
     delete h;
@@ -401,11 +410,19 @@ static int put3(SphHandle *h, double4 *dst, const double *src, uint64_t n)
     return SPH_OK;
 }
 
-static int get3(SphHandle *h, double *dst, const double4 *src, uint64_t n)
+static int get3(SphHandle *h, double *dst, const double4 *src, uint64_t n,
+                cudaStream_t cs = nullptr)
 {
     if (!dst) return SPH_OK;
     std::vector<double4> tmp(n ? n : 1);
-    CUDA_TRY(h, cudaMemcpy(tmp.data(), src, sizeof(double4) * (n ? n : 1), cudaMemcpyDeviceToHost));
+    if (cs) {
+        CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), src, sizeof(double4) * (n ? n : 1),
+                                    cudaMemcpyDeviceToHost, cs));
+        CUDA_TRY(h, cudaStreamSynchronize(cs));
+    } else {
+        CUDA_TRY(h, cudaMemcpy(tmp.data(), src, sizeof(double4) * (n ? n : 1),
+                               cudaMemcpyDeviceToHost));
+    }
     for (uint64_t i = 0; i < n; ++i) {
         dst[3 * i] = tmp[i].x;
         dst[3 * i + 1] = tmp[i].y;
@@ -723,34 +740,39 @@ int sph_advance(SphHandle *h, double time_total, double file_dt, double *time_cu
     return st;
 }
 
-int sph_download(SphHandle *h, SphParticles *p, SphBonds *b)
+}  // extern "C"
+
+// Copy the particle and bond state held in S (the live arrays or the
+// snapshot copies) to the host layouts; cs: stream for the copies (null:
+// synchronous copies).
+static int download_from(SphHandle *h, const StepArgs &S, cudaStream_t cs, SphParticles *p,
+                         SphBonds *b)
 {
-    if (!h) return SPH_ERR_INPUT;
-    cudaSetDevice(h->device);
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     const uint64_t n = h->ntot, nb = h->nbonds;
-    const StepArgs &A = h->A;
+    auto d2h = [&](void *dst, const void *src, size_t bytes) -> cudaError_t {
+        if (!cs) return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, cs);
+        return e == cudaSuccess ? cudaStreamSynchronize(cs) : e;
+    };
     int st;
     if (p) {
-        if (p->x && n) CUDA_TRY(h, cudaMemcpy(p->x, A.x, sizeof(double4) * n, cudaMemcpyDeviceToHost));
-        if (p->vel && n)
-            CUDA_TRY(h, cudaMemcpy(p->vel, A.vel, sizeof(double4) * n, cudaMemcpyDeviceToHost));
-        if ((st = get3(h, p->xyzsum, A.xyzsum, n)) || (st = get3(h, p->force, A.force, n)) ||
-            (st = get3(h, p->angpos, A.angpos, n)) || (st = get3(h, p->angvel, A.angvel, n)) ||
-            (st = get3(h, p->torque, A.torque, n)))
+        if (p->x && n) CUDA_TRY(h, d2h(p->x, S.x, sizeof(double4) * n));
+        if (p->vel && n) CUDA_TRY(h, d2h(p->vel, S.vel, sizeof(double4) * n));
+        if ((st = get3(h, p->xyzsum, S.xyzsum, n, cs)) || (st = get3(h, p->force, S.force, n, cs)) ||
+            (st = get3(h, p->angpos, S.angpos, n, cs)) || (st = get3(h, p->angvel, S.angvel, n, cs)) ||
+            (st = get3(h, p->torque, S.torque, n, cs)))
             return st;
         double *dst[5] = {p->es_dot, p->es, p->ev_dot, p->ev, p->p};
-        double *src[5] = {A.es_dot, A.es, A.ev_dot, A.ev, A.p};
+        double *src[5] = {S.es_dot, S.es, S.ev_dot, S.ev, S.p};
         for (int k = 0; k < 5; ++k)
-            if (dst[k] && n)
-                CUDA_TRY(h, cudaMemcpy(dst[k], src[k], sizeof(double) * n, cudaMemcpyDeviceToHost));
+            if (dst[k] && n) CUDA_TRY(h, d2h(dst[k], src[k], sizeof(double) * n));
     }
     if (b && nb) {
         std::vector<uint2> pairs(nb);
         std::vector<double4> dl(nb), om(nb);
-        CUDA_TRY(h, cudaMemcpy(pairs.data(), A.bonds, sizeof(uint2) * nb, cudaMemcpyDeviceToHost));
-        CUDA_TRY(h, cudaMemcpy(dl.data(), A.bdelta, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
-        CUDA_TRY(h, cudaMemcpy(om.data(), A.bomega, sizeof(double4) * nb, cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, d2h(pairs.data(), S.bonds, sizeof(uint2) * nb));
+        CUDA_TRY(h, d2h(dl.data(), S.bdelta, sizeof(double4) * nb));
+        CUDA_TRY(h, d2h(om.data(), S.bomega, sizeof(double4) * nb));
         for (uint64_t q = 0; q < nb; ++q) {
             if (b->pairs) { b->pairs[2 * q] = pairs[q].x; b->pairs[2 * q + 1] = pairs[q].y; }
             if (b->delta_n) b->delta_n[q] = dl[q].w;
@@ -762,13 +784,10 @@ int sph_download(SphHandle *h, SphParticles *p, SphBonds *b)
     return SPH_OK;
 }
 
-int sph_get_boxes(SphHandle *h, SphBox *boxes)
+// The boxes as created, with the fields the step changes taken from the
+// device box table image d.
+static void boxes_from(SphHandle *h, const std::vector<DevBox> &d, SphBox *boxes)
 {
-    if (!h || !boxes) return SPH_ERR_INPUT;
-    cudaSetDevice(h->device);
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    std::vector<DevBox> d(h->nbox);
-    CUDA_TRY(h, cudaMemcpy(d.data(), h->A.boxes, sizeof(DevBox) * h->nbox, cudaMemcpyDeviceToHost));
     for (uint32_t k = 0; k < h->nbox; ++k) {
         SphBox b = h->boxes[k];
         for (int c = 0; c < 2; ++c) b.grid.L[c] = d[k].L[c];
@@ -781,6 +800,104 @@ int sph_get_boxes(SphHandle *h, SphBox *boxes)
         b.t_current = d[k].t_current;
         boxes[k] = b;
     }
+}
+
+extern "C" {
+
+int sph_download(SphHandle *h, SphParticles *p, SphBonds *b)
+{
+    if (!h) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return download_from(h, h->A, nullptr, p, b);
+}
+
+int sph_get_boxes(SphHandle *h, SphBox *boxes)
+{
+    if (!h || !boxes) return SPH_ERR_INPUT;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    std::vector<DevBox> d(h->nbox);
+    CUDA_TRY(h, cudaMemcpy(d.data(), h->A.boxes, sizeof(DevBox) * h->nbox, cudaMemcpyDeviceToHost));
+    boxes_from(h, d, boxes);
+    return SPH_OK;
+}
+
+int sph_snapshot(SphHandle *h)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_snapshot before sph_upload");
+    cudaSetDevice(h->device);
+    const uint64_t n = h->ntot, nb = h->nbonds;
+    StepArgs &S = h->snap;
+    if (!h->snap_alloc) {
+        int st;
+        if ((st = dalloc(h, &S.x, n)) || (st = dalloc(h, &S.vel, n)) ||
+            (st = dalloc(h, &S.angvel, n)) || (st = dalloc(h, &S.angpos, n)) ||
+            (st = dalloc(h, &S.xyzsum, n)) || (st = dalloc(h, &S.force, n)) ||
+            (st = dalloc(h, &S.torque, n)) || (st = dalloc(h, &S.es_dot, n)) ||
+            (st = dalloc(h, &S.es, n)) || (st = dalloc(h, &S.ev_dot, n)) ||
+            (st = dalloc(h, &S.ev, n)) || (st = dalloc(h, &S.p, n)) ||
+            (st = dalloc(h, &S.bonds, nb)) || (st = dalloc(h, &S.bdelta, nb)) ||
+            (st = dalloc(h, &S.bomega, nb)) || (st = dalloc(h, &S.boxes, h->nbox)) ||
+            (st = dalloc(h, &S.err, 1)))
+            return st;
+        CUDA_TRY(h, cudaEventCreateWithFlags(&h->snap_ev, cudaEventDisableTiming));
+        CUDA_TRY(h, cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
+        h->snap_alloc = true;
+    }
+    const StepArgs &A = h->A;
+    auto d2d = [&](void *dst, const void *src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream);
+    };
+    const size_t n4 = sizeof(double4) * (n ? n : 1), n1 = sizeof(double) * (n ? n : 1);
+    CUDA_TRY(h, d2d(S.x, A.x, n4));
+    CUDA_TRY(h, d2d(S.vel, A.vel, n4));
+    CUDA_TRY(h, d2d(S.angvel, A.angvel, n4));
+    CUDA_TRY(h, d2d(S.angpos, A.angpos, n4));
+    CUDA_TRY(h, d2d(S.xyzsum, A.xyzsum, n4));
+    CUDA_TRY(h, d2d(S.force, A.force, n4));
+    CUDA_TRY(h, d2d(S.torque, A.torque, n4));
+    CUDA_TRY(h, d2d(S.es_dot, A.es_dot, n1));
+    CUDA_TRY(h, d2d(S.es, A.es, n1));
+    CUDA_TRY(h, d2d(S.ev_dot, A.ev_dot, n1));
+    CUDA_TRY(h, d2d(S.ev, A.ev, n1));
+    CUDA_TRY(h, d2d(S.p, A.p, n1));
+    if (nb) {
+        CUDA_TRY(h, d2d(S.bonds, A.bonds, sizeof(uint2) * nb));
+        CUDA_TRY(h, d2d(S.bdelta, A.bdelta, sizeof(double4) * nb));
+        CUDA_TRY(h, d2d(S.bomega, A.bomega, sizeof(double4) * nb));
+    }
+    CUDA_TRY(h, d2d(S.boxes, A.boxes, sizeof(DevBox) * h->nbox));
+    CUDA_TRY(h, d2d(S.err, A.err, sizeof(uint32_t)));
+    // errors are reported once: by the snapshot that saw them
+    CUDA_TRY(h, cudaMemsetAsync(A.err, 0, sizeof(uint32_t), h->stream));
+    CUDA_TRY(h, cudaEventRecord(h->snap_ev, h->stream));
+    h->snap_pending = true;
+    return SPH_OK;
+}
+
+int sph_snapshot_read(SphHandle *h, SphParticles *p, SphBonds *b, SphBox *boxes)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (!h->snap_pending) return fail(h, SPH_ERR_STATE, "no snapshot to read");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaEventSynchronize(h->snap_ev));
+    h->snap_pending = false;
+    int st = download_from(h, h->snap, h->snap_stream, p, b);
+    if (st != SPH_OK) return st;
+    uint32_t bits = 0;
+    std::vector<DevBox> d(h->nbox);
+    CUDA_TRY(h, cudaMemcpyAsync(d.data(), h->snap.boxes, sizeof(DevBox) * h->nbox,
+                                cudaMemcpyDeviceToHost, h->snap_stream));
+    CUDA_TRY(h, cudaMemcpyAsync(&bits, h->snap.err, sizeof bits, cudaMemcpyDeviceToHost,
+                                h->snap_stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->snap_stream));
+    if (boxes) boxes_from(h, d, boxes);
+    if (!bits) return SPH_OK;
+    static const int order[] = {SPH_ERR_NAN, SPH_ERR_OUT_OF_GRID, SPH_ERR_INPUT, SPH_ERR_NC_OVERFLOW};
+    for (int code : order)
+        if (bits & (1u << code)) return fail(h, code, sph_status_string(code));
     return SPH_OK;
 }
 

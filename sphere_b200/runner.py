@@ -294,10 +294,35 @@ class Stepper(object):
     def kernel_launches(self):
         return int(self.lib.sph_kernel_launches(self.h))
 
-    def to_sims(self):
-        """Copy device state into the sim objects (as an output file would)."""
-        hp, hb = self.download()
-        boxes = self.boxes()
+    def snapshot(self):
+        """Enqueue a device copy of the downloadable state after the steps
+        queued so far (sph_snapshot); returns at once."""
+        self._check(self.lib.sph_snapshot(self.h), "sph_snapshot")
+
+    def snapshot_read(self):
+        """Wait for the last snapshot and read it (sph_snapshot_read).
+        Returns (status, HostParticles, HostBonds, boxes); status is the
+        first device error raised since the previous snapshot."""
+        hp = HostParticles(self.ntot)
+        hb = HostBonds(self.nbonds)
+        ps = hp.struct()
+        bs = hb.struct()
+        out = (_abi.SphBox * len(self.sims))()
+        st = self.lib.sph_snapshot_read(self.h, C.byref(ps), C.byref(bs) if self.nbonds else None,
+                                        out)
+        if st not in (0, _abi.SPH_ERR_NAN, _abi.SPH_ERR_OUT_OF_GRID, _abi.SPH_ERR_INPUT,
+                      _abi.SPH_ERR_NC_OVERFLOW):
+            self._check(st, "sph_snapshot_read")
+        return st, hp, hb, list(out)
+
+    def to_sims(self, state=None):
+        """Copy device state (or a (HostParticles, HostBonds, boxes) triple
+        read earlier) into the sim objects, as an output file would."""
+        if state is None:
+            hp, hb = self.download()
+            boxes = self.boxes()
+        else:
+            hp, hb, boxes = state
         o = ob = 0
         for s, b, k, kb in zip(self.sims, boxes, self.np, self.nb):
             s.x = hp.x[o:o + k, :3].copy()
@@ -317,6 +342,153 @@ class Stepper(object):
             o += k
             ob += kb
         return self.sims
+
+
+# src/sphere.cpp:145-345 checkValues (host side, before any device work)
+def check_values(s):
+    if int(s.nd[0]) != 3:
+        return "Error: nd = %d, ND = 3" % int(s.nd[0])
+    if s.time_current[0] > s.time_total[0] or s.time_current[0] < 0.0:
+        return "Error: time.current = %g s, time.total = %g s" % (s.time_current[0], s.time_total[0])
+    if (numpy.asarray(s.origo) < 0.0).any():
+        return "Error: Negative values in grid.origo are known to cause problems."
+    if (numpy.asarray(s.L) <= 0.0).any():
+        return "Error: grid.L must be positive"
+    if (numpy.asarray(s.num) <= 0).any():
+        return "Error: grid.num must be positive"
+    if s.periodic[0] == 2 and s.num[0] < 3:
+        return "Error: When 1st dimension boundaries are periodic, there must be at least 3 cells in that dimension."
+    if s.periodic[0] == 1 and (s.num[0] < 3 or s.num[1] < 3):
+        return ("Error: When 1st and 2nd dimension boundaries are periodic, there must be at "
+                "least 3 cells in each of those dimensions.")
+    n = int(s.np[0])
+    if n:
+        if (s.radius <= 0.0).any():
+            return "Error: Particle %d has a radius of %g m." % (int(numpy.argmax(s.radius <= 0.0)),
+                                                                  float(s.radius.min()))
+        if numpy.isnan(s.x).any() or numpy.isnan(s.vel).any() or numpy.isnan(s.fixvel).any():
+            return "Error: NaN particle position or velocity"
+        out = (s.x < numpy.asarray(s.origo)).any(axis=1) | (s.x > numpy.asarray(s.L)).any(axis=1)
+        if out.any():
+            return "Error: Particle %d is outside of the computational grid" % int(numpy.argmax(out))
+        if s.nw[0] > 0 and s.w_x[0] < max(0.0, float(s.x[:, 2].max())):
+            return "Error: One or more particles have centres above the upper, dynamic wall"
+    if s.k_n[0] <= 0.0:
+        return "Error: k_n = %g N/m" % s.k_n[0]
+    if s.E[0] < 0.0:
+        return "Error: E = %g N/m^3" % s.E[0]
+    if s.rho[0] <= 0.0:
+        return "Error: rho = %g kg/m3" % s.rho[0]
+    return None
+
+
+def report_values(s):
+    """The `--dry` report of src/sphere.cpp:349-466."""
+    print("  - Number of dimensions: nd = %d" % s.nd[0])
+    print("  - Number of particles:  np = %d" % s.np[0])
+    print("  - Compiled for double precision")
+    print("  - Timestep length:      time.dt         = %g s" % s.time_dt[0])
+    print("  - Start at time:        time.current    = %g s" % s.time_current[0])
+    print("  - Total sim. time:      time.total      = %g s" % s.time_total[0])
+    print("  - File output interval: time.file_dt    = %g s" % s.time_file_dt[0])
+    print("  - Start at step count:  time.step_count = %d" % s.time_step_count[0])
+    cm = int(s.contactmodel[0])
+    names = {1: "Linear-elastic-viscous (n), visco-frictional (t)",
+             2: "Linear-elastic-visco-frictional", 3: "Nonlinear-elastic-visco-frictional"}
+    print("  - Contact model: " + names.get(cm, "unknown (%d)" % cm))
+    print("  - Using Young's modulus for contact stiffness" if s.E[0] > 0.01 else
+          "  - Using global value for contact stiffness")
+    print("  - Number of dynamic walls: %d" % s.nw[0])
+    print("  - Grid: %d * %d * %d cells" % tuple(int(v) for v in s.num))
+    print("  - Domain size: %g * %g * %g m" % tuple(float(v) for v in s.L))
+    print("  - No. of particle bonds: %d" % s.nb0[0])
+
+
+def _write_status(path, s):
+    with open(path, "w") as fh:
+        cur = float(s.time_current[0])
+        tot = float(s.time_total[0])
+        fh.write("%2.4e %2.4e %d\n" % (cur, 100.0 * cur / tot if tot else 0.0,
+                                       int(s.time_step_count[0])))
+
+
+def run_sim(s, root="..", verbose=True, device=-1, precision="fp64", length="reference"):
+    """Run `s` to time_total, writing the reference's output files.  Returns
+    0 or the SphStatus of the first failure (as the binary's exit status)."""
+    msg = check_values(s)
+    if msg:
+        print(msg)
+        return 1
+    # the caller's object keeps its input state, as with the reference binary
+    s = copy.deepcopy(s)
+    outdir = os.path.join(root, "output")
+    os.makedirs(outdir, exist_ok=True)
+    status_path = os.path.join(outdir, s.sid + ".status.dat")
+    # device.cu:840-842: output file 0 before the first step
+    if int(s.time_step_count[0]) == 0:
+        binio.write_bin(os.path.join(outdir, s.sid + ".output00000.bin"), s)
+    st = Stepper([s], precision=precision, length=length, device=device)
+    try:
+        st.upload()
+        _write_status(status_path, s)
+        cur = float(s.time_current[0])
+        total = float(s.time_total[0])
+        file_dt = float(s.time_file_dt[0])
+        dt = float(s.time_dt[0])
+        ftc = 0.0
+        state = {"status": 0, "stop": False}
+
+        def write_snapshot(t_out):
+            # the output due at time t_out, read back while later steps run
+            code, hp, hb, boxes = st.snapshot_read()
+            if code != 0:
+                state["status"] = code
+                if verbose:
+                    print("sphere_b200: " + st._msg(st.h))
+                # an overflowing contact list is reported and the run goes
+                # on (the reference ignores it); anything else ends the run
+                if code != _abi.SPH_ERR_NC_OVERFLOW:
+                    state["stop"] = True
+                    return
+            st.to_sims((hp, hb, boxes))
+            s.time_current[0] = t_out
+            s.time_step_count[0] += 1
+            binio.write_bin(os.path.join(outdir, "%s.output%05d.bin" %
+                                         (s.sid, int(s.time_step_count[0]))), s)
+            _write_status(status_path, s)
+
+        pending = None   # time of the queued snapshot not yet written
+        while cur <= total and not state["stop"]:
+            # steps up to the next output, counted as the reference's loop
+            # does (src/device.cu:1031 loop condition, :2536-2537
+            # increments, :2569 output test)
+            k = 0
+            while cur <= total:
+                cur += dt
+                ftc += dt
+                k += 1
+                if ftc >= file_dt:
+                    break
+            st.step_async(k)
+            if pending is not None:     # overlaps with the steps just queued
+                write_snapshot(pending)
+                pending = None
+            if ftc >= file_dt and not state["stop"]:
+                st.snapshot()
+                pending = cur
+                ftc = 0.0
+        if pending is not None and not state["stop"]:
+            write_snapshot(pending)
+        code = st.sync(raise_on_error=False)
+        if code != 0 and state["status"] == 0:
+            state["status"] = code
+            if verbose:
+                print("sphere_b200: " + st._msg(st.h))
+        if verbose:
+            print("  - Last output file number: %d" % int(s.time_step_count[0]))
+        return state["status"]
+    finally:
+        st.close()
 
 
 # src/sphere.cpp:145-345 checkValues (host side, before any device work)

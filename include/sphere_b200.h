@@ -298,6 +298,24 @@ int sph_set_variant(SphHandle *h, int variant);
 int sph_snapshot(SphHandle *h);
 int sph_snapshot_read(SphHandle *h, SphParticles *p, SphBonds *b, SphBox *boxes);
 
+/* Porosity profile of box `box` in z_slices horizontal slabs from the
+ * current state: DEM::porosity (src/sphere.cpp:487-606, the reference's
+ * `porosity` program), the same arithmetic in the same order; the top is
+ * wall 0's position when the box has walls, else L[2].  z_pos and porosity
+ * are host arrays of z_slices.  Slabs not thicker than 2 r_max:
+ * SPH_ERR_INPUT (the reference exits). */
+int sph_porosity(SphHandle *h, uint32_t box, uint32_t z_slices, double *z_pos, double *porosity);
+
+/* Overlapping sphere pairs of box `box` in the current state:
+ * DEM::findOverlaps (src/sphere.cpp:677-725, behind `sphere --contacts`):
+ * pairs (i, j) of box-local indexes with i < j, ascending in i then j,
+ * |x_j - x_i| - (r_i + r_j) < 0 without periodic images, both spheres free
+ * (fixvel 0), delta_n = that distance.  Writes up to max_pairs entries of
+ * pairs [max_pairs][2] and delta_n [max_pairs] (either may be NULL) and the
+ * total count in *npairs. */
+int sph_overlaps(SphHandle *h, uint32_t box, uint64_t max_pairs, uint32_t *pairs, double *delta_n,
+                 uint64_t *npairs);
+
 /* Message of the last error on this handle (or a static message for a NULL
  * handle).  Returns the number of characters written. */
 int sph_last_error(const SphHandle *h, char *buf, size_t n);

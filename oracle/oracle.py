@@ -10,6 +10,7 @@ Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline/reference
 legs use this module, as the checker; the product never imports it.
 """
 import ctypes as C
+import sys
 import os
 import subprocess
 
@@ -189,3 +190,75 @@ class CpuRun(object):
             s.w_force[i] = b.walls.mvfd[i][2]
         s.time_current[0] = b.t_current
         return s
+
+
+# ------------------------------------------------------------------ analysis
+
+def _alib():
+    lib = C.CDLL(LIBS["oracle"])
+    dp = C.POINTER(C.c_double)
+    lib.or_porosity.argtypes = [dp, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                C.c_uint32, dp, dp]
+    lib.or_porosity.restype = C.c_int
+    lib.or_overlaps.argtypes = [dp, dp, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), dp]
+    lib.or_overlaps.restype = C.c_uint64
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def porosity(s, slices):
+    """DEM::porosity of sim s (src/sphere.cpp:487-606) by the C restatement:
+    (z positions, porosities), or None where the reference exits."""
+    x = _f4(s.x, s.radius)
+    top = float(s.w_x[0]) if int(s.nw[0]) > 0 else float(s.L[2])
+    z = numpy.zeros(slices)
+    p = numpy.zeros(slices)
+    st = _alib().or_porosity(_dp(x), int(s.np[0]), top, float(s.origo[2]), float(s.L[0]),
+                             float(s.L[1]), int(slices), _dp(z), _dp(p))
+    return None if st != 0 else (z, p)
+
+
+def overlaps(s):
+    """DEM::findOverlaps of sim s (src/sphere.cpp:677-725) by the C
+    restatement: (pairs [n, 2] uint32, delta_n [n])."""
+    x = _f4(s.x, s.radius)
+    v = _f4(s.vel, s.fixvel)
+    lib = _alib()
+    n = int(lib.or_overlaps(_dp(x), _dp(v), int(s.np[0]), 0, None, None))
+    pairs = numpy.zeros((max(n, 1), 2), dtype=numpy.uint32)
+    d = numpy.zeros(max(n, 1))
+    lib.or_overlaps(_dp(x), _dp(v), int(s.np[0]), n, pairs.ctypes.data_as(C.POINTER(C.c_uint32)),
+                    _dp(d))
+    return pairs[:n], d[:n]
+
+
+def reference_analysis(s, what, slices=10, workdir=None):
+    """Run the reference's own analysis code (oracle/_ref/sphere_analysis_ref)
+    on sim s written as a .bin file; None when it is not built.  Returns
+    (z, porosity) for what='porosity', (pairs, delta_n) for 'contacts'."""
+    import os
+    import subprocess
+    import tempfile
+    exe = os.path.join(HERE, "_ref", "sphere_analysis_ref")
+    if not os.path.exists(exe):
+        return None
+    sys.path.insert(0, os.path.dirname(HERE))
+    from sphere_b200 import binio
+    d = workdir or tempfile.mkdtemp()
+    path = os.path.join(d, "analysis.bin")
+    binio.write_bin(path, s)
+    args = [exe, what, path] + ([str(slices)] if what == "porosity" else [])
+    out = subprocess.run(args, capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError(out.stderr)
+    rows = [r.split("\t") for r in out.stdout.strip().splitlines() if r.strip()]
+    if what == "porosity":
+        a = numpy.array([[float(c) for c in r] for r in rows])
+        return a[:, 0], a[:, 1]
+    if not rows:
+        return numpy.zeros((0, 2), dtype=numpy.uint32), numpy.zeros(0)
+    pairs = numpy.array([[int(r[0]), int(r[1])] for r in rows], dtype=numpy.uint32)
+    return pairs, numpy.array([float(r[2]) for r in rows])

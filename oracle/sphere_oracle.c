@@ -855,3 +855,74 @@ int or_step(OrState *s, uint64_t nsteps)
     }
     return s->error_flags;
 }
+
+/* ----------------------------------------------------------- analysis */
+
+/* M_PI of the C library, which src/sphere.cpp uses (not the 3.14159265358979
+ * of the step kernels) */
+static const double OR_M_PI = 3.14159265358979323846;
+
+/* src/sphere.cpp:468-471 sphericalCap */
+static double or_cap(double h, double r) { return OR_M_PI * h * h / 3.0 * (3.0 * r - h); }
+
+/* src/sphere.cpp:487-606 DEM::porosity: per slab, the slab volume less
+ * every sphere's volume inside it, with the reference's cap terms (a sphere
+ * cut by a slab face subtracts the sphere volume plus the cap, as the
+ * reference writes it), spheres in index order. */
+int or_porosity(const double *x, uint32_t np, double top, double origo_z, double L0, double L1,
+                uint32_t z_slices, double *z_pos, double *porosity)
+{
+    double r_max = 0.0;
+    for (uint32_t i = 0; i < np; ++i)
+        if (x[4 * (size_t)i + 3] > r_max) r_max = x[4 * (size_t)i + 3];
+    const double h_slice = (top - origo_z) / (double)z_slices;
+    if (h_slice <= r_max * 2.0) return -1;
+    const double V_slice = h_slice * L0 * L1;
+    for (uint32_t iz = 0; iz < z_slices; ++iz) {
+        double V_void = V_slice;
+        const double z_low = iz * h_slice;
+        const double z_high = z_low + h_slice;
+        for (uint32_t i = 0; i < np; ++i) {
+            const double zc = x[4 * (size_t)i + 2], r = x[4 * (size_t)i + 3];
+            const double zl = zc - r, zh = zc + r;
+            const double V_s = 4.0 / 3.0 * OR_M_PI * r * r * r;
+            if (z_low <= zl && zh <= z_high) {
+                V_void -= V_s;
+            } else {
+                if (z_low >= zc && z_low <= zh) V_void -= or_cap(zh - z_low, r);
+                else if (z_low < zc && z_low > zl) V_void -= V_s + or_cap(z_low - zl, r);
+                if (z_high <= zc && z_high >= zl) V_void -= or_cap(z_high - zl, r);
+                else if (z_high > zc && z_high < zh) V_void -= V_s + or_cap(zh - z_high, r);
+            }
+        }
+        z_pos[iz] = z_low + 0.5 * h_slice;
+        porosity[iz] = V_void / V_slice;
+    }
+    return 0;
+}
+
+/* src/sphere.cpp:677-725 DEM::findOverlaps: all pairs i < j (no periodic
+ * images) with |x_j - x_i| - (r_i + r_j) < 0 and both fixvel == 0. */
+uint64_t or_overlaps(const double *x, const double *vel, uint32_t np, uint64_t max_pairs,
+                     uint32_t *pairs, double *delta_n)
+{
+    uint64_t n = 0;
+    for (uint32_t i = 0; i < np; ++i)
+        for (uint32_t j = i + 1; j < np; ++j) {
+            const double *xi = x + 4 * (size_t)i, *xj = x + 4 * (size_t)j;
+            const double dx = xj[0] - xi[0], dy = xj[1] - xi[1], dz = xj[2] - xi[2];
+            const double len = sqrt(dx * dx + dy * dy + dz * dz);
+            const double d = len - (xi[3] + xj[3]);
+            if (d < 0.0 && vel[4 * (size_t)i + 3] == 0.0 && vel[4 * (size_t)j + 3] == 0.0) {
+                if (n < max_pairs) {
+                    if (pairs) {
+                        pairs[2 * n] = i;
+                        pairs[2 * n + 1] = j;
+                    }
+                    if (delta_n) delta_n[n] = d;
+                }
+                ++n;
+            }
+        }
+    return n;
+}

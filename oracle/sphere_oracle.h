@@ -52,6 +52,17 @@ typedef struct OrState {
 /* Run nsteps iterations of the fluid == 0 step loop.  Returns the OR of the
  * error flags raised (0 = clean). */
 int or_step(OrState *s, uint64_t nsteps);
+
+/* Analysis (TEST INFRASTRUCTURE ONLY), restated from src/sphere.cpp.
+ * x: [np][4] (x, y, z, r); vel: [np][4] (fixvel in w).
+ * or_porosity: DEM::porosity (:487-606); returns -1 when a slab is not
+ * thicker than 2 r_max (the reference exits), else 0.
+ * or_overlaps: DEM::findOverlaps (:677-725); writes up to max_pairs pairs
+ * (i, j) and their delta_n, returns the total count. */
+int or_porosity(const double *x, uint32_t np, double top, double origo_z, double L0, double L1,
+                uint32_t z_slices, double *z_pos, double *porosity);
+uint64_t or_overlaps(const double *x, const double *vel, uint32_t np, uint64_t max_pairs,
+                     uint32_t *pairs, double *delta_n);
 int ref_step(OrState *s, uint64_t nsteps);
 
 #ifdef __cplusplus

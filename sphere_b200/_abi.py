@@ -202,6 +202,11 @@ def load_library():
     lib.sph_relax.restype = C.c_int
     lib.sph_step_async.argtypes = [H, C.c_uint64]
     lib.sph_set_neighbor_lists.argtypes = [H, C.c_uint32]
+    lib.sph_porosity.argtypes = [H, C.c_uint32, C.c_uint32, _dp, _dp]
+    lib.sph_porosity.restype = C.c_int
+    lib.sph_overlaps.argtypes = [H, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), _dp,
+                                 C.POINTER(C.c_uint64)]
+    lib.sph_overlaps.restype = C.c_int
     lib.sph_snapshot.argtypes = [H]
     lib.sph_snapshot.restype = C.c_int
     lib.sph_snapshot_read.argtypes = [H, C.POINTER(SphParticles), C.POINTER(SphBonds), C.POINTER(SphBox)]

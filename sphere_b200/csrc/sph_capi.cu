@@ -21,6 +21,9 @@ int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                       uint64_t *launches, Prof *prof);
 int relax_sweep(const StepArgs &A, cudaStream_t st, double alpha, double z_top,
                 unsigned long long *d_max, uint64_t *launches);
+int porosity_profile(const double4 *x, uint32_t p0, uint32_t np, double h_slice, double V_slice,
+                     uint32_t nslices, double *z_pos, double *por, cudaStream_t st);
+int find_overlaps(OverlapArgs O, uint32_t ncells, uint32_t *scan_tmp, cudaStream_t st, int stage);
 int adjoint_step(const DevBox *box, uint32_t n, uint64_t iter, const double4 *x,
                  const double4 *vel, const double4 *angvel, const uint32_t *rows_pre,
                  const uint32_t *rows_post, const double4 *hist, const double4 *const lnext[5],
@@ -58,6 +61,7 @@ struct SphHandle {
     std::vector<void *> allocs;
     unsigned long long *d_count = nullptr;
     uint32_t *vlist_mem = nullptr;   // neighbour-list storage (A.vlist is null when off)
+    std::vector<double> rmax_box;    // largest radius per box (at upload)
     // output snapshot (sph_snapshot): device copies of what sph_download and
     // sph_get_boxes return, the error word, an event after the copies and a
     // stream for reading them back
@@ -540,6 +544,8 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
             for (uint32_t j = 0; j < d.np; ++j) rmax = fmax(rmax, p->x[4 * (size_t)(d.p_base + j) + 3]);
             for (int c = 0; c < 3; ++c) lmax = fmax(lmax, fabs(d.L[c]) + fabs(d.origo[c]));
             d.pre_margin = (float)(ldexp(2.0 * lmax + 2.0 * rmax, -19));
+            h->rmax_box.resize(h->nbox);
+            h->rmax_box[k] = rmax;
             // neighbour lists: skin 0.1 r_min; the list is rebuilt once a
             // sphere has moved half the skin less the rounding allowance;
             // the build searches the cells that can hold a sphere within
@@ -1323,6 +1329,122 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
     if (st != SPH_OK) return fail(h, st, "autotune step failed");
     if (chosen) *chosen = best;
     return st2;
+}
+
+int sph_porosity(SphHandle *h, uint32_t box, uint32_t z_slices, double *z_pos, double *porosity)
+{
+    if (!h || !z_pos || !porosity || z_slices == 0) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_porosity before sph_upload");
+    if (box >= h->nbox) return fail(h, SPH_ERR_INPUT, "no such box");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    DevBox d;
+    CUDA_TRY(h, cudaMemcpy(&d, h->A.boxes + box, sizeof d, cudaMemcpyDeviceToHost));
+    // src/sphere.cpp:492-515: the top is wall 0 when there are walls
+    const double top = d.nw > 0 ? d.wnx[0][3] : d.L[2];
+    const double h_slice = (top - d.origo[2]) / (double)z_slices;
+    if (h_slice <= h->rmax_box[box] * 2.0)
+        return fail(h, SPH_ERR_INPUT, "the number of z-slices is too high (slab <= 2 r_max)");
+    const double V_slice = h_slice * d.L[0] * d.L[1];
+    double *dz = nullptr, *dp = nullptr;
+    if (cudaMalloc((void **)&dz, sizeof(double) * z_slices) != cudaSuccess ||
+        cudaMalloc((void **)&dp, sizeof(double) * z_slices) != cudaSuccess) {
+        cudaFree(dz);
+        return fail(h, SPH_ERR_NOMEM, "porosity buffers");
+    }
+    int st = sph::porosity_profile(h->A.x, d.p_base, d.np, h_slice, V_slice, z_slices, dz, dp,
+                                   h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (st == SPH_OK && e == cudaSuccess) {
+        e = cudaMemcpy(z_pos, dz, sizeof(double) * z_slices, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(porosity, dp, sizeof(double) * z_slices, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(dz);
+    cudaFree(dp);
+    if (st != SPH_OK) return fail(h, st, "porosity kernel launch failed");
+    if (e != cudaSuccess) return fail(h, SPH_ERR_CUDA, cudaGetErrorString(e));
+    return SPH_OK;
+}
+
+int sph_overlaps(SphHandle *h, uint32_t box, uint64_t max_pairs, uint32_t *pairs, double *delta_n,
+                 uint64_t *npairs)
+{
+    if (!h || !npairs) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_overlaps before sph_upload");
+    if (box >= h->nbox) return fail(h, SPH_ERR_INPUT, "no such box");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    DevBox d;
+    CUDA_TRY(h, cudaMemcpy(&d, h->A.boxes + box, sizeof d, cudaMemcpyDeviceToHost));
+    sph::OverlapArgs O{};
+    O.x = h->A.x;
+    O.vel = h->A.vel;
+    O.p0 = d.p_base;
+    O.np = d.np;
+    double cmin = 1e300;
+    for (int c = 0; c < 3; ++c) {
+        O.origo[c] = d.origo[c];
+        O.cw[c] = d.L[c] / d.num[c];
+        O.num[c] = (int)d.num[c];
+        cmin = fmin(cmin, O.cw[c]);
+    }
+    O.R = (int)ceil(2.0 * h->rmax_box[box] / cmin);
+    if (O.R < 1) O.R = 1;
+    const uint64_t ncells = (uint64_t)d.num[0] * d.num[1] * d.num[2];
+    const uint64_t n = d.np ? d.np : 1;
+    if (n > 4096ull * 4096ull) return fail(h, SPH_ERR_UNSUPPORTED, "box too large for sph_overlaps");
+    std::vector<void *> mine;
+    auto get = [&](size_t bytes) -> void * {
+        void *q = nullptr;
+        if (cudaMalloc(&q, bytes) != cudaSuccess) return nullptr;
+        mine.push_back(q);
+        return q;
+    };
+    auto release = [&]() {
+        for (void *q : mine) cudaFree(q);
+    };
+    O.cell_of = (uint32_t *)get(4 * n);
+    O.slot = (uint32_t *)get(4 * n);
+    O.count = (uint32_t *)get(4 * (ncells + 1));
+    O.coff = (uint32_t *)get(4 * (ncells + 1));
+    O.items = (uint32_t *)get(4 * n);
+    O.npair = (uint32_t *)get(4 * (n + 1));
+    O.poff = (uint32_t *)get(4 * (n + 1));
+    uint32_t *scan_tmp = (uint32_t *)get(4 * (ncells / 4096 + n / 4096 + 2));
+    if (!O.cell_of || !O.slot || !O.count || !O.coff || !O.items || !O.npair || !O.poff ||
+        !scan_tmp) {
+        release();
+        return fail(h, SPH_ERR_NOMEM, "overlap-search buffers");
+    }
+    int st = sph::find_overlaps(O, (uint32_t)ncells, scan_tmp, h->stream, 0);
+    uint32_t total = 0;
+    cudaError_t e = cudaSuccess;
+    if (st == SPH_OK) {
+        e = cudaMemcpyAsync(&total, O.poff + d.np, sizeof total, cudaMemcpyDeviceToHost,
+                            h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+    if (st == SPH_OK && e == cudaSuccess && total > 0 && max_pairs > 0 && (pairs || delta_n)) {
+        O.pairs = (uint32_t *)get(8 * (size_t)total);
+        O.delta = (double *)get(8 * (size_t)total);
+        if (!O.pairs || !O.delta) {
+            release();
+            return fail(h, SPH_ERR_NOMEM, "overlap list buffers");
+        }
+        st = sph::find_overlaps(O, (uint32_t)ncells, scan_tmp, h->stream, 1);
+        const uint64_t m = total < max_pairs ? total : max_pairs;
+        if (st == SPH_OK && pairs)
+            e = cudaMemcpyAsync(pairs, O.pairs, 8 * m, cudaMemcpyDeviceToHost, h->stream);
+        if (st == SPH_OK && e == cudaSuccess && delta_n)
+            e = cudaMemcpyAsync(delta_n, O.delta, 8 * m, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+    release();
+    if (st != SPH_OK) return fail(h, st, "overlap-search launch failed");
+    if (e != cudaSuccess) return fail(h, SPH_ERR_CUDA, cudaGetErrorString(e));
+    *npairs = total;
+    return SPH_OK;
 }
 
 int sph_set_neighbor_lists(SphHandle *h, uint32_t capacity)

@@ -71,6 +71,19 @@ constexpr int VL_MAX = 48;   // neighbour-list capacity per sphere
 constexpr int INTERACT_VARIANTS = 4;   // launch variants of the interact stage (sph_autotune)
 constexpr int SPLIT_VARIANT = 3;       // the split step (k_search / k_contacts / k_finish)
 
+// Overlap search of one box (sph_overlaps): positions and velocities, the
+// box's spheres [p0, p0 + np), its grid (origin, cell widths, cell counts),
+// the search range R in cells, and scratch / output arrays.
+struct OverlapArgs {
+    const double4 *x, *vel;
+    uint32_t p0, np;
+    double origo[3], cw[3];
+    int num[3], R;
+    uint32_t *cell_of, *slot, *count, *coff, *items, *npair, *poff;
+    uint32_t *pairs;
+    double *delta;
+};
+
 struct StepConfig {
     int lenmode;
     bool unfused;     // some box has a shear-stress (wmode 3) top wall

@@ -577,6 +577,165 @@ int relax_sweep(const StepArgs &A, cudaStream_t st, double alpha, double z_top,
     return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
 }
 
+// ---------------------------------------------------------------- analysis
+
+// src/sphere.cpp:487-606 DEM::porosity, one thread per slab: the slab
+// volume less the spheres' volumes inside it (with the reference's cap
+// terms), spheres in index order, so that every slab's sum is the
+// reference's, operation for operation.  All threads of a warp read the
+// same sphere at a time (broadcast).
+__global__ void k_porosity(const double4 *x, uint32_t p0, uint32_t np, double h_slice,
+                           double V_slice, uint32_t nslices, double *z_pos, double *por)
+{
+    const uint32_t iz = blockIdx.x * blockDim.x + threadIdx.x;
+    const double z_low = (double)iz * h_slice;
+    const double z_high = z_low + h_slice;
+    double V_void = V_slice;
+    for (uint32_t i = 0; i < np; ++i) {
+        const double4 p = x[p0 + i];
+        const double zc = p.z, r = p.w;
+        const double zl = zc - r, zh = zc + r;
+        const double V_s = 4.0 / 3.0 * M_PI * r * r * r;
+        if (z_low <= zl && zh <= z_high) {
+            V_void -= V_s;
+        } else {
+            if (z_low >= zc && z_low <= zh) {
+                const double h = zh - z_low;
+                V_void -= M_PI * h * h / 3.0 * (3.0 * r - h);
+            } else if (z_low < zc && z_low > zl) {
+                const double h = z_low - zl;
+                V_void -= V_s + M_PI * h * h / 3.0 * (3.0 * r - h);
+            }
+            if (z_high <= zc && z_high >= zl) {
+                const double h = z_high - zl;
+                V_void -= M_PI * h * h / 3.0 * (3.0 * r - h);
+            } else if (z_high > zc && z_high < zh) {
+                const double h = zh - z_high;
+                V_void -= V_s + M_PI * h * h / 3.0 * (3.0 * r - h);
+            }
+        }
+    }
+    if (iz < nslices) {
+        z_pos[iz] = z_low + 0.5 * h_slice;
+        por[iz] = V_void / V_slice;
+    }
+}
+
+int porosity_profile(const double4 *x, uint32_t p0, uint32_t np, double h_slice, double V_slice,
+                     uint32_t nslices, double *z_pos, double *por, cudaStream_t st)
+{
+    k_porosity<<<blocks_for(nslices, 32), 32, 0, st>>>(x, p0, np, h_slice, V_slice, nslices, z_pos,
+                                                       por);
+    return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+}
+
+// src/sphere.cpp:677-725 DEM::findOverlaps on the device: the box's spheres
+// binned into its own grid (clamped cells), each sphere i testing the
+// spheres j > i in the cells within +-R (no periodic images), first
+// counting, then writing its pairs in ascending j after an exclusive scan
+// of the counts, so that the list is the reference's, in its order.
+
+__device__ __forceinline__ void ov_cell(const OverlapArgs &O, double4 p, int c[3])
+{
+    const double v[3] = {p.x, p.y, p.z};
+    for (int d = 0; d < 3; ++d) {
+        double f = floor((v[d] - O.origo[d]) / O.cw[d]);
+        if (!(f >= 0.0)) f = 0.0;
+        if (f > (double)(O.num[d] - 1)) f = (double)(O.num[d] - 1);
+        c[d] = (int)f;
+    }
+}
+
+__global__ void k_ov_bin(OverlapArgs O)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= O.np) return;
+    int c[3];
+    ov_cell(O, O.x[O.p0 + i], c);
+    const uint32_t cell = (uint32_t)((c[2] * O.num[1] + c[1]) * O.num[0] + c[0]);
+    O.cell_of[i] = cell;
+    O.slot[i] = atomicAdd(&O.count[cell], 1u);
+}
+
+__global__ void k_ov_scatter(OverlapArgs O)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= O.np) return;
+    O.items[O.coff[O.cell_of[i]] + O.slot[i]] = i;
+}
+
+// WRITE = false: count the pairs of sphere i; true: write them sorted by j.
+template <bool WRITE>
+__global__ void k_ov_pairs(OverlapArgs O)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= O.np) return;
+    const double4 xi = O.x[O.p0 + i];
+    const bool free_i = O.vel[O.p0 + i].w == 0.0;
+    int c[3];
+    ov_cell(O, xi, c);
+    uint32_t n = 0;
+    const uint32_t base = WRITE ? O.poff[i] : 0u;
+    const uint32_t cnt = WRITE ? O.npair[i] : 0u;
+    for (int dz = -O.R; dz <= O.R; ++dz)
+        for (int dy = -O.R; dy <= O.R; ++dy)
+            for (int dx = -O.R; dx <= O.R; ++dx) {
+                const int tx = c[0] + dx, ty = c[1] + dy, tz = c[2] + dz;
+                if (tx < 0 || ty < 0 || tz < 0 || tx >= O.num[0] || ty >= O.num[1] ||
+                    tz >= O.num[2])
+                    continue;
+                const uint32_t cell = (uint32_t)((tz * O.num[1] + ty) * O.num[0] + tx);
+                for (uint32_t q = O.coff[cell]; q < O.coff[cell + 1]; ++q) {
+                    const uint32_t j = O.items[q];
+                    if (j <= i) continue;
+                    const double4 xj = O.x[O.p0 + j];
+                    const double ddx = xj.x - xi.x, ddy = xj.y - xi.y, ddz = xj.z - xi.z;
+                    const double len = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+                    const double d = len - (xi.w + xj.w);
+                    if (!(d < 0.0 && free_i && O.vel[O.p0 + j].w == 0.0)) continue;
+                    if (WRITE && n < cnt) {
+                        // insertion by j into this sphere's part of the list
+                        uint32_t k = n;
+                        while (k > 0 && O.pairs[2 * (size_t)(base + k - 1) + 1] > j) {
+                            O.pairs[2 * (size_t)(base + k)] = O.pairs[2 * (size_t)(base + k - 1)];
+                            O.pairs[2 * (size_t)(base + k) + 1] =
+                                O.pairs[2 * (size_t)(base + k - 1) + 1];
+                            O.delta[base + k] = O.delta[base + k - 1];
+                            --k;
+                        }
+                        O.pairs[2 * (size_t)(base + k)] = i;
+                        O.pairs[2 * (size_t)(base + k) + 1] = j;
+                        O.delta[base + k] = d;
+                    }
+                    ++n;
+                }
+            }
+    if (!WRITE) O.npair[i] = n;
+}
+
+int find_overlaps(OverlapArgs O, uint32_t ncells, uint32_t *scan_tmp, cudaStream_t st,
+                  int stage)
+{
+    const unsigned gb = blocks_for(O.np, 256);
+    if (stage == 0) {
+        cudaMemsetAsync(O.count, 0, sizeof(uint32_t) * ncells, st);
+        k_ov_bin<<<gb, 256, 0, st>>>(O);
+        const uint32_t nb = blocks_for(ncells, SCAN_TILE);
+        k_scan_reduce<<<nb, SCAN_THREADS, 0, st>>>(O.count, ncells, scan_tmp);
+        k_scan_top<<<1, SCAN_THREADS, 0, st>>>(scan_tmp, nb);
+        k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(O.count, ncells, scan_tmp, nb, O.coff);
+        k_ov_scatter<<<gb, 256, 0, st>>>(O);
+        k_ov_pairs<false><<<gb, 256, 0, st>>>(O);
+        const uint32_t np_b = blocks_for(O.np, SCAN_TILE);
+        k_scan_reduce<<<np_b, SCAN_THREADS, 0, st>>>(O.npair, O.np, scan_tmp);
+        k_scan_top<<<1, SCAN_THREADS, 0, st>>>(scan_tmp, np_b);
+        k_scan_down<<<np_b, SCAN_THREADS, 0, st>>>(O.npair, O.np, scan_tmp, np_b, O.poff);
+    } else {
+        k_ov_pairs<true><<<gb, 256, 0, st>>>(O);
+    }
+    return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+}
+
 // Live directed contacts (non-empty slots), for the roofline byte count.
 __global__ void k_count_live(const uint32_t *slots, uint64_t nslots, unsigned long long *count)
 {

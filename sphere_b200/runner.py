@@ -202,6 +202,28 @@ class Stepper(object):
         self._check(self.lib.sph_set_neighbor_lists(self.h, int(capacity)),
                     "sph_set_neighbor_lists")
 
+    def porosity(self, slices, box=0):
+        """(z positions, porosities) of box `box` in `slices` slabs
+        (sph_porosity)."""
+        z = numpy.zeros(int(slices))
+        p = numpy.zeros(int(slices))
+        self._check(self.lib.sph_porosity(self.h, int(box), int(slices), _abi.dptr(z),
+                                          _abi.dptr(p)), "sph_porosity")
+        return z, p
+
+    def overlaps(self, box=0):
+        """(pairs [n, 2] uint32, delta_n [n]) of box `box` (sph_overlaps)."""
+        n = C.c_uint64(0)
+        self._check(self.lib.sph_overlaps(self.h, int(box), 0, None, None, C.byref(n)),
+                    "sph_overlaps")
+        m = int(n.value)
+        pairs = numpy.zeros((max(m, 1), 2), dtype=numpy.uint32)
+        d = numpy.zeros(max(m, 1))
+        if m:
+            self._check(self.lib.sph_overlaps(self.h, int(box), m, _abi.uptr(pairs), _abi.dptr(d),
+                                              C.byref(n)), "sph_overlaps")
+        return pairs[:m], d[:m]
+
     def neighbor_stats(self):
         """(spheres with a list, spheres whose list overflowed, entries,
         longest list, builds so far): sph_neighbor_stats."""

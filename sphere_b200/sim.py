@@ -778,8 +778,191 @@ class sim(object):
         m = self.rho[0] * V_sphere(self.radius)
         return numpy.sum(m[:, None] * self.vel, axis=0)
 
+    # ------------------------------------------------------- shear analysis
     def shearDisplacement(self):
-        return self.xyzsum[:, 0]
+        """Shear displacement: the largest x displacement (xyzsum) of the
+        spheres with a prescribed velocity (python/sphere.py:4777)."""
+        fixed = numpy.nonzero(self.fixvel > 0.0)
+        return numpy.max(self.xyzsum[fixed, 0])
+
+    def shearVelocity(self):
+        """Shear velocity: the largest x velocity of the spheres with a
+        prescribed velocity (python/sphere.py:4794)."""
+        fixed = numpy.nonzero(self.fixvel > 0.0)
+        return numpy.max(self.vel[fixed, 0])
+
+    def shearVel(self):
+        return self.shearVelocity()
+
+    def shearStrain(self):
+        """Shear displacement over the top wall height (python/sphere.py:4816)."""
+        return self.shearDisplacement() / self.w_x[0]
+
+    def shearStrainRate(self):
+        """Shear velocity over the top wall height (python/sphere.py:4837)."""
+        return self.shearVelocity() / self.w_x[0]
+
+    def shearStress(self, type='effective'):
+        """'defined': the prescribed top-wall shear stress; 'effective': minus
+        the x force on the spheres moving at positive prescribed x velocity,
+        per unit box area (python/sphere.py:6407)."""
+        if type == 'defined':
+            return self.w_tau_x[0]
+        if type == 'effective':
+            moving = (self.fixvel > 0.0) & (self.vel[:, 0] > 0.0)
+            force = numpy.zeros(3)
+            for i in numpy.nonzero(moving)[0]:      # in index order, as summed there
+                force += -self.force[i, :]
+            return force[0] / (self.L[0] * self.L[1])
+        raise Exception('Shear stress type ' + type + ' not understood')
+
+    def inertiaParameterPlanarShear(self):
+        """I = shear strain rate * mean radius * sqrt(rho / normal stress)
+        (python/sphere.py:4855)."""
+        return self.shearStrainRate() * numpy.mean(self.radius) * \
+            numpy.sqrt(self.rho[0] / self.currentNormalStress())
+
+    def acceleration(self, idx=-1):
+        """Acceleration force / mass + g of one or more spheres
+        (python/sphere.py:6278)."""
+        if idx == -1:
+            idx = range(int(self.np[0]))
+        return self.force[idx, :] / (V_sphere(self.radius[idx]) * self.rho[0]) + self.g
+
+    def setTopWallNormalStressModulation(self, A, f, plot=False):
+        """Sine modulation of the top wall's normal stress, amplitude A and
+        frequency f (python/sphere.py:6188); plotting is not provided."""
+        self.w_sigma0_A[0] = A
+        self.w_sigma0_f[0] = f
+
+    def disableTopWallNormalStressModulation(self):
+        self.setTopWallNormalStressModulation(A=0.0, f=0.0)
+
+    # ---------------------------------------- contact and porosity analysis
+    def _analysis_stepper(self, device=-1):
+        from .runner import Stepper
+        st = Stepper([self], precision='fp64', length='reference', device=device)
+        st.upload()
+        return st
+
+    def porosity(self, slices=10, verbose=False, device=-1):
+        """Porosity in `slices` horizontal slabs and the slab mid-depths:
+        the reference's `porosity` program (src/sphere.cpp:487-606), run on
+        the GPU (sph_porosity) at full FP64 precision.  Returns (porosity,
+        depth) as python/sphere.py:4437 does."""
+        st = self._analysis_stepper(device)
+        try:
+            z, p = st.porosity(slices)
+        finally:
+            st.close()
+        return p, z
+
+    def findOverlaps(self, device=-1):
+        """All overlapping sphere pairs: the reference's n^2 search
+        (src/sphere.cpp:677-725, `sphere --contacts`), on the GPU
+        (sph_overlaps).  Sets self.pairs ([2, n] int32, i < j) and
+        self.overlaps (the negative distances), as python/sphere.py:4868."""
+        st = self._analysis_stepper(device)
+        try:
+            pairs, d = st.overlaps()
+        finally:
+            st.close()
+        self.pairs = numpy.array((pairs[:, 0], pairs[:, 1]), dtype=numpy.int32)
+        self.overlaps = numpy.array(d)
+
+    def findCoordinationNumber(self):
+        """Contacts per sphere from self.pairs (python/sphere.py:4885)."""
+        self.coordinationnumber = numpy.zeros(int(self.np[0]), dtype=numpy.int64)
+        numpy.add.at(self.coordinationnumber, self.pairs[0, :], 1)
+        numpy.add.at(self.coordinationnumber, self.pairs[1, :], 1)
+
+    def findMeanCoordinationNumber(self):
+        return numpy.mean(self.coordinationnumber)
+
+    def findNormalForces(self):
+        """|f_n| = k_n |overlap| of every overlapping pair
+        (python/sphere.py:4906)."""
+        self.findOverlaps()
+        self.f_n_magn = self.k_n * numpy.abs(self.overlaps)
+
+    def contactSurfaceArea(self, i, j, overlap):
+        """Area of the circle where spheres i and j intersect
+        (python/sphere.py:4919)."""
+        r_i = self.radius[i]
+        r_j = self.radius[j]
+        d = r_i + r_j + overlap
+        contact_radius = 1. / (2. * d) * ((-d + r_i - r_j) * (-d - r_i + r_j) *
+                                          (-d + r_i + r_j) * (d + r_i + r_j)) ** 0.5
+        return numpy.pi * contact_radius ** 2.
+
+    def contactParticleArea(self, i, j):
+        """Cross-section of the pair's mean radius (python/sphere.py:4941)."""
+        r_bar = (self.radius[i] + self.radius[j]) * 0.5
+        return numpy.pi * r_bar ** 2.
+
+    def findAllContactSurfaceAreas(self):
+        return self.contactSurfaceArea(self.pairs[0, :], self.pairs[1, :], self.overlaps)
+
+    def findAllAverageParticlePairAreas(self):
+        return self.contactParticleArea(self.pairs[0, :], self.pairs[1, :])
+
+    def findContactStresses(self, area='average'):
+        """Normal stress of every contact: |f_n| over the mean-radius area
+        ('average') or the contact area ('contact') (python/sphere.py:4980)."""
+        self.findNormalForces()
+        if area == 'average':
+            areas = self.findAllAverageParticlePairAreas()
+        elif area == 'contact':
+            areas = self.findAllContactSurfaceAreas()
+        else:
+            raise Exception('Contact area type "' + area + '" not understood')
+        self.sigma_contacts = self.f_n_magn / areas
+
+    def findLoadedContacts(self, threshold):
+        """Indexes of the contacts whose stress is at least `threshold`
+        (python/sphere.py:5004)."""
+        self.findContactStresses()
+        return numpy.nonzero(self.sigma_contacts >= threshold)
+
+    def forcechains(self, lc=200.0, uc=650.0, outformat='txt', disp='2d', path=None):
+        """Force-chain data as the reference's `forcechains` program writes it
+        (src/sphere.cpp:727-902): every overlapping pair with f_n = -k_n
+        delta_n >= lc, as text rows (outformat 'txt') or as a gnuplot script
+        (other formats), written to `path` (default <sid>-fc.txt / .gp) and
+        returned as a string.  The script is not rendered here."""
+        self.findOverlaps()
+        threedim = disp != '2d'
+        x = self.x
+        pairs = self.pairs.T
+        d = self.overlaps
+        lines = []
+        if outformat == 'txt':
+            head = ["x_1, [m]"] + (["y_1, [m]"] if threedim else []) + ["z_1, [m]", "x_2, [m]"] + \
+                (["y_2, [m]"] if threedim else []) + ["z_2, [m]", "||f_n||, [N]i", "j"]
+            lines.append("\t".join(head))
+        else:
+            lines.append("set size ratio -1")
+            lines.append("set cbrange [%g:%g]" % (lc, uc))
+        f_n_max = -self.k_n[0] * (numpy.min(d) if d.size else 0.0)
+        for n, ((i, j), dn) in enumerate(zip(pairs, d)):
+            f_n = -self.k_n[0] * dn
+            if f_n < lc:
+                continue
+            a = [x[i, 0]] + ([x[i, 1]] if threedim else []) + [x[i, 2]]
+            b = [x[j, 0]] + ([x[j, 1]] if threedim else []) + [x[j, 2]]
+            if outformat == 'txt':
+                lines.append("\t".join("%.17g" % v for v in a + b) + "\t%.17g%d\t%d" % (f_n, i, j))
+            elif f_n > lc and (self.fixvel[i] + self.fixvel[j]) == 0.0:
+                lines.append("set arrow %d from %s to %s nohead lw %.17g lc palette cb %.17g" %
+                             (n + 1, ",".join("%.17g" % v for v in a),
+                              ",".join("%.17g" % v for v in b),
+                              f_n / f_n_max * 16.0, f_n))
+        text = "\n".join(lines) + "\n"
+        if path is None:
+            path = self.sid + ('-fc.txt' if outformat == 'txt' else '-fc.gp')
+        with open(path, 'w') as fh:
+            fh.write(text)
+        return text
 
     # ---------------------------------------------------------------- run
     def run(self, verbose=True, hideinputfile=False, dry=False, valgrind=False,

@@ -316,6 +316,22 @@ int sph_porosity(SphHandle *h, uint32_t box, uint32_t z_slices, double *z_pos, d
 int sph_overlaps(SphHandle *h, uint32_t box, uint64_t max_pairs, uint32_t *pairs, double *delta_n,
                  uint64_t *npairs);
 
+/* Ray-traced image of box `box` in the current state: DEM::render
+ * (src/raytracer.cuh:379-560, behind `sphere --render`) with its camera
+ * (eye at (2.3 L0, -5 L1, 1.3 L2), looking at maxPos()/2, image plane
+ * 1.35 L0 wide), its rays (including the row index taken modulo the width)
+ * and its shading.  method: 0 uniform colour, 1 pressure, 2 |vel|,
+ * 3 |angvel|, 4 xyzsum.x, 5 |angpos| (colour map from 0 to maxval);
+ * lower_cutoff > 0 hides spheres of methods 1-5 at or below it and spheres
+ * with a fixed velocity.  focal_length is accepted and unused, as in the
+ * reference.  rgb: host array of width * height * 3 bytes, written row by
+ * row (the body of the reference's PPM file, src/file_io.cpp:734-757).
+ * Arithmetic: the reference's FP32 expressions in its order, without FMA
+ * contraction, with IEEE division and square root and a normalisation by
+ * 1 / sqrtf.  Other methods or a zero width or height: SPH_ERR_INPUT. */
+int sph_render(SphHandle *h, uint32_t box, int method, float maxval, float lower_cutoff,
+               float focal_length, uint32_t width, uint32_t height, uint8_t *rgb);
+
 /* Message of the last error on this handle (or a static message for a NULL
  * handle).  Returns the number of characters written. */
 int sph_last_error(const SphHandle *h, char *buf, size_t n);

@@ -202,6 +202,9 @@ def _alib():
     lib.or_porosity.restype = C.c_int
     lib.or_overlaps.argtypes = [dp, dp, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), dp]
     lib.or_overlaps.restype = C.c_uint64
+    lib.or_render.argtypes = [dp, dp, dp, dp, dp, dp, C.c_uint32, dp, C.c_int, C.c_float,
+                              C.c_float, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint8)]
+    lib.or_render.restype = None
     return lib
 
 
@@ -235,6 +238,24 @@ def overlaps(s):
     return pairs[:n], d[:n]
 
 
+def render(s, method=1, maxval=1.0e3, lower_cutoff=0.0, width=800, height=800):
+    """DEM::render of sim s (src/raytracer.cuh:379-560) by the C
+    restatement, every sphere tested for every pixel: [height, width, 3]
+    uint8."""
+    x = _f4(s.x, s.radius)
+    v = _f4(s.vel, s.fixvel)
+    av = _f4(s.angvel, numpy.zeros(len(s.radius)))
+    ap = _f4(s.angpos, numpy.zeros(len(s.radius)))
+    xs = _f4(s.xyzsum, numpy.zeros(len(s.radius)))
+    p = numpy.ascontiguousarray(s.p, dtype=numpy.float64)
+    L = numpy.ascontiguousarray(s.L, dtype=numpy.float64)
+    img = numpy.zeros((int(height), int(width), 3), dtype=numpy.uint8)
+    _alib().or_render(_dp(x), _dp(v), _dp(av), _dp(ap), _dp(xs), _dp(p), int(s.np[0]), _dp(L),
+                      int(method), float(maxval), float(lower_cutoff), int(width), int(height),
+                      img.ctypes.data_as(C.POINTER(C.c_uint8)))
+    return img
+
+
 def reference_analysis(s, what, slices=10, workdir=None):
     """Run the reference's own analysis code (oracle/_ref/sphere_analysis_ref)
     on sim s written as a .bin file; None when it is not built.  Returns
@@ -262,3 +283,30 @@ def reference_analysis(s, what, slices=10, workdir=None):
         return numpy.zeros((0, 2), dtype=numpy.uint32), numpy.zeros(0)
     pairs = numpy.array([[int(r[0]), int(r[1])] for r in rows], dtype=numpy.uint32)
     return pairs, numpy.array([float(r[2]) for r in rows])
+
+
+def reference_render(s, method=1, maxval=1.0e3, lower_cutoff=0.0, width=800, height=800,
+                     workdir=None):
+    """Run the reference's own ray-tracer kernels and camera
+    (oracle/_ref/sphere_render_ref) on sim s written as a .bin file: the
+    image [height, width, 3] uint8, or None when the program is not built.
+    maxval and lower_cutoff travel as text with 9 significant digits, which
+    the program's atof reads back to the same float."""
+    import os
+    import subprocess
+    import tempfile
+    exe = os.path.join(HERE, "_ref", "sphere_render_ref")
+    if not os.path.exists(exe):
+        return None
+    sys.path.insert(0, os.path.dirname(HERE))
+    from sphere_b200 import binio
+    d = workdir or tempfile.mkdtemp()
+    path = os.path.join(d, "render.bin")
+    out = os.path.join(d, "render.rgb")
+    binio.write_bin(path, s)
+    args = [exe, path, str(int(method)), "%.9g" % numpy.float32(maxval),
+            "%.9g" % numpy.float32(lower_cutoff), str(int(width)), str(int(height)), out]
+    r = subprocess.run(args, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr)
+    return numpy.fromfile(out, dtype=numpy.uint8).reshape(int(height), int(width), 3)

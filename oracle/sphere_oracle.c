@@ -926,3 +926,146 @@ uint64_t or_overlaps(const double *x, const double *vel, uint32_t np, uint64_t m
         }
     return n;
 }
+
+/* ---- ray tracer (src/raytracer.cuh), FP32 as the reference computes it.
+ * One ray per pixel, every sphere in index order, the first strictly
+ * smallest |t| kept; normalisation by 1 / sqrtf, IEEE division and square
+ * root, no contraction (the build's -ffp-contract=off). */
+typedef struct {
+    float x, y, z;
+} of3;
+
+static of3 o3(float x, float y, float z)
+{
+    of3 r = {x, y, z};
+    return r;
+}
+static of3 o_add(of3 a, of3 b) { return o3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static of3 o_sub(of3 a, of3 b) { return o3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static of3 o_mul(float s, of3 a) { return o3(s * a.x, s * a.y, s * a.z); }
+static of3 o_div(of3 a, float s) { return o3(a.x / s, a.y / s, a.z / s); }
+static of3 o_neg(of3 a) { return o3(-a.x, -a.y, -a.z); }
+static float o_dot(of3 a, of3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static of3 o_cross(of3 a, of3 b)
+{
+    return o3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static float o_len(of3 a) { return sqrtf(o_dot(a, a)); }
+static of3 o_unit(of3 a) { return o_mul(1.0f / sqrtf(o_dot(a, a)), a); }
+
+/* src/colorbar.h:7-20 */
+static float o_red(float r) { return fminf(1.0f, 0.209f * r * r * r - 2.49f * r * r + 3.0f * r + 0.0109f); }
+static float o_green(float r) { return fminf(1.0f, -2.44f * r * r + 2.15f * r + 0.369f); }
+static float o_blue(float r) { return fminf(1.0f, -2.21f * r * r + 1.61f * r + 0.573f); }
+
+/* |(v.x, v.y, v.z)| in double, as render() fills its linear array */
+static double o_mag(const double *v) { return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+void or_render(const double *x, const double *vel, const double *angvel, const double *angpos,
+               const double *xyzsum, const double *p, uint32_t np, const double *L, int method,
+               float maxval, float lower_cutoff, uint32_t width, uint32_t height, uint8_t *rgb)
+{
+    /* src/sphere.cpp:641-670 maxPos: componentwise max of the positions and 0 */
+    double mx[3] = {0.0, 0.0, 0.0};
+    for (uint32_t i = 0; i < np; ++i)
+        for (int a = 0; a < 3; ++a)
+            if (mx[a] < x[4 * (size_t)i + a]) mx[a] = x[4 * (size_t)i + a];
+    /* src/raytracer.cuh:379-400 render, :291-333 cameraInit */
+    const float imgw = (float)(L[0] * 1.35f);
+    const of3 lookat = o_div(o3((float)mx[0], (float)mx[1], (float)mx[2]), 2.0f);
+    const of3 eye = o3((float)(L[0] * 2.3f), (float)(L[1] * -5.0f), (float)(L[2] * 1.3f));
+    const float hw_ratio = (float)(height / width);
+    const float pl = -0.5f * imgw, pr = 0.5f * imgw;
+    const float pb = -0.5f * imgw * hw_ratio, pt = 0.5f * imgw * hw_ratio;
+    const of3 view = o_sub(eye, lookat);
+    const of3 up = o3(0.0f, 0.0f, 1.0f);
+    const of3 w = o_div(o_neg(view), o_len(view));
+    const of3 u = o_div(o_cross(up, w), o_len(o_cross(up, w)));
+    const of3 v = o_cross(w, u);
+    const float dfoc = o_len(view) * 0.8f;
+    const of3 le = o_mul(-1.0f, eye);
+    const of3 light = o_unit(o3(le.x * 1.0f, le.y * 0.2f, le.z * 0.6f));
+    const int64_t pixels = (int64_t)width * height;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t m = 0; m < pixels; ++m) {
+        const unsigned int mempos = (unsigned int)m;
+        /* :29-56 rayInitPerspective */
+        const unsigned int i = mempos % width;
+        const unsigned int j = (unsigned int)(int)floorf((float)mempos / width) % width;
+        const float p_u = pl + (pr - pl) * (i + 0.5f) / width;
+        const float p_v = pb + (pt - pb) * (j + 0.5f) / height;
+        const of3 e = eye;
+        const of3 d = o_add(o_add(o_mul(-dfoc, w), o_mul(p_u, u)), o_mul(p_v, v));
+        /* :59-144 rayIntersectSpheres, :146-288 rayIntersectSpheresColormap */
+        float tdist = 1e10f;
+        of3 n = o3(0.0f, 0.0f, 0.0f);
+        uint32_t hitidx = 0;
+        for (uint32_t k = 0; k < np; ++k) {
+            const double *xk = x + 4 * (size_t)k;
+            const of3 c = o3((float)xk[0], (float)xk[1], (float)xk[2]);
+            const float R = (float)xk[3];
+            const float Delta = (2.0f * o_dot(d, o_sub(e, c))) * (2.0f * o_dot(d, o_sub(e, c))) -
+                                4.0f * o_dot(d, d) * (o_dot(o_sub(e, c), o_sub(e, c)) - R * R);
+            int take = Delta > 0.0f;
+            if (method != 0 && lower_cutoff > 0.0) {
+                double val;
+                switch (method) {
+                case 1: val = p[k]; break;
+                case 2: val = o_mag(vel + 4 * (size_t)k); break;
+                case 3: val = o_mag(angvel + 4 * (size_t)k); break;
+                case 4: val = xyzsum[4 * (size_t)k]; break;
+                default: val = o_mag(angpos + 4 * (size_t)k); break;
+                }
+                const float fval = (float)val;
+                const float fixvel = (float)vel[4 * (size_t)k + 3];
+                take = take && fval > lower_cutoff && fixvel == 0.f;
+            }
+            if (!take) continue;
+            const float t_minus =
+                (o_dot(o_neg(d), o_sub(e, c)) -
+                 sqrtf(o_dot(d, o_sub(e, c)) * o_dot(d, o_sub(e, c)) -
+                       o_dot(d, d) * (o_dot(o_sub(e, c), o_sub(e, c)) - R * R))) /
+                o_dot(d, d);
+            if (fabsf(t_minus) < tdist) {
+                const of3 pt3 = o_add(e, o_mul(t_minus, d));
+                tdist = fabsf(t_minus);
+                n = o_unit(o_mul(2.0f, o_sub(pt3, c)));
+                hitidx = k;
+            }
+        }
+        uint8_t *px = rgb + 3 * (size_t)mempos;
+        if (!(tdist < 1e10f)) {
+            px[0] = px[1] = px[2] = 255; /* :14-27 imageInit */
+            continue;
+        }
+        const float dotprod = fmaxf(0.0f, o_dot(n, light));
+        const float I_d = 40.0f, k_d = 5.0f, k_a = 10.0f, I_a = 5.0f;
+        if (method == 0) {
+            px[0] = (uint8_t)((k_d * I_d * dotprod + k_a * I_a) * 0.48f);
+            px[1] = (uint8_t)((k_d * I_d * dotprod + k_a * I_a) * 0.41f);
+            px[2] = (uint8_t)((k_d * I_d * dotprod + k_a * I_a) * 0.27f);
+            continue;
+        }
+        double val;
+        switch (method) {
+        case 1: val = p[hitidx]; break;
+        case 2: val = o_mag(vel + 4 * (size_t)hitidx); break;
+        case 3: val = o_mag(angvel + 4 * (size_t)hitidx); break;
+        case 4: val = xyzsum[4 * (size_t)hitidx]; break;
+        default: val = o_mag(angpos + 4 * (size_t)hitidx); break;
+        }
+        const float fixvel = (float)vel[4 * (size_t)hitidx + 3];
+        float ratio = (float)(val / maxval);
+        if (ratio < 0.01f) ratio = 0.01f;
+        if (ratio > 0.99f) ratio = 0.99f;
+        float redv = o_red(ratio), greenv = o_green(ratio), bluev = o_blue(ratio);
+        if (fixvel > 0.f) {
+            redv = 0.5f;
+            greenv = 0.5f;
+            bluev = 0.5f;
+        }
+        px[0] = (uint8_t)((k_d * I_d * dotprod + k_a * I_a) * redv);
+        px[1] = (uint8_t)((k_d * I_d * dotprod + k_a * I_a) * greenv);
+        px[2] = (uint8_t)((k_d * I_d * dotprod + k_a * I_a) * bluev);
+    }
+}

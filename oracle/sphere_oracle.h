@@ -63,6 +63,13 @@ int or_porosity(const double *x, uint32_t np, double top, double origo_z, double
                 uint32_t z_slices, double *z_pos, double *porosity);
 uint64_t or_overlaps(const double *x, const double *vel, uint32_t np, uint64_t max_pairs,
                      uint32_t *pairs, double *delta_n);
+/* Ray tracer (TEST INFRASTRUCTURE ONLY), restated from src/raytracer.cuh:
+ * DEM::render (:379-560) with its camera (:291-333) and kernels (:14-288),
+ * every sphere tested for every pixel.  x, vel, angvel, angpos, xyzsum:
+ * [np][4]; p: [np]; L: grid.L; rgb: width * height * 3 bytes, row-major. */
+void or_render(const double *x, const double *vel, const double *angvel, const double *angpos,
+               const double *xyzsum, const double *p, uint32_t np, const double *L, int method,
+               float maxval, float lower_cutoff, uint32_t width, uint32_t height, uint8_t *rgb);
 int ref_step(OrState *s, uint64_t nsteps);
 
 #ifdef __cplusplus

@@ -207,6 +207,9 @@ def load_library():
     lib.sph_overlaps.argtypes = [H, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), _dp,
                                  C.POINTER(C.c_uint64)]
     lib.sph_overlaps.restype = C.c_int
+    lib.sph_render.argtypes = [H, C.c_uint32, C.c_int, C.c_float, C.c_float, C.c_float,
+                               C.c_uint32, C.c_uint32, C.POINTER(C.c_uint8)]
+    lib.sph_render.restype = C.c_int
     lib.sph_snapshot.argtypes = [H]
     lib.sph_snapshot.restype = C.c_int
     lib.sph_snapshot_read.argtypes = [H, C.POINTER(SphParticles), C.POINTER(SphBonds), C.POINTER(SphBox)]

@@ -28,6 +28,7 @@ SOURCES = [
     ("sph_mixed.cu", ["-fmad=true"]),
     ("sph_adjoint.cu", ["-fmad=false"]),
     ("sph_noalloc.cu", []),
+    ("sph_render.cu", ["-fmad=false"]),
 ]
 
 

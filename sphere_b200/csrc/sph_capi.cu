@@ -1,5 +1,6 @@
 // sph_capi.cu -- C ABI of include/sphere_b200.h: handle, device memory,
 // host<->device transfers and the CUDA-graph step driver.
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <algorithm>
@@ -1444,6 +1445,39 @@ int sph_overlaps(SphHandle *h, uint32_t box, uint64_t max_pairs, uint32_t *pairs
     if (st != SPH_OK) return fail(h, st, "overlap-search launch failed");
     if (e != cudaSuccess) return fail(h, SPH_ERR_CUDA, cudaGetErrorString(e));
     *npairs = total;
+    return SPH_OK;
+}
+
+int sph_render(SphHandle *h, uint32_t box, int method, float maxval, float lower_cutoff,
+               float focal_length, uint32_t width, uint32_t height, uint8_t *rgb)
+{
+    (void)focal_length;   // src/raytracer.cuh:313: the focal distance is 0.8 |eye - lookat|
+    if (!h || !rgb) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_render before sph_upload");
+    if (box >= h->nbox) return fail(h, SPH_ERR_INPUT, "no such box");
+    if (method < 0 || method > 5)
+        return fail(h, SPH_ERR_INPUT, "render method must be 0 (normal) to 5 (angpos)");
+    if (width == 0 || height == 0 || (uint64_t)width * height > (1ull << 31))
+        return fail(h, SPH_ERR_INPUT, "image size out of range");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    DevBox d;
+    CUDA_TRY(h, cudaMemcpy(&d, h->A.boxes + box, sizeof d, cudaMemcpyDeviceToHost));
+    const double *d_L = reinterpret_cast<const double *>(
+        reinterpret_cast<const char *>(h->A.boxes + box) + offsetof(DevBox, L));
+    const size_t bytes = (size_t)width * height * 3;
+    uint8_t *img = nullptr;
+    if (cudaMalloc((void **)&img, bytes) != cudaSuccess)
+        return fail(h, SPH_ERR_NOMEM, "image buffer");
+    sph::RenderStats rs;
+    int st = sph::render_image(h->A, d.p_base, d.np, d_L, method, maxval, lower_cutoff, width,
+                               height, img, h->stream, &rs);
+    h->launches += (uint64_t)rs.launches;
+    cudaError_t e = cudaSuccess;
+    if (st == SPH_OK) e = cudaMemcpy(rgb, img, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(img);
+    if (st != SPH_OK) return fail(h, st, "ray-tracing kernels failed");
+    if (e != cudaSuccess) return fail(h, SPH_ERR_CUDA, cudaGetErrorString(e));
     return SPH_OK;
 }
 

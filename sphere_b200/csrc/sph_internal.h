@@ -117,4 +117,18 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
 int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                       uint64_t *launches, Prof *prof);
 
+// Ray-traced image of one box (sph_render): tiles of the screen, entries of
+// the tile lists, kernels launched.
+struct RenderStats {
+    uint32_t tiles = 0, entries = 0;
+    int launches = 0;
+};
+// Renders spheres [p0, p0 + np) into d_img (width * height * 3 bytes,
+// row-major RGB).  d_L is the box's grid.L in device memory.  Allocates and
+// frees its own scratch; synchronises st once (to size the tile lists) and
+// at the end.
+int render_image(const StepArgs &A, uint32_t p0, uint32_t np, const double *d_L, int method,
+                 float maxval, float lower_cutoff, uint32_t width, uint32_t height,
+                 uint8_t *d_img, cudaStream_t st, RenderStats *stats);
+
 }  // namespace sph

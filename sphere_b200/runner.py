@@ -224,6 +224,18 @@ class Stepper(object):
                                               C.byref(n)), "sph_overlaps")
         return pairs[:m], d[:m]
 
+    def render(self, box=0, method=1, maxval=1.0e3, lower_cutoff=0.0, width=800, height=800,
+               focal_length=1.0):
+        """RGB image [height, width, 3] uint8 of box `box` by the ray tracer
+        (sph_render); method as DEM::render's: 0 normal, 1 pres, 2 vel,
+        3 angvel, 4 xdisp, 5 angpos."""
+        img = numpy.zeros((int(height), int(width), 3), dtype=numpy.uint8)
+        self._check(self.lib.sph_render(self.h, int(box), int(method), float(maxval),
+                                        float(lower_cutoff), float(focal_length), int(width),
+                                        int(height), img.ctypes.data_as(C.POINTER(C.c_uint8))),
+                    "sph_render")
+        return img
+
     def neighbor_stats(self):
         """(spheres with a list, spheres whose list overflowed, entries,
         longest list, builds so far): sph_neighbor_stats."""

@@ -964,6 +964,38 @@ class sim(object):
             fh.write(text)
         return text
 
+    # ------------------------------------------------------------ ray tracer
+    def renderImage(self, method='pres', max_val=1e3, lower_cutoff=0.0, width=800, height=800,
+                    device=-1):
+        """RGB image [height, width, 3] uint8 of the current state by the
+        reference's ray tracer (src/raytracer.cuh:379-560, `sphere
+        --render`), on the GPU (sph_render).  method: 'normal', 'pres',
+        'vel', 'angvel', 'xdisp' or 'angpos' (src/main.cpp:130-147)."""
+        if method not in RENDER_METHODS:
+            raise ValueError("Visualization method not understood: " + str(method))
+        st = self._analysis_stepper(device)
+        try:
+            return st.render(method=RENDER_METHODS[method], maxval=max_val,
+                             lower_cutoff=lower_cutoff, width=width, height=height)
+        finally:
+            st.close()
+
+    def render(self, method='pres', max_val=1e3, lower_cutoff=0.0, graphics_format='png',
+               verbose=True, root=None, device=-1):
+        """Render every output file of this simulation
+        (<root>/output/<sid>*.bin) into <root>/img_out/<name>.ppm with the
+        ray tracer, then convert the images to graphics_format
+        (python/sphere.py:4693).  'png' is written here (no Imagemagick);
+        'ppm' keeps the ray tracer's own files.  Returns the image paths."""
+        import glob
+        root = root if root is not None else default_root()
+        if verbose:
+            print("Rendering {} images with the raytracer".format(self.sid))
+        files = sorted(glob.glob(os.path.join(root, "output", self.sid + "*.bin")))
+        return [render(f, method=method, max_val=max_val, lower_cutoff=lower_cutoff,
+                       graphics_format=graphics_format, verbose=verbose, root=root,
+                       device=device) for f in files]
+
     # ---------------------------------------------------------------- run
     def run(self, verbose=True, hideinputfile=False, dry=False, valgrind=False,
             cudamemcheck=False, device=-1, precision='fp64', length='reference', root=None,
@@ -998,6 +1030,93 @@ class sim(object):
 
     def cleanup(self, root=None):
         cleanup(self, root=root)
+
+
+RENDER_METHODS = {'normal': 0, 'pres': 1, 'vel': 2, 'angvel': 3, 'xdisp': 4, 'angpos': 5}
+
+
+def write_ppm(path, img):
+    """Binary PPM of an RGB image [height, width, 3] uint8, the layout of
+    DEM::writePPM (src/file_io.cpp:734-757)."""
+    img = numpy.ascontiguousarray(img, dtype=numpy.uint8)
+    with open(path, 'wb') as fh:
+        fh.write("P6 {} {} 255\n".format(img.shape[1], img.shape[0]).encode())
+        fh.write(img.tobytes())
+
+
+def read_ppm(path):
+    """RGB image of a binary PPM written by write_ppm."""
+    with open(path, 'rb') as fh:
+        data = fh.read()
+    head = data.split(b"\n", 1)
+    tag, w, h, depth = head[0].split()
+    if tag != b"P6" or depth != b"255":
+        raise ValueError("not an 8-bit binary PPM: " + path)
+    w, h = int(w), int(h)
+    return numpy.frombuffer(head[1][:w * h * 3], dtype=numpy.uint8).reshape(h, w, 3)
+
+
+def write_png(path, img):
+    """8-bit RGB PNG of an image [height, width, 3] uint8 (filter 0 on every
+    row, one zlib stream)."""
+    import struct
+    import zlib
+    img = numpy.ascontiguousarray(img, dtype=numpy.uint8)
+    h, w = img.shape[:2]
+    raw = numpy.zeros((h, 1 + 3 * w), dtype=numpy.uint8)
+    raw[:, 1:] = img.reshape(h, 3 * w)
+
+    def chunk(kind, body):
+        return (struct.pack(">I", len(body)) + kind + body +
+                struct.pack(">I", zlib.crc32(kind + body) & 0xffffffff))
+
+    with open(path, 'wb') as fh:
+        fh.write(b"\x89PNG\r\n\x1a\n")
+        fh.write(chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)))
+        fh.write(chunk(b"IDAT", zlib.compress(raw.tobytes(), 6)))
+        fh.write(chunk(b"IEND", b""))
+
+
+def convert(graphics_format='png', folder='../img_out'):
+    """Convert every PPM image in folder to graphics_format and remove the
+    PPM files (python/sphere.py:7450).  Only 'png' is written here; 'ppm'
+    leaves the files as they are."""
+    import glob
+    if graphics_format == 'ppm':
+        return
+    if graphics_format != 'png':
+        raise ValueError("graphics_format must be 'png' or 'ppm' here")
+    for f in sorted(glob.glob(os.path.join(folder, "*.ppm"))):
+        write_png(f[:-4] + ".png", read_ppm(f))
+        os.remove(f)
+
+
+def render(binary, method='pres', max_val=1e3, lower_cutoff=0.0, graphics_format='png',
+           verbose=True, root=None, device=-1):
+    """Render one .bin file with the ray tracer into <root>/img_out/<name>.ppm
+    (`sphere --render`, src/raytracer.cuh:556, name = the file name without
+    its extension), then convert it (python/sphere.py:7472).  Returns the
+    image path."""
+    root = root if root is not None else default_root()
+    s = sim(fluid=False)
+    s.readbin(binary, verbose=False)
+    img = s.renderImage(method=method, max_val=max_val, lower_cutoff=lower_cutoff,
+                        device=device)
+    outdir = os.path.join(root, "img_out")
+    os.makedirs(outdir, exist_ok=True)
+    name = os.path.splitext(os.path.basename(binary))[0]
+    path = os.path.join(outdir, name + ".ppm")
+    write_ppm(path, img)
+    if verbose:
+        print("  Saving image: " + path)
+    if graphics_format == 'ppm':
+        return path
+    if graphics_format != 'png':
+        raise ValueError("graphics_format must be 'png' or 'ppm' here")
+    png = path[:-4] + ".png"
+    write_png(png, img)
+    os.remove(path)
+    return png
 
 
 def status(project, root=None):

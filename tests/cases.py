@@ -101,3 +101,51 @@ CASES = ["periodic_xy_wall_stress", "walls_all_sides", "periodic_x_wall_velocity
 # Cases whose results go through a transcendental function (sin) that CUDA
 # and the C library round differently in the last bit.
 APPROX = {"sinusoidal_stress"}
+
+
+def render_scene(name):
+    """A parity scene with seeded non-zero pressures, velocities, spins,
+    rotations and displacements, so that every colour method of the ray
+    tracer has values to map."""
+    s, _, _ = make(name)
+    rng = numpy.random.default_rng(5)
+    n = len(s.radius)
+    s.vel[:] = rng.normal(0.0, 1.0, (n, 3))
+    s.angvel[:] = rng.normal(0.0, 10.0, (n, 3))
+    s.angpos[:] = rng.normal(0.0, 1.0, (n, 3))
+    s.xyzsum[:] = rng.normal(0.0, 0.01, (n, 3))
+    s.p[:] = rng.uniform(0.0, 2.0e3, n)
+    return s
+
+
+def render_values(s, method):
+    """The value a colour method maps (src/raytracer.cuh:452-499), FP64."""
+    if method == 1:
+        return numpy.asarray(s.p, dtype=numpy.float64)
+    if method == 4:
+        return numpy.asarray(s.xyzsum[:, 0], dtype=numpy.float64)
+    a = {2: s.vel, 3: s.angvel, 5: s.angpos}[method]
+    return numpy.sqrt(a[:, 0] * a[:, 0] + a[:, 1] * a[:, 1] + a[:, 2] * a[:, 2])
+
+
+# (width, height) of the ray-tracer cases: square; wide, where the integer
+# hw_ratio = height / width is 0 and the image plane is flat; tall, where the
+# row index wraps modulo the width
+RENDER_SHAPES = [(64, 64), (48, 32), (32, 72)]
+
+
+def render_runs(s):
+    """(method, maxval, lower_cutoff, width, height) of the ray-tracer
+    cases of scene s: every method on every shape, the middle shape with
+    the median as the cutoff."""
+    out = []
+    for method in range(6):
+        vals = render_values(s, method) if method else numpy.zeros(1)
+        maxval = float(numpy.quantile(vals, 0.9)) if method else 1e3
+        cut = float(numpy.median(vals)) if method else 0.0
+        for k, (w, h) in enumerate(RENDER_SHAPES):
+            out.append((method, maxval if maxval > 0.0 else 1.0, cut if k == 1 else 0.0, w, h))
+    return out
+
+
+RENDER_SCENES = ["fixvel_modes", "walls_all_sides"]

@@ -842,7 +842,7 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             else
                 k_search<SPH_LEN_REFERENCE><<<gs, SEARCH_THREADS, 0, st>>>(A);
             mark(prof, st, "k_search");
-            contact(A, st, blocks_for((uint64_t)A.ntot * CONTACT_LANES, CONTACT_THREADS),
+            contact(A, st, blocks_for(A.ntot, CONTACT_THREADS),
                     cfg.lenmode);
             mark(prof, st, "k_contacts");
             if (cfg.lenmode == SPH_LEN_FP64)

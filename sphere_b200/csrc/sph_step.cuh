@@ -166,7 +166,10 @@ __device__ __forceinline__ uint16_t list_key(const StepArgs &A, const DevBox &B,
 }
 
 // list_key for entries k0 .. k0 + KB - 1 (those below vc), their loads
-// issued together so that KB gathers are in flight at once.
+// issued together so that KB gathers are in flight at once.  For the split
+// step only: the partner's position is read in original order (A.x), which
+// holds the step's start positions until k_finish, one gather fewer than
+// the sorted copy through rank.
 constexpr int KB = 4;
 
 template <int LM>
@@ -174,7 +177,7 @@ __device__ __forceinline__ void list_keys_batch(const StepArgs &A, const DevBox 
                                                 const int g[3], const uint32_t *lst, uint32_t k0,
                                                 uint32_t vc, uint16_t out[KB])
 {
-    uint32_t bo[KB], rk[KB];
+    uint32_t bo[KB];
     uint64_t cc[KB];
     double4 xb[KB];
 #pragma unroll
@@ -182,10 +185,8 @@ __device__ __forceinline__ void list_keys_batch(const StepArgs &A, const DevBox 
 #pragma unroll
     for (int j = 0; j < KB; ++j) {
         cc[j] = k0 + j < vc ? A.cellc[bo[j]] : 0ull;
-        rk[j] = k0 + j < vc ? A.rank[bo[j]] : 0u;
+        xb[j] = k0 + j < vc ? A.x[bo[j]] : make_double4(0.0, 0.0, 0.0, 0.0);
     }
-#pragma unroll
-    for (int j = 0; j < KB; ++j) xb[j] = k0 + j < vc ? A.xs[rk[j]] : make_double4(0.0, 0.0, 0.0, 0.0);
 #pragma unroll
     for (int j = 0; j < KB; ++j) {
         out[j] = NO_KEY;
@@ -236,9 +237,13 @@ __device__ __forceinline__ bool insert_keys(const StepArgs &A, const uint16_t *k
         }
         if (cpos < 0) cpos = ~occ ? 31 - __clz(~occ) : nc;
         if (cpos < NC) {
-            row[cpos * RS] = b_orig | (((key >> 6) & 15u) << CODE_SHIFT);
+            // the row goes back to memory only if an entry changed
+            const uint32_t v = b_orig | (((key >> 6) & 15u) << CODE_SHIFT);
+            if (row[cpos * RS] != v) {
+                row[cpos * RS] = v;
+                dirty = true;
+            }
             occ |= 1u << cpos;
-            dirty = true;
         } else {
             raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
         }
@@ -300,8 +305,11 @@ __device__ __forceinline__ bool search_cells(const StepArgs &A, const DevBox &B,
                             else if ((w & ID_MASK) == b_orig) { cpos = s; break; }
                         }
                         if (cpos < NC) {
-                            row[cpos * RS] = b_orig | (shift_code(sx, sy) << CODE_SHIFT);
-                            dirty = true;
+                            const uint32_t v = b_orig | (shift_code(sx, sy) << CODE_SHIFT);
+                            if (row[cpos * RS] != v) {
+                                row[cpos * RS] = v;
+                                dirty = true;
+                            }
                         } else {
                             raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
                         }
@@ -621,17 +629,17 @@ __global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
 //   k_search   one thread per sphere: contact search on the slot row (kept
 //              with a bitmask of the slots in use), the list of live slots
 //              (ascending);
-//   k_contacts CONTACT_LANES threads per sphere, one live contact each: the
-//              contact law with its additions recorded (ContactRec), the
-//              new history written, ended contacts removed from the row;
-//              the records go by warp shuffle to the sphere's first lane,
-//              which adds them in slot order and stores the sums;
+//   k_contacts one warp per 32 spheres, the warp's live contacts dealt to
+//              its lanes 32 at a time: the contact law with its additions
+//              recorded (ContactRec), the new history written, ended
+//              contacts removed from the row; the records go through shared
+//              memory to the lane of their sphere, which adds them in slot
+//              order and stores the sums;
 //   k_finish   one thread per sphere, original order: walls, bonds, sums,
 //              integration.
 // Each contact's arithmetic and the order of every sum are those of
 // k_interact, so the results are bit-identical.
 constexpr int SEARCH_THREADS = 128;
-constexpr int CONTACT_LANES = 4;
 constexpr int CONTACT_THREADS = 128;
 constexpr int FINISH_THREADS = 128;
 
@@ -712,7 +720,7 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
         const int s = __ffs(m) - 1;
         const uint32_t w = row[s * RS];
         live[nl] = (uint8_t)s;
-        livew[nl] = __ldg(A.rank + (w & ID_MASK)) | (w & ~ID_MASK);   // sorted position
+        livew[nl] = w;   // the partner's original id and image code
         ++nl;
     }
     A.nlive[a] = nl;
@@ -725,51 +733,93 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
     }
 }
 
-// Shuffle a contact's record from lane src of the warp.
-__device__ __forceinline__ ContactRec shfl_rec(const ContactRec &r, int src)
+// One warp-round of contact records in shared memory, field by field
+// (consecutive lanes hit consecutive words).
+struct RecSlab {
+    double f[10][CONTACT_THREADS];   // F.x F.y F.z T.x T.y T.z ev0 ev1 es p
+    int32_t n[CONTACT_THREADS];      // (nev + 1) | nes << 4
+};
+
+__device__ __forceinline__ void put_rec(RecSlab &S, int t, const ContactRec &r)
 {
-    ContactRec o;
-    o.F = mk(__shfl_sync(0xffffffffu, r.F.x, src), __shfl_sync(0xffffffffu, r.F.y, src),
-             __shfl_sync(0xffffffffu, r.F.z, src));
-    o.T = mk(__shfl_sync(0xffffffffu, r.T.x, src), __shfl_sync(0xffffffffu, r.T.y, src),
-             __shfl_sync(0xffffffffu, r.T.z, src));
-    o.ev0 = __shfl_sync(0xffffffffu, r.ev0, src);
-    o.ev1 = __shfl_sync(0xffffffffu, r.ev1, src);
-    o.es = __shfl_sync(0xffffffffu, r.es, src);
-    o.p = __shfl_sync(0xffffffffu, r.p, src);
-    o.nev = __shfl_sync(0xffffffffu, r.nev, src);
-    o.nes = __shfl_sync(0xffffffffu, r.nes, src);
-    return o;
+    S.f[0][t] = r.F.x;
+    S.f[1][t] = r.F.y;
+    S.f[2][t] = r.F.z;
+    S.f[3][t] = r.T.x;
+    S.f[4][t] = r.T.y;
+    S.f[5][t] = r.T.z;
+    S.f[6][t] = r.ev0;
+    S.f[7][t] = r.ev1;
+    S.f[8][t] = r.es;
+    S.f[9][t] = r.p;
+    S.n[t] = (r.nev + 1) | (r.nes << 4);
 }
 
+__device__ __forceinline__ ContactRec get_rec(const RecSlab &S, int t)
+{
+    ContactRec r;
+    r.F = mk(S.f[0][t], S.f[1][t], S.f[2][t]);
+    r.T = mk(S.f[3][t], S.f[4][t], S.f[5][t]);
+    r.ev0 = S.f[6][t];
+    r.ev1 = S.f[7][t];
+    r.es = S.f[8][t];
+    r.p = S.f[9][t];
+    const int32_t n = S.n[t];
+    r.nev = (n & 15) - 1;
+    r.nes = n >> 4;
+    return r;
+}
+
+// One warp per 32 consecutive spheres (sorted positions), its lanes dealt
+// the warp's live contacts in order: round r computes contacts 32r .. 32r +
+// 31 of the warp's list (the spheres' live lists one after the other), so a
+// lane is idle only in the last round.  Each lane then adds, in slot order,
+// the round's records of its own sphere.
 template <int LM, bool MIXED>
 __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t a = t / CONTACT_LANES, lane = t % CONTACT_LANES;
-    const bool valid = a < A.ntot;
-    const uint32_t i = valid ? A.perm[a] : 0u;
-    const uint32_t nl = valid ? A.nlive[a] : 0u;
-    // the whole warp runs the same number of rounds (its shuffles need
-    // every lane); round r computes live contacts 4r .. 4r + 3 of each sphere
-    const uint32_t rounds =
-        __reduce_max_sync(0xffffffffu, (nl + CONTACT_LANES - 1) / CONTACT_LANES);
+    __shared__ RecSlab S;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int wbase = (int)(threadIdx.x & ~31u);
+    const uint32_t a_own = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t a0 = a_own - lane;
+    const bool valid = a_own < A.ntot;
+    const uint32_t nl_own = valid ? A.nlive[a_own] : 0u;
+    // inclusive prefix sum of the live counts over the warp
+    uint32_t incl = nl_own;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+    }
+    const uint32_t excl = incl - nl_own;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     Acc acc;
     acc.F = mk(0.0, 0.0, 0.0);
     acc.T = mk(0.0, 0.0, 0.0);
     acc.es_dot = 0.0;
     acc.ev_dot = 0.0;
     acc.p = 0.0;
-    const int base = (int)(threadIdx.x & 31u) & ~(CONTACT_LANES - 1);
-    for (uint32_t rd = 0; rd < rounds; ++rd) {
-        const uint32_t q = rd * CONTACT_LANES + lane;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t f = base + lane;
+        // the lane k whose list holds entry f: the first with incl_k > f
+        int k = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const uint32_t v = __shfl_sync(0xffffffffu, incl, k + step - 1);
+            if (v <= f) k += step;
+        }
+        const uint32_t ex_k = __shfl_sync(0xffffffffu, excl, k & 31);
         ContactRec r;
         r.F = mk(0.0, 0.0, 0.0);
         r.T = mk(0.0, 0.0, 0.0);
         r.ev0 = r.ev1 = r.es = r.p = 0.0;
         r.nev = -1;   // nothing to add unless a live contact is computed
         r.nes = 0;
-        if (q < nl) {
+        if (f < total) {
+            const uint32_t a = a0 + (uint32_t)k;
+            const uint32_t q = f - ex_k;
+            const uint32_t i = A.perm[a];
             const DevBox &B = A.boxes[A.box_of[i]];
             const SphParams &P = B.P;
             const double dt = B.dt;
@@ -782,14 +832,16 @@ __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
             double4 *hist = A.hist + (size_t)i * NC;
             const int s = A.live[(size_t)a * NC + q];
             const uint32_t w = A.livew[(size_t)a * NC + q];
-            const uint32_t bs = w & ID_MASK;   // partner's sorted position
+            const uint32_t bo = w & ID_MASK;   // partner's original id
             int sx, sy;
             decode_shift(w >> CODE_SHIFT, sx, sy);
             const d3 dm = shift_vec(B, sx, sy);
-            // the partner's data and the history are loaded together
-            const double4 xb = A.xs[bs];
-            const double4 vb4 = A.vs[bs];
-            const double4 wb4 = A.ws[bs];
+            // the partner's data (original order: A.x, A.vel, A.angvel hold
+            // the step's start state until k_finish) and the history are
+            // loaded together
+            const double4 xb = A.x[bo];
+            const double4 vb4 = A.vel[bo];
+            const double4 wb4 = A.angvel[bo];
             const double4 h4 = hist[s];
             const d3 x_ab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
             const double x_ab_length = vlen<LM>(x_ab);
@@ -819,13 +871,17 @@ __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
                 hist[s] = make_double4(0.0, 0.0, 0.0, 0.0);
             }
         }
-        // lane 0 of the sphere adds the round's contacts in slot order
-        for (int j = 0; j < CONTACT_LANES; ++j) {
-            const ContactRec o = shfl_rec(r, base + j);
-            if (lane == 0 && o.nev >= 0) replay(acc, o);
+        put_rec(S, (int)threadIdx.x, r);
+        __syncwarp();
+        // this lane's sphere: its entries of this round, in slot order
+        const uint32_t lo = max(excl, base), hi = min(incl, base + 32u);
+        for (uint32_t e = lo; e < hi; ++e) {
+            const ContactRec o = get_rec(S, wbase + (int)(e - base));
+            if (o.nev >= 0) replay(acc, o);
         }
+        __syncwarp();
     }
-    if (valid && lane == 0) A.csum[i] = acc;
+    if (valid) A.csum[A.perm[a_own]] = acc;
 }
 
 template <int LM>

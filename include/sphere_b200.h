@@ -273,7 +273,7 @@ int sph_neighbor_stats(SphHandle *h, uint64_t *stats);
  * (different occupancy); 3 = the split step (contact search, one thread
  * per contact for the contact laws, one thread per sphere for the sums and
  * integration), for contact models 2 and 3 with neighbour lists on, which
- * allocates 236 B per sphere when first chosen.  sph_autotune times
+ * allocates 332 B per sphere when first chosen.  sph_autotune times
  * `steps` steps with each applicable variant from the current state, keeps
  * the fastest for this handle and puts the state back as it was
  * (ms_per_step[SPH_TUNE_VARIANTS] may be NULL; -1 for a variant not

@@ -1245,15 +1245,17 @@ static int ensure_split(SphHandle *h)
 {
     if (h->A.csum) return SPH_OK;
     const uint64_t n = h->ntot;
-    uint8_t *live = nullptr;
-    uint32_t *livew = nullptr, *nlive = nullptr;
+    // a live entry holds the sphere index in 27 bits
+    if (n > (uint64_t)sph::SPLIT_ID_MASK + 1u)
+        return fail(h, SPH_ERR_UNSUPPORTED, "split step: more than 2^27 spheres");
+    uint2 *lent = nullptr;
+    uint32_t *nlive = nullptr;
     sph::Acc *csum = nullptr;
     int st;
-    if ((st = dalloc(h, &live, n * sph::NC)) || (st = dalloc(h, &livew, n * sph::NC)) ||
-        (st = dalloc(h, &nlive, n)) || (st = dalloc(h, &csum, n)))
+    if ((st = dalloc(h, &lent, n * sph::NC)) || (st = dalloc(h, &nlive, n)) ||
+        (st = dalloc(h, &csum, n)))
         return st;
-    h->A.live = live;
-    h->A.livew = livew;
+    h->A.lent = lent;
     h->A.nlive = nlive;
     h->A.csum = csum;
     return SPH_OK;

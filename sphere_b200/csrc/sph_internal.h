@@ -51,13 +51,13 @@ struct StepArgs {
     float4 *xref;
     uint64_t *cellc;
     uint32_t vcap;             // list capacity in use (<= VL_MAX)
-    // split step (k_search / k_contacts / k_finish): per sphere, by sorted
-    // position, the live slots in ascending order (slot index, and the
-    // partner's sorted position | image code << 28) and their number; by
-    // original index, the sums of its contacts (null until the split step
-    // is first used)
-    uint8_t *live;
-    uint32_t *livew;
+    // split step (k_search / k_contacts / k_finish): per warp of 32 sorted
+    // positions, a region of 32 * NC entries holding the warp's live
+    // contacts from its start, sphere after sphere, each in slot order
+    // (slot word; original index | slot << 27); per sphere, by sorted position, their
+    // number; by original index, the sums of its contacts (null until the
+    // split step is first used)
+    uint2 *lent;
     uint32_t *nlive;
     Acc *csum;
     // adjoint tape of the current step (null outside a recorded segment):
@@ -70,6 +70,7 @@ struct StepArgs {
 constexpr int VL_MAX = 48;   // neighbour-list capacity per sphere
 constexpr int INTERACT_VARIANTS = 4;   // launch variants of the interact stage (sph_autotune)
 constexpr int SPLIT_VARIANT = 3;       // the split step (k_search / k_contacts / k_finish)
+constexpr uint32_t SPLIT_ID_MASK = 0x07ffffffu;   // sphere index bits of a live entry
 
 // Overlap search of one box (sph_overlaps): positions and velocities, the
 // box's spheres [p0, p0 + np), its grid (origin, cell widths, cell counts),

@@ -11,7 +11,7 @@
 //   k_scatter       perm[cell_off[c] + slot] = i
 //   k_cellsort      order each cell by original index: the stable order of
 //                   thrust::sort_by_key (device.cu:1075)
-//   k_reorder       sorted copies of x, vel, angvel + rank  (sorting.cuh:56-132)
+//   k_reorder       sorted copies of x (+ vel, angvel, rank)  (sorting.cuh:56-132)
 //   k_bonds         bond forces into per-bond buffers       (cohesion.cuh:8-233)
 //   k_interact      topology + interact + walls + bond gather + integrate
 //                   (contactsearch.cuh:329-726, integration.cuh:14-305)
@@ -184,6 +184,10 @@ __global__ void k_cellsort(StepArgs A)
 }
 
 // sorting.cuh:118-130: sorted copies of x, vel, angvel; rank = inverse of perm
+// ALL = false for the split step, which reads velocities and partners in
+// original order and needs only the sorted positions (its own contact
+// search, the neighbour-list build and the cell-search fallback).
+template <bool ALL>
 __global__ void k_reorder(StepArgs A)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -192,9 +196,11 @@ __global__ void k_reorder(StepArgs A)
     const double4 x = A.x[i];
     A.xs[j] = x;
     A.xf[j] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
-    A.vs[j] = A.vel[i];
-    A.ws[j] = A.angvel[i];
-    A.rank[i] = j;
+    if (ALL) {
+        A.vs[j] = A.vel[i];
+        A.ws[j] = A.angvel[i];
+        A.rank[i] = j;
+    }
 }
 
 // --------------------------------------------------------- neighbour lists
@@ -569,7 +575,7 @@ int relax_sweep(const StepArgs &A, cudaStream_t st, double alpha, double z_top,
     k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(A.cell_count, A.ncells, A.scan_tmp, nb, A.cell_off);
     k_scatter<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
     k_cellsort<<<blocks_for(A.ncells, 256), 256, 0, st>>>(A);
-    k_reorder<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+    k_reorder<true><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
     cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
     k_relax<<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, alpha, z_top, d_max);
     k_relax_apply<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
@@ -817,7 +823,10 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         mark(prof, st, "k_scatter");
         k_cellsort<<<blocks_for(A.ncells, 256), 256, 0, st>>>(A);
         mark(prof, st, "k_cellsort");
-        k_reorder<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+        const bool split = cfg.variant == SPLIT_VARIANT && !cfg.unfused && cfg.all_cm23 &&
+                           A.vlist && A.csum;
+        if (split) k_reorder<false><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+        else k_reorder<true><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
         mark(prof, st, "k_reorder");
         nl += 8;
         if (A.vlist) {
@@ -833,8 +842,6 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             nl += 1;
         }
         const unsigned gi = blocks_for(A.ntot, INTERACT_THREADS);
-        const bool split = cfg.variant == SPLIT_VARIANT && !cfg.unfused && cfg.all_cm23 &&
-                           A.vlist && A.csum;
         if (split) {
             const unsigned gs = blocks_for(A.ntot, SEARCH_THREADS);
             if (cfg.lenmode == SPH_LEN_FP64)

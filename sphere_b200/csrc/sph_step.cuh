@@ -25,6 +25,13 @@ __device__ __forceinline__ bool maybe_touching(float4 xa, float4 xb, float sx, f
     return dx * dx + dy * dy + dz * dz < rr * rr;
 }
 
+// Box of sphere i; a single box needs no lookup (one dependent load fewer
+// on the way to the box's parameters).
+__device__ __forceinline__ uint32_t box_index(const StepArgs &A, uint32_t i)
+{
+    return A.nboxes == 1 ? 0u : A.box_of[i];
+}
+
 // ---------------------------------------------------------------- integrate
 
 // integration.cuh:14-305 integrate (TY3) for one particle.
@@ -174,14 +181,11 @@ constexpr int KB = 4;
 
 template <int LM>
 __device__ __forceinline__ void list_keys_batch(const StepArgs &A, const DevBox &B, double4 xa,
-                                                const int g[3], const uint32_t *lst, uint32_t k0,
+                                                const int g[3], const uint32_t bo[KB], uint32_t k0,
                                                 uint32_t vc, uint16_t out[KB])
 {
-    uint32_t bo[KB];
     uint64_t cc[KB];
     double4 xb[KB];
-#pragma unroll
-    for (int j = 0; j < KB; ++j) bo[j] = k0 + j < vc ? lst[k0 + j] : 0u;
 #pragma unroll
     for (int j = 0; j < KB; ++j) {
         cc[j] = k0 + j < vc ? A.cellc[bo[j]] : 0ull;
@@ -464,7 +468,7 @@ __global__ void __launch_bounds__(INTERACT_THREADS, MINB) k_interact(StepArgs A)
     uint32_t *row = s_row + threadIdx.x;
     const int RS = INTERACT_THREADS;
     const uint32_t i = A.perm[a];
-    const DevBox &B = A.boxes[A.box_of[i]];
+    const DevBox &B = A.boxes[box_index(A, i)];
     const SphParams &P = B.P;
     const double dt = B.dt;
     const double4 xa = A.xs[a];
@@ -643,18 +647,14 @@ constexpr int SEARCH_THREADS = 128;
 constexpr int CONTACT_THREADS = 128;
 constexpr int FINISH_THREADS = 128;
 
+// Contact search of sphere a (sorted position) on its slot row, staged in
+// shared memory (row[s * RS]); returns the bitmask of occupied slots.
 template <int LM>
-__global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
+__device__ __forceinline__ uint32_t search_sphere(const StepArgs &A, uint32_t a, uint32_t *row,
+                                                  uint16_t *keys, int RS)
 {
-    __shared__ uint32_t s_row[NC * SEARCH_THREADS];
-    __shared__ uint16_t s_keys[VL_MAX * SEARCH_THREADS];
-    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A.ntot) return;
-    const int RS = SEARCH_THREADS;
-    uint32_t *row = s_row + threadIdx.x;
-    uint16_t *keys = s_keys + threadIdx.x;
     const uint32_t i = A.perm[a];
-    const DevBox &B = A.boxes[A.box_of[i]];
+    const DevBox &B = A.boxes[box_index(A, i)];
     const double4 xa = A.xs[a];
     const uint4 *grow = reinterpret_cast<const uint4 *>(A.slots + (size_t)i * NC);
     uint32_t occ = 0;
@@ -679,14 +679,26 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
     g[0] = (int)floor((xa.x - B.origo[0]) / (B.L[0] / B.num[0]));
     g[1] = (int)floor((xa.y - B.origo[1]) / (B.L[1] / B.num[1]));
     g[2] = (int)floor((xa.z - B.origo[2]) / (B.L[2] / B.num[2]));
-    const uint32_t vc = A.vlist ? A.vcount[i] : (uint32_t)VL_MAX + 1u;
+    const uint32_t *lst = A.vlist ? A.vlist + (size_t)i * VL_MAX : nullptr;
+    const uint32_t vc = lst ? A.vcount[i] : (uint32_t)VL_MAX + 1u;
+    // the first entries are read together with the count (the list row
+    // holds VL_MAX >= 2 KB entries; those at or past the count go unused)
+    uint32_t nb[KB];
+#pragma unroll
+    for (int j = 0; j < KB; ++j) nb[j] = lst ? lst[j] : 0u;
     bool dirty;
     if (vc <= (uint32_t)VL_MAX) {
-        const uint32_t *lst = A.vlist + (size_t)i * VL_MAX;
         int nk = 0;
         for (uint32_t k0 = 0; k0 < vc; k0 += KB) {
+            uint32_t bo[KB];
+#pragma unroll
+            for (int j = 0; j < KB; ++j) bo[j] = nb[j];
+            if (k0 + KB < vc) {
+#pragma unroll
+                for (int j = 0; j < KB; ++j) nb[j] = lst[k0 + KB + j];
+            }
             uint16_t kb[KB];
-            list_keys_batch<LM>(A, B, xa, g, lst, k0, vc, kb);
+            list_keys_batch<LM>(A, B, xa, g, bo, k0, vc, kb);
 #pragma unroll
             for (int j = 0; j < KB; ++j) {
                 const uint16_t key = kb[j];
@@ -713,17 +725,6 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
             if (w != EMPTY) A.tape_hist[(size_t)i * NC + s] = hist[s];
         }
     }
-    uint8_t *live = A.live + (size_t)a * NC;
-    uint32_t *livew = A.livew + (size_t)a * NC;
-    uint32_t nl = 0;
-    for (uint32_t m = occ; m; m &= m - 1u) {
-        const int s = __ffs(m) - 1;
-        const uint32_t w = row[s * RS];
-        live[nl] = (uint8_t)s;
-        livew[nl] = w;   // the partner's original id and image code
-        ++nl;
-    }
-    A.nlive[a] = nl;
     if (dirty) {
         uint4 *wrow = reinterpret_cast<uint4 *>(A.slots + (size_t)i * NC);
 #pragma unroll
@@ -731,6 +732,38 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
             wrow[q] = make_uint4(row[(4 * q) * RS], row[(4 * q + 1) * RS], row[(4 * q + 2) * RS],
                                  row[(4 * q + 3) * RS]);
     }
+    return occ;
+}
+
+template <int LM>
+__global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
+{
+    __shared__ uint32_t s_row[NC * SEARCH_THREADS];
+    __shared__ uint16_t s_keys[VL_MAX * SEARCH_THREADS];
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int RS = SEARCH_THREADS;
+    uint32_t *row = s_row + threadIdx.x;
+    const uint32_t occ =
+        a < A.ntot ? search_sphere<LM>(A, a, row, s_keys + threadIdx.x, RS) : 0u;
+    // the warp's live contacts, sphere after sphere, each in slot order,
+    // written contiguously from the start of the warp's region
+    const uint32_t nl = __popc(occ);
+    uint32_t incl = nl;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+    }
+    if (a >= A.ntot) return;
+    uint2 *ent = A.lent + (size_t)(a - lane) * NC + (incl - nl);
+    uint32_t q = 0;
+    for (uint32_t m = occ; m; m &= m - 1u) {
+        const int sl = __ffs(m) - 1;
+        // slot word (partner's original id | image code), i | slot << 27
+        ent[q++] = make_uint2(row[sl * RS], A.perm[a] | ((uint32_t)sl << 27));
+    }
+    A.nlive[a] = nl;
 }
 
 // One warp-round of contact records in shared memory, field by field
@@ -800,16 +833,9 @@ __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
     acc.es_dot = 0.0;
     acc.ev_dot = 0.0;
     acc.p = 0.0;
+    const uint2 *ent = A.lent + (size_t)a0 * NC;
     for (uint32_t base = 0; base < total; base += 32) {
         const uint32_t f = base + lane;
-        // the lane k whose list holds entry f: the first with incl_k > f
-        int k = 0;
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1) {
-            const uint32_t v = __shfl_sync(0xffffffffu, incl, k + step - 1);
-            if (v <= f) k += step;
-        }
-        const uint32_t ex_k = __shfl_sync(0xffffffffu, excl, k & 31);
         ContactRec r;
         r.F = mk(0.0, 0.0, 0.0);
         r.T = mk(0.0, 0.0, 0.0);
@@ -817,21 +843,22 @@ __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
         r.nev = -1;   // nothing to add unless a live contact is computed
         r.nes = 0;
         if (f < total) {
-            const uint32_t a = a0 + (uint32_t)k;
-            const uint32_t q = f - ex_k;
-            const uint32_t i = A.perm[a];
-            const DevBox &B = A.boxes[A.box_of[i]];
+            const uint2 e = ent[f];
+            const uint32_t i = e.y & SPLIT_ID_MASK;
+            const int s = (int)(e.y >> 27);
+            const uint32_t w = e.x;
+            const DevBox &B = A.boxes[box_index(A, i)];
             const SphParams &P = B.P;
             const double dt = B.dt;
             const uint32_t cm = P.contactmodel;
-            const double4 xa = A.xs[a];
+            // the sphere's own data in original order (the step's start
+            // state until k_finish), like its partner's
+            const double4 xa = A.x[i];
             const double radius_a = xa.w;
-            const d3 vel_a = xyz(A.vs[a]);
-            const d3 angvel_a = xyz(A.ws[a]);
+            const d3 vel_a = xyz(A.vel[i]);
+            const d3 angvel_a = xyz(A.angvel[i]);
             uint32_t *slots = A.slots + (size_t)i * NC;
             double4 *hist = A.hist + (size_t)i * NC;
-            const int s = A.live[(size_t)a * NC + q];
-            const uint32_t w = A.livew[(size_t)a * NC + q];
             const uint32_t bo = w & ID_MASK;   // partner's original id
             int sx, sy;
             decode_shift(w >> CODE_SHIFT, sx, sy);
@@ -892,7 +919,7 @@ __global__ void __launch_bounds__(FINISH_THREADS, 4) k_finish(StepArgs A)
     // state at the start of the step: only this thread rewrites them)
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.ntot) return;
-    const DevBox &B = A.boxes[A.box_of[i]];
+    const DevBox &B = A.boxes[box_index(A, i)];
     const double4 xa = A.x[i];
     const double4 va4 = A.vel[i];
     const double4 wa4 = A.angvel[i];

@@ -324,6 +324,7 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_m
         (st = dalloc(h, &A.ev_dot, n)) || (st = dalloc(h, &A.ev, n)) ||
         (st = dalloc(h, &A.p, n)) || (st = dalloc(h, &box_of, n)) ||
         (st = dalloc(h, &A.cell_id, n)) || (st = dalloc(h, &A.local_off, n)) ||
+        (st = dalloc(h, &A.unsorted, n)) ||
         (st = dalloc(h, &A.cell_count, h->ncells)) || (st = dalloc(h, &A.cell_off, h->ncells + 1)) ||
         (st = dalloc(h, &A.scan_tmp, scan_blocks + 1)) || (st = dalloc(h, &A.perm, n)) ||
         (st = dalloc(h, &A.rank, n)) || (st = dalloc(h, &A.xs, n)) || (st = dalloc(h, &A.vs, n)) ||

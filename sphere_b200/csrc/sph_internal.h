@@ -26,6 +26,7 @@ struct StepArgs {
     const uint32_t *box_of;
     // cell sort
     uint32_t *cell_id, *local_off, *cell_count, *cell_off, *scan_tmp, *perm, *rank;
+    uint32_t *unsorted;        // ids by cell in arrival order (k_scatter)
     double4 *xs, *vs, *ws;     // sorted copies
     float4 *xf;                // sorted FP32 copy of x+r for the candidate prefilter
     // contact rows: slot word = partner | image code << 28, EMPTY when free

@@ -8,10 +8,10 @@
 //   memset cell_count
 //   k_hash          cell id + atomic slot within the cell  (sorting.cuh:7-51)
 //   scan (3)        exclusive scan of cell counts -> cell_off
-//   k_scatter       perm[cell_off[c] + slot] = i
-//   k_cellsort      order each cell by original index: the stable order of
-//                   thrust::sort_by_key (device.cu:1075)
-//   k_reorder       sorted copies of x (+ vel, angvel, rank)  (sorting.cuh:56-132)
+//   k_scatter       unsorted[cell_off[c] + slot] = i
+//   k_place         perm: each cell ordered by original index, the stable
+//                   order of thrust::sort_by_key (device.cu:1075); sorted
+//                   copies of x (+ vel, angvel, rank)  (sorting.cuh:56-132)
 //   k_bonds         bond forces into per-bond buffers       (cohesion.cuh:8-233)
 //   k_interact      topology + interact + walls + bond gather + integrate
 //                   (contactsearch.cuh:329-726, integration.cuh:14-305)
@@ -160,39 +160,26 @@ __global__ void k_scatter(StepArgs A)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.ntot) return;
-    A.perm[A.cell_off[A.cell_id[i]] + A.local_off[i]] = i;
+    A.unsorted[A.cell_off[A.cell_id[i]] + A.local_off[i]] = i;
 }
 
-// Within each cell, order particles by original index (insertion sort of
-// the short segment); the result is the stable sort by cell id.
-__global__ void k_cellsort(StepArgs A)
-{
-    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.ncells) return;
-    const uint32_t s = A.cell_off[c], e = A.cell_off[c + 1];
-    for (uint32_t j = s + 1; j < e; ++j) {
-        const uint32_t v = A.perm[j];
-        uint32_t k = j;
-        while (k > s) {
-            const uint32_t u = A.perm[k - 1];
-            if (u <= v) break;
-            A.perm[k] = u;
-            --k;
-        }
-        A.perm[k] = v;
-    }
-}
-
-// sorting.cuh:118-130: sorted copies of x, vel, angvel; rank = inverse of perm
+// The stable sort by cell id and the sorted copies (sorting.cuh:118-130)
+// in one pass over the particles in original order: particle i goes to
+// cell_off[c] + (the number of particles of its cell with a smaller index),
+// so each cell is ordered by original index.  rank = inverse of perm.
 // ALL = false for the split step, which reads velocities and partners in
 // original order and needs only the sorted positions (its own contact
 // search, the neighbour-list build and the cell-search fallback).
 template <bool ALL>
-__global__ void k_reorder(StepArgs A)
+__global__ void k_place(StepArgs A)
 {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= A.ntot) return;
-    const uint32_t i = A.perm[j];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.ntot) return;
+    const uint32_t c = A.cell_id[i];
+    const uint32_t s = A.cell_off[c], e = A.cell_off[c + 1];
+    uint32_t j = s;
+    for (uint32_t k = s; k < e; ++k) j += A.unsorted[k] < i ? 1u : 0u;
+    A.perm[j] = i;
     const double4 x = A.x[i];
     A.xs[j] = x;
     A.xf[j] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
@@ -440,8 +427,19 @@ __global__ void __launch_bounds__(BOX_THREADS) k_box_step(StepArgs A)
             for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x)
                 s_part[k] = A.wall_partial[B.part_base + base + k];
             __syncthreads();
-            if (threadIdx.x == 0)
-                for (uint32_t k = 0; k < cnt; ++k) fsum += s_part[k];
+            if (threadIdx.x == 0) {
+                // the sequential sum of integrateWalls, its loads issued
+                // eight at a time ahead of the additions
+                uint32_t k = 0;
+                for (; k + 8 <= cnt; k += 8) {
+                    double v[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) v[q] = s_part[k + q];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) fsum += v[q];
+                }
+                for (; k < cnt; ++k) fsum += s_part[k];
+            }
         }
     }
     if (threadIdx.x != 0) return;
@@ -574,12 +572,11 @@ int relax_sweep(const StepArgs &A, cudaStream_t st, double alpha, double z_top,
     k_scan_top<<<1, SCAN_THREADS, 0, st>>>(A.scan_tmp, nb);
     k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(A.cell_count, A.ncells, A.scan_tmp, nb, A.cell_off);
     k_scatter<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
-    k_cellsort<<<blocks_for(A.ncells, 256), 256, 0, st>>>(A);
-    k_reorder<true><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+    k_place<true><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
     cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
     k_relax<<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, alpha, z_top, d_max);
     k_relax_apply<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
-    if (launches) *launches += 10;
+    if (launches) *launches += 9;
     return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
 }
 
@@ -821,14 +818,12 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         mark(prof, st, "k_scan(3)");
         k_scatter<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
         mark(prof, st, "k_scatter");
-        k_cellsort<<<blocks_for(A.ncells, 256), 256, 0, st>>>(A);
-        mark(prof, st, "k_cellsort");
         const bool split = cfg.variant == SPLIT_VARIANT && !cfg.unfused && cfg.all_cm23 &&
                            A.vlist && A.csum;
-        if (split) k_reorder<false><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
-        else k_reorder<true><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
-        mark(prof, st, "k_reorder");
-        nl += 8;
+        if (split) k_place<false><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+        else k_place<true><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+        mark(prof, st, "k_place");
+        nl += 7;
         if (A.vlist) {
             k_vlist_build<<<blocks_for(A.ntot, VLIST_THREADS), VLIST_THREADS, 0, st>>>(A);
             k_vlist_done<<<1, 1, 0, st>>>(A);

@@ -38,9 +38,10 @@ static inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n
 // sorting.cuh:7-51 calcParticleCellID + device.cu:241-276 position checks
 __global__ void k_hash(StepArgs A)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.ntot) return;
-    const DevBox &B = A.boxes[A.box_of[i]];
+    const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i0 < A.ntot;
+    const uint32_t i = valid ? i0 : 0u;
+    const DevBox &B = A.boxes[A.nboxes == 1 ? 0u : A.box_of[i]];
     const double4 x = A.x[i];
     const double xv[3] = {x.x, x.y, x.z};
     uint32_t c[3];
@@ -52,13 +53,24 @@ __global__ void k_hash(StepArgs A)
         if (f >= (double)B.num[d]) { outside = true; f = (double)(B.num[d] - 1); }
         c[d] = (uint32_t)f;
     }
-    if (nonfinite) raise_flag(A.err, SPH_ERR_NAN);
-    else if (outside || x.x > B.L[0] || x.y > B.L[1] || x.z > B.L[2])
-        raise_flag(A.err, SPH_ERR_OUT_OF_GRID);
+    if (valid) {
+        if (nonfinite) raise_flag(A.err, SPH_ERR_NAN);
+        else if (outside || x.x > B.L[0] || x.y > B.L[1] || x.z > B.L[2])
+            raise_flag(A.err, SPH_ERR_OUT_OF_GRID);
+    }
     const uint32_t cell = B.cell_base + (c[2] * B.num[1]) * B.num[0] + c[1] * B.num[0] + c[0];
+    // lanes of the warp in the same cell take consecutive slots with one
+    // atomic (the slot order within a cell is free: k_place orders by index)
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, valid ? cell : 0xffffffffu);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (valid && (int)lane == leader) base = atomicAdd(&A.cell_count[cell], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!valid) return;
     A.cell_id[i] = cell;
     if (A.cellc) A.cellc[i] = pack_cell(c[0], c[1], c[2]);
-    A.local_off[i] = atomicAdd(&A.cell_count[cell], 1u);
+    A.local_off[i] = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
 // Exclusive scan of n uint32 (3 launches): per-block totals, a one-block

@@ -48,3 +48,32 @@ def test_oracle_matches_reference_kernels(name):
         assert a.box.grid.L[2] == b.box.grid.L[2]
         assert a.box.t_current == b.box.t_current
     assert int((a.contacts != s.np[0]).sum()) > 0 or s.contactmodel[0] == 1
+
+
+FIXTURES = "/root/reference/output"
+
+
+@needs_ref
+@pytest.mark.skipif(not __import__("os").path.isdir(FIXTURES),
+                    reason="the reference's output fixtures are not present")
+@pytest.mark.parametrize("fname,steps", [("cube-init.output00029.bin", 20),
+                                         ("init-1e4.output00199.bin", 6)])
+def test_oracle_matches_reference_kernels_on_its_fixtures(fname, steps):
+    """The reference's own output files as inputs (output/cube-init: 1,000
+    spheres in a 3 x 3 x 112 periodic grid, the smallest grid with periodic
+    images on both sides; output/init-1e4: 10,000 settled spheres)."""
+    import os
+    from sphere_b200 import sim
+    if not O.available("ref"):
+        O.build()
+    s = sim()
+    s.readbin(os.path.join(FIXTURES, fname), verbose=False)
+    a = O.CpuRun(s, "oracle")
+    b = O.CpuRun(s, "ref")
+    for chunk in range(2):
+        a.step(steps // 2)
+        b.step(steps // 2)
+        for f in FIELDS:
+            A, B = getattr(a, f), getattr(b, f)
+            assert _same(A, B), "%s differs after %d steps" % (f, (chunk + 1) * steps // 2)
+    assert int((a.contacts != s.np[0]).sum()) > 0

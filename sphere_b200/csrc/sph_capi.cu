@@ -46,6 +46,13 @@ struct SphHandle {
     StepConfig cfg{};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    // runs of steps: head of the first step, then steps that overlap the
+    // previous step's wall stage (side stream), then the last wall stage
+    // (indexed by sph::StepPhase; [0] unused)
+    cudaGraph_t pgraph_ph[4] = {};
+    cudaGraphExec_t pexec_ph[4] = {};
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     uint64_t launches_per_step = 0;
     uint64_t launches = 0;
     // profiling: a ring of captured step graphs with event-record nodes
@@ -226,6 +233,13 @@ void sph_destroy(SphHandle *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
+    for (int k = 1; k < 4; ++k) {
+        if (h->pexec_ph[k]) cudaGraphExecDestroy(h->pexec_ph[k]);
+        if (h->pgraph_ph[k]) cudaGraphDestroy(h->pgraph_ph[k]);
+    }
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
     for (int r = 0; r < SphHandle::PR; ++r) {
         if (h->pexec[r]) cudaGraphExecDestroy(h->pexec[r]);
         if (h->pgraph[r]) cudaGraphDestroy(h->pgraph[r]);
@@ -575,13 +589,18 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
 // Capture one step (optionally with event-record nodes between kernels)
 // into a CUDA graph.
 static int capture_step(SphHandle *h, sph::Prof *prof, cudaGraph_t *g, cudaGraphExec_t *ge,
-                        uint64_t *nl)
+                        uint64_t *nl, int phase = sph::STEP_WHOLE)
 {
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    StepConfig cfg = h->cfg;
+    cfg.phase = phase;
+    cfg.side = h->side;
+    cfg.fork = h->ev_fork;
+    cfg.join = h->ev_join;
     CUDA_TRY(h, cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
     int st = h->precision == SPH_PREC_MIXED
-                 ? sph::launch_step_mixed(h->A, h->cfg, h->own, nl, prof)
-                 : sph::launch_step(h->A, h->cfg, h->own, nl, prof);
+                 ? sph::launch_step_mixed(h->A, cfg, h->own, nl, prof)
+                 : sph::launch_step(h->A, cfg, h->own, nl, prof);
     cudaError_t e = cudaStreamEndCapture(h->own, g);
     if (st != SPH_OK) return fail(h, st, "step launch failed during graph capture");
     if (e != cudaSuccess) return fail(h, SPH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -596,6 +615,33 @@ static int build_graph(SphHandle *h)
     int st = capture_step(h, nullptr, &h->graph, &h->gexec, &nl);
     if (st != SPH_OK) return st;
     h->launches_per_step = nl;
+    return SPH_OK;
+}
+
+// Whether runs of steps may overlap a step's wall stage with the next
+// step: not when a box's grid follows its wall (the next step's cell hash
+// reads L[2]) nor for the unfused kernels.
+static bool overlap_ok(const SphHandle *h)
+{
+    if (h->cfg.unfused) return false;
+    for (uint32_t k = 0; k < h->nbox; ++k)
+        if (h->boxes[k].grid.adaptive) return false;
+    return true;
+}
+
+static int build_phase_graphs(SphHandle *h)
+{
+    if (h->pexec_ph[1]) return SPH_OK;
+    if (!h->side) {
+        CUDA_TRY(h, cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+        CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    }
+    for (int k = 1; k < 4; ++k) {
+        uint64_t nl = 0;
+        int st = capture_step(h, nullptr, &h->pgraph_ph[k], &h->pexec_ph[k], &nl, k);
+        if (st != SPH_OK) return st;
+    }
     return SPH_OK;
 }
 
@@ -658,8 +704,21 @@ int sph_step_async(SphHandle *h, uint64_t nsteps)
     cudaSetDevice(h->device);
     int st;
     if ((st = build_graph(h)) != SPH_OK) return st;
-    for (uint64_t s = 0; s < nsteps; ++s)
-        if ((st = launch_one(h)) != SPH_OK) return st;
+    if (nsteps >= 2 && !h->prof_on && overlap_ok(h)) {
+        // the head of step 1, steps 2..n each beside the wall stage of the
+        // step before, then the wall stage of step n: every step's work, in
+        // an order that respects each read of the wall stage's results
+        if ((st = build_phase_graphs(h)) != SPH_OK) return st;
+        for (uint64_t s = 0; s <= nsteps; ++s) {
+            const int ph = s == 0 ? sph::STEP_HEAD : (s < nsteps ? sph::STEP_OVERLAP : sph::STEP_TAIL);
+            CUDA_TRY(h, cudaGraphLaunch(h->pexec_ph[ph], h->stream));
+        }
+        for (uint64_t s = 0; s < nsteps; ++s)
+            for (uint32_t k = 0; k < h->nbox; ++k) h->t_host[k] += h->boxes[k].dt;
+    } else {
+        for (uint64_t s = 0; s < nsteps; ++s)
+            if ((st = launch_one(h)) != SPH_OK) return st;
+    }
     h->launches += nsteps * h->launches_per_step;
     return SPH_OK;
 }
@@ -1231,6 +1290,12 @@ static int drop_graphs(SphHandle *h)
     if (h->graph) cudaGraphDestroy(h->graph);
     h->gexec = nullptr;
     h->graph = nullptr;
+    for (int k = 1; k < 4; ++k) {
+        if (h->pexec_ph[k]) cudaGraphExecDestroy(h->pexec_ph[k]);
+        if (h->pgraph_ph[k]) cudaGraphDestroy(h->pgraph_ph[k]);
+        h->pexec_ph[k] = nullptr;
+        h->pgraph_ph[k] = nullptr;
+    }
     for (int r = 0; r < SphHandle::PR; ++r) {
         if (h->pexec[r]) cudaGraphExecDestroy(h->pexec[r]);
         if (h->pgraph[r]) cudaGraphDestroy(h->pgraph[r]);

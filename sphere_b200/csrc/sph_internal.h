@@ -86,12 +86,25 @@ struct OverlapArgs {
     double *delta;
 };
 
+// Parts of a step a captured graph holds.  A step ends with the wall stage
+// (wall-force partial sums, integrateWalls, time and state of the box),
+// which the next step's sort and contact search do not read: in a run of
+// steps the wall stage of step t can run beside step t+1 up to its
+// integration.  STEP_WHOLE: the whole step; STEP_HEAD: the step without
+// its wall stage; STEP_OVERLAP: the previous step's wall stage on the side
+// stream beside this step's head, joined before the integration;
+// STEP_TAIL: the wall stage alone.
+enum StepPhase { STEP_WHOLE = 0, STEP_HEAD = 1, STEP_OVERLAP = 2, STEP_TAIL = 3 };
+
 struct StepConfig {
     int lenmode;
     bool unfused;     // some box has a shear-stress (wmode 3) top wall
     bool any_walls;   // some box has nw > 0
     int variant = 1;  // interact launch variant (sph_autotune)
     bool all_cm23 = false;   // every box uses contact model 2 or 3
+    int phase = STEP_WHOLE;
+    cudaStream_t side = nullptr;                       // STEP_OVERLAP only
+    cudaEvent_t fork = nullptr, join = nullptr;        // STEP_OVERLAP only
 };
 
 // Per-kernel timing of an un-graphed step (the counterpart of the

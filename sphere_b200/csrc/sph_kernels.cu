@@ -819,6 +819,30 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         prof->n = 0;
         record(prof->ev[0], st);
     }
+    // the wall stage: wall-force partial sums and integrateWalls, time and
+    // box state (integration.cuh:309-450, device.cu:2504-2537)
+    auto wall_stage = [&](cudaStream_t s) {
+        if (A.ntot > 0 && cfg.any_walls) {
+            k_block_sums<<<A.npartials, 256, 0, s>>>(A, A.wf_pp, A.wall_partial, 0);
+            mark(prof, s, "k_block_sums");
+            nl += 1;
+        }
+        k_box_step<<<A.nboxes, BOX_THREADS, 0, s>>>(A);
+        mark(prof, s, "k_box_step");
+        nl += 1;
+    };
+    if (cfg.phase == STEP_TAIL) {
+        wall_stage(st);
+        if (launches) *launches += nl;
+        return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+    }
+    const bool overlap = cfg.phase == STEP_OVERLAP;
+    if (overlap) {
+        cudaEventRecord(cfg.fork, st);
+        cudaStreamWaitEvent(cfg.side, cfg.fork, 0);
+        wall_stage(cfg.side);
+        cudaEventRecord(cfg.join, cfg.side);
+    }
     if (A.ntot > 0) {
         cudaMemsetAsync(A.cell_count, 0, sizeof(uint32_t) * A.ncells, st);
         k_hash<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
@@ -859,6 +883,7 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             contact(A, st, blocks_for(A.ntot, CONTACT_THREADS),
                     cfg.lenmode);
             mark(prof, st, "k_contacts");
+            if (overlap) cudaStreamWaitEvent(st, cfg.join, 0);
             if (cfg.lenmode == SPH_LEN_FP64)
                 k_finish<SPH_LEN_FP64><<<blocks_for(A.ntot, FINISH_THREADS), FINISH_THREADS, 0, st>>>(A);
             else
@@ -866,11 +891,13 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             mark(prof, st, "k_finish");
             nl += 3;
         } else if (!cfg.unfused) {
+            if (overlap) cudaStreamWaitEvent(st, cfg.join, 0);
             interact(A, st, gi, true, cfg.lenmode,
                      cfg.variant == SPLIT_VARIANT ? 1 : cfg.variant);
             mark(prof, st, "k_interact");
             nl += 1;
         } else {
+            if (overlap) cudaStreamWaitEvent(st, cfg.join, 0);
             interact(A, st, gi, false, cfg.lenmode,
                      cfg.variant == SPLIT_VARIANT ? 1 : cfg.variant);
             mark(prof, st, "k_interact");
@@ -882,15 +909,10 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             mark(prof, st, "k_integrate");
             nl += 5;
         }
-        if (cfg.any_walls) {
-            k_block_sums<<<A.npartials, 256, 0, st>>>(A, A.wf_pp, A.wall_partial, 0);
-            mark(prof, st, "k_block_sums");
-            nl += 1;
-        }
+    } else if (overlap) {
+        cudaStreamWaitEvent(st, cfg.join, 0);
     }
-    k_box_step<<<A.nboxes, BOX_THREADS, 0, st>>>(A);
-    mark(prof, st, "k_box_step");
-    nl += 1;
+    if (cfg.phase == STEP_WHOLE) wall_stage(st);
     if (launches) *launches += nl;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

@@ -484,8 +484,10 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
     CUDA_TRY(h, cudaMemset(A.wf_pp, 0, sizeof(double) * (n ? n : 1)));
     CUDA_TRY(h, cudaMemset(A.tau_pp, 0, sizeof(double) * (n ? n : 1)));
     // src/device.cu:458-464: empty contact lists; histories start at zero
-    CUDA_TRY(h, cudaMemset(A.slots, 0xff, sizeof(uint32_t) * (n ? n : 1) * sph::NC));
-    CUDA_TRY(h, cudaMemset(A.hist, 0, sizeof(double4) * (n ? n : 1) * sph::NC));
+    if (n) {
+        CUDA_TRY(h, cudaMemset(A.slots, 0xff, sizeof(uint32_t) * n * sph::NC));
+        CUDA_TRY(h, cudaMemset(A.hist, 0, sizeof(double4) * n * sph::NC));
+    }
 
     // bonds (local indexes) and the per-particle list of bond endpoints in
     // ascending bond order
@@ -592,6 +594,9 @@ static int capture_step(SphHandle *h, sph::Prof *prof, cudaGraph_t *g, cudaGraph
                         uint64_t *nl, int phase = sph::STEP_WHOLE)
 {
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    // an error left by an earlier failed call (already returned to its
+    // caller) must not be taken for a launch error of this capture
+    (void)cudaGetLastError();
     StepConfig cfg = h->cfg;
     cfg.phase = phase;
     cfg.side = h->side;

@@ -214,14 +214,9 @@ constexpr int VLIST_THREADS = 128;
 // integration against xref) keeps every sphere it can touch in its list.
 // Runs only when vflag[0] is set; a list that overflows vcap (<= VL_MAX) is
 // marked VL_MAX + 1 and that sphere uses the cell search.
-__global__ void __launch_bounds__(VLIST_THREADS) k_vlist_build(StepArgs A)
+__device__ __forceinline__ void vlist_build_one(const StepArgs &A, uint32_t a, uint32_t *lst)
 {
-    if (A.vflag[0] == 0u) return;
-    __shared__ uint32_t s_list[VL_MAX * VLIST_THREADS];
-    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A.ntot) return;
     const int RS = VLIST_THREADS;
-    uint32_t *lst = s_list + threadIdx.x;
     const uint32_t i = A.perm[a];
     const DevBox &B = A.boxes[A.box_of[i]];
     const float4 xaf = A.xf[a];
@@ -272,6 +267,19 @@ __global__ void __launch_bounds__(VLIST_THREADS) k_vlist_build(StepArgs A)
     uint32_t *out = A.vlist + (size_t)i * VL_MAX;
     for (int k = 0; k < n; ++k) out[k] = lst[k * RS];
     A.vcount[i] = (uint32_t)n;
+}
+
+// A grid of a few blocks per SM that strides over the spheres, so that the
+// launch costs little on the steps that build nothing.
+constexpr unsigned VLIST_BLOCKS = 148u * 8u;
+
+__global__ void __launch_bounds__(VLIST_THREADS) k_vlist_build(StepArgs A)
+{
+    if (A.vflag[0] == 0u) return;
+    __shared__ uint32_t s_list[VL_MAX * VLIST_THREADS];
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < A.ntot;
+         a += gridDim.x * blockDim.x)
+        vlist_build_one(A, a, s_list + threadIdx.x);
 }
 
 // After the (possible) build: clear the request, count builds.
@@ -861,7 +869,8 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         mark(prof, st, "k_place");
         nl += 7;
         if (A.vlist) {
-            k_vlist_build<<<blocks_for(A.ntot, VLIST_THREADS), VLIST_THREADS, 0, st>>>(A);
+            const unsigned gv = blocks_for(A.ntot, VLIST_THREADS);
+            k_vlist_build<<<gv < VLIST_BLOCKS ? gv : VLIST_BLOCKS, VLIST_THREADS, 0, st>>>(A);
             k_vlist_done<<<1, 1, 0, st>>>(A);
             mark(prof, st, "k_vlist");
             nl += 2;

@@ -17,9 +17,9 @@ from CUDA events recorded inside 8 step graphs run after the timed region
 of the dominant kernel, the end-to-end time through the C ABI with host
 buffers, and (rank 0, N = 1) the CPU baseline: the reference's own step
 kernels compiled for the CPU (oracle/_ref) on a bounded sample.  Rank 0
-also reports the cost of the adjoint (time_adjoint) under "adjoint" and the
+also reports the cost of the adjoint (time_adjoint) under "adjoint", the
 batched-ensemble throughput and per-box error (time_ensemble) under
-"ensemble".
+"ensemble", and the bonded-pack throughput (time_bonded) under "bonded".
 
 --impl reference times that CPU reference alone (rank 0; other ranks exit).
 
@@ -260,6 +260,39 @@ def time_ensemble(device, stream, nboxes=256, steps=200, err_steps=100):
             "per_box_dx_over_rmean_max_after_%d_steps" % err_steps: max(xerr)}
 
 
+def time_bonded(device, stream, n=200000, nbonds=300000, steps=200):
+    """The bonded-pack workload: 2e5 spheres U[0.008, 0.012] m at porosity
+    0.38, 3e5 linear bonds between touching pairs (k = 1e9, sigma_b = 1 MPa),
+    Young's-modulus contacts (E = 70 GPa), top wall at -0.005 m/s
+    (uniaxialStrainRate), FP32-mixed; launch variant picked by sph_autotune."""
+    import torch
+    from sphere_b200 import scenes
+    from sphere_b200.runner import Stepper
+    s = scenes.bonded_pack(n=n, nbonds=nbonds, seed=0, device=device)
+    nb = int(s.nb0[0])
+    st = Stepper([s], precision="mixed", length="reference", device=device)
+    st.set_stream(stream.cuda_stream)
+    st.upload()
+    variant, variant_ms = st.autotune(steps=10)
+    st.step(5)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    st.step_async(steps)
+    end.record(stream)
+    end.synchronize()
+    code = st.sync(raise_on_error=False)
+    ms = start.elapsed_time(end)
+    st.close()
+    return {"workload": "bonded pack: %d spheres U[0.008, 0.012] m, porosity 0.38, %d linear "
+                        "bonds between touching pairs (k_n = k_t = 1e9, sigma_b = 1 MPa), "
+                        "E = 70 GPa contacts, top wall at -0.005 m/s, FP32-mixed" % (n, nb),
+            "value": n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "spheres": n, "bonds": nb, "variant": variant,
+            "variant_ms_per_step": variant_ms, "device_status": code}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -272,6 +305,7 @@ def main():
     ap.add_argument("--pack-sweeps", type=int, default=3000)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-bonded", action="store_true")
     ap.add_argument("--variant", type=int, default=-1,
                     help="interact launch variant (0-3); default: picked by sph_autotune")
     args = ap.parse_args()
@@ -465,6 +499,9 @@ def main():
     ens = None
     if rank == 0 and not args.no_ensemble:
         ens = time_ensemble(local, stream)
+    bonded = None
+    if rank == 0 and not args.no_bonded:
+        bonded = time_bonded(local, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -504,6 +541,8 @@ def main():
         line["adjoint"] = adj
     if ens is not None:
         line["ensemble"] = ens
+    if bonded is not None:
+        line["bonded"] = bonded
     print(json.dumps(line))
     return 0
 

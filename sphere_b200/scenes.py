@@ -199,6 +199,60 @@ def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.00
     return s, worst
 
 
+def bonded_pack(n=200000, nbonds=300000, seed=0, porosity=0.38, r_range=(0.008, 0.012),
+                E=70.0e9, k_bond=1.0e9, sigma_b=1.0e6, wvel=-0.005, sweeps=3000, device=-1,
+                sid="bonded"):
+    """The bonded-pack workload: n spheres of radii U[r_range] packed on the
+    GPU to the porosity (FCC start + overlap removal, radii grown so that
+    neighbours touch), nbonds linear bonds between touching pairs (the
+    first nbonds pairs of the overlap listing, i < j ascending), contact
+    stiffness from Young's modulus E (k_n = pi/2 E r, contact model 2),
+    bond stiffness k_n = k_t = k_bond, bond strength sigma_b (tau_b
+    unlimited), and a top wall moving at wvel (uniaxialStrainRate, wmode 2);
+    dt = 0.17 sqrt(m_min / k) with k = pi/2 E r_max."""
+    from .runner import Stepper
+    rng = numpy.random.default_rng(seed)
+    r = rng.uniform(r_range[0], r_range[1], n)
+    s, H = _fcc_start(n, rng, r, porosity, 0.5, float(numpy.mean(r)), sid)
+    st = Stepper([s], device=device)
+    st.upload()
+    st.relax(sweeps, alpha=0.6, z_top=H)
+    st.to_sims()
+    s.radius *= 1.0 + 2.0e-7
+    st.close()
+    st = Stepper([s], device=device)
+    st.upload()
+    pairs, _ = st.overlaps()
+    st.close()
+    nb = min(int(nbonds), len(pairs))
+    s.nb0[0] = nb
+    s.bonds = numpy.array(pairs[:nb], dtype=numpy.uint32)
+    s.bonds_delta_n = numpy.zeros(nb)
+    s.bonds_delta_t = numpy.zeros((nb, 3))
+    s.bonds_omega_n = numpy.zeros(nb)
+    s.bonds_omega_t = numpy.zeros((nb, 3))
+    s.lambda_bar[0] = 1.0
+    s.sigma_b[0] = sigma_b
+    s.tau_b[0] = numpy.inf
+    s.g[:] = [0.0, 0.0, -9.81]
+    s.E[0] = E
+    s.k_n[0] = s.k_t[0] = k_bond
+    s.gamma_n[0] = 0.0
+    s.gamma_t[0] = 0.0
+    s.mu_s[0] = s.mu_d[0] = 0.5
+    s.contactmodel[0] = 2
+    s.time_current[0] = 0.0
+    s.uniaxialStrainRate(wvel=wvel)
+    # adjustWall rounds the z cell count up; keep every cell 2.1 r_max wide
+    s.num[2] = max(int(float(s.L[2]) / (2.1 * float(s.radius.max()))), 3)
+    m_min = float(s.rho[0]) * V_sphere(float(r.min()))
+    k = math.pi / 2.0 * E * float(s.radius.max())
+    s.time_dt[0] = 0.17 * math.sqrt(m_min / k)
+    s.time_total[0] = 10000 * s.time_dt[0]
+    s.time_file_dt[0] = s.time_total[0]
+    return s
+
+
 def _shear_setup(s, sigma0, mu, k_n=1.16e9, gamma_n=1.0e3, top_vel=0.01, steps=5000):
     """Turn a relaxed pack into a shear box: gravity, linear contacts, a top
     wall at normal stress sigma0 (wmode 1, mass = total particle mass as in

@@ -452,10 +452,7 @@ class sim(object):
         cellsize = self.L[0] / self.num[0]
         self.num[dim] = numpy.ceil(((xmax - xmin) * adjust + xmin) / cellsize)
         self.L[dim] = (xmax - xmin) * adjust + xmin
-        if idx in (0, 1, 3):
-            self.w_x[idx] = numpy.array([xmax])
-        else:
-            self.w_x[idx] = numpy.array([xmin])
+        self.w_x[idx] = xmax if idx in (0, 1, 3) else xmin
         self.w_m[idx] = self.totalMass()
 
     def consolidate(self, normal_stress=10e3):

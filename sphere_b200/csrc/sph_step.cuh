@@ -177,19 +177,25 @@ __device__ __forceinline__ uint16_t list_key(const StepArgs &A, const DevBox &B,
 // step only: the partner's position is read in original order (A.x), which
 // holds the step's start positions until k_finish, one gather fewer than
 // the sorted copy through rank.
-constexpr int KB = 4;
+constexpr int KB = 4;   // (the overflow path of k_search spells out KB entries)
 
-template <int LM>
+// FILTER: entries whose partner already holds a slot of the row (srow[j] >=
+// 0) are not tested: only their image code is brought up to date (in place,
+// *dirty set when it changes); the caller uses this when the row cannot
+// overflow, where such entries do not change where the new ones go.
+template <int LM, bool FILTER>
 __device__ __forceinline__ void list_keys_batch(const StepArgs &A, const DevBox &B, double4 xa,
                                                 const int g[3], const uint32_t bo[KB], uint32_t k0,
-                                                uint32_t vc, uint16_t out[KB])
+                                                uint32_t vc, uint16_t out[KB], const int srow[KB],
+                                                uint32_t *row, int RS, bool *dirty)
 {
     uint64_t cc[KB];
     double4 xb[KB];
 #pragma unroll
     for (int j = 0; j < KB; ++j) {
+        const bool test = k0 + j < vc && (!FILTER || srow[j] < 0);
         cc[j] = k0 + j < vc ? A.cellc[bo[j]] : 0ull;
-        xb[j] = k0 + j < vc ? A.x[bo[j]] : make_double4(0.0, 0.0, 0.0, 0.0);
+        xb[j] = test ? A.x[bo[j]] : make_double4(0.0, 0.0, 0.0, 0.0);
     }
 #pragma unroll
     for (int j = 0; j < KB; ++j) {
@@ -198,6 +204,14 @@ __device__ __forceinline__ void list_keys_batch(const StepArgs &A, const DevBox 
         int bx, by, bz, dx, dy, dz, sx, sy;
         unpack_cell(cc[j], bx, by, bz);
         if (!relative_cell(B, g, bx, by, bz, dx, dy, dz, sx, sy)) continue;
+        if (FILTER && srow[j] >= 0) {
+            const uint32_t v = bo[j] | (shift_code(sx, sy) << CODE_SHIFT);
+            if (row[srow[j] * RS] != v) {
+                row[srow[j] * RS] = v;
+                *dirty = true;
+            }
+            continue;
+        }
         const d3 dm = shift_vec(B, sx, sy);
         d3 x_ab = mk(xa.x - xb[j].x, xa.y - xb[j].y, xa.z - xb[j].z);
         x_ab = vadd(x_ab, dm);
@@ -686,19 +700,37 @@ __device__ __forceinline__ uint32_t search_sphere(const StepArgs &A, uint32_t a,
     uint32_t nb[KB];
 #pragma unroll
     for (int j = 0; j < KB; ++j) nb[j] = lst ? lst[j] : 0u;
-    bool dirty;
+    bool dirty = false;
     if (vc <= (uint32_t)VL_MAX) {
+        // Partners already in the row keep their slots whatever the order,
+        // so when the row cannot overflow only the other entries are
+        // tested and inserted (in visit order, each into the highest free
+        // slot); otherwise every entry goes through the reference's
+        // counting of touching entries.
+        const uint32_t occ0 = occ;
         int nk = 0;
         for (uint32_t k0 = 0; k0 < vc; k0 += KB) {
             uint32_t bo[KB];
+            int srow[KB];
 #pragma unroll
-            for (int j = 0; j < KB; ++j) bo[j] = nb[j];
+            for (int j = 0; j < KB; ++j) {
+                bo[j] = nb[j];
+                srow[j] = -1;
+                if (k0 + j < vc)
+                    for (uint32_t m = occ0; m; m &= m - 1u) {
+                        const int sl = __ffs(m) - 1;
+                        if ((row[sl * RS] & ID_MASK) == bo[j]) {
+                            srow[j] = sl;
+                            break;
+                        }
+                    }
+            }
             if (k0 + KB < vc) {
 #pragma unroll
                 for (int j = 0; j < KB; ++j) nb[j] = lst[k0 + KB + j];
             }
             uint16_t kb[KB];
-            list_keys_batch<LM>(A, B, xa, g, bo, k0, vc, kb);
+            list_keys_batch<LM, true>(A, B, xa, g, bo, k0, vc, kb, srow, row, RS, &dirty);
 #pragma unroll
             for (int j = 0; j < KB; ++j) {
                 const uint16_t key = kb[j];
@@ -712,7 +744,31 @@ __device__ __forceinline__ uint32_t search_sphere(const StepArgs &A, uint32_t a,
                 ++nk;
             }
         }
-        dirty = insert_keys(A, keys, nk, RS, lst, row, RS, occ);
+        if (__popc(occ0) + nk > NC) {
+            // the row may overflow: all touching entries, counted in order
+            nk = 0;
+            const int none[KB] = {-1, -1, -1, -1};
+            for (uint32_t k0 = 0; k0 < vc; k0 += KB) {
+                uint32_t bo[KB];
+#pragma unroll
+                for (int j = 0; j < KB; ++j) bo[j] = k0 + j < vc ? lst[k0 + j] : 0u;
+                uint16_t kb[KB];
+                list_keys_batch<LM, false>(A, B, xa, g, bo, k0, vc, kb, none, row, RS, &dirty);
+#pragma unroll
+                for (int j = 0; j < KB; ++j) {
+                    const uint16_t key = kb[j];
+                    if (key == NO_KEY) continue;
+                    int q = nk;
+                    while (q > 0 && keys[(q - 1) * RS] > key) {
+                        keys[q * RS] = keys[(q - 1) * RS];
+                        --q;
+                    }
+                    keys[q * RS] = key;
+                    ++nk;
+                }
+            }
+        }
+        if (insert_keys(A, keys, nk, RS, lst, row, RS, occ)) dirty = true;
     } else {
         dirty = search_cells<LM>(A, B, a, xa, g, A.xf[a], row, RS);
         occ = occupancy(row, RS);

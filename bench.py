@@ -473,8 +473,11 @@ def main():
         st2._check(st2.lib.sph_upload(st2.h, C.byref(ps), None), "sph_upload")
         boxbuf = (_abi.SphBox * 1)()
         for _ in range(args.steps):
-            st2._check(st2.lib.sph_step(st2.h, 1), "sph_step")
+            # each step's result (time, wall force and position) read back
+            # before the next step is queued; device errors collected once
+            st2._check(st2.lib.sph_step_async(st2.h, 1), "sph_step_async")
             st2._check(st2.lib.sph_get_boxes(st2.h, boxbuf), "sph_get_boxes")
+        st2._check(st2.lib.sph_sync(st2.h), "sph_sync")
         out = HostParticles(n)
         po = out.struct()
         st2._check(st2.lib.sph_download(st2.h, C.byref(po), None), "sph_download")
@@ -489,8 +492,8 @@ def main():
         e2e = {"value": world * n * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "seconds": t_e2e,
-               "what": "sph_upload from pinned host arrays + K x (sph_step + sph_get_boxes) + "
-                       "sph_download"}
+               "what": "sph_upload from pinned host arrays + K x (sph_step_async + "
+                       "sph_get_boxes) + sph_sync + sph_download"}
         st2.close()
 
     adj = None

@@ -70,6 +70,7 @@ struct SphHandle {
     unsigned long long *d_count = nullptr;
     uint32_t *vlist_mem = nullptr;   // neighbour-list storage (A.vlist is null when off)
     std::vector<double> rmax_box;    // largest radius per box (at upload)
+    double *stage = nullptr;         // [np][3] staging of the host 3-vector layout
     // output snapshot (sph_snapshot): device copies of what sph_download and
     // sph_get_boxes return, the error word, an event after the copies and a
     // stream for reading them back
@@ -420,34 +421,59 @@ static int check_particles(SphHandle *h, const SphParticles *p)
     return SPH_OK;
 }
 
+// [np][3] host layout <-> double4 device arrays: one copy of the host
+// buffer into (or out of) a device staging array, and the repacking on the
+// GPU (a pinned host buffer then moves at DMA speed).
+__global__ void k_unpack3(double4 *dst, const double *src, uint64_t n)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = make_double4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0);
+}
+
+__global__ void k_pack3(double *dst, const double4 *src, uint64_t n)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double4 v = src[i];
+        dst[3 * i] = v.x;
+        dst[3 * i + 1] = v.y;
+        dst[3 * i + 2] = v.z;
+    }
+}
+
+static int ensure_stage(SphHandle *h)
+{
+    if (h->stage) return SPH_OK;
+    return dalloc(h, &h->stage, 3 * h->ntot);
+}
+
 static int put3(SphHandle *h, double4 *dst, const double *src, uint64_t n)
 {
-    std::vector<double4> tmp(n ? n : 1);
-    for (uint64_t i = 0; i < n; ++i)
-        tmp[i] = src ? make_double4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0)
-                     : make_double4(0.0, 0.0, 0.0, 0.0);
-    CUDA_TRY(h, cudaMemcpy(dst, tmp.data(), sizeof(double4) * (n ? n : 1), cudaMemcpyHostToDevice));
+    if (!src || n == 0) {
+        CUDA_TRY(h, cudaMemset(dst, 0, sizeof(double4) * (n ? n : 1)));
+        return SPH_OK;
+    }
+    int st;
+    if ((st = ensure_stage(h)) != SPH_OK) return st;
+    CUDA_TRY(h, cudaMemcpyAsync(h->stage, src, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                                h->stream));
+    k_unpack3<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(dst, h->stage, n);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return SPH_OK;
 }
 
 static int get3(SphHandle *h, double *dst, const double4 *src, uint64_t n,
                 cudaStream_t cs = nullptr)
 {
-    if (!dst) return SPH_OK;
-    std::vector<double4> tmp(n ? n : 1);
-    if (cs) {
-        CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), src, sizeof(double4) * (n ? n : 1),
-                                    cudaMemcpyDeviceToHost, cs));
-        CUDA_TRY(h, cudaStreamSynchronize(cs));
-    } else {
-        CUDA_TRY(h, cudaMemcpy(tmp.data(), src, sizeof(double4) * (n ? n : 1),
-                               cudaMemcpyDeviceToHost));
-    }
-    for (uint64_t i = 0; i < n; ++i) {
-        dst[3 * i] = tmp[i].x;
-        dst[3 * i + 1] = tmp[i].y;
-        dst[3 * i + 2] = tmp[i].z;
-    }
+    if (!dst || n == 0) return SPH_OK;
+    int st;
+    if ((st = ensure_stage(h)) != SPH_OK) return st;
+    cudaStream_t s = cs ? cs : h->stream;
+    k_pack3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->stage, src, n);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(dst, h->stage, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(h, cudaStreamSynchronize(s));
     return SPH_OK;
 }
 

@@ -14,6 +14,13 @@
 
 namespace sph {
 
+// Wait for the kernel before this one in the stream when launched as a
+// programmatic dependent launch (launch_k); returns at once otherwise.
+__device__ __forceinline__ void grid_dependency_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 constexpr int NC = SPH_NC;
 constexpr uint32_t EMPTY = 0xffffffffu;     // free contact slot
 constexpr uint32_t ID_MASK = 0x0fffffffu;   // partner index bits of a slot word

@@ -125,7 +125,33 @@ typedef void (*InteractLauncher)(const StepArgs &A, cudaStream_t st, unsigned gr
                                  int lenmode, int variant);
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
                 Prof *prof = nullptr);
-typedef void (*ContactLauncher)(const StepArgs &A, cudaStream_t st, unsigned grid, int lenmode);
+typedef void (*ContactLauncher)(const StepArgs &A, cudaStream_t st, unsigned grid, int lenmode,
+                                bool pdl);
+
+// Launch kern<<<grid, block, 0, st>>>(args...); with pdl, as a programmatic
+// dependent launch: the grid may be scheduled while the kernel before it
+// in the stream finishes, and waits (grid_dependency_wait) before reading
+// what that kernel wrote.
+template <typename... P, typename... Q>
+inline void launch_k(bool pdl, void (*kern)(P...), unsigned grid, unsigned block,
+                     cudaStream_t st, Q... args)
+{
+    if (!pdl) {
+        kern<<<grid, block, 0, st>>>(args...);
+        return;
+    }
+    cudaLaunchConfig_t c = {};
+    c.gridDim = dim3(grid);
+    c.blockDim = dim3(block);
+    c.dynamicSmemBytes = 0;
+    c.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    c.attrs = at;
+    c.numAttrs = 1;
+    cudaLaunchKernelEx(&c, kern, args...);
+}
 int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                      uint64_t *launches, Prof *prof, InteractLauncher interact,
                      ContactLauncher contact);

@@ -112,6 +112,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const uint32_t *in, uint64_t n,
                                                               uint32_t *bsum)
 {
+    grid_dependency_wait();
     __shared__ uint32_t smem[33];
     const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
     uint32_t s = 0;
@@ -125,6 +126,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const uint32_t *in
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_top(uint32_t *bsum, uint32_t nb)
 {
+    grid_dependency_wait();
     __shared__ uint32_t smem[33];
     uint32_t v[SCAN_ITEMS];
     uint32_t s = 0;
@@ -149,6 +151,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t *in, 
                                                             const uint32_t *bsum, uint32_t nb,
                                                             uint32_t *out)
 {
+    grid_dependency_wait();
     __shared__ uint32_t smem[33];
     const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
     uint32_t v[SCAN_ITEMS];
@@ -170,6 +173,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const uint32_t *in, 
 
 __global__ void k_scatter(StepArgs A)
 {
+    grid_dependency_wait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.ntot) return;
     A.unsorted[A.cell_off[A.cell_id[i]] + A.local_off[i]] = i;
@@ -185,6 +189,7 @@ __global__ void k_scatter(StepArgs A)
 template <bool ALL>
 __global__ void k_place(StepArgs A)
 {
+    grid_dependency_wait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.ntot) return;
     const uint32_t c = A.cell_id[i];
@@ -275,6 +280,7 @@ constexpr unsigned VLIST_BLOCKS = 148u * 8u;
 
 __global__ void __launch_bounds__(VLIST_THREADS) k_vlist_build(StepArgs A)
 {
+    grid_dependency_wait();
     if (A.vflag[0] == 0u) return;
     __shared__ uint32_t s_list[VL_MAX * VLIST_THREADS];
     for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < A.ntot;
@@ -285,6 +291,7 @@ __global__ void __launch_bounds__(VLIST_THREADS) k_vlist_build(StepArgs A)
 // After the (possible) build: clear the request, count builds.
 __global__ void k_vlist_done(StepArgs A)
 {
+    grid_dependency_wait();
     if (A.vflag[0] != 0u) {
         A.vflag[0] = 0u;
         A.vflag[1] += 1u;
@@ -807,9 +814,9 @@ static void interact_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, boo
     launch_interact<false>(A, st, grid, fused, lm, variant);
 }
 
-static void contacts_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, int lm)
+static void contacts_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, int lm, bool pdl)
 {
-    launch_contacts<false>(A, st, grid, lm);
+    launch_contacts<false>(A, st, grid, lm, pdl);
 }
 
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,
@@ -823,6 +830,9 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                      ContactLauncher contact)
 {
     uint64_t nl = 0;
+    // programmatic dependent launches along the step's chain of kernels,
+    // except where events are recorded between them (profiling)
+    const bool pdl = prof == nullptr;
     if (prof) {
         prof->n = 0;
         record(prof->ev[0], st);
@@ -856,22 +866,24 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         k_hash<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
         mark(prof, st, "k_hash");
         const uint32_t nb = blocks_for(A.ncells, SCAN_TILE);
-        k_scan_reduce<<<nb, SCAN_THREADS, 0, st>>>(A.cell_count, A.ncells, A.scan_tmp);
-        k_scan_top<<<1, SCAN_THREADS, 0, st>>>(A.scan_tmp, nb);
-        k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(A.cell_count, A.ncells, A.scan_tmp, nb, A.cell_off);
+        launch_k(pdl, k_scan_reduce, nb, SCAN_THREADS, st, (const uint32_t *)A.cell_count,
+                 A.ncells, A.scan_tmp);
+        launch_k(pdl, k_scan_top, 1, SCAN_THREADS, st, A.scan_tmp, nb);
+        launch_k(pdl, k_scan_down, nb, SCAN_THREADS, st, (const uint32_t *)A.cell_count, A.ncells,
+                 (const uint32_t *)A.scan_tmp, nb, A.cell_off);
         mark(prof, st, "k_scan(3)");
-        k_scatter<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+        launch_k(pdl, k_scatter, blocks_for(A.ntot, 256), 256, st, A);
         mark(prof, st, "k_scatter");
         const bool split = cfg.variant == SPLIT_VARIANT && !cfg.unfused && cfg.all_cm23 &&
                            A.vlist && A.csum;
-        if (split) k_place<false><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
-        else k_place<true><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+        if (split) launch_k(pdl, k_place<false>, blocks_for(A.ntot, 256), 256, st, A);
+        else launch_k(pdl, k_place<true>, blocks_for(A.ntot, 256), 256, st, A);
         mark(prof, st, "k_place");
         nl += 7;
         if (A.vlist) {
             const unsigned gv = blocks_for(A.ntot, VLIST_THREADS);
-            k_vlist_build<<<gv < VLIST_BLOCKS ? gv : VLIST_BLOCKS, VLIST_THREADS, 0, st>>>(A);
-            k_vlist_done<<<1, 1, 0, st>>>(A);
+            launch_k(pdl, k_vlist_build, gv < VLIST_BLOCKS ? gv : VLIST_BLOCKS, VLIST_THREADS, st, A);
+            launch_k(pdl, k_vlist_done, 1, 1, st, A);
             mark(prof, st, "k_vlist");
             nl += 2;
         }
@@ -884,13 +896,14 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
         const unsigned gi = blocks_for(A.ntot, INTERACT_THREADS);
         if (split) {
             const unsigned gs = blocks_for(A.ntot, SEARCH_THREADS);
+            // after k_bonds (when there are bonds) an ordinary launch
+            const bool pdl_s = pdl && !A.nbonds;
             if (cfg.lenmode == SPH_LEN_FP64)
-                k_search<SPH_LEN_FP64><<<gs, SEARCH_THREADS, 0, st>>>(A);
+                launch_k(pdl_s, k_search<SPH_LEN_FP64>, gs, SEARCH_THREADS, st, A);
             else
-                k_search<SPH_LEN_REFERENCE><<<gs, SEARCH_THREADS, 0, st>>>(A);
+                launch_k(pdl_s, k_search<SPH_LEN_REFERENCE>, gs, SEARCH_THREADS, st, A);
             mark(prof, st, "k_search");
-            contact(A, st, blocks_for(A.ntot, CONTACT_THREADS),
-                    cfg.lenmode);
+            contact(A, st, blocks_for(A.ntot, CONTACT_THREADS), cfg.lenmode, pdl);
             mark(prof, st, "k_contacts");
             if (overlap) cudaStreamWaitEvent(st, cfg.join, 0);
             if (cfg.lenmode == SPH_LEN_FP64)

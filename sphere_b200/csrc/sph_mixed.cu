@@ -16,9 +16,9 @@ static void interact_mixed(const StepArgs &A, cudaStream_t st, unsigned grid, bo
     launch_interact<true>(A, st, grid, fused, lm, variant);
 }
 
-static void contacts_mixed(const StepArgs &A, cudaStream_t st, unsigned grid, int lm)
+static void contacts_mixed(const StepArgs &A, cudaStream_t st, unsigned grid, int lm, bool pdl)
 {
-    launch_contacts<true>(A, st, grid, lm);
+    launch_contacts<true>(A, st, grid, lm, pdl);
 }
 
 int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,

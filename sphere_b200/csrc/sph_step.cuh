@@ -796,6 +796,7 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
 {
     __shared__ uint32_t s_row[NC * SEARCH_THREADS];
     __shared__ uint16_t s_keys[VL_MAX * SEARCH_THREADS];
+    grid_dependency_wait();
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
     const int RS = SEARCH_THREADS;
@@ -868,6 +869,7 @@ template <int LM, bool MIXED>
 __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
 {
     __shared__ RecSlab S;
+    grid_dependency_wait();
     const uint32_t lane = threadIdx.x & 31u;
     const int wbase = (int)(threadIdx.x & ~31u);
     const uint32_t a_own = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1005,10 +1007,10 @@ inline void launch_interact_lm(const StepArgs &A, cudaStream_t st, unsigned grid
 }
 
 template <bool MIXED>
-inline void launch_contacts(const StepArgs &A, cudaStream_t st, unsigned grid, int lm)
+inline void launch_contacts(const StepArgs &A, cudaStream_t st, unsigned grid, int lm, bool pdl)
 {
-    if (lm == SPH_LEN_FP64) k_contacts<SPH_LEN_FP64, MIXED><<<grid, CONTACT_THREADS, 0, st>>>(A);
-    else k_contacts<SPH_LEN_REFERENCE, MIXED><<<grid, CONTACT_THREADS, 0, st>>>(A);
+    if (lm == SPH_LEN_FP64) launch_k(pdl, k_contacts<SPH_LEN_FP64, MIXED>, grid, CONTACT_THREADS, st, A);
+    else launch_k(pdl, k_contacts<SPH_LEN_REFERENCE, MIXED>, grid, CONTACT_THREADS, st, A);
 }
 
 template <bool MIXED>

@@ -52,12 +52,12 @@ struct StepArgs {
     float4 *xref;
     uint64_t *cellc;
     uint32_t vcap;             // list capacity in use (<= VL_MAX)
-    // split step (k_search / k_contacts / k_finish): per warp of 32 sorted
-    // positions, a region of 32 * NC entries holding the warp's live
+    // split step (k_search / k_contacts / k_finish): per warp of 32
+    // original indexes, a region of 32 * NC entries holding the warp's live
     // contacts from its start, sphere after sphere, each in slot order
-    // (slot word; original index | slot << 27); per sphere, by sorted position, their
-    // number; by original index, the sums of its contacts (null until the
-    // split step is first used)
+    // (slot word; original index | slot << 27); per sphere their
+    // number and the sums of its contacts, all by original index (null until
+    // the split step is first used)
     uint2 *lent;
     uint32_t *nlive;
     Acc *csum;

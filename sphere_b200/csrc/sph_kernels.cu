@@ -184,8 +184,8 @@ __global__ void k_scatter(StepArgs A)
 // cell_off[c] + (the number of particles of its cell with a smaller index),
 // so each cell is ordered by original index.  rank = inverse of perm.
 // ALL = false for the split step, which reads velocities and partners in
-// original order and needs only the sorted positions (its own contact
-// search, the neighbour-list build and the cell-search fallback).
+// original order and needs only the sorted positions and rank (the
+// neighbour-list build and the cell-search fallback).
 template <bool ALL>
 __global__ void k_place(StepArgs A)
 {
@@ -200,10 +200,10 @@ __global__ void k_place(StepArgs A)
     const double4 x = A.x[i];
     A.xs[j] = x;
     A.xf[j] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+    A.rank[i] = j;
     if (ALL) {
         A.vs[j] = A.vel[i];
         A.ws[j] = A.angvel[i];
-        A.rank[i] = j;
     }
 }
 

@@ -661,15 +661,15 @@ constexpr int SEARCH_THREADS = 128;
 constexpr int CONTACT_THREADS = 128;
 constexpr int FINISH_THREADS = 128;
 
-// Contact search of sphere a (sorted position) on its slot row, staged in
-// shared memory (row[s * RS]); returns the bitmask of occupied slots.
+// Contact search of sphere i (original index: its row, list and state are
+// read without a permutation lookup) on its slot row, staged in shared
+// memory (row[s * RS]); returns the bitmask of occupied slots.
 template <int LM>
-__device__ __forceinline__ uint32_t search_sphere(const StepArgs &A, uint32_t a, uint32_t *row,
+__device__ __forceinline__ uint32_t search_sphere(const StepArgs &A, uint32_t i, uint32_t *row,
                                                   uint16_t *keys, int RS)
 {
-    const uint32_t i = A.perm[a];
     const DevBox &B = A.boxes[box_index(A, i)];
-    const double4 xa = A.xs[a];
+    const double4 xa = A.x[i];
     const uint4 *grow = reinterpret_cast<const uint4 *>(A.slots + (size_t)i * NC);
     uint32_t occ = 0;
 #pragma unroll
@@ -770,6 +770,7 @@ __device__ __forceinline__ uint32_t search_sphere(const StepArgs &A, uint32_t a,
         }
         if (insert_keys(A, keys, nk, RS, lst, row, RS, occ)) dirty = true;
     } else {
+        const uint32_t a = A.rank[i];   // the cell search walks the sorted copies
         dirty = search_cells<LM>(A, B, a, xa, g, A.xf[a], row, RS);
         occ = occupancy(row, RS);
     }
@@ -797,12 +798,12 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
     __shared__ uint32_t s_row[NC * SEARCH_THREADS];
     __shared__ uint16_t s_keys[VL_MAX * SEARCH_THREADS];
     grid_dependency_wait();
-    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
     const int RS = SEARCH_THREADS;
     uint32_t *row = s_row + threadIdx.x;
     const uint32_t occ =
-        a < A.ntot ? search_sphere<LM>(A, a, row, s_keys + threadIdx.x, RS) : 0u;
+        i < A.ntot ? search_sphere<LM>(A, i, row, s_keys + threadIdx.x, RS) : 0u;
     // the warp's live contacts, sphere after sphere, each in slot order,
     // written contiguously from the start of the warp's region
     const uint32_t nl = __popc(occ);
@@ -812,15 +813,15 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_search(StepArgs A)
         const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= (uint32_t)o) incl += v;
     }
-    if (a >= A.ntot) return;
-    uint2 *ent = A.lent + (size_t)(a - lane) * NC + (incl - nl);
+    if (i >= A.ntot) return;
+    uint2 *ent = A.lent + (size_t)(i - lane) * NC + (incl - nl);
     uint32_t q = 0;
     for (uint32_t m = occ; m; m &= m - 1u) {
         const int sl = __ffs(m) - 1;
         // slot word (partner's original id | image code), i | slot << 27
-        ent[q++] = make_uint2(row[sl * RS], A.perm[a] | ((uint32_t)sl << 27));
+        ent[q++] = make_uint2(row[sl * RS], i | ((uint32_t)sl << 27));
     }
-    A.nlive[a] = nl;
+    A.nlive[i] = nl;
 }
 
 // One warp-round of contact records in shared memory, field by field
@@ -860,7 +861,7 @@ __device__ __forceinline__ ContactRec get_rec(const RecSlab &S, int t)
     return r;
 }
 
-// One warp per 32 consecutive spheres (sorted positions), its lanes dealt
+// One warp per 32 consecutive spheres (original indexes), its lanes dealt
 // the warp's live contacts in order: round r computes contacts 32r .. 32r +
 // 31 of the warp's list (the spheres' live lists one after the other), so a
 // lane is idle only in the last round.  Each lane then adds, in slot order,
@@ -872,10 +873,10 @@ __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
     grid_dependency_wait();
     const uint32_t lane = threadIdx.x & 31u;
     const int wbase = (int)(threadIdx.x & ~31u);
-    const uint32_t a_own = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t a0 = a_own - lane;
-    const bool valid = a_own < A.ntot;
-    const uint32_t nl_own = valid ? A.nlive[a_own] : 0u;
+    const uint32_t i_own = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i0 = i_own - lane;
+    const bool valid = i_own < A.ntot;
+    const uint32_t nl_own = valid ? A.nlive[i_own] : 0u;
     // inclusive prefix sum of the live counts over the warp
     uint32_t incl = nl_own;
 #pragma unroll
@@ -891,7 +892,7 @@ __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
     acc.es_dot = 0.0;
     acc.ev_dot = 0.0;
     acc.p = 0.0;
-    const uint2 *ent = A.lent + (size_t)a0 * NC;
+    const uint2 *ent = A.lent + (size_t)i0 * NC;
     for (uint32_t base = 0; base < total; base += 32) {
         const uint32_t f = base + lane;
         ContactRec r;
@@ -966,7 +967,7 @@ __global__ void __launch_bounds__(CONTACT_THREADS, 6) k_contacts(StepArgs A)
         }
         __syncwarp();
     }
-    if (valid) A.csum[A.perm[a_own]] = acc;
+    if (valid) A.csum[i_own] = acc;
 }
 
 template <int LM>

@@ -614,38 +614,82 @@ int relax_sweep(const StepArgs &A, cudaStream_t st, double alpha, double z_top,
 // terms), spheres in index order, so that every slab's sum is the
 // reference's, operation for operation.  All threads of a warp read the
 // same sphere at a time (broadcast).
-__global__ void k_porosity(const double4 *x, uint32_t p0, uint32_t np, double h_slice,
-                           double V_slice, uint32_t nslices, double *z_pos, double *por)
+// One block per slab.  The slab's void volume is the reference's sequential
+// subtraction over the spheres in index order (one or two subtractions per
+// sphere that reaches into the slab, none otherwise); the threads compute
+// the terms of 256 spheres at a time and thread 0 applies them in index
+// order, skipping the spheres without a term (src/sphere.cpp:520-587).
+constexpr int POR_THREADS = 256;
+
+__global__ void __launch_bounds__(POR_THREADS) k_porosity(const double4 *x, uint32_t p0,
+                                                          uint32_t np, double h_slice,
+                                                          double V_slice, uint32_t nslices,
+                                                          double *z_pos, double *por)
 {
-    const uint32_t iz = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double s_t[2][POR_THREADS];
+    __shared__ int s_n[POR_THREADS];
+    __shared__ uint32_t s_mask[POR_THREADS / 32];
+    const uint32_t iz = blockIdx.x;
     const double z_low = (double)iz * h_slice;
     const double z_high = z_low + h_slice;
     double V_void = V_slice;
-    for (uint32_t i = 0; i < np; ++i) {
-        const double4 p = x[p0 + i];
-        const double zc = p.z, r = p.w;
-        const double zl = zc - r, zh = zc + r;
-        const double V_s = 4.0 / 3.0 * M_PI * r * r * r;
-        if (z_low <= zl && zh <= z_high) {
-            V_void -= V_s;
-        } else {
-            if (z_low >= zc && z_low <= zh) {
-                const double h = zh - z_low;
-                V_void -= M_PI * h * h / 3.0 * (3.0 * r - h);
-            } else if (z_low < zc && z_low > zl) {
-                const double h = z_low - zl;
-                V_void -= V_s + M_PI * h * h / 3.0 * (3.0 * r - h);
-            }
-            if (z_high <= zc && z_high >= zl) {
-                const double h = z_high - zl;
-                V_void -= M_PI * h * h / 3.0 * (3.0 * r - h);
-            } else if (z_high > zc && z_high < zh) {
-                const double h = zh - z_high;
-                V_void -= V_s + M_PI * h * h / 3.0 * (3.0 * r - h);
+    for (uint32_t base = 0; base < np; base += POR_THREADS) {
+        const uint32_t i = base + threadIdx.x;
+        int n = 0;
+        double t0 = 0.0, t1 = 0.0;
+        if (i < np) {
+            const double4 p = x[p0 + i];
+            const double zc = p.z, r = p.w;
+            const double zl = zc - r, zh = zc + r;
+            const double V_s = 4.0 / 3.0 * M_PI * r * r * r;
+            if (z_low <= zl && zh <= z_high) {
+                t0 = V_s;
+                n = 1;
+            } else {
+                if (z_low >= zc && z_low <= zh) {
+                    const double h = zh - z_low;
+                    t0 = M_PI * h * h / 3.0 * (3.0 * r - h);
+                    n = 1;
+                } else if (z_low < zc && z_low > zl) {
+                    const double h = z_low - zl;
+                    t0 = V_s + M_PI * h * h / 3.0 * (3.0 * r - h);
+                    n = 1;
+                }
+                double tb = 0.0;
+                bool hb = false;
+                if (z_high <= zc && z_high >= zl) {
+                    const double h = z_high - zl;
+                    tb = M_PI * h * h / 3.0 * (3.0 * r - h);
+                    hb = true;
+                } else if (z_high > zc && z_high < zh) {
+                    const double h = zh - z_high;
+                    tb = V_s + M_PI * h * h / 3.0 * (3.0 * r - h);
+                    hb = true;
+                }
+                if (hb) {
+                    if (n == 0) t0 = tb;
+                    else t1 = tb;
+                    ++n;
+                }
             }
         }
+        s_t[0][threadIdx.x] = t0;
+        s_t[1][threadIdx.x] = t1;
+        s_n[threadIdx.x] = n;
+        const uint32_t m = __ballot_sync(0xffffffffu, n > 0);
+        if ((threadIdx.x & 31) == 0) s_mask[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 0; w < POR_THREADS / 32; ++w)
+                for (uint32_t b = s_mask[w]; b; b &= b - 1u) {
+                    const int t = w * 32 + __ffs(b) - 1;
+                    V_void -= s_t[0][t];
+                    if (s_n[t] > 1) V_void -= s_t[1][t];
+                }
+        }
+        __syncthreads();
     }
-    if (iz < nslices) {
+    if (threadIdx.x == 0 && iz < nslices) {
         z_pos[iz] = z_low + 0.5 * h_slice;
         por[iz] = V_void / V_slice;
     }
@@ -654,8 +698,7 @@ __global__ void k_porosity(const double4 *x, uint32_t p0, uint32_t np, double h_
 int porosity_profile(const double4 *x, uint32_t p0, uint32_t np, double h_slice, double V_slice,
                      uint32_t nslices, double *z_pos, double *por, cudaStream_t st)
 {
-    k_porosity<<<blocks_for(nslices, 32), 32, 0, st>>>(x, p0, np, h_slice, V_slice, nslices, z_pos,
-                                                       por);
+    k_porosity<<<nslices, POR_THREADS, 0, st>>>(x, p0, np, h_slice, V_slice, nslices, z_pos, por);
     return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
 }
 

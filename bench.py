@@ -313,6 +313,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-bonded", action="store_true")
+    ap.add_argument("--kernel-tour", action="store_true",
+                    help="run every kernel family once inside the NVTX range 'k' (for profiling) "
+                         "and exit")
     ap.add_argument("--variant", type=int, default=-1,
                     help="interact launch variant (0-3); default: picked by sph_autotune")
     args = ap.parse_args()
@@ -345,6 +348,30 @@ def main():
     import torch
     import torch.distributed as dist
     from sphere_b200.runner import Stepper, HostParticles
+
+    if args.kernel_tour:
+        # every kernel family once, inside one NVTX range: split steps in
+        # both forms, fused steps, a render, a porosity profile, an overlap
+        # listing and packing sweeps
+        torch.cuda.set_device(local)
+        s = make_scene(args.n, 0, local, args.pack_sweeps)
+        torch.cuda.nvtx.range_push("k")
+        for prec in ("mixed", "fp64"):
+            st = Stepper([s], precision=prec, length="reference", device=local)
+            st.upload()
+            st.set_variant(3)
+            st.step(3)
+            if prec == "fp64":
+                st.set_variant(1)
+                st.step(2)
+                st.render(method=1, maxval=1e3, width=800, height=800)
+                st.porosity(10)
+                st.overlaps()
+                st.relax(2, alpha=0.5, z_top=float(s.L[2]))
+            st.close()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"kernel_tour": "done", "spheres": args.n}))
+        return 0
 
     torch.cuda.set_device(local)
     if world > 1:

@@ -498,22 +498,29 @@ def main():
             setattr(hp, name, pin)
         st2.hp = hp
         import ctypes as C
-        from sphere_b200 import _abi
         h2d = sum(getattr(hp, k).nbytes for k in ("x", "xyzsum", "vel", "force", "angpos",
                                                    "angvel", "torque", "es_dot", "es", "ev_dot",
                                                    "ev", "p"))
+        nbs = st2.box_state_bytes()
+        states = torch.empty((max(args.steps, args.warmup), nbs), dtype=torch.uint8,
+                             pin_memory=True).numpy()
+        # warm-up: the same calls untimed (graphs instantiated, pages touched);
+        # the timed upload below starts the scene again from the host arrays
+        ps = hp.struct()
+        st2._check(st2.lib.sph_upload(st2.h, C.byref(ps), None), "sph_upload")
+        st2.step_async_states(args.warmup, states)
+        st2._check(st2.lib.sph_sync(st2.h), "sph_sync")
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
         ps = hp.struct()
         st2._check(st2.lib.sph_upload(st2.h, C.byref(ps), None), "sph_upload")
-        boxbuf = (_abi.SphBox * 1)()
-        for _ in range(args.steps):
-            # each step's result (time, wall force and position) read back
-            # before the next step is queued; device errors collected once
-            st2._check(st2.lib.sph_step_async(st2.h, 1), "sph_step_async")
-            st2._check(st2.lib.sph_get_boxes(st2.h, boxbuf), "sph_get_boxes")
+        # every step's result (time, wall force and position) copied into
+        # pinned host memory as the step ends, the steps queued back to
+        # back; device errors collected once, then each state decoded
+        st2.step_async_states(args.steps, states[:args.steps])
         st2._check(st2.lib.sph_sync(st2.h), "sph_sync")
+        per_step = [st2.boxes_from_state(states[k]) for k in range(args.steps)]
         out = HostParticles(n)
         po = out.struct()
         st2._check(st2.lib.sph_download(st2.h, C.byref(po), None), "sph_download")
@@ -524,12 +531,14 @@ def main():
             t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             t_e2e = float(t.item())
-        d2h = h2d + C.sizeof(_abi.SphBox) * args.steps
+        d2h = h2d + nbs * args.steps
+        assert per_step[-1][0].t_current > per_step[0][0].t_current or args.steps == 1
         e2e = {"value": world * n * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "seconds": t_e2e,
-               "what": "sph_upload from pinned host arrays + K x (sph_step_async + "
-                       "sph_get_boxes) + sph_sync + sph_download"}
+               "what": "sph_upload from pinned host arrays + sph_step_async_states (K steps, "
+                       "the box state after each copied to pinned host memory) + sph_sync + "
+                       "decoding of the K states + sph_download"}
         st2.close()
 
     adj = None

@@ -195,6 +195,21 @@ int sph_download(SphHandle *h, SphParticles *p, SphBonds *b);
  * forces after integrateWalls; L[2] after an adaptive-grid update). */
 int sph_get_boxes(SphHandle *h, SphBox *boxes);
 
+/* The same box state read back without waiting (no counterpart in the
+ * reference, whose loop stops for every read).  A state is the raw device
+ * box table, sph_box_state_bytes long.  sph_get_boxes_async queues, on the
+ * handle's stream after the steps queued so far, a copy of it into
+ * `staging`; sph_step_async_states queues nsteps steps as sph_step_async
+ * does and the state after step s into states + s * sph_box_state_bytes
+ * (states_bytes >= nsteps times that).  Pinned host memory keeps the copies
+ * asynchronous.  After sph_sync, sph_boxes_from_staging turns one state
+ * into SphBox records, as sph_get_boxes returns them.  Lets a caller read
+ * every step's result while the steps run back to back. */
+int sph_box_state_bytes(const SphHandle *h, uint64_t *bytes);
+int sph_get_boxes_async(SphHandle *h, void *staging, uint64_t staging_bytes);
+int sph_step_async_states(SphHandle *h, uint64_t nsteps, void *states, uint64_t states_bytes);
+int sph_boxes_from_staging(SphHandle *h, const void *staging, SphBox *boxes);
+
 /* Contact bookkeeping in the reference's slot form (src/device.cu:428-432):
  * contacts [np][NC] (partner index local to the box, np_box = empty),
  * delta_t [np][NC][4], distmod [np][NC][4] (periodic shift xyz, partner

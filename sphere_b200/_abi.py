@@ -207,6 +207,14 @@ def load_library():
     lib.sph_overlaps.argtypes = [H, C.c_uint32, C.c_uint64, C.POINTER(C.c_uint32), _dp,
                                  C.POINTER(C.c_uint64)]
     lib.sph_overlaps.restype = C.c_int
+    lib.sph_box_state_bytes.argtypes = [H, C.POINTER(C.c_uint64)]
+    lib.sph_box_state_bytes.restype = C.c_int
+    lib.sph_get_boxes_async.argtypes = [H, C.c_void_p, C.c_uint64]
+    lib.sph_get_boxes_async.restype = C.c_int
+    lib.sph_step_async_states.argtypes = [H, C.c_uint64, C.c_void_p, C.c_uint64]
+    lib.sph_step_async_states.restype = C.c_int
+    lib.sph_boxes_from_staging.argtypes = [H, C.c_void_p, C.POINTER(SphBox)]
+    lib.sph_boxes_from_staging.restype = C.c_int
     lib.sph_render.argtypes = [H, C.c_uint32, C.c_int, C.c_float, C.c_float, C.c_float,
                                C.c_uint32, C.c_uint32, C.POINTER(C.c_uint8)]
     lib.sph_render.restype = C.c_int

@@ -728,30 +728,59 @@ int sph_step(SphHandle *h, uint64_t nsteps)
     return collect_errors(h);
 }
 
+// Queue nsteps steps on the handle's stream; with states, the box table
+// after step s is copied to states + s * (nbox * sizeof(DevBox)) as soon as
+// that step's wall stage has run.
+static int queue_steps(SphHandle *h, uint64_t nsteps, uint8_t *states)
+{
+    int st;
+    if ((st = build_graph(h)) != SPH_OK) return st;
+    const size_t bytes = sizeof(DevBox) * h->nbox;
+    if (nsteps >= 2 && !h->prof_on && overlap_ok(h)) {
+        // the head of step 1, steps 2..n each beside the wall stage of the
+        // step before, then the wall stage of step n: every step's work, in
+        // an order that respects each read of the wall stage's results.
+        // Graph s (s >= 1) ends with the wall stage of step s, and the
+        // heads only read the box table, so a copy after graph s holds the
+        // state after step s.
+        if ((st = build_phase_graphs(h)) != SPH_OK) return st;
+        for (uint64_t s = 0; s <= nsteps; ++s) {
+            const int ph = s == 0 ? sph::STEP_HEAD : (s < nsteps ? sph::STEP_OVERLAP : sph::STEP_TAIL);
+            CUDA_TRY(h, cudaGraphLaunch(h->pexec_ph[ph], h->stream));
+            if (states && s > 0)
+                CUDA_TRY(h, cudaMemcpyAsync(states + (s - 1) * bytes, h->A.boxes, bytes,
+                                            cudaMemcpyDeviceToHost, h->stream));
+        }
+        for (uint64_t s = 0; s < nsteps; ++s)
+            for (uint32_t k = 0; k < h->nbox; ++k) h->t_host[k] += h->boxes[k].dt;
+    } else {
+        for (uint64_t s = 0; s < nsteps; ++s) {
+            if ((st = launch_one(h)) != SPH_OK) return st;
+            if (states)
+                CUDA_TRY(h, cudaMemcpyAsync(states + s * bytes, h->A.boxes, bytes,
+                                            cudaMemcpyDeviceToHost, h->stream));
+        }
+    }
+    h->launches += nsteps * h->launches_per_step;
+    return SPH_OK;
+}
+
 int sph_step_async(SphHandle *h, uint64_t nsteps)
 {
     if (!h) return SPH_ERR_INPUT;
     if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_step_async before sph_upload");
     cudaSetDevice(h->device);
-    int st;
-    if ((st = build_graph(h)) != SPH_OK) return st;
-    if (nsteps >= 2 && !h->prof_on && overlap_ok(h)) {
-        // the head of step 1, steps 2..n each beside the wall stage of the
-        // step before, then the wall stage of step n: every step's work, in
-        // an order that respects each read of the wall stage's results
-        if ((st = build_phase_graphs(h)) != SPH_OK) return st;
-        for (uint64_t s = 0; s <= nsteps; ++s) {
-            const int ph = s == 0 ? sph::STEP_HEAD : (s < nsteps ? sph::STEP_OVERLAP : sph::STEP_TAIL);
-            CUDA_TRY(h, cudaGraphLaunch(h->pexec_ph[ph], h->stream));
-        }
-        for (uint64_t s = 0; s < nsteps; ++s)
-            for (uint32_t k = 0; k < h->nbox; ++k) h->t_host[k] += h->boxes[k].dt;
-    } else {
-        for (uint64_t s = 0; s < nsteps; ++s)
-            if ((st = launch_one(h)) != SPH_OK) return st;
-    }
-    h->launches += nsteps * h->launches_per_step;
-    return SPH_OK;
+    return queue_steps(h, nsteps, nullptr);
+}
+
+int sph_step_async_states(SphHandle *h, uint64_t nsteps, void *states, uint64_t states_bytes)
+{
+    if (!h || !states) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_step_async_states before sph_upload");
+    if (nsteps && states_bytes / nsteps < sizeof(DevBox) * (uint64_t)h->nbox)
+        return fail(h, SPH_ERR_INPUT, "states smaller than nsteps x sph_box_state_bytes");
+    cudaSetDevice(h->device);
+    return queue_steps(h, nsteps, static_cast<uint8_t *>(states));
 }
 
 int sph_profile(SphHandle *h, int enable)
@@ -917,6 +946,33 @@ int sph_get_boxes(SphHandle *h, SphBox *boxes)
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     std::vector<DevBox> d(h->nbox);
     CUDA_TRY(h, cudaMemcpy(d.data(), h->A.boxes, sizeof(DevBox) * h->nbox, cudaMemcpyDeviceToHost));
+    boxes_from(h, d, boxes);
+    return SPH_OK;
+}
+
+int sph_box_state_bytes(const SphHandle *h, uint64_t *bytes)
+{
+    if (!h || !bytes) return SPH_ERR_INPUT;
+    *bytes = sizeof(DevBox) * (uint64_t)h->nbox;
+    return SPH_OK;
+}
+
+int sph_get_boxes_async(SphHandle *h, void *staging, uint64_t staging_bytes)
+{
+    if (!h || !staging) return SPH_ERR_INPUT;
+    if (staging_bytes < sizeof(DevBox) * (uint64_t)h->nbox)
+        return fail(h, SPH_ERR_INPUT, "staging buffer smaller than sph_box_state_bytes");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaMemcpyAsync(staging, h->A.boxes, sizeof(DevBox) * h->nbox,
+                                cudaMemcpyDeviceToHost, h->stream));
+    return SPH_OK;
+}
+
+int sph_boxes_from_staging(SphHandle *h, const void *staging, SphBox *boxes)
+{
+    if (!h || !staging || !boxes) return SPH_ERR_INPUT;
+    std::vector<DevBox> d(h->nbox);
+    memcpy(d.data(), staging, sizeof(DevBox) * h->nbox);
     boxes_from(h, d, boxes);
     return SPH_OK;
 }

@@ -300,6 +300,37 @@ class Stepper(object):
         self._check(self.lib.sph_get_boxes(self.h, out), "sph_get_boxes")
         return list(out)
 
+    def box_state_bytes(self):
+        """Size of one raw box-state copy (sph_box_state_bytes)."""
+        b = C.c_uint64()
+        self._check(self.lib.sph_box_state_bytes(self.h, C.byref(b)), "sph_box_state_bytes")
+        return b.value
+
+    def get_boxes_async(self, staging):
+        """Queue a copy of the box state into `staging` (a C-contiguous
+        uint8 numpy array of at least box_state_bytes(); pinned memory keeps
+        it asynchronous).  Read it with boxes_from_state after sync()."""
+        assert staging.dtype == numpy.uint8 and staging.flags["C_CONTIGUOUS"]
+        self._check(self.lib.sph_get_boxes_async(self.h, C.c_void_p(staging.ctypes.data),
+                                                 staging.nbytes), "sph_get_boxes_async")
+
+    def step_async_states(self, nsteps, states):
+        """Queue nsteps steps and the box state after each into `states`
+        (uint8, nsteps x box_state_bytes(), C-contiguous)."""
+        assert states.dtype == numpy.uint8 and states.flags["C_CONTIGUOUS"]
+        self._check(self.lib.sph_step_async_states(self.h, int(nsteps),
+                                                   C.c_void_p(states.ctypes.data), states.nbytes),
+                    "sph_step_async_states")
+
+    def boxes_from_state(self, state):
+        """SphBox records (as boxes() returns them) from one raw state."""
+        assert state.dtype == numpy.uint8 and state.flags["C_CONTIGUOUS"]
+        assert state.nbytes >= self.box_state_bytes()
+        out = (_abi.SphBox * len(self.sims))()
+        self._check(self.lib.sph_boxes_from_staging(self.h, C.c_void_p(state.ctypes.data), out),
+                    "sph_boxes_from_staging")
+        return list(out)
+
     def contacts(self):
         n = self.ntot
         c = numpy.zeros(n * NC, dtype=numpy.uint32)

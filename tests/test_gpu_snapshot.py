@@ -47,3 +47,58 @@ def test_snapshot_read_without_snapshot_is_refused():
     with pytest.raises(SphereError):
         a.snapshot_read()            # one read per snapshot
     a.close()
+
+
+def _box_fields(b):
+    return ([b.grid.L[c] for c in range(3)], [list(b.walls.nx[w]) for w in range(b.walls.nw)],
+            [list(b.walls.mvfd[w]) for w in range(b.walls.nw)], b.t_current)
+
+
+@pytest.mark.parametrize("name,nsteps", [("periodic_xy_wall_stress", 9),
+                                         ("periodic_x_wall_velocity", 6),
+                                         ("shear_stress_wall", 5), ("adaptive_grid", 7),
+                                         ("walls_all_sides", 1)])
+def test_step_states_equal_a_read_after_every_step(name, nsteps):
+    # two boxes in one handle; the queued run (the wall stage beside the
+    # next step where the handle allows it) against one synchronous read
+    # per step
+    s, _, _ = cases.make(name)
+    s2, _, _ = cases.make("fixvel_modes")
+    a = Stepper([s, s2], precision="fp64")
+    b = Stepper([s, s2], precision="fp64")
+    a.upload()
+    b.upload()
+    nb = a.box_state_bytes()
+    assert nb > 0 and nb % 8 == 0
+    states = numpy.zeros((nsteps, nb), dtype=numpy.uint8)
+    a.step_async_states(nsteps, states)
+    a.sync()
+    for k in range(nsteps):
+        b.step(1)
+        want = b.boxes()
+        got = a.boxes_from_state(states[k])
+        for bw, bg in zip(want, got):
+            assert _box_fields(bg) == _box_fields(bw), (name, k)
+    fa, _ = a.download()
+    fb, _ = b.download()
+    assert numpy.array_equal(fa.x, fb.x)
+    one = numpy.zeros(nb, dtype=numpy.uint8)
+    a.get_boxes_async(one)
+    a.sync()
+    assert [_box_fields(x) for x in a.boxes_from_state(one)] == \
+        [_box_fields(x) for x in a.boxes()]
+    a.close()
+    b.close()
+
+
+def test_step_states_buffer_too_small_is_refused():
+    s, _, _ = cases.make("periodic_xy_wall_stress")
+    a = Stepper([s], precision="fp64")
+    a.upload()
+    nb = a.box_state_bytes()
+    with pytest.raises(SphereError):
+        a.step_async_states(3, numpy.zeros(3 * nb - 1, dtype=numpy.uint8))
+    with pytest.raises(SphereError):
+        a.get_boxes_async(numpy.zeros(nb - 1, dtype=numpy.uint8))
+    a.step(1)
+    a.close()

@@ -313,6 +313,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-bonded", action="store_true")
+    ap.add_argument("--no-long-run", action="store_true",
+                    help="skip the mixed-vs-FP64 comparison over the whole run")
     ap.add_argument("--kernel-tour", action="store_true",
                     help="run every kernel family once inside the NVTX range 'k' (for profiling) "
                          "and exit")
@@ -550,6 +552,12 @@ def main():
     bonded = None
     if rank == 0 and not args.no_bonded:
         bonded = time_bonded(local, stream)
+    long_run = None
+    if rank == 0 and not args.no_long_run and "mixed" in res and "fp64" in res:
+        # the mixed form's error against the FP64 form over the workload's
+        # whole run (5,000 steps of the same pack): wall stress, porosity
+        from sphere_b200.mixed_error import compare_precisions
+        long_run = compare_precisions(s, slices=50, device=local, cuda_stream=stream.cuda_stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -591,6 +599,8 @@ def main():
         line["ensemble"] = ens
     if bonded is not None:
         line["bonded"] = bonded
+    if long_run is not None:
+        line["mixed_error_long_run"] = long_run
     print(json.dumps(line))
     return 0
 

@@ -63,3 +63,23 @@ def test_mixed_positions_after_100_steps():
     assert dev < 1e-4
     a.close()
     b.close()
+
+
+def test_mixed_wall_stress_and_porosity_over_a_long_run():
+    # a 20,000-sphere sheared dense pack (the benchmark's scene at a
+    # smaller size: 20 kPa on the top wall, top layer sheared), 2,000 steps
+    import json
+    from sphere_b200 import scenes
+    from sphere_b200.mixed_error import compare_precisions
+    s = scenes.sheared_dense_pack(n=20000, seed=3, device=0, sweeps=1500)
+    e = compare_precisions(s, nsteps=2000, slices=20, device=0)
+    print(json.dumps(e))
+    assert e["status"] == [0, 0]
+    assert e["times_equal"]
+    # measured on this scene: mean 5.6e-6, RMS 2.0e-3, bulk porosity
+    # 1.3e-9, profile 2.8e-7, positions 8.9e-4 r
+    assert e["wall_stress_mean_rel_diff_second_half"] < 1e-4
+    assert e["wall_stress_rms_diff_over_rms"] < 2e-2
+    assert e["bulk_porosity_max_abs_diff"] < 1e-7
+    assert e["porosity_profile_max_abs_diff"] < 1e-5
+    assert e["positions_max_diff_over_rmean"] < 1e-2

@@ -354,9 +354,31 @@ def main():
     if args.kernel_tour:
         # every kernel family once, inside one NVTX range: split steps in
         # both forms, fused steps, a render, a porosity profile, an overlap
-        # listing and packing sweeps
+        # listing, packing sweeps, the contact count and the download, the
+        # unfused step of a shear-stress wall, bonded steps (split and
+        # fused), an adjoint forward + backward pass and the cell-offset
+        # scan with caller-owned memory
+        import copy
+        import numpy
+        from sphere_b200 import scenes
         torch.cuda.set_device(local)
         s = make_scene(args.n, 0, local, args.pack_sweeps)
+        # the same pack under a shear-stress top wall (wmode 3: the unfused
+        # step), a bonded pack and the adjoint's loose pack, made before the
+        # range
+        s3 = copy.deepcopy(s)
+        s3.wmode[0] = 3
+        s3.w_tau_x[0] = 500.0
+        nbd = min(args.n, 200000)
+        sb = scenes.bonded_pack(n=nbd, nbonds=3 * nbd // 2, seed=0, device=local)
+        sa = scenes.loose_pack(50000, seed=0, device=local)
+        import ctypes as C
+        from sphere_b200 import _abi
+        lib = _abi.load_library()
+        ncell = 4_000_000
+        d_counts = torch.randint(0, 8, (ncell,), dtype=torch.int32, device="cuda")
+        d_off = torch.empty(ncell + 1, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("k")
         for prec in ("mixed", "fp64"):
             st = Stepper([s], precision=prec, length="reference", device=local)
@@ -370,7 +392,33 @@ def main():
                 st.porosity(10)
                 st.overlaps()
                 st.relax(2, alpha=0.5, z_top=float(s.L[2]))
+                st.count_contacts()
+                st.download()
             st.close()
+        st = Stepper([s3], precision="fp64", length="reference", device=local)
+        st.upload()
+        st.step(2)
+        st.close()
+        st = Stepper([sb], precision="mixed", length="reference", device=local)
+        st.upload()
+        st.set_variant(3)
+        st.step(2)
+        st.set_variant(1)
+        st.step(1)
+        st.close()
+        st = Stepper([sa], precision="fp64", length="fp64", device=local)
+        st.upload()
+        st.adjoint_forward(4, 2)
+        hp, _ = st.download()
+        st.adjoint_backward(numpy.ascontiguousarray(hp.x[:, :3]) * 1e-3)
+        st.close()
+        # the cell-offset scan with caller-owned memory (4e6 cells)
+        rc = lib.sph_cell_offsets_static(
+            C.c_void_p(d_counts.data_ptr()), C.c_uint64(ncell), C.c_void_p(d_off.data_ptr()),
+            C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError("sph_cell_offsets_static: status %d" % rc)
         torch.cuda.nvtx.range_pop()
         print(json.dumps({"kernel_tour": "done", "spheres": args.n}))
         return 0

@@ -415,25 +415,53 @@ __global__ void __launch_bounds__(256) k_block_sums(StepArgs A, const double *in
     if (threadIdx.x == 0) out[part] = cache[0];
 }
 
-// Sum of the shear-stress partials per box (integration.cuh:65-68), once
-// per box instead of once per particle.
-__global__ void k_tau_final(StepArgs A)
+// Per-box kernels: one block per box, partials staged in BOX_STAGE chunks.
+constexpr int BOX_THREADS = 256;
+constexpr int BOX_STAGE = 2048;
+
+// In-order sum of cnt doubles staged in shared memory, by one thread, its
+// loads issued eight at a time ahead of the additions.
+__device__ __forceinline__ double ordered_sum(const double *v_s, uint32_t cnt, double acc)
 {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k = 0;
+    for (; k + 8 <= cnt; k += 8) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = v_s[k + q];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc += v[q];
+    }
+    for (; k < cnt; ++k) acc += v_s[k];
+    return acc;
+}
+
+// Sum of the shear-stress partials per box (integration.cuh:65-68), once
+// per box instead of once per particle: one block per box stages the
+// partials in shared memory with coalesced loads and thread 0 adds them in
+// block order, the reference's order.
+__global__ void __launch_bounds__(BOX_THREADS) k_tau_final(StepArgs A)
+{
+    __shared__ double s_part[BOX_STAGE];
+    const uint32_t b = blockIdx.x;
     if (b >= A.nboxes) return;
     DevBox &B = A.boxes[b];
     double tau = 0.0;
-    if (B.nw > 0 && B.wmode[0] == 3)
-        for (uint32_t k = 0; k < B.nblocks; ++k) tau += A.tau_partial[B.part_base + k];
-    B.tau_eff_x = tau;
+    if (B.nw > 0 && B.wmode[0] == 3) {
+        for (uint32_t base = 0; base < B.nblocks; base += BOX_STAGE) {
+            const uint32_t cnt = min((uint32_t)BOX_STAGE, B.nblocks - base);
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x)
+                s_part[k] = A.tau_partial[B.part_base + base + k];
+            __syncthreads();
+            if (threadIdx.x == 0) tau = ordered_sum(s_part, cnt, tau);
+        }
+    }
+    if (threadIdx.x == 0) B.tau_eff_x = tau;
 }
 
 // integration.cuh:344-450 integrateWalls, then the loop bookkeeping of
 // device.cu:2536-2538, the adaptive grid of device.cu:1050 and the
 // velocity-step state of device.cu:2455-2462 for the next step.
-constexpr int BOX_THREADS = 256;
-constexpr int BOX_STAGE = 2048;
-
 // One block per box.  The wall-force total is the sequential sum of the
 // per-block partials in block order (as the reference's integrateWalls
 // loop); the block stages the partials in shared memory with coalesced
@@ -454,19 +482,8 @@ __global__ void __launch_bounds__(BOX_THREADS) k_box_step(StepArgs A)
             for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x)
                 s_part[k] = A.wall_partial[B.part_base + base + k];
             __syncthreads();
-            if (threadIdx.x == 0) {
-                // the sequential sum of integrateWalls, its loads issued
-                // eight at a time ahead of the additions
-                uint32_t k = 0;
-                for (; k + 8 <= cnt; k += 8) {
-                    double v[8];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) v[q] = s_part[k + q];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) fsum += v[q];
-                }
-                for (; k < cnt; ++k) fsum += s_part[k];
-            }
+            // the sequential sum of integrateWalls
+            if (threadIdx.x == 0) fsum = ordered_sum(s_part, cnt, fsum);
         }
     }
     if (threadIdx.x != 0) return;
@@ -968,7 +985,7 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             mark(prof, st, "k_interact");
             k_shear_stress<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
             k_block_sums<<<A.npartials, 256, 0, st>>>(A, A.tau_pp, A.tau_partial, 1);
-            k_tau_final<<<blocks_for(A.nboxes, 128), 128, 0, st>>>(A);
+            k_tau_final<<<A.nboxes, BOX_THREADS, 0, st>>>(A);
             mark(prof, st, "k_shear_stress+sums");
             k_integrate<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
             mark(prof, st, "k_integrate");

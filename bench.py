@@ -560,22 +560,32 @@ def main():
         st2._check(st2.lib.sph_upload(st2.h, C.byref(ps), None), "sph_upload")
         st2.step_async_states(args.warmup, states)
         st2._check(st2.lib.sph_sync(st2.h), "sph_sync")
+        # the final state goes to pinned host arrays as well
+        out = HostParticles(n)
+        for name in ("x", "xyzsum", "vel", "force", "angpos", "angvel", "torque", "es_dot", "es",
+                     "ev_dot", "ev", "p"):
+            a = getattr(out, name)
+            setattr(out, name, torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy())
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
         ps = hp.struct()
         st2._check(st2.lib.sph_upload(st2.h, C.byref(ps), None), "sph_upload")
+        t1 = time.perf_counter()
         # every step's result (time, wall force and position) copied into
         # pinned host memory as the step ends, the steps queued back to
         # back; device errors collected once, then each state decoded
         st2.step_async_states(args.steps, states[:args.steps])
         st2._check(st2.lib.sph_sync(st2.h), "sph_sync")
-        per_step = [st2.boxes_from_state(states[k]) for k in range(args.steps)]
-        out = HostParticles(n)
+        t2 = time.perf_counter()
+        per_step = st2.boxes_from_states(states, args.steps)
+        t3 = time.perf_counter()
         po = out.struct()
         st2._check(st2.lib.sph_download(st2.h, C.byref(po), None), "sph_download")
         torch.cuda.synchronize()
         t_e2e = time.perf_counter() - t0
+        parts = {"upload_s": t1 - t0, "steps_and_sync_s": t2 - t1, "decode_s": t3 - t2,
+                 "download_s": t_e2e - (t3 - t0)}
         barrier()
         if world > 1:
             t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
@@ -585,10 +595,10 @@ def main():
         assert per_step[-1][0].t_current > per_step[0][0].t_current or args.steps == 1
         e2e = {"value": world * n * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "seconds": t_e2e,
+               "seconds": t_e2e, "parts": parts,
                "what": "sph_upload from pinned host arrays + sph_step_async_states (K steps, "
                        "the box state after each copied to pinned host memory) + sph_sync + "
-                       "decoding of the K states + sph_download"}
+                       "decoding of the K states + sph_download into pinned host arrays"}
         st2.close()
 
     adj = None

@@ -202,13 +202,14 @@ int sph_get_boxes(SphHandle *h, SphBox *boxes);
  * `staging`; sph_step_async_states queues nsteps steps as sph_step_async
  * does and the state after step s into states + s * sph_box_state_bytes
  * (states_bytes >= nsteps times that).  Pinned host memory keeps the copies
- * asynchronous.  After sph_sync, sph_boxes_from_staging turns one state
- * into SphBox records, as sph_get_boxes returns them.  Lets a caller read
+ * asynchronous.  After sph_sync, sph_boxes_from_staging turns nstates
+ * consecutive states into nstates x nbox SphBox records (state-major), as
+ * sph_get_boxes returns them.  Lets a caller read
  * every step's result while the steps run back to back. */
 int sph_box_state_bytes(const SphHandle *h, uint64_t *bytes);
 int sph_get_boxes_async(SphHandle *h, void *staging, uint64_t staging_bytes);
 int sph_step_async_states(SphHandle *h, uint64_t nsteps, void *states, uint64_t states_bytes);
-int sph_boxes_from_staging(SphHandle *h, const void *staging, SphBox *boxes);
+int sph_boxes_from_staging(SphHandle *h, const void *staging, uint64_t nstates, SphBox *boxes);
 
 /* Contact bookkeeping in the reference's slot form (src/device.cu:428-432):
  * contacts [np][NC] (partner index local to the box, np_box = empty),

@@ -213,7 +213,7 @@ def load_library():
     lib.sph_get_boxes_async.restype = C.c_int
     lib.sph_step_async_states.argtypes = [H, C.c_uint64, C.c_void_p, C.c_uint64]
     lib.sph_step_async_states.restype = C.c_int
-    lib.sph_boxes_from_staging.argtypes = [H, C.c_void_p, C.POINTER(SphBox)]
+    lib.sph_boxes_from_staging.argtypes = [H, C.c_void_p, C.c_uint64, C.POINTER(SphBox)]
     lib.sph_boxes_from_staging.restype = C.c_int
     lib.sph_render.argtypes = [H, C.c_uint32, C.c_int, C.c_float, C.c_float, C.c_float,
                                C.c_uint32, C.c_uint32, C.POINTER(C.c_uint8)]

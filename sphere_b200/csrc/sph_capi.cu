@@ -385,16 +385,23 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_m
     return SPH_OK;
 }
 
-static int check_particles(SphHandle *h, const SphParticles *p)
+// One pass over the particles, which also gives each box's largest and
+// smallest radius (0 for an empty box).
+static int check_particles(SphHandle *h, const SphParticles *p, std::vector<double> &rmax_box,
+                           std::vector<double> &rmin_box)
 {
     char buf[256];
+    rmax_box.assign(h->nbox, 0.0);
+    rmin_box.assign(h->nbox, 0.0);
     for (uint32_t k = 0; k < h->nbox; ++k) {
         const DevBox &d = h->dbox[k];
         const SphBox &b = h->boxes[k];
-        double zmax = 0.0;
+        double zmax = 0.0, rmax = 0.0, rmin = HUGE_VAL;
         for (uint32_t j = 0; j < d.np; ++j) {
             const double *x = p->x + 4 * (size_t)(d.p_base + j);
             const double *v = p->vel + 4 * (size_t)(d.p_base + j);
+            rmax = fmax(rmax, x[3]);
+            rmin = fmin(rmin, x[3]);
             if (!(x[3] > 0.0)) {
                 snprintf(buf, sizeof buf, "box %u particle %u has a radius of %g m", k, j, x[3]);
                 return fail(h, SPH_ERR_INPUT, buf);
@@ -412,6 +419,8 @@ static int check_particles(SphHandle *h, const SphParticles *p)
             }
             if (x[2] > zmax) zmax = x[2];
         }
+        rmax_box[k] = rmax;
+        rmin_box[k] = d.np ? rmin : 0.0;
         if (b.walls.nw > 0 && b.walls.nx[0][3] < zmax) {
             snprintf(buf, sizeof buf,
                      "box %u: one or more particles have centres above the upper, dynamic wall", k);
@@ -492,7 +501,8 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
     if (n > 0 && (!p->x || !p->vel)) return fail(h, SPH_ERR_INPUT, "x and vel are required");
     if (nb > 0 && (!b || !b->pairs)) return fail(h, SPH_ERR_INPUT, "bond pairs are required");
     int st;
-    if ((st = check_particles(h, p)) != SPH_OK) return st;
+    std::vector<double> rmax_in, rmin_in;
+    if ((st = check_particles(h, p, rmax_in, rmin_in)) != SPH_OK) return st;
     StepArgs &A = h->A;
     cudaStreamSynchronize(h->stream);
     if (n > 0) {
@@ -517,8 +527,9 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
 
     // bonds (local indexes) and the per-particle list of bond endpoints in
     // ascending bond order
-    std::vector<uint32_t> cnt(n + 1, 0);
+    std::vector<uint32_t> cnt;
     if (nb > 0) {
+        cnt.assign(n + 1, 0);
         std::vector<uint2> pairs(nb);
         std::vector<double4> dl(nb), om(nb);
         for (uint32_t k = 0; k < h->nbox; ++k) {
@@ -561,8 +572,11 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
         CUDA_TRY(h, cudaMemcpy((void *)A.bcsr_ent, ent.data(), sizeof(uint32_t) * ent.size(),
                                cudaMemcpyHostToDevice));
     }
-    CUDA_TRY(h, cudaMemcpy((void *)A.bcsr_off, cnt.data(), sizeof(uint32_t) * (n + 1),
-                           cudaMemcpyHostToDevice));
+    if (nb > 0)
+        CUDA_TRY(h, cudaMemcpy((void *)A.bcsr_off, cnt.data(), sizeof(uint32_t) * (n + 1),
+                               cudaMemcpyHostToDevice));
+    else
+        CUDA_TRY(h, cudaMemset((void *)A.bcsr_off, 0, sizeof(uint32_t) * (n + 1)));
     // a new run: time state from the boxes, TY3 iteration counter at zero
     for (uint32_t k = 0; k < h->nbox; ++k) {
         init_dev_box(h->dbox[k], h->boxes[k]);
@@ -584,8 +598,8 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
             // FP32 prefilter margin: bounds the rounding of FP32 coordinates
             // (|x| <= 2 max L), their differences and periodic shifts, and
             // of the reference's FP32-rounded lengths, with room to spare.
-            double rmax = 0.0, lmax = 0.0;
-            for (uint32_t j = 0; j < d.np; ++j) rmax = fmax(rmax, p->x[4 * (size_t)(d.p_base + j) + 3]);
+            const double rmax = rmax_in[k];
+            double lmax = 0.0;
             for (int c = 0; c < 3; ++c) lmax = fmax(lmax, fabs(d.L[c]) + fabs(d.origo[c]));
             d.pre_margin = (float)(ldexp(2.0 * lmax + 2.0 * rmax, -19));
             h->rmax_box.resize(h->nbox);
@@ -594,8 +608,7 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
             // sphere has moved half the skin less the rounding allowance;
             // the build searches the cells that can hold a sphere within
             // 2 r_max + skin (up to +-3 cells, else lists are off)
-            double rmin = rmax;
-            for (uint32_t j = 0; j < d.np; ++j) rmin = fmin(rmin, p->x[4 * (size_t)(d.p_base + j) + 3]);
+            const double rmin = rmin_in[k];
             const double skin = 0.1 * rmin;
             const double cmin = fmin(d.L[0] / d.num[0], fmin(d.L[1] / d.num[1], d.L[2] / d.num[2]));
             const double half = 0.5 * skin - 4.0 * (double)d.pre_margin;
@@ -968,12 +981,15 @@ int sph_get_boxes_async(SphHandle *h, void *staging, uint64_t staging_bytes)
     return SPH_OK;
 }
 
-int sph_boxes_from_staging(SphHandle *h, const void *staging, SphBox *boxes)
+int sph_boxes_from_staging(SphHandle *h, const void *staging, uint64_t nstates, SphBox *boxes)
 {
-    if (!h || !staging || !boxes) return SPH_ERR_INPUT;
+    if (!h || (nstates && (!staging || !boxes))) return SPH_ERR_INPUT;
     std::vector<DevBox> d(h->nbox);
-    memcpy(d.data(), staging, sizeof(DevBox) * h->nbox);
-    boxes_from(h, d, boxes);
+    const uint8_t *src = static_cast<const uint8_t *>(staging);
+    for (uint64_t s = 0; s < nstates; ++s) {
+        memcpy(d.data(), src + s * sizeof(DevBox) * h->nbox, sizeof(DevBox) * h->nbox);
+        boxes_from(h, d, boxes + s * h->nbox);
+    }
     return SPH_OK;
 }
 

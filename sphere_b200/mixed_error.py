@@ -26,7 +26,7 @@ def _run(sim, precision, nsteps, slices, device, cuda_stream, max_slices=0):
         states = numpy.zeros((nsteps, nbs), dtype=numpy.uint8)
         st.step_async_states(nsteps, states)
         code = st.sync(raise_on_error=False)
-        boxes = [st.boxes_from_state(states[k])[0] for k in range(nsteps)]
+        boxes = [b[0] for b in st.boxes_from_states(states, nsteps)]
         if slices is None:
             # slabs thicker than 2 r_max (src/sphere.cpp:492-515), one to
             # spare so that both forms' wall positions allow the same count

@@ -324,12 +324,22 @@ class Stepper(object):
 
     def boxes_from_state(self, state):
         """SphBox records (as boxes() returns them) from one raw state."""
-        assert state.dtype == numpy.uint8 and state.flags["C_CONTIGUOUS"]
-        assert state.nbytes >= self.box_state_bytes()
-        out = (_abi.SphBox * len(self.sims))()
-        self._check(self.lib.sph_boxes_from_staging(self.h, C.c_void_p(state.ctypes.data), out),
+        return self.boxes_from_states(state, 1)[0]
+
+    def boxes_from_states(self, states, nstates=None):
+        """Per state, the list of SphBox records, from `nstates` raw states
+        (default: all rows of `states`), decoded in one call."""
+        assert states.dtype == numpy.uint8 and states.flags["C_CONTIGUOUS"]
+        nb = self.box_state_bytes()
+        if nstates is None:
+            nstates = states.nbytes // nb
+        assert states.nbytes >= nstates * nb
+        nbox = len(self.sims)
+        out = (_abi.SphBox * (nstates * nbox))()
+        self._check(self.lib.sph_boxes_from_staging(self.h, C.c_void_p(states.ctypes.data),
+                                                    int(nstates), out),
                     "sph_boxes_from_staging")
-        return list(out)
+        return [list(out[k * nbox:(k + 1) * nbox]) for k in range(nstates)]
 
     def contacts(self):
         n = self.ntot

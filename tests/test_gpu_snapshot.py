@@ -57,7 +57,9 @@ def _box_fields(b):
 @pytest.mark.parametrize("name,nsteps", [("periodic_xy_wall_stress", 9),
                                          ("periodic_x_wall_velocity", 6),
                                          ("shear_stress_wall", 5), ("adaptive_grid", 7),
-                                         ("walls_all_sides", 1)])
+                                         ("walls_all_sides", 1),
+                                         # more steps than the 128-step ring
+                                         ("fixvel_modes", 300)])
 def test_step_states_equal_a_read_after_every_step(name, nsteps):
     # two boxes in one handle; the queued run (the wall stage beside the
     # next step where the handle allows it) against one synchronous read
@@ -73,12 +75,15 @@ def test_step_states_equal_a_read_after_every_step(name, nsteps):
     states = numpy.zeros((nsteps, nb), dtype=numpy.uint8)
     a.step_async_states(nsteps, states)
     a.sync()
+    bulk = a.boxes_from_states(states)
+    assert len(bulk) == nsteps
     for k in range(nsteps):
         b.step(1)
         want = b.boxes()
         got = a.boxes_from_state(states[k])
-        for bw, bg in zip(want, got):
+        for bw, bg, bb in zip(want, got, bulk[k]):
             assert _box_fields(bg) == _box_fields(bw), (name, k)
+            assert _box_fields(bb) == _box_fields(bw), (name, k)
     fa, _ = a.download()
     fb, _ = b.download()
     assert numpy.array_equal(fa.x, fb.x)

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "sph_device.cuh"
@@ -385,39 +386,90 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_m
     return SPH_OK;
 }
 
-// One pass over the particles, which also gives each box's largest and
-// smallest radius (0 for an empty box).
+// The checks of one particle range [j0, j1) of a box: the first failing
+// particle (bad, with kind 1 radius, 2 NaN, 3 outside the grid) stops the
+// range; otherwise the range's largest z and largest/smallest radius.
+struct CheckRange {
+    uint32_t bad = UINT32_MAX;
+    int kind = 0;
+    double zmax = 0.0, rmax = 0.0, rmin = HUGE_VAL;
+};
+
+static void check_range(const SphParticles *p, const SphBox &b, uint64_t base, uint32_t j0,
+                        uint32_t j1, CheckRange &r)
+{
+    for (uint32_t j = j0; j < j1; ++j) {
+        const double *x = p->x + 4 * (size_t)(base + j);
+        const double *v = p->vel + 4 * (size_t)(base + j);
+        r.rmax = fmax(r.rmax, x[3]);
+        r.rmin = fmin(r.rmin, x[3]);
+        int kind = 0;
+        if (!(x[3] > 0.0)) kind = 1;
+        else {
+            for (int c = 0; c < 4; ++c)
+                if (x[c] != x[c] || v[c] != v[c]) kind = 2;
+            if (!kind && (x[0] < b.grid.origo[0] || x[1] < b.grid.origo[1] ||
+                          x[2] < b.grid.origo[2] || x[0] > b.grid.L[0] || x[1] > b.grid.L[1] ||
+                          x[2] > b.grid.L[2]))
+                kind = 3;
+        }
+        if (kind) {
+            r.bad = j;
+            r.kind = kind;
+            return;
+        }
+        if (x[2] > r.zmax) r.zmax = x[2];
+    }
+}
+
+// One pass over the particles (split over host threads for large boxes),
+// which also gives each box's largest and smallest radius (0 for an empty
+// box).  The error reported is that of the first failing particle in index
+// order, as a sequential pass finds it.
 static int check_particles(SphHandle *h, const SphParticles *p, std::vector<double> &rmax_box,
                            std::vector<double> &rmin_box)
 {
     char buf[256];
     rmax_box.assign(h->nbox, 0.0);
     rmin_box.assign(h->nbox, 0.0);
+    const unsigned hw = std::thread::hardware_concurrency();
     for (uint32_t k = 0; k < h->nbox; ++k) {
         const DevBox &d = h->dbox[k];
         const SphBox &b = h->boxes[k];
+        const uint32_t nt = d.np >= (1u << 17) ? std::max(1u, std::min(8u, hw)) : 1u;
+        std::vector<CheckRange> res(nt);
+        const uint32_t per = (d.np + nt - 1) / nt;
+        std::vector<std::thread> pool;
+        for (uint32_t t = 1; t < nt; ++t) {
+            const uint32_t j0 = std::min(d.np, t * per), j1 = std::min(d.np, (t + 1) * per);
+            try {
+                pool.emplace_back(check_range, p, std::cref(b), (uint64_t)d.p_base, j0, j1,
+                                  std::ref(res[t]));
+            } catch (...) {
+                check_range(p, b, d.p_base, j0, j1, res[t]);   // no thread to be had
+            }
+        }
+        check_range(p, b, d.p_base, 0, std::min(d.np, per), res[0]);
+        for (auto &th : pool) th.join();
         double zmax = 0.0, rmax = 0.0, rmin = HUGE_VAL;
-        for (uint32_t j = 0; j < d.np; ++j) {
-            const double *x = p->x + 4 * (size_t)(d.p_base + j);
-            const double *v = p->vel + 4 * (size_t)(d.p_base + j);
-            rmax = fmax(rmax, x[3]);
-            rmin = fmin(rmin, x[3]);
-            if (!(x[3] > 0.0)) {
-                snprintf(buf, sizeof buf, "box %u particle %u has a radius of %g m", k, j, x[3]);
+        for (const CheckRange &r : res) {
+            if (r.kind == 1) {
+                snprintf(buf, sizeof buf, "box %u particle %u has a radius of %g m", k, r.bad,
+                         p->x[4 * (size_t)(d.p_base + r.bad) + 3]);
                 return fail(h, SPH_ERR_INPUT, buf);
             }
-            for (int c = 0; c < 4; ++c)
-                if (x[c] != x[c] || v[c] != v[c]) {
-                    snprintf(buf, sizeof buf, "box %u particle %u has NaN values", k, j);
-                    return fail(h, SPH_ERR_INPUT, buf);
-                }
-            if (x[0] < b.grid.origo[0] || x[1] < b.grid.origo[1] || x[2] < b.grid.origo[2] ||
-                x[0] > b.grid.L[0] || x[1] > b.grid.L[1] || x[2] > b.grid.L[2]) {
+            if (r.kind == 2) {
+                snprintf(buf, sizeof buf, "box %u particle %u has NaN values", k, r.bad);
+                return fail(h, SPH_ERR_INPUT, buf);
+            }
+            if (r.kind == 3) {
                 snprintf(buf, sizeof buf, "box %u particle %u is outside of the computational grid",
-                         k, j);
+                         k, r.bad);
                 return fail(h, SPH_ERR_INPUT, buf);
             }
-            if (x[2] > zmax) zmax = x[2];
+            zmax = fmax(zmax, r.zmax);
+            rmax = fmax(rmax, r.rmax);
+            rmin = fmin(rmin, r.rmin);
         }
         rmax_box[k] = rmax;
         rmin_box[k] = d.np ? rmin : 0.0;

@@ -51,6 +51,32 @@ def test_bad_positions_are_refused_at_upload():
         st.close()
 
 
+def test_first_bad_particle_is_named_in_a_large_box():
+    # a box large enough for the check to be split over host threads: the
+    # message names the first failing particle in index order
+    from sphere_b200 import scenes
+    s = scenes.lattice_pack(200000, seed=5, periodic=1, nw=0)
+    n = int(s.np[0])
+    late, later = n - 7, n - 3
+    s.x[later, 0] = numpy.nan
+    s.radius[late] = -1.0
+    st = Stepper([s], precision="fp64")
+    with pytest.raises(SphereError) as e:
+        st.upload()
+    assert e.value.status == _status("SPH_ERR_INPUT")
+    assert "particle %d has a radius" % late in str(e.value)
+    s.radius[late] = float(numpy.median(s.radius))
+    with pytest.raises(SphereError) as e:
+        st.upload()
+    assert "particle %d has NaN values" % later in str(e.value)
+    s.x[later, 0] = s.x[later - 1, 0]
+    s.x[n // 3, 2] = 10.0 * float(s.L[2])
+    with pytest.raises(SphereError) as e:
+        st.upload()
+    assert "particle %d is outside" % (n // 3) in str(e.value)
+    st.close()
+
+
 def test_sphere_leaving_the_grid_is_reported():
     """A sphere that crosses the top of the grid during the steps (walls on
     all sides are implicit in the reference only at L; z is never

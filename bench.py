@@ -300,6 +300,55 @@ def time_bonded(device, stream, n=200000, nbonds=300000, steps=200):
             "variant_ms_per_step": variant_ms, "device_status": code}
 
 
+def time_settling(device, stream, n=10000, steps=1000):
+    """The FP64 gravity-settling workload (scenes.gravity_settling: 10,000
+    spheres U[0.010, 0.012] m on a jittered cubic lattice, 0.5 x 0.5 m box
+    with wall sides, k_n = k_t = 1.16e9, no damping, mu = 0.5,
+    dt = 0.17 sqrt(m_min / k_n)), its whole run of 1,000 steps queued at once
+    and timed with CUDA events on the launching stream: a small box whose
+    step time is set by launch latency and the few dependent kernels of a
+    step, not by bandwidth."""
+    import torch
+    from sphere_b200 import scenes
+    from sphere_b200.runner import Stepper
+    s = scenes.gravity_settling(n=n, seed=0, steps=steps)
+    st = Stepper([s], precision="fp64", length="reference", device=device)
+    st.set_stream(stream.cuda_stream)
+    st.upload()
+    variant, variant_ms = st.autotune(steps=20)
+    st.step(5)
+    st.upload()    # the timed run starts from the workload's initial state
+    st.step(3)     # graphs of the overlapped steps instantiated, untimed
+    st.upload()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    launches0 = st.kernel_launches()
+    start.record(stream)
+    st.step_async(steps)
+    end.record(stream)
+    end.synchronize()
+    code = st.sync(raise_on_error=False)
+    ms = start.elapsed_time(end)
+    launches = st.kernel_launches() - launches0
+    st.close()
+    return {"workload": "FP64 gravity settling, %d spheres U[0.010, 0.012] m, jittered cubic "
+                        "lattice (spacing 2.5 r_max), 0.5 x 0.5 x 1.25 m box with wall sides, "
+                        "k_n=k_t=1.16e9, gamma=0, mu=0.5, dt=0.17 sqrt(m_min/k_n), %d steps "
+                        "(the whole run)" % (n, steps),
+            "value": n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "spheres": n, "variant": variant,
+            "variant_ms_per_step": variant_ms, "gpu_launches": launches,
+            "device_status": code}
+
+
+def bench_config(args):
+    """The `config` object of the JSON line, the same in both arms."""
+    return {"workload": WORKLOAD, "spheres_per_gpu": args.n, "length_mode": "reference",
+            "l2": "working set > L2 (no flush needed)",
+            "parallelism": "replicas only (one independent pack per GPU)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -313,6 +362,10 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-bonded", action="store_true")
+    ap.add_argument("--no-settling", action="store_true")
+    ap.add_argument("--ref-n", type=int, default=100000,
+                    help="spheres of the reference arm's sample of the workload (the same "
+                         "construction, packed on the CPU)")
     ap.add_argument("--no-long-run", action="store_true",
                     help="skip the mixed-vs-FP64 comparison over the whole run")
     ap.add_argument("--kernel-tour", action="store_true",
@@ -329,19 +382,37 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
+        # The reference's own step kernels compiled for the CPU
+        # (oracle/_ref), all host threads, on a bounded sample of the
+        # workload: the same construction (log-normal FCC start, the packing
+        # sweeps, radii grown, shear set-up) at args.ref_n spheres, packed
+        # on the CPU by the C restatement of the packing sweeps, which gives
+        # the GPU's pack bit for bit.  Nothing of this arm runs on a GPU or
+        # loads this project's CUDA library.
         if rank != 0:
             return 0
-        s = make_scene(args.n, 0, local, args.pack_sweeps)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        from sphere_b200 import scenes
+        nref = min(args.ref_n, args.n)
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        s = scenes.sheared_dense_pack(
+            n=nref, seed=0, sweeps=args.pack_sweeps,
+            relax=lambda q, k, a, z: O.relax(q, k, alpha=a, z_top=z, nthreads=threads))
+        t_pack = time.perf_counter() - t0
         rate, done, secs, threads, kind, warm = cpu_reference_rate(s, args.steps, 120.0,
                                                                    warmup=args.warmup)
+        sample = ("%d whole steps after %d untimed ones, of the workload's construction at "
+                  "%d spheres (packed on the CPU in %.0f s by the packing sweeps' C "
+                  "restatement)" % (done, warm, nref, t_pack))
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
                 "n_gpus": args.gpus, "steps": done, "warmup": warm,
                 "ms_per_step": secs / done * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "spheres": args.n},
+                "config": bench_config(args),
                 "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-                                 "sample": "%d whole steps of the %d-sphere pack after %d "
-                                           "untimed ones" % (done, args.n, warm)},
+                                 "sample": sample},
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -610,6 +681,9 @@ def main():
     bonded = None
     if rank == 0 and not args.no_bonded:
         bonded = time_bonded(local, stream)
+    settling = None
+    if rank == 0 and not args.no_settling:
+        settling = time_settling(local, stream)
     long_run = None
     if rank == 0 and not args.no_long_run and "mixed" in res and "fp64" in res:
         # the mixed form's error against the FP64 form over the workload's
@@ -633,10 +707,8 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if head == "fp64" else "f64+f32",
         "data": "synthetic (seeded GPU-relaxed pack per rank)",
-        "config": {"workload": WORKLOAD, "spheres_per_gpu": n, "precision": head,
-                   "forms_timed": forms, "length_mode": "reference",
-                   "l2": "working set > L2 (no flush needed)",
-                   "parallelism": "replicas only (one independent pack per GPU)"},
+        "config": bench_config(args),
+        "precision": head, "forms_timed": forms,
         "roofline": H["roofline"],
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -657,6 +729,8 @@ def main():
         line["ensemble"] = ens
     if bonded is not None:
         line["bonded"] = bonded
+    if settling is not None:
+        line["settling"] = settling
     if long_run is not None:
         line["mixed_error_long_run"] = long_run
     print(json.dumps(line))

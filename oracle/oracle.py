@@ -52,9 +52,23 @@ class OrState(C.Structure):
 _loaded = {}
 
 
+def reference_root():
+    """The reference's checkout: $SPHERE_REFERENCE, else a directory named
+    'reference' beside this repository; None when neither exists (the
+    reference builds and the tests that read its files are then skipped)."""
+    cand = os.environ.get("SPHERE_REFERENCE") or os.path.join(
+        os.path.dirname(os.path.dirname(HERE)), "reference")
+    return cand if os.path.isdir(os.path.join(cand, "src")) else None
+
+
 def build():
-    """Compile the CPU oracles in place (make -C oracle)."""
-    subprocess.check_call(["make", "-s", "-C", HERE])
+    """Compile the CPU oracles in place (make -C oracle); the reference's
+    kernels too when its checkout is found (reference_root)."""
+    env = dict(os.environ)
+    root = reference_root()
+    if root:
+        env["SPHERE_REFERENCE"] = root
+    subprocess.check_call(["make", "-s", "-C", HERE], env=env)
 
 
 def available(which):
@@ -310,3 +324,26 @@ def reference_render(s, method=1, maxval=1.0e3, lower_cutoff=0.0, width=800, hei
     if r.returncode != 0:
         raise RuntimeError(r.stderr)
     return numpy.fromfile(out, dtype=numpy.uint8).reshape(int(height), int(width), 3)
+
+
+def relax(s, sweeps, alpha=0.6, z_top=1e300, nthreads=0):
+    """The packing sweeps of sph_relax (sphere_b200 scene preparation) on
+    the CPU, restated in C (or_relax): moves s.x in place for one box and
+    returns the largest overlap of the last sweep.  Bit for bit the GPU's
+    result (the checker of sph_relax, and the CPU packer of bench.py's
+    reference arm)."""
+    lib = C.CDLL(LIBS["oracle"])
+    dp = C.POINTER(C.c_double)
+    lib.or_relax.argtypes = [dp, C.c_uint32, dp, dp, C.POINTER(C.c_uint32), C.c_int, C.c_uint32,
+                             C.c_double, C.c_double, C.c_int, dp]
+    lib.or_relax.restype = None
+    x = _f4(s.x, s.radius)
+    origo = numpy.ascontiguousarray(s.origo, dtype=numpy.float64)
+    L = numpy.ascontiguousarray(s.L, dtype=numpy.float64)
+    num = numpy.ascontiguousarray(s.num, dtype=numpy.uint32)
+    worst = C.c_double(0.0)
+    lib.or_relax(_dp(x), int(s.np[0]), _dp(origo), _dp(L), num.ctypes.data_as(C.POINTER(C.c_uint32)),
+                 int(s.periodic[0]), int(sweeps), float(alpha), float(z_top), int(nthreads),
+                 C.byref(worst))
+    s.x = x[:, :3].copy()
+    return worst.value

@@ -1069,3 +1069,158 @@ void or_render(const double *x, const double *vel, const double *angvel, const d
         px[2] = (uint8_t)((k_d * I_d * dotprod + k_a * I_a) * bluev);
     }
 }
+
+/* ------------------------------------------------------------ packing sweep */
+
+/* The project's scene-preparation sweep (sphere_b200 sph_relax: kernels
+ * k_hash, k_place, k_relax, k_relax_apply; no counterpart in the reference,
+ * whose packs come from running the DEM itself), restated for one box as the
+ * checker of that kernel chain and as a CPU packer for bench.py's reference
+ * arm.  Per sweep: spheres binned into the grid's cells (cell ids clamped
+ * into the grid), ordered by cell and, within a cell, by index; for each
+ * sphere in that order, every overlapping sphere of the 27 cells around it
+ * (periodic images by the rule of calc_cell_id / find_dist_mod, visited in
+ * (z, y, x) order, a cell's spheres in index order) adds alpha * overlap / 2
+ * along the centre line; the floor, the ceiling z_top and the side walls of
+ * non-periodic axes push back; then every sphere moves (Jacobi), periodic
+ * axes wrap, and positions are clamped into [origo, L (1 - 1e-12)].
+ * x4: [np][4] (x, y, z, r), updated.  *max_ov: the largest overlap seen in
+ * the last sweep.  Arithmetic in the operand order of the CUDA kernels,
+ * without contraction, so the result is the GPU's bit for bit. */
+void or_relax(double *x4, uint32_t np, const double origo[3], const double L[3],
+              const uint32_t num[3], int periodic, uint32_t sweeps, double alpha, double z_top,
+              int nthreads, double *max_ov)
+{
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    const size_t ncells = (size_t)num[0] * num[1] * num[2];
+    uint32_t *cell = (uint32_t *)malloc(sizeof(uint32_t) * (np ? np : 1));
+    uint32_t *off = (uint32_t *)calloc(ncells + 1, sizeof(uint32_t));
+    uint32_t *perm = (uint32_t *)malloc(sizeof(uint32_t) * (np ? np : 1));
+    double *xs = (double *)malloc(sizeof(double) * 4 * (np ? np : 1));
+    double *disp = (double *)malloc(sizeof(double) * 3 * (np ? np : 1));
+    double worst_all = 0.0;
+    for (uint32_t sw = 0; sw < sweeps; ++sw) {
+        memset(off, 0, sizeof(uint32_t) * (ncells + 1));
+        for (uint32_t i = 0; i < np; ++i) {
+            unsigned c[3];
+            for (int d = 0; d < 3; ++d) {
+                double f = floor((x4[4 * (size_t)i + d] - origo[d]) / (L[d] / num[d]));
+                if (!(f >= 0.0)) f = 0.0;
+                if (f >= (double)num[d]) f = (double)(num[d] - 1);
+                c[d] = (unsigned)f;
+            }
+            cell[i] = (c[2] * num[1]) * num[0] + c[1] * num[0] + c[0];
+            off[cell[i] + 1]++;
+        }
+        for (size_t k = 0; k < ncells; ++k) off[k + 1] += off[k];
+        {
+            uint32_t *fill = (uint32_t *)malloc(sizeof(uint32_t) * (ncells ? ncells : 1));
+            memcpy(fill, off, sizeof(uint32_t) * ncells);
+            for (uint32_t i = 0; i < np; ++i) {   /* ascending index within a cell */
+                const uint32_t a = fill[cell[i]]++;
+                perm[a] = i;
+                memcpy(xs + 4 * (size_t)a, x4 + 4 * (size_t)i, 4 * sizeof(double));
+            }
+            free(fill);
+        }
+        double worst = 0.0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(max : worst)
+        for (long long aa = 0; aa < (long long)np; ++aa) {
+            const uint32_t a = (uint32_t)aa;
+            const double *xa = xs + 4 * (size_t)a;
+            int g[3];
+            for (int d = 0; d < 3; ++d) g[d] = (int)floor((xa[d] - origo[d]) / (L[d] / num[d]));
+            double dx = 0.0, dy = 0.0, dz = 0.0, w = 0.0;
+            for (int oz = -1; oz < 2; ++oz)
+                for (int oy = -1; oy < 2; ++oy)
+                    for (int ox = -1; ox < 2; ++ox) {
+                        int tx = g[0] + ox, ty = g[1] + oy;
+                        const int tz = g[2] + oz;
+                        int sx = 0, sy = 0;
+                        const int nx = (int)num[0], ny = (int)num[1], nz = (int)num[2];
+                        if (periodic == 1) {
+                            if (tx < 0) { tx += nx; sx = 1; }
+                            if (tx >= nx) { tx -= nx; sx = -1; }
+                            if (ty < 0) { ty += ny; sy = 1; }
+                            if (ty >= ny) { ty -= ny; sy = -1; }
+                        } else if (periodic == 2) {
+                            if (tx < 0) { tx += nx; sx = 1; }
+                            if (tx >= nx) { tx -= nx; sx = -1; }
+                            if (ty < 0 || ty >= ny) continue;
+                        } else {
+                            if (tx < 0 || tx >= nx || ty < 0 || ty >= ny) continue;
+                        }
+                        if (tz < 0 || tz >= nz) continue;
+                        if (tx < 0 || tx >= nx || ty < 0 || ty >= ny) continue;
+                        const double dmx = sx == 0 ? 0.0 : (sx > 0 ? L[0] : -L[0]);
+                        const double dmy = sy == 0 ? 0.0 : (sy > 0 ? L[1] : -L[1]);
+                        const double dmz = 0.0;
+                        const uint32_t c = (uint32_t)(tx + ty * nx + (nx * ny) * tz);
+                        for (uint32_t b = off[c]; b < off[c + 1]; ++b) {
+                            if (b == a) continue;
+                            const double *xb = xs + 4 * (size_t)b;
+                            const double rx = xa[0] - xb[0] + dmx, ry = xa[1] - xb[1] + dmy,
+                                         rz = xa[2] - xb[2] + dmz;
+                            const double len = sqrt(rx * rx + ry * ry + rz * rz);
+                            const double ov = xa[3] + xb[3] - len;
+                            if (ov > 0.0 && len > 0.0) {
+                                const double s = 0.5 * alpha * ov / len;
+                                dx += s * rx;
+                                dy += s * ry;
+                                dz += s * rz;
+                                w = fmax(w, ov);
+                            }
+                        }
+                    }
+            const double below = (origo[2] + xa[3]) - xa[2];
+            if (below > 0.0) { dz += below; w = fmax(w, below); }
+            const double above = xa[2] + xa[3] - z_top;
+            if (above > 0.0) { dz -= above; w = fmax(w, above); }
+            if (periodic == 0) {
+                const double lo = (origo[0] + xa[3]) - xa[0], hi = xa[0] + xa[3] - L[0];
+                if (lo > 0.0) { dx += lo; w = fmax(w, lo); }
+                if (hi > 0.0) { dx -= hi; w = fmax(w, hi); }
+            }
+            if (periodic != 1) {
+                const double lo = (origo[1] + xa[3]) - xa[1], hi = xa[1] + xa[3] - L[1];
+                if (lo > 0.0) { dy += lo; w = fmax(w, lo); }
+                if (hi > 0.0) { dy -= hi; w = fmax(w, hi); }
+            }
+            double *d = disp + 3 * (size_t)perm[a];
+            d[0] = dx;
+            d[1] = dy;
+            d[2] = dz;
+            if (w > worst) worst = w;
+        }
+#pragma omp parallel for schedule(static)
+        for (long long ii = 0; ii < (long long)np; ++ii) {
+            double *x = x4 + 4 * (size_t)ii;
+            const double *d = disp + 3 * (size_t)ii;
+            x[0] += d[0];
+            x[1] += d[1];
+            x[2] += d[2];
+            if (periodic == 1 || periodic == 2) {
+                if (x[0] < origo[0]) x[0] += L[0] - origo[0];
+                if (x[0] >= L[0]) x[0] -= L[0] - origo[0];
+            }
+            if (periodic == 1) {
+                if (x[1] < origo[1]) x[1] += L[1] - origo[1];
+                if (x[1] >= L[1]) x[1] -= L[1] - origo[1];
+            }
+            x[0] = fmin(fmax(x[0], origo[0]), L[0] * (1.0 - 1e-12));
+            x[1] = fmin(fmax(x[1], origo[1]), L[1] * (1.0 - 1e-12));
+            x[2] = fmin(fmax(x[2], origo[2]), L[2] * (1.0 - 1e-12));
+        }
+        worst_all = worst;
+    }
+    if (max_ov) *max_ov = worst_all;
+    free(cell);
+    free(off);
+    free(perm);
+    free(xs);
+    free(disp);
+}

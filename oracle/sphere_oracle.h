@@ -70,6 +70,13 @@ uint64_t or_overlaps(const double *x, const double *vel, uint32_t np, uint64_t m
 void or_render(const double *x, const double *vel, const double *angvel, const double *angpos,
                const double *xyzsum, const double *p, uint32_t np, const double *L, int method,
                float maxval, float lower_cutoff, uint32_t width, uint32_t height, uint8_t *rgb);
+/* Packing sweeps of the project's scene preparation (sph_relax), restated
+ * for one box (TEST INFRASTRUCTURE, and the CPU packer of bench.py's
+ * reference arm): x4 [np][4] updated in place, *max_ov = the largest overlap
+ * of the last sweep. */
+void or_relax(double *x4, uint32_t np, const double origo[3], const double L[3],
+              const uint32_t num[3], int periodic, uint32_t sweeps, double alpha, double z_top,
+              int nthreads, double *max_ov);
 int ref_step(OrState *s, uint64_t nsteps);
 
 #ifdef __cplusplus

@@ -176,24 +176,37 @@ def _fcc_start(n, rng, r, porosity, aspect_z, zlift, sid):
     return s, H
 
 
-def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.005, 0.02),
-               aspect_z=0.5, sweeps=3000, alpha=0.6, inflate=2.0e-7, device=-1, sid="dense"):
-    """A dense x-y periodic pack of n log-normal spheres at the given
-    porosity, made on the GPU: FCC lattice start in a box of aspect
-    1 : 1 : aspect_z sized for the porosity, then geometric overlap removal
-    (sph_relax) between the floor and the box top, then radii grown by the
-    factor (1 + inflate) so that touching spheres overlap by ~inflate * r
-    and form contacts.  Returns the sim (no walls yet) and the largest
-    residual overlap of the relaxation."""
+def gpu_relax(s, sweeps, alpha, z_top, device=-1):
+    """Overlap removal of one box on the GPU (sph_relax): moves s.x and
+    returns the largest overlap of the last sweep."""
     from .runner import Stepper
+    st = Stepper([s], device=device)
+    st.upload()
+    worst = st.relax(sweeps, alpha=alpha, z_top=z_top)
+    hp, _ = st.download()
+    st.close()
+    s.x = hp.x[:, :3].copy()
+    return worst
+
+
+def dense_pack(n, seed=0, porosity=0.40, median=0.01, sigma_ln=0.2, r_clip=(0.005, 0.02),
+               aspect_z=0.5, sweeps=3000, alpha=0.6, inflate=2.0e-7, device=-1, sid="dense",
+               relax=None):
+    """A dense x-y periodic pack of n log-normal spheres at the given
+    porosity: FCC lattice start in a box of aspect 1 : 1 : aspect_z sized
+    for the porosity, then geometric overlap removal between the floor and
+    the box top (`relax(s, sweeps, alpha, z_top)`, by default sph_relax on
+    GPU `device`; any function with the same sweeps gives the same pack),
+    then radii grown by the factor (1 + inflate) so that touching spheres
+    overlap by ~inflate * r and form contacts.  Returns the sim (no walls
+    yet) and the largest residual overlap of the relaxation."""
     rng = numpy.random.default_rng(seed)
     r = numpy.clip(numpy.exp(rng.normal(math.log(median), sigma_ln, n)), *r_clip)
     s, H = _fcc_start(n, rng, r, porosity, aspect_z, median, sid)
-    st = Stepper([s], device=device)
-    st.upload()
-    worst = st.relax(sweeps, alpha=alpha, z_top=H)
-    st.to_sims()
-    st.close()
+    if relax is None:
+        worst = gpu_relax(s, sweeps, alpha, H, device=device)
+    else:
+        worst = relax(s, sweeps, alpha, H)
     s.radius *= 1.0 + inflate
     s.time_current[0] = 0.0
     return s, worst
@@ -315,7 +328,7 @@ def shear_ensemble(nboxes=256, seed=0, device=-1, counts=(500, 20000), r_range=(
     return sims
 
 
-def sheared_dense_pack(n=1000000, seed=0, device=-1, sweeps=3000):
+def sheared_dense_pack(n=1000000, seed=0, device=-1, sweeps=3000, relax=None):
     """The 1e6-sphere sheared dense pack: log-normal radii (median 0.01 m,
     sigma_ln 0.2, clipped to [0.005, 0.02]) packed to porosity ~0.40 in an
     x-y periodic box of aspect 1:1:0.5 (dense_pack, on the GPU), a top wall
@@ -323,8 +336,9 @@ def sheared_dense_pack(n=1000000, seed=0, device=-1, sweeps=3000):
     sim.consolidate), the top layer moving at +x 0.01 m/s and the bottom
     layer held (fixvel, as in sim.shear), linear contacts
     k_n = k_t = 1.16e9 N/m, gamma_n = 1e3, mu = 0.5, NC = 32 slots,
-    dt = 0.17 * sqrt(m_min / k_n), 5,000 steps."""
-    s, _worst = dense_pack(n, seed=seed, device=device, sweeps=sweeps, sid="shear1e6")
+    dt = 0.17 * sqrt(m_min / k_n), 5,000 steps.  `relax`: as in dense_pack."""
+    s, _worst = dense_pack(n, seed=seed, device=device, sweeps=sweeps, sid="shear1e6",
+                           relax=relax)
     return _shear_setup(s, sigma0=2.0e4, mu=0.5, steps=5000)
 
 

@@ -578,7 +578,7 @@ class sim(object):
         else:
             self.kappa[0] = 0.0
             self.V_b[0] = 0.0
-        self.db[0] = (1.0 + theta / 2.0) * self.V_b ** (1.0 / 3.0)
+        self.db[0] = (1.0 + theta / 2.0) * self.V_b[0] ** (1.0 / 3.0)
 
     def setStiffnessNormal(self, k_n):
         self.k_n[0] = k_n

@@ -84,6 +84,19 @@ def make(name):
         s.w_sigma0_A[0] = 2.0e3
         s.w_sigma0_f[0] = 50.0
         return s, True, 10
+    if name == "capillary_cohesion":
+        # contact model 1 with capillary bonds (contactsearch.cuh:163-168,
+        # cohesion.cuh:237-277): a lattice a little wider than the spheres,
+        # so that most neighbours sit at gaps between 0 and db, soft
+        # contacts (k_n = 1e4) and kappa = 10, so that the capillary forces
+        # are ~1/4 of the force field (relative L2 after one step: 0.23)
+        s = scenes.lattice_pack(500, seed=14, periodic=1, contactmodel=1, gamma_n=0.0,
+                                gamma_t=1.0, k_n=1.0e4, r_min=0.0095, r_max=0.0105,
+                                spacing=0.0203, jitter=0.0006, nw=0)
+        s.kappa[0] = 10.0
+        s.V_b[0] = 1.0e-9
+        s.db[0] = 1.0e-3
+        return s, True, 20
     if name == "fast_spheres":
         # fast enough that spheres cross cells and periodic boundaries and
         # the neighbour lists are rebuilt several times
@@ -96,11 +109,21 @@ def make(name):
 CASES = ["periodic_xy_wall_stress", "walls_all_sides", "periodic_x_wall_velocity",
          "contact_model_1", "contact_model_3_hertz", "youngs_modulus", "bonds", "bonds_breaking",
          "fixvel_modes", "shear_stress_wall", "adaptive_grid", "sinusoidal_stress",
-         "fast_spheres"]
+         "fast_spheres", "capillary_cohesion"]
 
-# Cases whose results go through a transcendental function (sin) that CUDA
-# and the C library round differently in the last bit.
-APPROX = {"sinusoidal_stress"}
+# Cases whose results go through a transcendental function that CUDA and the
+# C library may round differently, with the tolerance (relative to each
+# field's largest magnitude) of the GPU-vs-oracle comparison:
+#  * sinusoidal_stress: the wall stress through sin() in FP64 (a last-bit
+#    difference of the wall force);
+#  * capillary_cohesion: the capillary force through the FP32 expf()
+#    (cohesion.cuh:270), which may differ by an FP32 ulp or two between CUDA
+#    and glibc, ~1e-7 of each capillary force; the tolerance, 1e-6 of each
+#    field's scale after 20 steps, is 2e5 times smaller than the capillary
+#    forces' share of the force field (0.23), so a capillary law that is
+#    wrong or missing fails it.  The oracle itself equals the reference's
+#    kernels bit for bit on this case (both call glibc's expf on the CPU).
+APPROX = {"sinusoidal_stress": 1e-12, "capillary_cohesion": 1e-6}
 
 
 def render_scene(name):

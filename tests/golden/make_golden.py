@@ -2,7 +2,9 @@
 holds the reference sources; the fixtures are committed, the script is the
 record of how they were made):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
+
+(the reference checkout may instead be given as $SPHERE_REFERENCE)
 
 1. bin_*.bin: .bin files written by the reference's own python/sphere.py
    (sim.writebin) for seeded scenes built with the reference's own set-up
@@ -163,4 +165,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SPHERE_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set SPHERE_REFERENCE)")
+    main(ref)

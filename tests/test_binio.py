@@ -7,6 +7,7 @@ import os
 import numpy
 import pytest
 
+import oracle as O
 from sphere_b200 import binio
 from sphere_b200.sim import sim
 
@@ -48,13 +49,13 @@ def test_truncated_file_is_an_error(tmp_path):
         sim().readbin(str(p), verbose=False)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/output"),
+@pytest.mark.skipif(O.reference_root() is None,
                     reason="reference fixtures not present")
 @pytest.mark.parametrize("fname,n", [("cube-init.output00029.bin", 1000),
                                      ("init-1e4.output00199.bin", 10000)])
 def test_reads_reference_output_files(fname, n):
     s = sim()
-    s.readbin(os.path.join("/root/reference/output", fname), verbose=False)
+    s.readbin(os.path.join(O.reference_root(), "output", fname), verbose=False)
     assert int(s.np[0]) == n
     assert s.x.shape == (n, 3) and (s.radius > 0).all()
     assert numpy.isfinite(s.x).all()

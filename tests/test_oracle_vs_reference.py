@@ -6,6 +6,8 @@ this project's restatement.  On every parity case they must agree bit for
 bit: positions, velocities, forces, torques, energies, contact lists,
 tangential histories, the sorted permutation and the walls.
 """
+import os
+
 import numpy
 import pytest
 
@@ -16,8 +18,8 @@ FIELDS = ["x", "vel", "angvel", "angpos", "xyzsum", "force", "torque", "es", "ev
           "ev_dot", "p", "contacts", "delta_t", "perm", "cell_id", "bonds", "bonds_delta",
           "bonds_omega"]
 
-needs_ref = pytest.mark.skipif(not O.available("ref") and not __import__("os").path.isdir(
-    "/root/reference/src"), reason="reference sources unavailable to build oracle/_ref")
+needs_ref = pytest.mark.skipif(not O.available("ref") and O.reference_root() is None,
+                               reason="reference sources unavailable to build oracle/_ref")
 
 
 def _same(a, b):
@@ -50,11 +52,12 @@ def test_oracle_matches_reference_kernels(name):
     assert int((a.contacts != s.np[0]).sum()) > 0 or s.contactmodel[0] == 1
 
 
-FIXTURES = "/root/reference/output"
+# the reference's own output files (its checkout's output/ directory)
+FIXTURES = os.path.join(O.reference_root() or "", "output")
 
 
 @needs_ref
-@pytest.mark.skipif(not __import__("os").path.isdir(FIXTURES),
+@pytest.mark.skipif(O.reference_root() is None or not os.path.isdir(FIXTURES),
                     reason="the reference's output fixtures are not present")
 @pytest.mark.parametrize("fname,steps", [("cube-init.output00029.bin", 20),
                                          ("init-1e4.output00199.bin", 6)])
@@ -62,7 +65,6 @@ def test_oracle_matches_reference_kernels_on_its_fixtures(fname, steps):
     """The reference's own output files as inputs (output/cube-init: 1,000
     spheres in a 3 x 3 x 112 periodic grid, the smallest grid with periodic
     images on both sides; output/init-1e4: 10,000 settled spheres)."""
-    import os
     from sphere_b200 import sim
     if not O.available("ref"):
         O.build()
@@ -77,3 +79,19 @@ def test_oracle_matches_reference_kernels_on_its_fixtures(fname, steps):
             A, B = getattr(a, f), getattr(b, f)
             assert _same(A, B), "%s differs after %d steps" % (f, (chunk + 1) * steps // 2)
     assert int((a.contacts != s.np[0]).sum()) > 0
+
+
+def test_capillary_case_exercises_the_capillary_law():
+    """The capillary case is only a check of capillaryCohesion_exp if that
+    law carries a real share of the forces: one step with kappa = 0 must
+    differ from the case's forces by more than 10 % (relative L2)."""
+    import copy
+    s, _ok, _steps = cases.make("capillary_cohesion")
+    a = O.CpuRun(s, "oracle")
+    a.step(1)
+    s0 = copy.deepcopy(s)
+    s0.kappa[0] = 0.0
+    b = O.CpuRun(s0, "oracle")
+    b.step(1)
+    rel = numpy.linalg.norm(a.force - b.force) / numpy.linalg.norm(a.force)
+    assert rel > 0.1, rel

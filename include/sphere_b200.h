@@ -217,6 +217,15 @@ int sph_boxes_from_staging(SphHandle *h, const void *staging, uint64_t nstates, 
  * radius).  Any pointer may be NULL. */
 int sph_get_contacts(SphHandle *h, uint32_t *contacts, double *delta_t,
                      double *distmod);
+/* The inverse of sph_get_contacts, after sph_upload (no counterpart in the
+ * reference, whose .bin files carry no contact history, so that a restart
+ * begins with empty contact lists): contacts [np][NC] (partner index local
+ * to the box, np_box = empty slot) and delta_t [np][NC][4] (NULL: zero
+ * histories) become the handle's contact rows; each pair's periodic image
+ * is the nearest one at the current positions.  A partner index that is
+ * not a sphere of the box, or the sphere itself, is SPH_ERR_INPUT and
+ * changes nothing. */
+int sph_set_contacts(SphHandle *h, const uint32_t *contacts, const double *delta_t);
 
 /* Cell-sort products of the last step (src/sorting.cuh:25-132,
  * src/device.cu:1059-1107): per-particle cell id [np] (in original order),
@@ -284,17 +293,28 @@ int sph_set_neighbor_lists(SphHandle *h, uint32_t capacity);
 int sph_neighbor_stats(SphHandle *h, uint64_t *stats);
 
 /* Launch variants of the interact stage (no counterpart in the
- * reference), all with the same arithmetic and results: 0, 1, 2 = the
- * fused kernel compiled for up to 255, 128 and 80 registers per thread
- * (different occupancy); 3 = the split step (contact search, one thread
- * per contact for the contact laws, one thread per sphere for the sums and
- * integration), for contact models 2 and 3 with neighbour lists on, which
- * allocates 332 B per sphere when first chosen.  sph_autotune times
- * `steps` steps with each applicable variant from the current state, keeps
- * the fastest for this handle and puts the state back as it was
- * (ms_per_step[SPH_TUNE_VARIANTS] may be NULL; -1 for a variant not
- * tried).  sph_set_variant picks one directly.  Default 1. */
-#define SPH_TUNE_VARIANTS 4
+ * reference).  0, 1, 2 = the fused kernel compiled for up to 255, 128 and
+ * 80 registers per thread (different occupancy); 3 = the split step
+ * (contact search, one thread per contact for the contact laws, one thread
+ * per sphere for the sums and integration), for contact models 2 and 3
+ * with neighbour lists on, which allocates 332 B per sphere when first
+ * chosen.  Variants 0-3 have the same arithmetic and results.
+ * 4 = the list step of the FP32-mixed form (SPH_PREC_MIXED only; contact
+ * models 2 and 3, neighbour lists on, no bonds, no shear-stress wall, no
+ * adaptive grid; other handles run variant 1 when it is chosen): the
+ * tangential history of a touching pair is kept with its neighbour-list
+ * entry instead of an NC slot, each sphere's contacts are summed in list
+ * order, and one kernel per step runs the contact laws, walls and
+ * integration on compact state (FP32 where the mixed form allows); it
+ * allocates about 2.7 kB per sphere when first chosen.  Its contacts are
+ * those of the other variants (the same FP64 overlap test); sph_get_contacts
+ * returns them in list order in slots 0, 1, ...; its results are held to
+ * the mixed form's stated error, not to the other variants' bits.
+ * sph_autotune times `steps` steps with each applicable variant from the
+ * current state, keeps the fastest for this handle and puts the state back
+ * as it was (ms_per_step[SPH_TUNE_VARIANTS] may be NULL; -1 for a variant
+ * not tried).  sph_set_variant picks one directly.  Default 1. */
+#define SPH_TUNE_VARIANTS 5
 int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen);
 int sph_set_variant(SphHandle *h, int variant);
 

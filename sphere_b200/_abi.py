@@ -8,6 +8,7 @@ import os
 
 NC = 32
 MAXWALLS = 6
+TUNE_VARIANTS = 5   # SPH_TUNE_VARIANTS: launch variants sph_autotune times
 BIN_VERSION = 2.15
 
 SPH_OK = 0
@@ -185,6 +186,8 @@ def load_library():
     lib.sph_download.argtypes = [H, C.POINTER(SphParticles), C.POINTER(SphBonds)]
     lib.sph_get_boxes.argtypes = [H, C.POINTER(SphBox)]
     lib.sph_get_contacts.argtypes = [H, _up, _dp, _dp]
+    lib.sph_set_contacts.argtypes = [H, _up, _dp]
+    lib.sph_set_contacts.restype = C.c_int
     lib.sph_get_sort.argtypes = [H, _up, _up, _up, _up]
     lib.sph_total_cells.argtypes = [H]
     lib.sph_total_cells.restype = C.c_uint64

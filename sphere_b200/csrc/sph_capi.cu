@@ -3,6 +3,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -83,6 +84,17 @@ struct SphHandle {
     char *adj_snaps = nullptr;
     uint64_t adj_nsteps = 0, adj_iter0 = 0;
     uint32_t adj_ckpt = 0;
+    // the list step of the FP32-mixed form (launch variant 4): its compact
+    // state (allocated when the variant is first chosen); pair_valid: the
+    // compact arrays hold the current state; pair_ahead: the FP64 arrays
+    // of A are behind them (brought up to date by sync_public)
+    sph::PairArgs P{};
+    bool pair_alloc = false, pair_valid = false, pair_ahead = false;
+    // steps launched kernel by kernel instead of as captured graphs
+    // (SPHERE_B200_EAGER=1 at sph_create): for profilers that cannot see
+    // into graphs with conditional nodes; the list step then reads its
+    // rebuild request on the host each step
+    bool eager = false;
 };
 
 static int fail(SphHandle *h, int code, const std::string &msg)
@@ -109,6 +121,116 @@ static int dalloc(SphHandle *h, T **p, uint64_t count)
         return fail(h, SPH_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     h->allocs.push_back(q);
     *p = static_cast<T *>(q);
+    return SPH_OK;
+}
+
+// Whether the list step (launch variant 4) can run this handle: the
+// FP32-mixed form, contact models 2/3 in every box, no shear-stress wall,
+// no bonds, no adaptive grid, neighbour lists on and possible in every
+// populated box (set at sph_upload).
+static bool pair_eligible(const SphHandle *h)
+{
+    if (h->precision != SPH_PREC_MIXED || !h->cfg.all_cm23 || h->cfg.unfused || !h->A.vlist ||
+        h->nbonds != 0 || h->ntot == 0 || !h->uploaded)
+        return false;
+    for (uint32_t k = 0; k < h->nbox; ++k) {
+        if (h->boxes[k].grid.adaptive) return false;
+        if (h->dbox[k].np > 0 && h->dbox[k].vrange < 1) return false;
+    }
+    return true;
+}
+
+static bool pair_active(const SphHandle *h)
+{
+    return h->cfg.variant == sph::PAIR_VARIANT && pair_eligible(h);
+}
+
+static int ensure_pair(SphHandle *h)
+{
+    if (h->pair_alloc) return SPH_OK;
+    const uint64_t n = h->ntot;
+    sph::PairArgs &P = h->P;
+    std::vector<uint32_t> cbox, c0(h->nbox);
+    for (uint32_t k = 0; k < h->nbox; ++k) {
+        c0[k] = (uint32_t)cbox.size();
+        const uint32_t nch = (h->dbox[k].np + (1u << sph::PAIR_CHUNK_LOG2) - 1) >> sph::PAIR_CHUNK_LOG2;
+        for (uint32_t c = 0; c < nch; ++c) cbox.push_back(k);
+    }
+    uint32_t *chunk_box = nullptr, *box_chunk0 = nullptr, *words = nullptr;
+    int st;
+    if ((st = dalloc(h, &P.xr[0], n)) || (st = dalloc(h, &P.xr[1], n)) ||
+        (st = dalloc(h, &P.vw[0], 2 * n)) || (st = dalloc(h, &P.vw[1], 2 * n)) ||
+        (st = dalloc(h, &P.vel, n)) || (st = dalloc(h, &P.angpos, n)) ||
+        (st = dalloc(h, &P.acc, n)) || (st = dalloc(h, &P.angacc, n)) ||
+        (st = dalloc(h, &P.force, n)) || (st = dalloc(h, &P.torque, n)) ||
+        (st = dalloc(h, &P.epp, n)) || (st = dalloc(h, &P.eacc, n)) ||
+        (st = dalloc(h, &P.xyzsum, n)) ||
+        (st = dalloc(h, &P.ids[0], n * sph::VL_MAX)) || (st = dalloc(h, &P.ids[1], n * sph::VL_MAX)) ||
+        (st = dalloc(h, &P.cnt[0], n)) || (st = dalloc(h, &P.cnt[1], n)) ||
+        (st = dalloc(h, &P.live[0], n)) || (st = dalloc(h, &P.live[1], n)) ||
+        (st = dalloc(h, &P.hist[0], 3 * n * sph::VL_MAX)) ||
+        (st = dalloc(h, &P.hist[1], 3 * n * sph::VL_MAX)) || (st = dalloc(h, &words, 3)) ||
+        (st = dalloc(h, &P.chunk_part, cbox.size())) || (st = dalloc(h, &chunk_box, cbox.size())) ||
+        (st = dalloc(h, &box_chunk0, h->nbox)))
+        return st;
+    P.pp = words;
+    P.lsel = words + 1;
+    P.from_rows = words + 2;
+    P.chunk_box = chunk_box;
+    P.box_chunk0 = box_chunk0;
+    P.nchunks = (uint32_t)cbox.size();
+    P.chunk_log2 = sph::PAIR_CHUNK_LOG2;
+    CUDA_TRY(h, cudaMemset(words, 0, 3 * sizeof(uint32_t)));
+    for (int b = 0; b < 2; ++b) {
+        CUDA_TRY(h, cudaMemset(P.cnt[b], 0, sizeof(uint32_t) * n));
+        CUDA_TRY(h, cudaMemset(P.live[b], 0, sizeof(uint64_t) * n));
+    }
+    if (!cbox.empty())
+        CUDA_TRY(h, cudaMemcpy(chunk_box, cbox.data(), 4 * cbox.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(box_chunk0, c0.data(), 4 * c0.size(), cudaMemcpyHostToDevice));
+    h->pair_alloc = true;
+    return SPH_OK;
+}
+
+// Bring the FP64 arrays of A up to date with the list step's compact state
+// (before anything reads them); synchronises the handle's stream.
+static int sync_public(SphHandle *h)
+{
+    if (!h->pair_ahead) return SPH_OK;
+    int st = sph::pair_flush(h->A, h->P, h->stream);
+    if (st != SPH_OK) return fail(h, st, "list-step state flush failed");
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->pair_ahead = false;
+    return SPH_OK;
+}
+
+// The FP64 arrays were written: the compact state no longer holds the
+// current state.
+static void invalidate_pair(SphHandle *h)
+{
+    h->pair_valid = false;
+    h->pair_ahead = false;
+}
+
+// Before steps of the active launch variant are queued: the list step
+// loads its compact state when that is stale; every other variant needs
+// the FP64 arrays current, and leaves the compact state stale.
+static int prepare_steps(SphHandle *h)
+{
+    if (pair_active(h)) {
+        int st = ensure_pair(h);
+        if (st != SPH_OK) return st;
+        if (!h->pair_valid) {
+            st = sph::pair_load(h->A, h->P, h->stream);
+            if (st != SPH_OK) return fail(h, st, "list-step state load failed");
+            h->pair_valid = true;
+        }
+        h->pair_ahead = true;
+        return SPH_OK;
+    }
+    int st = sync_public(h);
+    if (st != SPH_OK) return st;
+    h->pair_valid = false;
     return SPH_OK;
 }
 
@@ -320,6 +442,10 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision, int length_m
     if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess)
         return bail(SPH_ERR_CUDA);
     h->stream = h->own;
+    {
+        const char *e = getenv("SPHERE_B200_EAGER");
+        h->eager = e && e[0] == '1';
+    }
 
     StepArgs &A = h->A;
     A.nboxes = nboxes;
@@ -502,6 +628,29 @@ __global__ void k_pack3(double *dst, const double4 *src, uint64_t n)
     }
 }
 
+// The image code of every occupied slot (sph_set_contacts): the nearest
+// periodic image of the partner at the current positions.
+__global__ void k_image_codes(StepArgs A, uint64_t ns)
+{
+    const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ns) return;
+    const uint32_t w = A.slots[q];
+    if (w == sph::EMPTY) return;
+    const uint32_t i = (uint32_t)(q / sph::NC), b = w & sph::ID_MASK;
+    const DevBox &B = A.boxes[A.nboxes == 1 ? 0u : A.box_of[i]];
+    const double dx = A.x[i].x - A.x[b].x, dy = A.x[i].y - A.x[b].y;
+    int sx = 0, sy = 0;
+    if (B.periodic == 1 || B.periodic == 2) {
+        if (dx > 0.5 * B.L[0]) sx = -1;
+        else if (dx < -0.5 * B.L[0]) sx = 1;
+    }
+    if (B.periodic == 1) {
+        if (dy > 0.5 * B.L[1]) sy = -1;
+        else if (dy < -0.5 * B.L[1]) sy = 1;
+    }
+    A.slots[q] = b | (sph::shift_code(sx, sy) << sph::CODE_SHIFT);
+}
+
 static int ensure_stage(SphHandle *h)
 {
     if (h->stage) return SPH_OK;
@@ -676,6 +825,7 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
     CUDA_TRY(h, cudaMemset(A.vflag, 0, 2 * sizeof(uint32_t)));
     CUDA_TRY(h, cudaMemset(A.vflag, 1, 1));   // build the lists in the first step
     h->uploaded = true;
+    invalidate_pair(h);
     return SPH_OK;
 }
 
@@ -693,8 +843,21 @@ static int capture_step(SphHandle *h, sph::Prof *prof, cudaGraph_t *g, cudaGraph
     cfg.side = h->side;
     cfg.fork = h->ev_fork;
     cfg.join = h->ev_join;
+    const bool pair = pair_active(h);
+    if (pair && !h->side) {
+        // the list step captures its rebuild body on the side stream
+        CUDA_TRY(h, cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+        CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    }
+    if (pair) {
+        int st = ensure_pair(h);
+        if (st != SPH_OK) return st;
+        cfg.side = h->side;
+    }
     CUDA_TRY(h, cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
-    int st = h->precision == SPH_PREC_MIXED
+    int st = pair ? sph::launch_step_pair(h->A, h->P, cfg, h->own, nl, prof)
+             : h->precision == SPH_PREC_MIXED
                  ? sph::launch_step_mixed(h->A, cfg, h->own, nl, prof)
                  : sph::launch_step(h->A, cfg, h->own, nl, prof);
     cudaError_t e = cudaStreamEndCapture(h->own, g);
@@ -719,7 +882,7 @@ static int build_graph(SphHandle *h)
 // reads L[2]) nor for the unfused kernels.
 static bool overlap_ok(const SphHandle *h)
 {
-    if (h->cfg.unfused) return false;
+    if (h->cfg.unfused || pair_active(h)) return false;
     for (uint32_t k = 0; k < h->nbox; ++k)
         if (h->boxes[k].grid.adaptive) return false;
     return true;
@@ -799,7 +962,28 @@ int sph_step(SphHandle *h, uint64_t nsteps)
 static int queue_steps(SphHandle *h, uint64_t nsteps, uint8_t *states)
 {
     int st;
+    if (h->eager) {
+        // kernel by kernel on the handle's stream (no graphs)
+        if ((st = prepare_steps(h)) != SPH_OK) return st;
+        const size_t bytes = sizeof(DevBox) * h->nbox;
+        StepConfig cfg = h->cfg;
+        for (uint64_t s = 0; s < nsteps; ++s) {
+            uint64_t nl = 0;
+            st = pair_active(h) ? sph::launch_step_pair(h->A, h->P, cfg, h->stream, &nl, nullptr)
+                 : h->precision == SPH_PREC_MIXED
+                     ? sph::launch_step_mixed(h->A, cfg, h->stream, &nl, nullptr)
+                     : sph::launch_step(h->A, cfg, h->stream, &nl, nullptr);
+            if (st != SPH_OK) return fail(h, st, "step launch failed");
+            h->launches += nl;
+            for (uint32_t k = 0; k < h->nbox; ++k) h->t_host[k] += h->boxes[k].dt;
+            if (states)
+                CUDA_TRY(h, cudaMemcpyAsync(states + s * bytes, h->A.boxes, bytes,
+                                            cudaMemcpyDeviceToHost, h->stream));
+        }
+        return SPH_OK;
+    }
     if ((st = build_graph(h)) != SPH_OK) return st;
+    if ((st = prepare_steps(h)) != SPH_OK) return st;
     const size_t bytes = sizeof(DevBox) * h->nbox;
     if (nsteps >= 2 && !h->prof_on && overlap_ok(h)) {
         // the head of step 1, steps 2..n each beside the wall stage of the
@@ -1001,6 +1185,8 @@ int sph_download(SphHandle *h, SphParticles *p, SphBonds *b)
     if (!h) return SPH_ERR_INPUT;
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    int st = sync_public(h);
+    if (st != SPH_OK) return st;
     return download_from(h, h->A, nullptr, p, b);
 }
 
@@ -1068,6 +1254,12 @@ int sph_snapshot(SphHandle *h)
         CUDA_TRY(h, cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
         h->snap_alloc = true;
     }
+    if (h->pair_ahead) {
+        // the compact state into the FP64 arrays, on the stream, before the copies
+        int st = sph::pair_flush(h->A, h->P, h->stream);
+        if (st != SPH_OK) return fail(h, st, "list-step state flush failed");
+        h->pair_ahead = false;
+    }
     const StepArgs &A = h->A;
     auto d2d = [&](void *dst, const void *src, size_t bytes) {
         return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream);
@@ -1128,6 +1320,10 @@ int sph_get_contacts(SphHandle *h, uint32_t *contacts, double *delta_t, double *
     if (!h) return SPH_ERR_INPUT;
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    {
+        int st = sync_public(h);
+        if (st != SPH_OK) return st;
+    }
     const uint64_t n = h->ntot, ns = n * sph::NC;
     if (n == 0) return SPH_OK;
     std::vector<uint32_t> w(ns);
@@ -1162,6 +1358,45 @@ int sph_get_contacts(SphHandle *h, uint32_t *contacts, double *delta_t, double *
     return SPH_OK;
 }
 
+int sph_set_contacts(SphHandle *h, const uint32_t *contacts, const double *delta_t)
+{
+    if (!h || !contacts) return SPH_ERR_INPUT;
+    if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_set_contacts before sph_upload");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const uint64_t n = h->ntot, ns = n * sph::NC;
+    if (n == 0) return SPH_OK;
+    std::vector<uint32_t> w(ns, sph::EMPTY);
+    for (uint32_t k = 0; k < h->nbox; ++k) {
+        const DevBox &d = h->dbox[k];
+        for (uint64_t i = d.p_base; i < (uint64_t)d.p_base + d.np; ++i)
+            for (int s = 0; s < sph::NC; ++s) {
+                const uint64_t q = i * sph::NC + s;
+                const uint32_t b = contacts[q];
+                if (b == d.np) continue;
+                if (b > d.np || (uint64_t)d.p_base + b == i) {
+                    char buf[160];
+                    snprintf(buf, sizeof buf, "box %u sphere %llu slot %d: partner %u is not "
+                             "another sphere of the box", k, (unsigned long long)(i - d.p_base), s, b);
+                    return fail(h, SPH_ERR_INPUT, buf);
+                }
+                w[q] = d.p_base + b;   // image code set on the device
+            }
+    }
+    std::vector<double4> hist(ns);
+    for (uint64_t q = 0; q < ns; ++q)
+        hist[q] = delta_t && w[q] != sph::EMPTY
+                      ? make_double4(delta_t[4 * q], delta_t[4 * q + 1], delta_t[4 * q + 2], 0.0)
+                      : make_double4(0.0, 0.0, 0.0, 0.0);
+    CUDA_TRY(h, cudaMemcpy(h->A.slots, w.data(), sizeof(uint32_t) * ns, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->A.hist, hist.data(), sizeof(double4) * ns, cudaMemcpyHostToDevice));
+    k_image_codes<<<(unsigned)((ns + 255) / 256), 256, 0, h->stream>>>(h->A, ns);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    invalidate_pair(h);
+    return SPH_OK;
+}
+
 uint64_t sph_total_cells(const SphHandle *h) { return h ? h->ncells : 0; }
 
 int sph_get_sort(SphHandle *h, uint32_t *cell_id, uint32_t *perm, uint32_t *cell_start,
@@ -1190,7 +1425,14 @@ int sph_count_contacts(SphHandle *h, uint64_t *ncontacts)
     if (!h || !ncontacts) return SPH_ERR_INPUT;
     cudaSetDevice(h->device);
     uint64_t nl = 0;
-    int st = sph::count_live_slots(h->A, h->stream, h->d_count, &nl);
+    int st;
+    if (pair_active(h) && h->pair_valid) {
+        st = sph::pair_count_live(h->A, h->P, h->stream, h->d_count);
+        nl = 1;
+    } else {
+        st = sync_public(h);
+        if (st == SPH_OK) st = sph::count_live_slots(h->A, h->stream, h->d_count, &nl);
+    }
     h->launches += nl;
     if (st != SPH_OK) return fail(h, st, "count_live_slots failed");
     unsigned long long c = 0;
@@ -1208,7 +1450,14 @@ int sph_neighbor_stats(SphHandle *h, uint64_t *stats)
     const uint64_t n = h->ntot;
     std::vector<uint32_t> vc(n ? n : 1);
     uint32_t flag[2] = {0, 0};
-    if (n) CUDA_TRY(h, cudaMemcpy(vc.data(), h->A.vcount, 4 * n, cudaMemcpyDeviceToHost));
+    const uint32_t *counts = h->A.vcount;
+    if (pair_active(h) && h->pair_valid) {
+        // the list step's lists in use
+        uint32_t ls = 0;
+        CUDA_TRY(h, cudaMemcpy(&ls, h->P.lsel, sizeof ls, cudaMemcpyDeviceToHost));
+        counts = h->P.cnt[ls & 1u];
+    }
+    if (n) CUDA_TRY(h, cudaMemcpy(vc.data(), counts, 4 * n, cudaMemcpyDeviceToHost));
     CUDA_TRY(h, cudaMemcpy(flag, h->A.vflag, sizeof flag, cudaMemcpyDeviceToHost));
     uint64_t with = 0, over = 0, sum = 0, mx = 0;
     for (uint64_t i = 0; i < n; ++i) {
@@ -1489,8 +1738,16 @@ int sph_set_variant(SphHandle *h, int variant)
         return fail(h, SPH_ERR_INPUT, "variant out of range");
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    {
+        int st = sync_public(h);
+        if (st != SPH_OK) return st;
+    }
     if (variant == sph::SPLIT_VARIANT) {
         int st = ensure_split(h);
+        if (st != SPH_OK) return st;
+    }
+    if (variant == sph::PAIR_VARIANT && pair_eligible(h)) {
+        int st = ensure_pair(h);
         if (st != SPH_OK) return st;
     }
     h->cfg.variant = variant;
@@ -1503,6 +1760,10 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
     if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_autotune before sph_upload");
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    {
+        int st0 = sync_public(h);
+        if (st0 != SPH_OK) return st0;
+    }
     const size_t sb = state_bytes(h);
     char *snap = nullptr;
     if (cudaMalloc((void **)&snap, sb) != cudaSuccess)
@@ -1522,9 +1783,13 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
         if (v == sph::SPLIT_VARIANT &&
             (!h->cfg.all_cm23 || h->cfg.unfused || !h->A.vlist || ensure_split(h) != SPH_OK))
             continue;
+        // the list step: the FP32-mixed form's cases it covers
+        if (v == sph::PAIR_VARIANT && (!pair_eligible(h) || ensure_pair(h) != SPH_OK)) continue;
         h->cfg.variant = v;
         if ((st = drop_graphs(h)) != SPH_OK || (st = build_graph(h)) != SPH_OK) break;
         copy_state(h, snap, 0, false);
+        invalidate_pair(h);
+        if ((st = prepare_steps(h)) != SPH_OK) break;
         // one untimed step (graph upload, list build), then the timed ones
         if ((st = launch_one(h)) != SPH_OK) break;
         cudaEventRecord(e0, h->stream);
@@ -1541,6 +1806,7 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
         }
     }
     copy_state(h, snap, 0, false);
+    invalidate_pair(h);
     cudaStreamSynchronize(h->stream);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1562,6 +1828,10 @@ int sph_porosity(SphHandle *h, uint32_t box, uint32_t z_slices, double *z_pos, d
     if (box >= h->nbox) return fail(h, SPH_ERR_INPUT, "no such box");
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    {
+        int st0 = sync_public(h);
+        if (st0 != SPH_OK) return st0;
+    }
     DevBox d;
     CUDA_TRY(h, cudaMemcpy(&d, h->A.boxes + box, sizeof d, cudaMemcpyDeviceToHost));
     // src/sphere.cpp:492-515: the top is wall 0 when there are walls
@@ -1599,6 +1869,10 @@ int sph_overlaps(SphHandle *h, uint32_t box, uint64_t max_pairs, uint32_t *pairs
     if (box >= h->nbox) return fail(h, SPH_ERR_INPUT, "no such box");
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    {
+        int st0 = sync_public(h);
+        if (st0 != SPH_OK) return st0;
+    }
     DevBox d;
     CUDA_TRY(h, cudaMemcpy(&d, h->A.boxes + box, sizeof d, cudaMemcpyDeviceToHost));
     sph::OverlapArgs O{};
@@ -1684,6 +1958,10 @@ int sph_render(SphHandle *h, uint32_t box, int method, float maxval, float lower
         return fail(h, SPH_ERR_INPUT, "image size out of range");
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    {
+        int st0 = sync_public(h);
+        if (st0 != SPH_OK) return st0;
+    }
     DevBox d;
     CUDA_TRY(h, cudaMemcpy(&d, h->A.boxes + box, sizeof d, cudaMemcpyDeviceToHost));
     const double *d_L = reinterpret_cast<const double *>(
@@ -1711,6 +1989,10 @@ int sph_set_neighbor_lists(SphHandle *h, uint32_t capacity)
         return fail(h, SPH_ERR_INPUT, "neighbour-list capacity above " + std::to_string(sph::VL_MAX));
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    {
+        int st = sync_public(h);
+        if (st != SPH_OK) return st;
+    }
     h->A.vlist = capacity ? h->vlist_mem : nullptr;
     h->A.vcap = capacity;
     CUDA_TRY(h, cudaMemset(h->A.vflag, 1, 1));
@@ -1722,6 +2004,11 @@ int sph_relax(SphHandle *h, uint32_t sweeps, double alpha, double z_top, double 
     if (!h || !(alpha > 0.0) || !(alpha <= 1.0)) return SPH_ERR_INPUT;
     if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_relax before sph_upload");
     cudaSetDevice(h->device);
+    {
+        int st0 = sync_public(h);
+        if (st0 != SPH_OK) return st0;
+        invalidate_pair(h);   // the sweeps move the spheres in the FP64 arrays
+    }
     uint64_t nl = 0;
     for (uint32_t k = 0; k < sweeps; ++k) {
         int st = sph::relax_sweep(h->A, h->stream, alpha, z_top, h->d_count, &nl);

@@ -69,9 +69,50 @@ struct StepArgs {
 };
 
 constexpr int VL_MAX = 48;   // neighbour-list capacity per sphere
-constexpr int INTERACT_VARIANTS = 4;   // launch variants of the interact stage (sph_autotune)
+constexpr int INTERACT_VARIANTS = 5;   // launch variants of the interact stage (sph_autotune)
 constexpr int SPLIT_VARIANT = 3;       // the split step (k_search / k_contacts / k_finish)
+constexpr int PAIR_VARIANT = 4;        // the list step of the FP32-mixed form (sph_pair.cu)
 constexpr uint32_t SPLIT_ID_MASK = 0x07ffffffu;   // sphere index bits of a live entry
+
+// The list step of the FP32-mixed form (launch variant 4, sph_pair.cu).
+// Its state lives in compact arrays of its own while it steps; the FP64
+// arrays of StepArgs are brought up to date from them (pair_flush) before
+// anything else reads them, and the compact arrays are loaded from them
+// (pair_load) before the first list step after anything wrote them.
+//  - ping-pong (selected by *pp: the current step reads [*pp], writes
+//    [*pp ^ 1]; k_pair_box flips *pp at the end of the step): what the
+//    contact laws read of a partner, x+r in FP64 (xr) and velocity and
+//    angular velocity in FP32 (vw: two float4 per sphere, (v, 0) and
+//    (w, 0));
+//  - the sphere's own state, read and written by its own thread only:
+//    velocity+fixvel FP64, angpos, acc, angacc (w: angacc_w), force,
+//    torque FP32, es_dot/ev_dot/p FP32 (epp), es/ev FP64 (eacc);
+//  - the contact lists, double buffered (selected by *lsel, flipped by a
+//    rebuild): per sphere up to VL_MAX neighbour ids in ascending order
+//    (ids, cnt), the tangential-displacement history of each entry (hist,
+//    three FP64 per entry) and a bit per entry that is set while the pair
+//    touches (live);
+//  - the wall force of each sphere (A.wf_pp) summed over chunks of
+//    PAIR_CHUNK spheres of one box (chunk_part), then per box.
+struct PairArgs {
+    double4 *xr[2];
+    float4 *vw[2];
+    double4 *vel;
+    float4 *angpos, *acc, *angacc, *force, *torque, *epp;
+    double2 *eacc;
+    double4 *xyzsum;
+    uint32_t *ids[2], *cnt[2];
+    uint64_t *live[2];
+    double *hist[2];
+    uint32_t *pp, *lsel;
+    uint32_t *from_rows;       // != 0: the next rebuild takes histories from A.slots / A.hist
+    double *chunk_part;        // [nchunks]
+    const uint32_t *chunk_box; // box of each chunk
+    uint32_t nchunks;
+    uint32_t chunk_log2;       // chunk = 1 << chunk_log2 spheres of one box
+    const uint32_t *box_chunk0;   // first chunk of each box
+};
+constexpr int PAIR_CHUNK_LOG2 = 11;
 
 // Overlap search of one box (sph_overlaps): positions and velocities, the
 // box's spheres [p0, p0 + np), its grid (origin, cell widths, cell counts),
@@ -157,6 +198,20 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                      ContactLauncher contact);
 int launch_step_mixed(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
                       uint64_t *launches, Prof *prof);
+
+// The list step (sph_pair.cu): one step; the public FP64 arrays from the
+// compact state and back; the number of touching list entries.
+int launch_step_pair(const StepArgs &A, const PairArgs &P, const StepConfig &cfg, cudaStream_t st,
+                     uint64_t *launches, Prof *prof);
+int pair_load(const StepArgs &A, const PairArgs &P, cudaStream_t st);
+int pair_flush(const StepArgs &A, const PairArgs &P, cudaStream_t st);
+int pair_count_live(const StepArgs &A, const PairArgs &P, cudaStream_t st,
+                    unsigned long long *d_count);
+// Sort and neighbour lists for a rebuild of the list step's lists
+// (sph_kernels.cu): the positions of the current state (xr[*pp]) into A.x,
+// the cell sort, and the lists into the buffers not in use
+// (ids / cnt [*lsel ^ 1]).
+void launch_pair_sort_build(const StepArgs &A, const PairArgs &P, cudaStream_t st);
 
 // Ray-traced image of one box (sph_render): tiles of the screen, entries of
 // the tile lists, kernels launched.

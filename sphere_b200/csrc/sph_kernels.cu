@@ -219,7 +219,8 @@ constexpr int VLIST_THREADS = 128;
 // integration against xref) keeps every sphere it can touch in its list.
 // Runs only when vflag[0] is set; a list that overflows vcap (<= VL_MAX) is
 // marked VL_MAX + 1 and that sphere uses the cell search.
-__device__ __forceinline__ void vlist_build_one(const StepArgs &A, uint32_t a, uint32_t *lst)
+__device__ __forceinline__ void vlist_build_one(const StepArgs &A, uint32_t a, uint32_t *lst,
+                                                uint32_t *vlist, uint32_t *vcount, uint32_t cap)
 {
     const int RS = VLIST_THREADS;
     const uint32_t i = A.perm[a];
@@ -229,7 +230,7 @@ __device__ __forceinline__ void vlist_build_one(const StepArgs &A, uint32_t a, u
     const int R = B.vrange;
     const uint32_t cm = B.P.contactmodel;
     if (R < 1 || (cm != 2 && cm != 3)) {
-        A.vcount[i] = VL_MAX + 1;
+        vcount[i] = VL_MAX + 1;
         return;
     }
     int g0, g1, g2;
@@ -256,7 +257,7 @@ __device__ __forceinline__ void vlist_build_one(const StepArgs &A, uint32_t a, u
                     int q = n;
                     while (q > 0 && lst[(q - 1) * RS] > bo) --q;
                     if (q > 0 && lst[(q - 1) * RS] == bo) continue;   // another image
-                    if (n == (int)A.vcap) {
+                    if (n == (int)cap) {
                         over = true;
                         break;
                     }
@@ -266,12 +267,12 @@ __device__ __forceinline__ void vlist_build_one(const StepArgs &A, uint32_t a, u
                 }
             }
     if (over) {
-        A.vcount[i] = VL_MAX + 1;
+        vcount[i] = VL_MAX + 1;
         return;
     }
-    uint32_t *out = A.vlist + (size_t)i * VL_MAX;
+    uint32_t *out = vlist + (size_t)i * VL_MAX;
     for (int k = 0; k < n; ++k) out[k] = lst[k * RS];
-    A.vcount[i] = (uint32_t)n;
+    vcount[i] = (uint32_t)n;
 }
 
 // A grid of a few blocks per SM that strides over the spheres, so that the
@@ -285,7 +286,24 @@ __global__ void __launch_bounds__(VLIST_THREADS) k_vlist_build(StepArgs A)
     __shared__ uint32_t s_list[VL_MAX * VLIST_THREADS];
     for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < A.ntot;
          a += gridDim.x * blockDim.x)
-        vlist_build_one(A, a, s_list + threadIdx.x);
+        vlist_build_one(A, a, s_list + threadIdx.x, A.vlist, A.vcount, A.vcap);
+}
+
+// The list step's rebuild (sph_pair.cu): its current positions into A.x for
+// the cell sort, and its lists built at full capacity into the buffers not
+// in use.
+__global__ void k_pair_sync_x(StepArgs A, PairArgs P)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < A.ntot) A.x[i] = P.xr[*P.pp][i];
+}
+
+__global__ void __launch_bounds__(VLIST_THREADS) k_pair_vlist(StepArgs A, PairArgs P)
+{
+    __shared__ uint32_t s_list[VL_MAX * VLIST_THREADS];
+    const uint32_t alt = *P.lsel ^ 1u;
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < A.ntot) vlist_build_one(A, a, s_list + threadIdx.x, P.ids[alt], P.cnt[alt], VL_MAX);
 }
 
 // After the (possible) build: clear the request, count builds.
@@ -487,37 +505,7 @@ __global__ void __launch_bounds__(BOX_THREADS) k_box_step(StepArgs A)
         }
     }
     if (threadIdx.x != 0) return;
-    const double dt = B.dt;
-    if (B.np > 0) {
-        for (uint32_t w = 0; w < B.nw; ++w) {
-            const int wmode = B.wmode[w];
-            if (wmode == 0) continue;
-            const double acc0 = B.iter == 0 ? 0.0 : B.wacc[w];
-            B.wmvfd[w][2] = fsum;
-            const double sigma_0 =
-                B.wmvfd[w][3] + B.P.sigma0_A * sin(2.0 * PI * B.P.sigma0_f * B.t_current);
-            const double N = -sigma_0 * B.L[0] * B.L[1];
-            double acc = (B.wmvfd[w][2] + N) / B.wmvfd[w][0];
-            if (wmode == 2) acc = 0.0;
-            const double dacc_dt = (acc - acc0) / dt;
-            B.wnx[w][3] += B.wmvfd[w][1] * dt + 0.5 * acc * dt * dt + 1.0 / 6.0 * dacc_dt * dt * dt * dt;
-            B.wmvfd[w][1] += acc * dt + 0.5 * dacc_dt * dt * dt;
-            B.wacc[w] = acc;
-        }
-    }
-    B.t_current += dt;
-    B.iter += 1;
-    B.L2_out = B.L[2];
-    if (B.adaptive == 1 && B.nw > 0) B.L[2] = B.wnx[0][3];
-    int change = 0;
-    if (B.t_current >= 10.0 && B.t_current < 15.0 && B.velocity_state == 1) {
-        change = 1;
-        B.velocity_state = 2;
-    } else if (B.t_current >= 15.0 && B.velocity_state == 2) {
-        change = -1;
-        B.velocity_state = 1;
-    }
-    B.change_velocity_state = change;
+    advance_box(B, fsum);
 }
 
 // ------------------------------------------------------------- scene packing
@@ -877,6 +865,20 @@ static void interact_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, boo
 static void contacts_fp64(const StepArgs &A, cudaStream_t st, unsigned grid, int lm, bool pdl)
 {
     launch_contacts<false>(A, st, grid, lm, pdl);
+}
+
+void launch_pair_sort_build(const StepArgs &A, const PairArgs &P, cudaStream_t st)
+{
+    k_pair_sync_x<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A, P);
+    cudaMemsetAsync(A.cell_count, 0, sizeof(uint32_t) * A.ncells, st);
+    k_hash<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+    const uint32_t nb = blocks_for(A.ncells, SCAN_TILE);
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, st>>>(A.cell_count, A.ncells, A.scan_tmp);
+    k_scan_top<<<1, SCAN_THREADS, 0, st>>>(A.scan_tmp, nb);
+    k_scan_down<<<nb, SCAN_THREADS, 0, st>>>(A.cell_count, A.ncells, A.scan_tmp, nb, A.cell_off);
+    k_scatter<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+    k_place<false><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
+    k_pair_vlist<<<blocks_for(A.ntot, VLIST_THREADS), VLIST_THREADS, 0, st>>>(A, P);
 }
 
 int launch_step(const StepArgs &A, const StepConfig &cfg, cudaStream_t st, uint64_t *launches,

@@ -80,7 +80,9 @@ __device__ __forceinline__ d3 contact_linear_mixed(const SphParams &P, double dt
     const float vel_t_length = flen(vel_t);
     const d3 nd = tod(n);
     const d3 delta_t0 = vsub(delta_t0_uncor, muls(nd, dot(nd, delta_t0_uncor)));
-    const float delta_t0_length = (float)sqrt(dot(delta_t0, delta_t0));
+    // the law reads the length of delta_t0 only as "> 0" (the FP64 law's
+    // length(delta_t0) > 0.0): its square says the same without a square root
+    const bool delta_t0_nonzero = dot(delta_t0, delta_t0) > 0.0;
     float k_n, k_t;
     mixed_stiffness(P, q.ra, q.rb, k_n, k_t);
     const float gn = (float)P.gamma_n, gt = (float)P.gamma_t;
@@ -91,7 +93,7 @@ __device__ __forceinline__ d3 contact_linear_mixed(const SphParams &P, double dt
     const f3 f_c = fmul(-(float)P.kappa * sqrtf(q.ra * q.rb), n);
     f3 f_t = fk(0.f, 0.f, 0.f);
     d3 delta_t = mk(0.0, 0.0, 0.0);
-    if (delta_t0_length > 0.0f || vel_t_length > 0.0f) {
+    if (delta_t0_nonzero || vel_t_length > 0.0f) {
         delta_t = vadd(delta_t0, muls(tod(vel_t), dt));
         f_t = fsub(fmul(-k_t, tof(delta_t)), fmul(gt, vel_t));
         const float f_t_length = flen(f_t);
@@ -129,7 +131,7 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
     const float vel_t_ab_length = flen(vel_t_ab);
     const d3 nd = tod(n);
     const d3 delta_t0 = vsub(delta_t0_uncor, muls(nd, dot(delta_t0_uncor, nd)));
-    const float delta_t0_length = (float)sqrt(dot(delta_t0, delta_t0));
+    const bool delta_t0_nonzero = dot(delta_t0, delta_t0) > 0.0;   // length > 0
     float k_n, k_t;
     mixed_stiffness(P, q.ra, q.rb, k_n, k_t);
     const float gn = (float)P.gamma_n, gt = (float)P.gamma_t;
@@ -141,7 +143,7 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
     f3 f_t = fk(0.f, 0.f, 0.f);
     f3 T_res = fk(0.f, 0.f, 0.f);
     d3 delta_t = mk(0.0, 0.0, 0.0);
-    if (delta_t0_length > 0.0f || vel_t_ab_length > 0.0f) {
+    if (delta_t0_nonzero || vel_t_ab_length > 0.0f) {
         const f3 f_t_elast = fmul(-k_t * d12, tof(delta_t0));
         const f3 f_t_visc = fmul(-gt * d14, vel_t_ab);
         const float fnc = flen(fsub(f_n, f_c));

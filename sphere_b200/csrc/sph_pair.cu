@@ -1,0 +1,670 @@
+// sph_pair.cu -- the list step of the FP32-mixed form (launch variant 4).
+//
+// The FP64 form reproduces the reference's NC-slot contact rows
+// (contactsearch.cuh:194-322): a new contact takes a free slot in the order
+// the 27-cell search meets it, and each sphere's sums run in slot order,
+// which is what makes its forces equal the reference's bit for bit.  The
+// FP32-mixed form is held to a stated error instead (per-step force
+// relative L2 <= 1e-5 against the FP64 form), so it keeps the contact
+// history where the neighbour list already has a place for it:
+//
+//  * contact set: the same exact FP64 overlap test on the same centre line
+//    as the FP64 form ((xa - xb) + image shift, FP64 length as the length
+//    mode says, no contraction), over every entry of the sphere's
+//    neighbour list (all spheres within ra + rb + skin at the list build),
+//    so the touching pairs are the FP64 form's;
+//  * history: the tangential displacement of a touching pair is kept with
+//    its list entry (three FP64), with a bit per entry that says whether the
+//    pair touched at the last step; a rebuild of the lists carries every
+//    history over to the entry of the same partner in the new list;
+//  * order: a sphere's contacts are summed in list order (ascending
+//    partner index) instead of slot order;
+//  * one kernel per step does the contact laws, the walls, the sums and the
+//    integration (k_pair_step): partners are read from the state of the
+//    step's start and the new state is written to the other half of a
+//    ping-pong pair, so no second pass is needed; the wall stage sums the
+//    wall force in fixed-order chunks (deterministic, FP64) and advances
+//    the walls and time (k_pair_chunks, k_pair_box);
+//  * storage: FP64 where the precision contract keeps FP64 (positions,
+//    velocities, the history, xyzsum, es/ev, the wall force), FP32 for the
+//    rest (angular velocity, angpos, acc, angacc, force, torque, energy
+//    rates) -- the per-sphere bytes of the mixed budget.
+//
+// The lists are rebuilt inside the step graph only when a sphere has moved
+// more than half the skin since the last build: a conditional graph node
+// whose body is the cell sort, the list build and the history carry-over
+// (launch_step_pair), set by k_pair_cond from the flag the integration
+// raises.  Compiled with FMA contraction; the overlap test is written with
+// explicitly rounded operations so that it matches the FP64 form.
+#include <cstdint>
+#include <cstdio>
+
+#include "sph_device.cuh"
+#include "sph_internal.h"
+#include "sph_mixed_laws.cuh"
+#include "sph_step.cuh"
+
+namespace sph {
+
+namespace {
+
+inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+constexpr int PAIR_THREADS = 128;
+
+// The centre line a - b of a touching pair under the image the cell search
+// uses (the nearest one: along a periodic axis a difference over half the
+// box is shifted by -+L), rounded as the FP64 form's (xa - xb) + shift;
+// code: the image code of a slot word (shift_code).
+__device__ __forceinline__ d3 centre_line(const DevBox &B, const double4 &xa, const double4 &xb,
+                                          uint32_t *code)
+{
+    double dx = __dsub_rn(xa.x, xb.x), dy = __dsub_rn(xa.y, xb.y);
+    const double dz = __dsub_rn(xa.z, xb.z);
+    int sx = 0, sy = 0;
+    if (B.periodic == 1 || B.periodic == 2) {
+        if (dx > 0.5 * B.L[0]) { dx = __dadd_rn(dx, -B.L[0]); sx = -1; }
+        else if (dx < -0.5 * B.L[0]) { dx = __dadd_rn(dx, B.L[0]); sx = 1; }
+    }
+    if (B.periodic == 1) {
+        if (dy > 0.5 * B.L[1]) { dy = __dadd_rn(dy, -B.L[1]); sy = -1; }
+        else if (dy < -0.5 * B.L[1]) { dy = __dadd_rn(dy, B.L[1]); sy = 1; }
+    }
+    if (code) *code = shift_code(sx, sy);
+    return mk(dx, dy, dz);
+}
+
+// vlen<LM> with the dot product rounded operation by operation.
+template <int LM>
+__device__ __forceinline__ double len_rn(d3 v)
+{
+    const double d = __dadd_rn(__dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y)),
+                               __dmul_rn(v.z, v.z));
+    if (LM == SPH_LEN_FP64) return __dsqrt_rn(d);
+    return (double)__fsqrt_rn(__double2float_rn(d));
+}
+
+__device__ __forceinline__ MixedPair mixed_pair_f(d3 x_ab, double x_length, double delta, float4 va,
+                                                  float4 vb, float4 wa, float4 wb, double ra,
+                                                  double rb)
+{
+    MixedPair q;
+    const float inv = 1.0f / (float)x_length;
+    q.n = fmul(inv, tof(x_ab));
+    q.vel_linear = fk(va.x - vb.x, va.y - vb.y, va.z - vb.z);
+    q.angvel_a = fk(wa.x, wa.y, wa.z);
+    q.angvel_b = fk(wb.x, wb.y, wb.z);
+    q.ra = (float)ra;
+    q.rb = (float)rb;
+    q.delta = (float)delta;
+    return q;
+}
+
+// The plane walls of contactsearch.cuh:428-465 and :602-701 for one sphere
+// of the list step: wall w is the box's wall w when w < nw, else the
+// default plane (top at L[2], sides at 0 and L); the normal force on wall 0
+// is returned.  Reads each wall from the box table where it is used.
+template <int LM>
+__device__ __forceinline__ double walls_pair(const DevBox &B, double4 xa, d3 vel_a, d3 angvel_a,
+                                             Acc &acc)
+{
+    const SphParams &Pm = B.P;
+    const double dt = B.dt, r = xa.w;
+    const uint32_t nw = B.nw;
+    auto plane = [&](uint32_t w, double dx, double dy, double dz, double dpos, d3 &n, double &pos,
+                     double &vel) {
+        if (w < nw) {
+            n = mk(B.wnx[w][0], B.wnx[w][1], B.wnx[w][2]);
+            pos = B.wnx[w][3];
+            vel = B.wmvfd[w][1];
+        } else {
+            n = mk(dx, dy, dz);
+            pos = dpos;
+            vel = 0.0;
+        }
+    };
+    d3 n;
+    double pos, wv, w0_force = 0.0;
+    plane(0, 0.0, 0.0, -1.0, B.L[2], n, pos, wv);
+    double delta_w = pos - (xa.z + r);
+    if (delta_w < 0.0) w0_force = contact_linear_wall<LM>(Pm, dt, acc, vel_a, angvel_a, r, n, delta_w, wv);
+    delta_w = xa.z - r - B.origo[2];
+    if (delta_w < 0.0)
+        (void)contact_linear_wall<LM>(Pm, dt, acc, vel_a, angvel_a, r, mk(0.0, 0.0, 1.0), delta_w, 0.0);
+    if (B.periodic == 0) {
+        plane(1, -1.0, 0.0, 0.0, B.L[0], n, pos, wv);
+        delta_w = pos - (xa.x + r);
+        if (delta_w < 0.0) (void)contact_linear_wall<LM>(Pm, dt, acc, vel_a, angvel_a, r, n, delta_w, wv);
+        plane(2, 1.0, 0.0, 0.0, 0.0, n, pos, wv);
+        delta_w = xa.x - r - pos;
+        if (delta_w < 0.0) (void)contact_linear_wall<LM>(Pm, dt, acc, vel_a, angvel_a, r, n, delta_w, wv);
+    }
+    if (B.periodic == 0 || B.periodic == 2) {
+        plane(3, 0.0, -1.0, 0.0, B.L[1], n, pos, wv);
+        delta_w = pos - (xa.y + r);
+        if (delta_w < 0.0) (void)contact_linear_wall<LM>(Pm, dt, acc, vel_a, angvel_a, r, n, delta_w, wv);
+        plane(4, 0.0, 1.0, 0.0, 0.0, n, pos, wv);
+        delta_w = xa.y - r - pos;
+        if (delta_w < 0.0) (void)contact_linear_wall<LM>(Pm, dt, acc, vel_a, angvel_a, r, n, delta_w, wv);
+    }
+    return w0_force;
+}
+
+// integration.cuh:14-305 (TY3) for one sphere of the list step: FP64
+// arithmetic on the compact state; the new state goes to the [nxt] half of
+// the ping-pong arrays and to the sphere's own arrays.
+__device__ __forceinline__ void integrate_pair(const StepArgs &A, const PairArgs &P,
+                                               const DevBox &B, uint32_t i, uint32_t nxt,
+                                               double4 x, double4 vel, float4 wf, d3 F, d3 T)
+{
+    const SphParams &Pm = B.P;
+    const double dt = B.dt;
+    const float4 apf = P.angpos[i];
+    double4 xyzsum = P.xyzsum[i];
+    double a0[3] = {0.0, 0.0, 0.0}, w0[3] = {0.0, 0.0, 0.0};
+    if (B.iter != 0) {
+        const float4 q = P.acc[i], r = P.angacc[i];
+        a0[0] = q.x; a0[1] = q.y; a0[2] = q.z;
+        w0[0] = r.x; w0[1] = r.y; w0[2] = r.z;
+    }
+    const double radius = x.w;
+    const double m = 4.0 / 3.0 * PI * radius * radius * radius * Pm.rho;
+    double acc[3], angacc[3];
+    acc[0] = F.x / m + Pm.g[0];
+    acc[1] = F.y / m + Pm.g[1];
+    acc[2] = F.z / m + Pm.g[2];
+    const double inertia = 2.0 / 5.0 * m * radius * radius;
+    angacc[0] = T.x / inertia;
+    angacc[1] = T.y / inertia;
+    angacc[2] = T.z / inertia;
+    if (vel.w > 0.0001 && vel.w < 10.0) {
+        acc[0] = 0.0;
+        acc[1] = 0.0;
+        acc[2] -= Pm.g[2];
+        angacc[0] = angacc[1] = angacc[2] = 0.0;
+    }
+    if (vel.w >= 10.0) {
+        acc[1] = 0.0;
+        angacc[0] = 0.0;
+        angacc[2] = 0.0;
+    }
+    if (vel.w < -0.0001) {
+        acc[0] = acc[1] = acc[2] = 0.0;
+        angacc[0] = angacc[1] = angacc[2] = 0.0;
+    }
+    const double xv[3] = {x.x, x.y, x.z};
+    const double vv[3] = {vel.x, vel.y, vel.z};
+    const double pv[3] = {apf.x, apf.y, apf.z};
+    const double wv[3] = {wf.x, wf.y, wf.z};
+    double sv[3] = {xyzsum.x, xyzsum.y, xyzsum.z};
+    double xn[3], vn[3], pn[3], wn[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double dacc = (acc[d] - a0[d]) / dt;
+        const double dangacc = (angacc[d] - w0[d]) / dt;
+        const double dx = vv[d] * dt + 0.5 * acc[d] * dt * dt + 1.0 / 6.0 * dacc * dt * dt * dt;
+        xn[d] = xv[d] + dx;
+        vn[d] = vv[d] + acc[d] * dt + 0.5 * dacc * dt * dt;
+        pn[d] = pv[d] + wv[d] * dt + 0.5 * angacc[d] * dt * dt + 1.0 / 6.0 * dangacc * dt * dt * dt;
+        wn[d] = wv[d] + angacc[d] * dt + 0.5 * dangacc * dt * dt;
+        sv[d] += dx;
+    }
+    if (B.periodic == 1) {
+        if (xn[0] < B.origo[0]) xn[0] += B.L[0];
+        if (xn[0] > B.L[0]) xn[0] -= B.L[0];
+        if (xn[1] < B.origo[1]) xn[1] += B.L[1];
+        if (xn[1] > B.L[1]) xn[1] -= B.L[1];
+    } else if (B.periodic == 2) {
+        if (xn[0] < B.origo[0]) xn[0] += B.L[0];
+        if (xn[0] > B.L[0]) xn[0] -= B.L[0];
+    }
+    {
+        // neighbour-list validity: displacement since the list build
+        // (nearest periodic image), FP32
+        const float4 r = A.xref[i];
+        float ex = (float)xn[0] - r.x, ey = (float)xn[1] - r.y;
+        const float ez = (float)xn[2] - r.z;
+        if (B.periodic == 1 || B.periodic == 2) {
+            const float lx = (float)B.L[0];
+            if (ex > 0.5f * lx) ex -= lx;
+            else if (ex < -0.5f * lx) ex += lx;
+        }
+        if (B.periodic == 1) {
+            const float ly = (float)B.L[1];
+            if (ey > 0.5f * ly) ey -= ly;
+            else if (ey < -0.5f * ly) ey += ly;
+        }
+        if (!(ex * ex + ey * ey + ez * ez <= B.vdisp2)) A.vflag[0] = 1u;
+    }
+    if (vel.w > 5.0 && vel.w < 10.0) {
+        if (B.change_velocity_state == 1) vn[0] *= 10.0;
+        else if (B.change_velocity_state == -1) vn[0] /= 10.0;
+    }
+    P.xyzsum[i] = make_double4(sv[0], sv[1], sv[2], 0.0);
+    P.acc[i] = make_float4((float)acc[0], (float)acc[1], (float)acc[2], 0.f);
+    P.angacc[i] = make_float4((float)angacc[0], (float)angacc[1], (float)angacc[2], 0.f);
+    P.angpos[i] = make_float4((float)pn[0], (float)pn[1], (float)pn[2], apf.w);
+    P.vel[i] = make_double4(vn[0], vn[1], vn[2], vel.w);
+    P.xr[nxt][i] = make_double4(xn[0], xn[1], xn[2], x.w);
+    P.vw[nxt][2 * i] = make_float4((float)vn[0], (float)vn[1], (float)vn[2], 0.f);
+    P.vw[nxt][2 * i + 1] = make_float4((float)wn[0], (float)wn[1], (float)wn[2], 0.f);
+}
+
+// One step of the list form, one thread per sphere: the sphere's list
+// entries in order, each tested with the exact FP64 overlap test and, for a
+// touching pair, the contact law with the entry's history (the loads of the
+// next entry -- partner state and, when its pair touched, its history --
+// issued before the current entry is computed); then walls, sums and the
+// integration of the sphere.
+template <int LM>
+__global__ void __launch_bounds__(PAIR_THREADS, 4) k_pair_step(StepArgs A, PairArgs P)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.ntot) return;
+    const uint32_t cur = *P.pp, nxt = cur ^ 1u, ls = *P.lsel;
+    const double4 *__restrict__ xr = P.xr[cur];
+    const float4 *__restrict__ vw = P.vw[cur];
+    const DevBox &B = A.boxes[box_index(A, i)];
+    uint32_t n = P.cnt[ls][i];
+    if (n > (uint32_t)VL_MAX) {   // the list overflowed at its build
+        raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+        n = 0;
+    }
+    const unsigned long long live_old = P.live[ls][i];
+    unsigned long long live_new = 0ull;
+    const uint32_t *__restrict__ lst = P.ids[ls] + (size_t)i * VL_MAX;
+    double *__restrict__ hist = P.hist[ls] + (size_t)i * VL_MAX * 3;
+    const double4 xa = xr[i];
+    const float4 va = vw[2 * i], wa = vw[2 * i + 1];
+    const double dt = B.dt;
+
+    Acc acc;
+    acc.F = mk(0.0, 0.0, 0.0);
+    acc.T = mk(0.0, 0.0, 0.0);
+    acc.es_dot = 0.0;
+    acc.ev_dot = 0.0;
+    acc.p = 0.0;
+    double4 xb = make_double4(0.0, 0.0, 0.0, 0.0);
+    float4 vb = make_float4(0.f, 0.f, 0.f, 0.f), wb = vb;
+    d3 hb = mk(0.0, 0.0, 0.0);
+    if (n) {
+        const uint32_t b = lst[0];
+        xb = xr[b];
+        vb = vw[2 * b];
+        wb = vw[2 * b + 1];
+        if (live_old & 1ull) hb = mk(hist[0], hist[1], hist[2]);
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+        double4 xq = xb;
+        float4 vq = vb, wq = wb;
+        d3 hq = mk(0.0, 0.0, 0.0);
+        if (k + 1 < n) {
+            const uint32_t b = lst[k + 1];
+            xq = xr[b];
+            vq = vw[2 * b];
+            wq = vw[2 * b + 1];
+            if ((live_old >> (k + 1)) & 1ull)
+                hq = mk(hist[3 * (k + 1)], hist[3 * (k + 1) + 1], hist[3 * (k + 1) + 2]);
+        }
+        const d3 x_ab = centre_line(B, xa, xb, nullptr);
+        const double x_ab_length = len_rn<LM>(x_ab);
+        const double delta_n = __dsub_rn(x_ab_length, __dadd_rn(xa.w, xb.w));
+        if (delta_n < 0.0) {
+            const MixedPair q = mixed_pair_f(x_ab, x_ab_length, delta_n, va, vb, wa, wb, xa.w, xb.w);
+            const d3 nd = B.P.contactmodel == 2 ? contact_linear_mixed(B.P, dt, acc, q, hb)
+                                                : contact_hertz_mixed(B.P, dt, acc, q, hb);
+            hist[3 * k] = nd.x;
+            hist[3 * k + 1] = nd.y;
+            hist[3 * k + 2] = nd.z;
+            live_new |= 1ull << k;
+        }
+        xb = xq;
+        vb = vq;
+        wb = wq;
+        hb = hq;
+    }
+    if (__popcll(live_new) > NC) raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+    if (live_new != live_old) P.live[ls][i] = live_new;
+
+    const double4 vel = P.vel[i];
+    const double w0_force = walls_pair<LM>(B, xa, xyz(vel), mk(wa.x, wa.y, wa.z), acc);
+    P.force[i] = make_float4((float)acc.F.x, (float)acc.F.y, (float)acc.F.z, 0.f);
+    P.torque[i] = make_float4((float)acc.T.x, (float)acc.T.y, (float)acc.T.z, 0.f);
+    P.epp[i] = make_float4((float)acc.es_dot, (float)acc.ev_dot, (float)acc.p, 0.f);
+    const double2 e0 = P.eacc[i];
+    P.eacc[i] = make_double2(e0.x + acc.es_dot * dt, e0.y + acc.ev_dot * dt);
+    if (B.nw > 0) A.wf_pp[i] = w0_force;
+    integrate_pair(A, P, B, i, nxt, xa, vel, wa, acc.F, acc.T);
+}
+
+// Wall-force sum of one chunk of 2^chunk_log2 spheres of one box: each
+// thread adds its strided share in index order, then a fixed shuffle tree
+// and the warps' sums in warp order (FP64, the same order every step).
+constexpr int CHUNK_THREADS = 256;
+
+__global__ void __launch_bounds__(CHUNK_THREADS) k_pair_chunks(StepArgs A, PairArgs P)
+{
+    grid_dependency_wait();
+    __shared__ double s_w[CHUNK_THREADS / 32];
+    const uint32_t c = blockIdx.x;
+    const uint32_t bx = P.chunk_box[c];
+    const DevBox &B = A.boxes[bx];
+    const uint32_t start = (c - P.box_chunk0[bx]) << P.chunk_log2;
+    const uint32_t end = min(B.np, start + (1u << P.chunk_log2));
+    double s = 0.0;
+    if (B.nw > 0)
+        for (uint32_t k = start + threadIdx.x; k < end; k += CHUNK_THREADS) s += A.wf_pp[B.p_base + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31u) == 0) s_w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < CHUNK_THREADS / 32; ++w) t += s_w[w];
+        P.chunk_part[c] = t;
+    }
+}
+
+// Per box: the chunks' sums in chunk order (FP64), then integrateWalls and
+// the time bookkeeping (advance_box); block 0 then hands the ping-pong
+// state to the next step.
+constexpr int PBOX_THREADS = 128;
+
+__global__ void __launch_bounds__(PBOX_THREADS) k_pair_box(StepArgs A, PairArgs P)
+{
+    grid_dependency_wait();
+    __shared__ double s_w[PBOX_THREADS / 32];
+    const uint32_t bx = blockIdx.x;
+    DevBox &B = A.boxes[bx];
+    bool any = false;
+    for (uint32_t w = 0; w < B.nw; ++w) any = any || B.wmode[w] != 0;
+    double s = 0.0;
+    if (B.np > 0 && any) {
+        const uint32_t c0 = P.box_chunk0[bx];
+        const uint32_t nch = (B.np + (1u << P.chunk_log2) - 1) >> P.chunk_log2;
+        for (uint32_t k = threadIdx.x; k < nch; k += PBOX_THREADS) s += P.chunk_part[c0 + k];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31u) == 0) s_w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double fsum = 0.0;
+    for (int w = 0; w < PBOX_THREADS / 32; ++w) fsum += s_w[w];
+    advance_box(B, fsum);
+    if (bx == 0) *P.pp ^= 1u;
+}
+
+// Rebuild request -> the condition of the rebuild node.
+__global__ void k_pair_cond(cudaGraphConditionalHandle hc, const uint32_t *vflag)
+{
+    cudaGraphSetConditional(hc, vflag[0] != 0u ? 1u : 0u);
+}
+
+// After a list build into the buffers not in use: each sphere's touching
+// entries (and their histories) carried over to the new list -- from the
+// old list, or, after pair_load, from the FP64 contact rows.
+__global__ void k_pair_remap(StepArgs A, PairArgs P)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.ntot) return;
+    const uint32_t ls = *P.lsel, nw = ls ^ 1u;
+    const uint32_t *nid = P.ids[nw] + (size_t)i * VL_MAX;
+    uint32_t nn = P.cnt[nw][i];
+    if (nn > (uint32_t)VL_MAX) nn = 0;   // overflowed: raised by the step kernel
+    double *nh = P.hist[nw] + (size_t)i * VL_MAX * 3;
+    unsigned long long live = 0ull;
+    auto find = [&](uint32_t b) -> int {
+        int lo = 0, hi = (int)nn;   // first entry >= b
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (nid[mid] < b) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo < (int)nn && nid[lo] == b ? lo : -1;
+    };
+    if (*P.from_rows) {
+        for (int s = 0; s < NC; ++s) {
+            const uint32_t w = A.slots[(size_t)i * NC + s];
+            if (w == EMPTY) continue;
+            const int k = find(w & ID_MASK);
+            if (k < 0) continue;
+            const double4 h = A.hist[(size_t)i * NC + s];
+            nh[3 * k] = h.x;
+            nh[3 * k + 1] = h.y;
+            nh[3 * k + 2] = h.z;
+            live |= 1ull << k;
+        }
+    } else {
+        const uint32_t *oid = P.ids[ls] + (size_t)i * VL_MAX;
+        const double *oh = P.hist[ls] + (size_t)i * VL_MAX * 3;
+        const uint32_t on = min(P.cnt[ls][i], (uint32_t)VL_MAX);
+        for (unsigned long long m = P.live[ls][i]; m; m &= m - 1ull) {
+            const int ko = __ffsll((long long)m) - 1;
+            if ((uint32_t)ko >= on) break;
+            const int k = find(oid[ko]);
+            if (k < 0) continue;
+            nh[3 * k] = oh[3 * ko];
+            nh[3 * k + 1] = oh[3 * ko + 1];
+            nh[3 * k + 2] = oh[3 * ko + 2];
+            live |= 1ull << k;
+        }
+    }
+    P.live[nw][i] = live;
+}
+
+__global__ void k_pair_done(StepArgs A, PairArgs P)
+{
+    *P.lsel ^= 1u;
+    *P.from_rows = 0u;
+    A.vflag[0] = 0u;
+    A.vflag[1] += 1u;
+}
+
+// The FP64 arrays -> the compact state (into the [*pp] half); the next step
+// rebuilds the lists and takes the histories from the contact rows.
+__global__ void k_pair_load(StepArgs A, PairArgs P)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t c = *P.pp;
+    if (i == 0) {
+        *P.from_rows = 1u;
+        A.vflag[0] = 1u;
+    }
+    if (i >= A.ntot) return;
+    const double4 v = A.vel[i], w = A.angvel[i], ap = A.angpos[i];
+    const double4 ac = A.acc[i], aa = A.angacc[i], f = A.force[i], t = A.torque[i];
+    P.xr[c][i] = A.x[i];
+    P.vel[i] = v;
+    P.vw[c][2 * i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+    P.vw[c][2 * i + 1] = make_float4((float)w.x, (float)w.y, (float)w.z, 0.f);
+    P.angpos[i] = make_float4((float)ap.x, (float)ap.y, (float)ap.z, (float)ap.w);
+    P.xyzsum[i] = A.xyzsum[i];
+    P.acc[i] = make_float4((float)ac.x, (float)ac.y, (float)ac.z, 0.f);
+    P.angacc[i] = make_float4((float)aa.x, (float)aa.y, (float)aa.z, (float)aa.w);
+    P.force[i] = make_float4((float)f.x, (float)f.y, (float)f.z, 0.f);
+    P.torque[i] = make_float4((float)t.x, (float)t.y, (float)t.z, 0.f);
+    P.epp[i] = make_float4((float)A.es_dot[i], (float)A.ev_dot[i], (float)A.p[i], 0.f);
+    P.eacc[i] = make_double2(A.es[i], A.ev[i]);
+}
+
+// The compact state -> the FP64 arrays, and the touching entries of each
+// list -> the sphere's contact row (in list order, slots 0, 1, ...) with
+// their histories and image codes.
+__global__ void k_pair_flush(StepArgs A, PairArgs P)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.ntot) return;
+    const uint32_t c = *P.pp, ls = *P.lsel;
+    const double4 xa = P.xr[c][i];
+    const float4 w = P.vw[c][2 * i + 1], ap = P.angpos[i], ac = P.acc[i], aa = P.angacc[i];
+    const float4 f = P.force[i], t = P.torque[i], e = P.epp[i];
+    const double2 ea = P.eacc[i];
+    A.x[i] = xa;
+    A.vel[i] = P.vel[i];
+    A.angvel[i] = make_double4(w.x, w.y, w.z, 0.0);
+    A.angpos[i] = make_double4(ap.x, ap.y, ap.z, ap.w);
+    A.xyzsum[i] = P.xyzsum[i];
+    A.acc[i] = make_double4(ac.x, ac.y, ac.z, 0.0);
+    A.angacc[i] = make_double4(aa.x, aa.y, aa.z, aa.w);
+    A.force[i] = make_double4(f.x, f.y, f.z, 0.0);
+    A.torque[i] = make_double4(t.x, t.y, t.z, 0.0);
+    A.es_dot[i] = e.x;
+    A.ev_dot[i] = e.y;
+    A.p[i] = e.z;
+    A.es[i] = ea.x;
+    A.ev[i] = ea.y;
+    const DevBox &B = A.boxes[box_index(A, i)];
+    const uint32_t *ids = P.ids[ls] + (size_t)i * VL_MAX;
+    const double *h = P.hist[ls] + (size_t)i * VL_MAX * 3;
+    const uint32_t nn = min(P.cnt[ls][i], (uint32_t)VL_MAX);
+    int s = 0;
+    for (unsigned long long m = P.live[ls][i]; m && s < NC; m &= m - 1ull) {
+        const int k = __ffsll((long long)m) - 1;
+        if ((uint32_t)k >= nn) break;
+        const uint32_t b = ids[k];
+        uint32_t code = 0;
+        (void)centre_line(B, xa, P.xr[c][b], &code);
+        A.slots[(size_t)i * NC + s] = b | (code << CODE_SHIFT);
+        A.hist[(size_t)i * NC + s] = make_double4(h[3 * k], h[3 * k + 1], h[3 * k + 2], 0.0);
+        ++s;
+    }
+    for (; s < NC; ++s) {
+        A.slots[(size_t)i * NC + s] = EMPTY;
+        A.hist[(size_t)i * NC + s] = make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+}
+
+__global__ void k_pair_count(StepArgs A, PairArgs P, unsigned long long *count)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t ls = *P.lsel;
+    const unsigned long long v = i < A.ntot ? (unsigned long long)__popcll(P.live[ls][i]) : 0ull;
+    unsigned long long s = v;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31u) == 0 && s) atomicAdd(count, s);
+}
+
+inline void record(cudaEvent_t ev, cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal);
+    else cudaEventRecord(ev, st);
+}
+
+inline void mark(Prof *prof, cudaStream_t st, const char *name)
+{
+    if (!prof || prof->n >= Prof::MAX) return;
+    prof->name[prof->n] = name;
+    record(prof->ev[prof->n + 1], st);
+    prof->n++;
+}
+
+void launch_rebuild_body(const StepArgs &A, const PairArgs &P, cudaStream_t st)
+{
+    launch_pair_sort_build(A, P, st);
+    k_pair_remap<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A, P);
+    k_pair_done<<<1, 1, 0, st>>>(A, P);
+}
+
+}  // namespace
+
+// One step of the list form on st.  Under stream capture the list rebuild
+// is a conditional node (run when the integration of the step before asked
+// for it); outside a capture the request is read on the host.  cfg.side:
+// a second stream, on which the conditional node's body is captured.
+int launch_step_pair(const StepArgs &A, const PairArgs &P, const StepConfig &cfg, cudaStream_t st,
+                     uint64_t *launches, Prof *prof)
+{
+    uint64_t nl = 0;
+    if (prof) {
+        prof->n = 0;
+        record(prof->ev[0], st);
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return SPH_ERR_CUDA;
+    if (cs == cudaStreamCaptureStatusActive) {
+        if (!cfg.side) return SPH_ERR_CUDA;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        cudaGraphConditionalHandle hc;
+        if (cudaGraphConditionalHandleCreate(&hc, g, 0u, cudaGraphCondAssignDefault) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        k_pair_cond<<<1, 1, 0, st>>>(hc, A.vflag);
+        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = hc;
+        np.conditional.type = cudaGraphCondTypeIf;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, g, deps, nd, &np) != cudaSuccess) return SPH_ERR_CUDA;
+        if (cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) !=
+            cudaSuccess)
+            return SPH_ERR_CUDA;
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        if (cudaStreamBeginCaptureToGraph(cfg.side, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        launch_rebuild_body(A, P, cfg.side);
+        cudaGraph_t done = nullptr;
+        if (cudaStreamEndCapture(cfg.side, &done) != cudaSuccess) return SPH_ERR_CUDA;
+        nl += 1;
+    } else {
+        uint32_t flag = 0;
+        if (cudaMemcpyAsync(&flag, A.vflag, sizeof flag, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        if (flag) launch_rebuild_body(A, P, st);
+    }
+    mark(prof, st, "k_pair_cond");
+    if (cfg.lenmode == SPH_LEN_FP64)
+        k_pair_step<SPH_LEN_FP64><<<blocks_for(A.ntot, PAIR_THREADS), PAIR_THREADS, 0, st>>>(A, P);
+    else
+        k_pair_step<SPH_LEN_REFERENCE><<<blocks_for(A.ntot, PAIR_THREADS), PAIR_THREADS, 0, st>>>(A, P);
+    mark(prof, st, "k_pair_step");
+    const bool pdl = prof == nullptr;
+    if (cfg.any_walls) {
+        launch_k(pdl, k_pair_chunks, P.nchunks, CHUNK_THREADS, st, A, P);
+        mark(prof, st, "k_pair_chunks");
+        nl += 1;
+    }
+    launch_k(pdl && cfg.any_walls, k_pair_box, A.nboxes, PBOX_THREADS, st, A, P);
+    mark(prof, st, "k_pair_box");
+    nl += 2;
+    if (launches) *launches += nl;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "sphere_b200: list-step launch failed: %s\n", cudaGetErrorString(e));
+        return SPH_ERR_CUDA;
+    }
+    return SPH_OK;
+}
+
+int pair_load(const StepArgs &A, const PairArgs &P, cudaStream_t st)
+{
+    k_pair_load<<<blocks_for(A.ntot ? A.ntot : 1, 256), 256, 0, st>>>(A, P);
+    return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+}
+
+int pair_flush(const StepArgs &A, const PairArgs &P, cudaStream_t st)
+{
+    if (A.ntot) k_pair_flush<<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, P);
+    return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+}
+
+int pair_count_live(const StepArgs &A, const PairArgs &P, cudaStream_t st,
+                    unsigned long long *d_count)
+{
+    cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st);
+    if (A.ntot) k_pair_count<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A, P, d_count);
+    return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+}
+
+}  // namespace sph

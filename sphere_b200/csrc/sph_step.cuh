@@ -147,6 +147,45 @@ __device__ __forceinline__ void integrate_particle(const StepArgs &A, const DevB
     A.x[i] = make_double4(xn[0], xn[1], xn[2], x.w);
 }
 
+// integration.cuh:344-450 integrateWalls with the wall-force total fsum,
+// then the loop bookkeeping of device.cu:2536-2538, the adaptive grid of
+// device.cu:1050 and the velocity-step state of device.cu:2455-2462 for
+// the next step.  One thread per box.
+__device__ __forceinline__ void advance_box(DevBox &B, double fsum)
+{
+    const double dt = B.dt;
+    if (B.np > 0) {
+        for (uint32_t w = 0; w < B.nw; ++w) {
+            const int wmode = B.wmode[w];
+            if (wmode == 0) continue;
+            const double acc0 = B.iter == 0 ? 0.0 : B.wacc[w];
+            B.wmvfd[w][2] = fsum;
+            const double sigma_0 =
+                B.wmvfd[w][3] + B.P.sigma0_A * sin(2.0 * PI * B.P.sigma0_f * B.t_current);
+            const double N = -sigma_0 * B.L[0] * B.L[1];
+            double acc = (B.wmvfd[w][2] + N) / B.wmvfd[w][0];
+            if (wmode == 2) acc = 0.0;
+            const double dacc_dt = (acc - acc0) / dt;
+            B.wnx[w][3] += B.wmvfd[w][1] * dt + 0.5 * acc * dt * dt + 1.0 / 6.0 * dacc_dt * dt * dt * dt;
+            B.wmvfd[w][1] += acc * dt + 0.5 * dacc_dt * dt * dt;
+            B.wacc[w] = acc;
+        }
+    }
+    B.t_current += dt;
+    B.iter += 1;
+    B.L2_out = B.L[2];
+    if (B.adaptive == 1 && B.nw > 0) B.L[2] = B.wnx[0][3];
+    int change = 0;
+    if (B.t_current >= 10.0 && B.t_current < 15.0 && B.velocity_state == 1) {
+        change = 1;
+        B.velocity_state = 2;
+    } else if (B.t_current >= 15.0 && B.velocity_state == 2) {
+        change = -1;
+        B.velocity_state = 1;
+    }
+    B.change_velocity_state = change;
+}
+
 // ------------------------------------------------------------------ interact
 
 // Neighbour-list entry k of sphere a (partner id bo): the cell search visits

@@ -248,7 +248,7 @@ class Stepper(object):
         """Time each launch variant of the interact kernel for `steps` steps
         from the current state, keep the fastest, restore the state
         (sph_autotune).  Returns (chosen, [ms per step of each variant])."""
-        ms = numpy.zeros(4)
+        ms = numpy.zeros(_abi.TUNE_VARIANTS)
         ch = C.c_int(-1)
         self._check(self.lib.sph_autotune(self.h, int(steps), _abi.dptr(ms), C.byref(ch)),
                     "sph_autotune")
@@ -349,6 +349,17 @@ class Stepper(object):
         self._check(self.lib.sph_get_contacts(self.h, _abi.uptr(c), _abi.dptr(dt), _abi.dptr(dm)),
                     "sph_get_contacts")
         return c, dt, dm
+
+    def set_contacts(self, contacts, delta_t=None):
+        """Contact rows and tangential histories in the layout contacts()
+        returns (sph_set_contacts), e.g. to continue a run in another handle
+        with its contact history."""
+        c = numpy.ascontiguousarray(contacts, dtype=numpy.uint32).reshape(-1)
+        d = None if delta_t is None else numpy.ascontiguousarray(delta_t,
+                                                                 dtype=numpy.float64).reshape(-1)
+        self._check(self.lib.sph_set_contacts(self.h, _abi.uptr(c),
+                                              _abi.dptr(d) if d is not None else None),
+                    "sph_set_contacts")
 
     def sort_products(self):
         n = self.ntot

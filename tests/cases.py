@@ -89,10 +89,16 @@ def make(name):
         # cohesion.cuh:237-277): a lattice a little wider than the spheres,
         # so that most neighbours sit at gaps between 0 and db, soft
         # contacts (k_n = 1e4) and kappa = 10, so that the capillary forces
-        # are ~1/4 of the force field (relative L2 after one step: 0.23)
+        # are ~1/4 of the force field (relative L2 after one step: 0.23).
+        # The capillary force jumps from ~3 N to 0 where a gap passes db;
+        # a short time step (dt_scale 0.02) and slow spheres keep the gaps'
+        # changes small over the 20 steps, so that the ~1e-11 m by which
+        # the FP32 expf roundings (below) move the spheres cannot put a gap
+        # on the other side of db in one run than in the other.
         s = scenes.lattice_pack(500, seed=14, periodic=1, contactmodel=1, gamma_n=0.0,
                                 gamma_t=1.0, k_n=1.0e4, r_min=0.0095, r_max=0.0105,
-                                spacing=0.0203, jitter=0.0006, nw=0)
+                                spacing=0.0203, jitter=0.0006, nw=0, dt_scale=0.02,
+                                vel_sigma=0.005, angvel_sigma=0.1)
         s.kappa[0] = 10.0
         s.V_b[0] = 1.0e-9
         s.db[0] = 1.0e-3

@@ -317,6 +317,15 @@ int sph_neighbor_stats(SphHandle *h, uint64_t *stats);
 #define SPH_TUNE_VARIANTS 5
 int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen);
 int sph_set_variant(SphHandle *h, int variant);
+/* Launch shape of the list step (variant 4): threads per block x resident
+ * blocks per SM, i.e. its register budget -- 0: 128 x 4, 1: 128 x 5,
+ * 2: 128 x 6, 3: 64 x 8, 4: 256 x 2 (SPH_PAIR_SHAPES); the results do not
+ * depend on it.  sph_autotune tries every shape of variant 4 and reports
+ * the best in ms_per_step[4]; sph_get_tuning returns the variant and shape
+ * in use. */
+#define SPH_PAIR_SHAPES 5
+int sph_set_launch_shape(SphHandle *h, int shape);
+int sph_get_tuning(const SphHandle *h, int *variant, int *shape);
 
 /* Output snapshot, the output path of the reference's loop
  * (transferFromGlobalDeviceMemory before each output file,

@@ -231,6 +231,10 @@ def load_library():
     lib.sph_autotune.restype = C.c_int
     lib.sph_set_variant.argtypes = [H, C.c_int]
     lib.sph_set_variant.restype = C.c_int
+    lib.sph_set_launch_shape.argtypes = [H, C.c_int]
+    lib.sph_set_launch_shape.restype = C.c_int
+    lib.sph_get_tuning.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.sph_get_tuning.restype = C.c_int
     lib.sph_set_neighbor_lists.restype = C.c_int
     lib.sph_adjoint_forward.argtypes = [H, C.c_uint64, C.c_uint32, _dp]
     lib.sph_cell_offsets_static.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]

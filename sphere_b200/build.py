@@ -26,7 +26,7 @@ SOURCES = [
     ("sph_kernels.cu", ["-fmad=false"]),
     ("sph_capi.cu", ["-fmad=false"]),
     ("sph_mixed.cu", ["-fmad=true"]),
-    ("sph_pair.cu", ["-fmad=true"]),
+    ("sph_pair.cu", ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("sph_adjoint.cu", ["-fmad=false"]),
     ("sph_noalloc.cu", []),
     ("sph_render.cu", ["-fmad=false"]),

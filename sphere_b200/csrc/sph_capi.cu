@@ -168,6 +168,7 @@ static int ensure_pair(SphHandle *h)
         (st = dalloc(h, &P.ids[0], n * sph::VL_MAX)) || (st = dalloc(h, &P.ids[1], n * sph::VL_MAX)) ||
         (st = dalloc(h, &P.cnt[0], n)) || (st = dalloc(h, &P.cnt[1], n)) ||
         (st = dalloc(h, &P.live[0], n)) || (st = dalloc(h, &P.live[1], n)) ||
+        (st = dalloc(h, &P.order[0], n)) || (st = dalloc(h, &P.order[1], n)) ||
         (st = dalloc(h, &P.hist[0], 3 * n * sph::VL_MAX)) ||
         (st = dalloc(h, &P.hist[1], 3 * n * sph::VL_MAX)) || (st = dalloc(h, &words, 3)) ||
         (st = dalloc(h, &P.chunk_part, cbox.size())) || (st = dalloc(h, &chunk_box, cbox.size())) ||
@@ -1754,6 +1755,24 @@ int sph_set_variant(SphHandle *h, int variant)
     return drop_graphs(h);
 }
 
+int sph_set_launch_shape(SphHandle *h, int shape)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (shape < 0 || shape >= sph::PAIR_SHAPES) return fail(h, SPH_ERR_INPUT, "shape out of range");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->cfg.pair_shape = shape;
+    return drop_graphs(h);
+}
+
+int sph_get_tuning(const SphHandle *h, int *variant, int *shape)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (variant) *variant = h->cfg.variant;
+    if (shape) *shape = h->cfg.pair_shape;
+    return SPH_OK;
+}
+
 int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
 {
     if (!h || steps == 0) return SPH_ERR_INPUT;
@@ -1774,10 +1793,13 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    int best = h->cfg.variant, st = SPH_OK;
+    int best = h->cfg.variant, best_shape = h->cfg.pair_shape, st = SPH_OK;
     double best_ms = 1e300;
-    for (int v = 0; v < sph::INTERACT_VARIANTS && st == SPH_OK; ++v) {
-        if (ms_per_step) ms_per_step[v] = -1.0;
+    // the variants, and the list step at each of its launch shapes
+    for (int t = 0; t < sph::INTERACT_VARIANTS - 1 + sph::PAIR_SHAPES && st == SPH_OK; ++t) {
+        const int v = t < sph::INTERACT_VARIANTS ? t : sph::PAIR_VARIANT;
+        const int shape = t < sph::PAIR_VARIANT ? 0 : t - sph::PAIR_VARIANT;
+        if (ms_per_step && t <= sph::PAIR_VARIANT) ms_per_step[v] = -1.0;
         // the split step needs contact models 2/3, fused integration,
         // neighbour lists and its buffers; otherwise it is not a candidate
         if (v == sph::SPLIT_VARIANT &&
@@ -1786,6 +1808,7 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
         // the list step: the FP32-mixed form's cases it covers
         if (v == sph::PAIR_VARIANT && (!pair_eligible(h) || ensure_pair(h) != SPH_OK)) continue;
         h->cfg.variant = v;
+        h->cfg.pair_shape = shape;
         if ((st = drop_graphs(h)) != SPH_OK || (st = build_graph(h)) != SPH_OK) break;
         copy_state(h, snap, 0, false);
         invalidate_pair(h);
@@ -1799,10 +1822,11 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         const double per = (double)ms / steps;
-        if (ms_per_step) ms_per_step[v] = per;
+        if (ms_per_step && (ms_per_step[v] < 0.0 || per < ms_per_step[v])) ms_per_step[v] = per;
         if (per < best_ms) {
             best_ms = per;
             best = v;
+            best_shape = shape;
         }
     }
     copy_state(h, snap, 0, false);
@@ -1815,6 +1839,7 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
     h->launches = launches_saved;
     cudaMemset(h->A.err, 0, sizeof(uint32_t));
     h->cfg.variant = best;
+    h->cfg.pair_shape = best_shape;
     const int st2 = drop_graphs(h);
     if (st != SPH_OK) return fail(h, st, "autotune step failed");
     if (chosen) *chosen = best;

@@ -104,6 +104,10 @@ struct PairArgs {
     uint32_t *ids[2], *cnt[2];
     uint64_t *live[2];
     double *hist[2];
+    // the order in which the step kernel's threads take the spheres: within
+    // each group of PAIR_ORDER_GROUP consecutive spheres, by list length
+    // (built with each list), so that a warp's lists are of similar length
+    uint32_t *order[2];
     uint32_t *pp, *lsel;
     uint32_t *from_rows;       // != 0: the next rebuild takes histories from A.slots / A.hist
     double *chunk_part;        // [nchunks]
@@ -113,6 +117,8 @@ struct PairArgs {
     const uint32_t *box_chunk0;   // first chunk of each box
 };
 constexpr int PAIR_CHUNK_LOG2 = 11;
+constexpr int PAIR_SHAPES = 5;
+constexpr int PAIR_ORDER_GROUP = 128;   // launch shapes of the list-step kernel (sph_pair.cu)
 
 // Overlap search of one box (sph_overlaps): positions and velocities, the
 // box's spheres [p0, p0 + np), its grid (origin, cell widths, cell counts),
@@ -142,6 +148,7 @@ struct StepConfig {
     bool unfused;     // some box has a shear-stress (wmode 3) top wall
     bool any_walls;   // some box has nw > 0
     int variant = 1;  // interact launch variant (sph_autotune)
+    int pair_shape = 0;   // register budget of the list-step kernel (sph_autotune)
     bool all_cm23 = false;   // every box uses contact model 2 or 3
     int phase = STEP_WHOLE;
     cudaStream_t side = nullptr;                       // STEP_OVERLAP only

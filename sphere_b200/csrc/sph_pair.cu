@@ -34,8 +34,10 @@
 // more than half the skin since the last build: a conditional graph node
 // whose body is the cell sort, the list build and the history carry-over
 // (launch_step_pair), set by k_pair_cond from the flag the integration
-// raises.  Compiled with FMA contraction; the overlap test is written with
-// explicitly rounded operations so that it matches the FP64 form.
+// raises.  Compiled with FMA contraction and with FP32 division and square
+// root to within an ulp or two (the contact laws' FP32 part); the overlap
+// test is written with explicitly rounded operations so that it matches the
+// FP64 form.
 #include <cstdint>
 #include <cstdio>
 
@@ -50,7 +52,6 @@ namespace {
 
 inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
-constexpr int PAIR_THREADS = 128;
 
 // The centre line a - b of a touching pair under the image the cell search
 // uses (the nearest one: along a periodic axis a difference over half the
@@ -169,14 +170,16 @@ __device__ __forceinline__ void integrate_pair(const StepArgs &A, const PairArgs
     }
     const double radius = x.w;
     const double m = 4.0 / 3.0 * PI * radius * radius * radius * Pm.rho;
+    // reciprocals once (FP64 divisions are long instruction sequences)
+    const double inv_m = 1.0 / m, inv_dt = 1.0 / dt;
+    const double inv_i = inv_m * (5.0 / 2.0) / (radius * radius);
     double acc[3], angacc[3];
-    acc[0] = F.x / m + Pm.g[0];
-    acc[1] = F.y / m + Pm.g[1];
-    acc[2] = F.z / m + Pm.g[2];
-    const double inertia = 2.0 / 5.0 * m * radius * radius;
-    angacc[0] = T.x / inertia;
-    angacc[1] = T.y / inertia;
-    angacc[2] = T.z / inertia;
+    acc[0] = F.x * inv_m + Pm.g[0];
+    acc[1] = F.y * inv_m + Pm.g[1];
+    acc[2] = F.z * inv_m + Pm.g[2];
+    angacc[0] = T.x * inv_i;
+    angacc[1] = T.y * inv_i;
+    angacc[2] = T.z * inv_i;
     if (vel.w > 0.0001 && vel.w < 10.0) {
         acc[0] = 0.0;
         acc[1] = 0.0;
@@ -200,8 +203,8 @@ __device__ __forceinline__ void integrate_pair(const StepArgs &A, const PairArgs
     double xn[3], vn[3], pn[3], wn[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const double dacc = (acc[d] - a0[d]) / dt;
-        const double dangacc = (angacc[d] - w0[d]) / dt;
+        const double dacc = (acc[d] - a0[d]) * inv_dt;
+        const double dangacc = (angacc[d] - w0[d]) * inv_dt;
         const double dx = vv[d] * dt + 0.5 * acc[d] * dt * dt + 1.0 / 6.0 * dacc * dt * dt * dt;
         xn[d] = xv[d] + dx;
         vn[d] = vv[d] + acc[d] * dt + 0.5 * dacc * dt * dt;
@@ -256,12 +259,13 @@ __device__ __forceinline__ void integrate_pair(const StepArgs &A, const PairArgs
 // next entry -- partner state and, when its pair touched, its history --
 // issued before the current entry is computed); then walls, sums and the
 // integration of the sphere.
-template <int LM>
-__global__ void __launch_bounds__(PAIR_THREADS, 4) k_pair_step(StepArgs A, PairArgs P)
+template <int LM, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_pair_step(StepArgs A, PairArgs P)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.ntot) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.ntot) return;
     const uint32_t cur = *P.pp, nxt = cur ^ 1u, ls = *P.lsel;
+    const uint32_t i = P.order[ls][t];
     const double4 *__restrict__ xr = P.xr[cur];
     const float4 *__restrict__ vw = P.vw[cur];
     const DevBox &B = A.boxes[box_index(A, i)];
@@ -284,9 +288,13 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4) k_pair_step(StepArgs A, PairA
     acc.es_dot = 0.0;
     acc.ev_dot = 0.0;
     acc.p = 0.0;
+    // entry k's partner state and history are loaded during entry k - 1,
+    // entry k's partner id during entry k - 2 (the row holds VL_MAX >= 2
+    // ids; those at or past n are not used)
     double4 xb = make_double4(0.0, 0.0, 0.0, 0.0);
     float4 vb = make_float4(0.f, 0.f, 0.f, 0.f), wb = vb;
     d3 hb = mk(0.0, 0.0, 0.0);
+    uint32_t b_next = lst[1];
     if (n) {
         const uint32_t b = lst[0];
         xb = xr[b];
@@ -299,7 +307,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4) k_pair_step(StepArgs A, PairA
         float4 vq = vb, wq = wb;
         d3 hq = mk(0.0, 0.0, 0.0);
         if (k + 1 < n) {
-            const uint32_t b = lst[k + 1];
+            const uint32_t b = b_next;
+            if (k + 2 < n) b_next = lst[k + 2];
             xq = xr[b];
             vq = vw[2 * b];
             wq = vw[2 * b + 1];
@@ -453,6 +462,26 @@ __global__ void k_pair_remap(StepArgs A, PairArgs P)
     P.live[nw][i] = live;
 }
 
+// The threads' order over the new lists (P.order[*lsel ^ 1]): within each
+// group of PAIR_ORDER_GROUP spheres, ascending list length, ties by index
+// (a stable rank), spheres past the end last.  One block per group.
+__global__ void __launch_bounds__(PAIR_ORDER_GROUP) k_pair_order(StepArgs A, PairArgs P)
+{
+    __shared__ uint32_t s_key[PAIR_ORDER_GROUP];
+    const uint32_t nw = *P.lsel ^ 1u;
+    const uint32_t base = blockIdx.x * PAIR_ORDER_GROUP, t = threadIdx.x, i = base + t;
+    uint32_t key = 0xffffffffu;
+    if (i < A.ntot) key = min(P.cnt[nw][i], (uint32_t)VL_MAX + 1u);
+    s_key[t] = key;
+    __syncthreads();
+    uint32_t rank = 0;
+    for (uint32_t u = 0; u < PAIR_ORDER_GROUP; ++u) {
+        const uint32_t k = s_key[u];
+        rank += (k < key || (k == key && u < t)) ? 1u : 0u;
+    }
+    if (i < A.ntot) P.order[nw][base + rank] = i;
+}
+
 __global__ void k_pair_done(StepArgs A, PairArgs P)
 {
     *P.lsel ^= 1u;
@@ -562,10 +591,36 @@ inline void mark(Prof *prof, cudaStream_t st, const char *name)
     prof->n++;
 }
 
+// The list-step kernel at one of its launch shapes (cfg.pair_shape, chosen
+// by sph_autotune): threads per block and resident blocks per SM, i.e. the
+// register budget per thread -- 0: 128 x 4 (128 registers), 1: 128 x 5
+// (102), 2: 128 x 6 (85), 3: 64 x 8 (128), 4: 256 x 2 (128).  Fewer
+// registers give more warps to hide the partner gathers, at the cost of
+// spilled values; the arithmetic is the same in every shape.
+template <int LM>
+void launch_pair_lm(const StepArgs &A, const PairArgs &P, int shape, cudaStream_t st)
+{
+    switch (shape) {
+    case 1: k_pair_step<LM, 128, 5><<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, P); break;
+    case 2: k_pair_step<LM, 128, 6><<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, P); break;
+    case 3: k_pair_step<LM, 64, 8><<<blocks_for(A.ntot, 64), 64, 0, st>>>(A, P); break;
+    case 4: k_pair_step<LM, 256, 2><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A, P); break;
+    default: k_pair_step<LM, 128, 4><<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, P); break;
+    }
+}
+
+void launch_pair_kernel(const StepArgs &A, const PairArgs &P, const StepConfig &cfg,
+                        cudaStream_t st)
+{
+    if (cfg.lenmode == SPH_LEN_FP64) launch_pair_lm<SPH_LEN_FP64>(A, P, cfg.pair_shape, st);
+    else launch_pair_lm<SPH_LEN_REFERENCE>(A, P, cfg.pair_shape, st);
+}
+
 void launch_rebuild_body(const StepArgs &A, const PairArgs &P, cudaStream_t st)
 {
     launch_pair_sort_build(A, P, st);
     k_pair_remap<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A, P);
+    k_pair_order<<<blocks_for(A.ntot, PAIR_ORDER_GROUP), PAIR_ORDER_GROUP, 0, st>>>(A, P);
     k_pair_done<<<1, 1, 0, st>>>(A, P);
 }
 
@@ -624,10 +679,7 @@ int launch_step_pair(const StepArgs &A, const PairArgs &P, const StepConfig &cfg
         if (flag) launch_rebuild_body(A, P, st);
     }
     mark(prof, st, "k_pair_cond");
-    if (cfg.lenmode == SPH_LEN_FP64)
-        k_pair_step<SPH_LEN_FP64><<<blocks_for(A.ntot, PAIR_THREADS), PAIR_THREADS, 0, st>>>(A, P);
-    else
-        k_pair_step<SPH_LEN_REFERENCE><<<blocks_for(A.ntot, PAIR_THREADS), PAIR_THREADS, 0, st>>>(A, P);
+    launch_pair_kernel(A, P, cfg, st);
     mark(prof, st, "k_pair_step");
     const bool pdl = prof == nullptr;
     if (cfg.any_walls) {

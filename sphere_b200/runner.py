@@ -257,6 +257,16 @@ class Stepper(object):
     def set_variant(self, variant):
         self._check(self.lib.sph_set_variant(self.h, int(variant)), "sph_set_variant")
 
+    def set_launch_shape(self, shape):
+        """Launch shape of the list step (sph_set_launch_shape)."""
+        self._check(self.lib.sph_set_launch_shape(self.h, int(shape)), "sph_set_launch_shape")
+
+    def tuning(self):
+        """(variant, list-step launch shape) in use (sph_get_tuning)."""
+        v, sh = C.c_int(0), C.c_int(0)
+        self._check(self.lib.sph_get_tuning(self.h, C.byref(v), C.byref(sh)), "sph_get_tuning")
+        return v.value, sh.value
+
     def adjoint_forward(self, nsteps, ckpt=100):
         """nsteps steps with a checkpoint every ckpt steps kept for
         adjoint_backward (sph_adjoint_forward); returns the device ms."""

@@ -220,6 +220,7 @@ def time_ensemble(device, stream, nboxes=256, steps=200, err_steps=100):
     st.set_stream(stream.cuda_stream)
     st.upload()
     variant, variant_ms = st.autotune(steps=10)
+    tuning = st.tuning()
     st.step(5)
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
@@ -261,6 +262,7 @@ def time_ensemble(device, stream, nboxes=256, steps=200, err_steps=100):
                         % (nboxes, min(counts), max(counts), n),
             "value": n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
             "steps": steps, "spheres": n, "variant": variant, "variant_ms_per_step": variant_ms,
+            "tuning": {"variant": tuning[0], "list_step_shape": tuning[1]},
             "device_status": code,
             "per_box_force_rel_l2_max": max(ferr), "per_box_force_rel_l2_median":
                 float(numpy.median(ferr)),
@@ -372,7 +374,9 @@ def main():
                     help="run every kernel family once inside the NVTX range 'k' (for profiling) "
                          "and exit")
     ap.add_argument("--variant", type=int, default=-1,
-                    help="interact launch variant (0-3); default: picked by sph_autotune")
+                    help="interact launch variant (0-4); default: picked by sph_autotune")
+    ap.add_argument("--shape", type=int, default=0,
+                    help="launch shape of the list step (variant 4) when --variant is given")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -456,6 +460,10 @@ def main():
             st.upload()
             st.set_variant(3)
             st.step(3)
+            if prec == "mixed":
+                # the list step (its first step rebuilds the lists)
+                st.set_variant(4)
+                st.step(3)
             if prec == "fp64":
                 st.set_variant(1)
                 st.step(2)
@@ -530,6 +538,7 @@ def main():
         # state is put back afterwards), then the warm-up steps
         if args.variant >= 0:
             st.set_variant(args.variant)
+            st.set_launch_shape(args.shape)
             variant, variant_ms = args.variant, None
         else:
             variant, variant_ms = st.autotune(steps=20)
@@ -569,10 +578,15 @@ def main():
         st.profile(False)
         contacts = st.count_contacts()
         nstats = st.neighbor_stats()
-        # the interact stage: the fused kernel, or the three kernels of the
-        # split step (same work, same algorithmic bytes)
-        stage = ["k_interact"] if "k_interact" in kernels else ["k_search", "k_contacts",
-                                                                   "k_finish"]
+        # the interact stage: the fused kernel, the three kernels of the
+        # split step or the list step's kernel (same work, same algorithmic
+        # bytes)
+        if "k_pair_step" in kernels:
+            stage = ["k_pair_step"]
+        elif "k_interact" in kernels:
+            stage = ["k_interact"]
+        else:
+            stage = ["k_search", "k_contacts", "k_finish"]
         parts = [kernels.get(k) for k in stage]
         t_int = sum(parts) if all(isinstance(v, float) for v in parts) else None
         b_int = interact_bytes(n, contacts, precision)
@@ -584,14 +598,18 @@ def main():
         try:
             with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
                 tr = json.load(fh)
-            roofline["traffic"] = tr[precision]["k_interact_bytes_per_sphere"] * n
-            roofline["traffic_source"] = tr.get("source")
+            key = "mixed_list" if stage == ["k_pair_step"] else precision
+            if tr[key]["kernels"] == "+".join(stage):
+                roofline["traffic"] = tr[key]["bytes_per_sphere"] * n
+                roofline["traffic_source"] = tr["source"] + "; " + tr[key]["capture"]
         except Exception:
             pass
+        tuning = st.tuning()
         st.close()
         ms_step = ms_max / args.steps
         return {"value": world * n * args.steps / (ms_max / 1e3), "ms_per_step": ms_step,
                 "variant": variant, "variant_ms_per_step": variant_ms,
+                "tuning": {"variant": tuning[0], "list_step_shape": tuning[1]},
                 "neighbor_lists": nstats,
                 "roofline": roofline, "kernel_ms": kernels, "live_contacts": contacts,
                 "gpu_launches": launches, "clocks": clk, "device_status": code,
@@ -609,7 +627,8 @@ def main():
     if rank == 0 or world > 1:
         st2 = Stepper([s], precision=head, length="reference", device=local)
         st2.set_stream(stream.cuda_stream)
-        st2.set_variant(H["variant"])
+        st2.set_variant(H["tuning"]["variant"])
+        st2.set_launch_shape(H["tuning"]["list_step_shape"])
         hp = HostParticles.from_sims([s])
         for name in ("x", "xyzsum", "vel", "force", "angpos", "angvel", "torque", "es_dot", "es",
                      "ev_dot", "ev", "p"):

@@ -318,12 +318,15 @@ int sph_neighbor_stats(SphHandle *h, uint64_t *stats);
 int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen);
 int sph_set_variant(SphHandle *h, int variant);
 /* Launch shape of the list step (variant 4): threads per block x resident
- * blocks per SM, i.e. its register budget -- 0: 128 x 4, 1: 128 x 5,
- * 2: 128 x 6, 3: 64 x 8, 4: 256 x 2 (SPH_PAIR_SHAPES); the results do not
+ * blocks per SM, i.e. its register budget, and for shapes 5-8 the number
+ * of list entries whose partner data each thread has in flight (staged in
+ * shared memory) -- 0: 128 x 4, 1: 128 x 5, 2: 128 x 6, 3: 64 x 8,
+ * 4: 256 x 2, 5: 64 x 8 staging 4, 6: 64 x 8 staging 6, 7: 128 x 4
+ * staging 4, 8: 64 x 10 staging 3 (SPH_PAIR_SHAPES); the results do not
  * depend on it.  sph_autotune tries every shape of variant 4 and reports
  * the best in ms_per_step[4]; sph_get_tuning returns the variant and shape
  * in use. */
-#define SPH_PAIR_SHAPES 5
+#define SPH_PAIR_SHAPES 9
 int sph_set_launch_shape(SphHandle *h, int shape);
 int sph_get_tuning(const SphHandle *h, int *variant, int *shape);
 

@@ -117,7 +117,7 @@ struct PairArgs {
     const uint32_t *box_chunk0;   // first chunk of each box
 };
 constexpr int PAIR_CHUNK_LOG2 = 11;
-constexpr int PAIR_SHAPES = 5;
+constexpr int PAIR_SHAPES = 9;
 constexpr int PAIR_ORDER_GROUP = 128;   // launch shapes of the list-step kernel (sph_pair.cu)
 
 // Overlap search of one box (sph_overlaps): positions and velocities, the

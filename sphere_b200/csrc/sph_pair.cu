@@ -253,6 +253,28 @@ __device__ __forceinline__ void integrate_pair(const StepArgs &A, const PairArgs
     P.vw[nxt][2 * i + 1] = make_float4((float)wn[0], (float)wn[1], (float)wn[2], 0.f);
 }
 
+// After a sphere's contacts: its touching bits, walls, sums and integration.
+template <int LM>
+__device__ __forceinline__ void finish_sphere(const StepArgs &A, const PairArgs &P,
+                                              const DevBox &B, uint32_t i, uint32_t nxt,
+                                              uint32_t ls, double4 xa, float4 wa, Acc &acc,
+                                              unsigned long long live_old,
+                                              unsigned long long live_new)
+{
+    const double dt = B.dt;
+    if (__popcll(live_new) > NC) raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+    if (live_new != live_old) P.live[ls][i] = live_new;
+    const double4 vel = P.vel[i];
+    const double w0_force = walls_pair<LM>(B, xa, xyz(vel), mk(wa.x, wa.y, wa.z), acc);
+    P.force[i] = make_float4((float)acc.F.x, (float)acc.F.y, (float)acc.F.z, 0.f);
+    P.torque[i] = make_float4((float)acc.T.x, (float)acc.T.y, (float)acc.T.z, 0.f);
+    P.epp[i] = make_float4((float)acc.es_dot, (float)acc.ev_dot, (float)acc.p, 0.f);
+    const double2 e0 = P.eacc[i];
+    P.eacc[i] = make_double2(e0.x + acc.es_dot * dt, e0.y + acc.ev_dot * dt);
+    if (B.nw > 0) A.wf_pp[i] = w0_force;
+    integrate_pair(A, P, B, i, nxt, xa, vel, wa, acc.F, acc.T);
+}
+
 // One step of the list form, one thread per sphere: the sphere's list
 // entries in order, each tested with the exact FP64 overlap test and, for a
 // touching pair, the contact law with the entry's history (the loads of the
@@ -332,18 +354,118 @@ __global__ void __launch_bounds__(NT, MINB) k_pair_step(StepArgs A, PairArgs P)
         wb = wq;
         hb = hq;
     }
-    if (__popcll(live_new) > NC) raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
-    if (live_new != live_old) P.live[ls][i] = live_new;
+    finish_sphere<LM>(A, P, B, i, nxt, ls, xa, wa, acc, live_old, live_new);
+}
 
-    const double4 vel = P.vel[i];
-    const double w0_force = walls_pair<LM>(B, xa, xyz(vel), mk(wa.x, wa.y, wa.z), acc);
-    P.force[i] = make_float4((float)acc.F.x, (float)acc.F.y, (float)acc.F.z, 0.f);
-    P.torque[i] = make_float4((float)acc.T.x, (float)acc.T.y, (float)acc.T.z, 0.f);
-    P.epp[i] = make_float4((float)acc.es_dot, (float)acc.ev_dot, (float)acc.p, 0.f);
-    const double2 e0 = P.eacc[i];
-    P.eacc[i] = make_double2(e0.x + acc.es_dot * dt, e0.y + acc.ev_dot * dt);
-    if (B.nw > 0) A.wf_pp[i] = w0_force;
-    integrate_pair(A, P, B, i, nxt, xa, vel, wa, acc.F, acc.T);
+// cp.async (global -> shared, issued per thread, completion per thread by
+// commit groups): the staging of partner data below.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Partner data of D list entries per thread in flight, staged in shared
+// memory (field-major: slot, field, thread, so that a warp's accesses to
+// one field are consecutive): position+radius, velocity, angular velocity
+// and the entry's history.
+template <int NT, int D>
+struct PairStage {
+    double4 x[D][NT];
+    float4 v[D][NT];
+    float4 w[D][NT];
+    double h[D][3][NT];
+};
+
+// The list step with the partner data of entry k + D copied into shared
+// memory (cp.async) while entry k is computed: D entries' loads in flight
+// per thread without holding them in registers.  The same arithmetic as
+// k_pair_step.
+template <int LM, int NT, int MINB, int D>
+__global__ void __launch_bounds__(NT, MINB) k_pair_step_async(StepArgs A, PairArgs P)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    PairStage<NT, D> &S = *reinterpret_cast<PairStage<NT, D> *>(s_raw);
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tx = (int)threadIdx.x;
+    if (t >= A.ntot) return;
+    const uint32_t cur = *P.pp, nxt = cur ^ 1u, ls = *P.lsel;
+    const uint32_t i = P.order[ls][t];
+    const double4 *__restrict__ xr = P.xr[cur];
+    const float4 *__restrict__ vw = P.vw[cur];
+    const DevBox &B = A.boxes[box_index(A, i)];
+    uint32_t n = P.cnt[ls][i];
+    if (n > (uint32_t)VL_MAX) {   // the list overflowed at its build
+        raise_flag(A.err, SPH_ERR_NC_OVERFLOW);
+        n = 0;
+    }
+    const unsigned long long live_old = P.live[ls][i];
+    unsigned long long live_new = 0ull;
+    const uint32_t *__restrict__ lst = P.ids[ls] + (size_t)i * VL_MAX;
+    double *__restrict__ hist = P.hist[ls] + (size_t)i * VL_MAX * 3;
+    auto stage = [&](uint32_t k) {
+        // entry k into slot k % D (an empty commit group past the list's end)
+        if (k < n) {
+            const int q = (int)(k % D);
+            const uint32_t b = lst[k];
+            const double4 *gx = xr + b;
+            cp_async16(&S.x[q][tx], gx);
+            cp_async16(reinterpret_cast<char *>(&S.x[q][tx]) + 16, reinterpret_cast<const char *>(gx) + 16);
+            cp_async16(&S.v[q][tx], vw + 2 * b);
+            cp_async16(&S.w[q][tx], vw + 2 * b + 1);
+            if ((live_old >> k) & 1ull) {
+                cp_async8(&S.h[q][0][tx], hist + 3 * k);
+                cp_async8(&S.h[q][1][tx], hist + 3 * k + 1);
+                cp_async8(&S.h[q][2][tx], hist + 3 * k + 2);
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int k = 0; k < D; ++k) stage((uint32_t)k);
+    const double4 xa = xr[i];
+    const float4 va = vw[2 * i], wa = vw[2 * i + 1];
+    const double dt = B.dt;
+
+    Acc acc;
+    acc.F = mk(0.0, 0.0, 0.0);
+    acc.T = mk(0.0, 0.0, 0.0);
+    acc.es_dot = 0.0;
+    acc.ev_dot = 0.0;
+    acc.p = 0.0;
+    for (uint32_t k = 0; k < n; ++k) {
+        cp_async_wait<D - 1>();
+        const int q = (int)(k % D);
+        const double4 xb = S.x[q][tx];
+        const float4 vb = S.v[q][tx], wb = S.w[q][tx];
+        d3 hb = mk(0.0, 0.0, 0.0);
+        if ((live_old >> k) & 1ull) hb = mk(S.h[q][0][tx], S.h[q][1][tx], S.h[q][2][tx]);
+        const d3 x_ab = centre_line(B, xa, xb, nullptr);
+        const double x_ab_length = len_rn<LM>(x_ab);
+        const double delta_n = __dsub_rn(x_ab_length, __dadd_rn(xa.w, xb.w));
+        if (delta_n < 0.0) {
+            const MixedPair mp = mixed_pair_f(x_ab, x_ab_length, delta_n, va, vb, wa, wb, xa.w, xb.w);
+            const d3 nd = B.P.contactmodel == 2 ? contact_linear_mixed(B.P, dt, acc, mp, hb)
+                                                : contact_hertz_mixed(B.P, dt, acc, mp, hb);
+            hist[3 * k] = nd.x;
+            hist[3 * k + 1] = nd.y;
+            hist[3 * k + 2] = nd.z;
+            live_new |= 1ull << k;
+        }
+        // slot k % D is refilled only after its values were used (the copy
+        // cannot overtake the reads)
+        stage(k + D);
+    }
+    cp_async_wait<0>();
+    finish_sphere<LM>(A, P, B, i, nxt, ls, xa, wa, acc, live_old, live_new);
 }
 
 // Wall-force sum of one chunk of 2^chunk_log2 spheres of one box: each
@@ -592,11 +714,29 @@ inline void mark(Prof *prof, cudaStream_t st, const char *name)
 }
 
 // The list-step kernel at one of its launch shapes (cfg.pair_shape, chosen
-// by sph_autotune): threads per block and resident blocks per SM, i.e. the
-// register budget per thread -- 0: 128 x 4 (128 registers), 1: 128 x 5
-// (102), 2: 128 x 6 (85), 3: 64 x 8 (128), 4: 256 x 2 (128).  Fewer
-// registers give more warps to hide the partner gathers, at the cost of
-// spilled values; the arithmetic is the same in every shape.
+// by sph_autotune): threads per block x resident blocks per SM (the
+// register budget per thread) and, for the staged kernel, the entries in
+// flight per thread --
+//   0: 128 x 4 (128 registers)       3: 64 x 8 (128)       4: 256 x 2 (128)
+//   1: 128 x 5 (102)                 2: 128 x 6 (85)
+//   5: staged, 64 x 8, 4 entries     6: staged, 64 x 8, 6 entries
+//   7: staged, 128 x 4, 4 entries    8: staged, 64 x 10, 3 entries
+// Fewer registers give more warps to hide the partner gathers, at the cost
+// of spilled values; staging keeps more gathers in flight per thread; the
+// arithmetic is the same in every shape.
+template <int LM, int NT, int MINB, int D>
+void launch_staged(const StepArgs &A, const PairArgs &P, cudaStream_t st)
+{
+    const size_t sm = sizeof(PairStage<NT, D>);
+    static bool attr = false;   // per instantiation: allow more than 48 KB of shared memory
+    if (!attr) {
+        cudaFuncSetAttribute(k_pair_step_async<LM, NT, MINB, D>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = true;
+    }
+    k_pair_step_async<LM, NT, MINB, D><<<blocks_for(A.ntot, NT), NT, sm, st>>>(A, P);
+}
+
 template <int LM>
 void launch_pair_lm(const StepArgs &A, const PairArgs &P, int shape, cudaStream_t st)
 {
@@ -605,6 +745,10 @@ void launch_pair_lm(const StepArgs &A, const PairArgs &P, int shape, cudaStream_
     case 2: k_pair_step<LM, 128, 6><<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, P); break;
     case 3: k_pair_step<LM, 64, 8><<<blocks_for(A.ntot, 64), 64, 0, st>>>(A, P); break;
     case 4: k_pair_step<LM, 256, 2><<<blocks_for(A.ntot, 256), 256, 0, st>>>(A, P); break;
+    case 5: launch_staged<LM, 64, 8, 4>(A, P, st); break;
+    case 6: launch_staged<LM, 64, 8, 6>(A, P, st); break;
+    case 7: launch_staged<LM, 128, 4, 4>(A, P, st); break;
+    case 8: launch_staged<LM, 64, 10, 3>(A, P, st); break;
     default: k_pair_step<LM, 128, 4><<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, P); break;
     }
 }

@@ -396,17 +396,20 @@ int sph_struct_sizes(uint64_t *sizes);
  * search, src/sorting.cuh:56-116 reorderArrays, as a stand-alone call):
  * offsets[k] = counts[0] + ... + counts[k-1] for k = 0..n (n + 1 words;
  * offsets[n] is the total), on device pointers, enqueued on `stream` (a
- * cudaStream_t; NULL = default stream).  For callers that must not allocate device
+ * cudaStream_t of the current device, else SPH_ERR_INPUT; NULL = default
+ * stream).  For callers that must not allocate device
  * memory at the call (a framework that owns all device memory, a
  * steady-state loop where an allocation could block or fail): the scratch
  * is a fixed file-scope device array of SPH_SCAN_STATIC_MAX / 4096 + 1
  * words (16 KiB + 4 B), so n > SPH_SCAN_STATIC_MAX returns
  * SPH_ERR_UNSUPPORTED.  The scratch needs no initial value.  The first call
- * on each device looks up the array's address with the device current
- * (cudaGetSymbolAddress, which may load the module): make that first call
- * before any stream capture begins.  Calls on one device share the array,
- * so calls that may overlap in time (other streams or host threads without
- * ordering between them) race and give wrong offsets. */
+ * on each device (and the first after a device reset) looks up the array's
+ * address with the device current (cudaGetSymbolAddress, which may load
+ * the module, and the driver may allocate device memory for it): make that
+ * first call at initialisation, before any stream capture begins; later
+ * calls allocate nothing.  Calls on one device share the array, so calls
+ * that may overlap in time (other streams or host threads without ordering
+ * between them) race and give wrong offsets. */
 #define SPH_SCAN_STATIC_MAX 16777216u
 int sph_cell_offsets_static(const uint32_t *counts, uint64_t n, uint32_t *offsets, void *stream);
 

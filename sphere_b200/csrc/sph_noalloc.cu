@@ -121,21 +121,49 @@ __global__ void __launch_bounds__(THREADS) k_tile_offsets(const uint32_t *in, ui
     if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = sums[ntiles];
 }
 
-// Device address of g_tile_sums, looked up once per device (with that
-// device current) and cached.
+// Device address of g_tile_sums, looked up with the device current and
+// cached per device together with the context it belongs to: a device
+// reset (cudaDeviceReset) ends the context, the module is loaded again in
+// the next one and the array may move, so a call that finds another
+// context current looks the address up again.  The current context is
+// read through the driver's cuCtxGetCurrent, obtained from the runtime
+// (no link against the driver library).
 std::mutex g_lock;
 constexpr int MAX_DEVICES = 64;
 uint32_t *g_addr[MAX_DEVICES] = {};
+void *g_ctx[MAX_DEVICES] = {};
+
+typedef int (*CtxGetCurrentFn)(void **ctx);
+
+void *current_context()
+{
+    static CtxGetCurrentFn fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(f);
+        looked = true;
+    }
+    void *ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
 
 int scratch_address(uint32_t **out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return SPH_ERR_CUDA;
     std::lock_guard<std::mutex> guard(g_lock);
-    if (!g_addr[dev]) {
+    void *ctx = current_context();
+    if (!g_addr[dev] || !ctx || ctx != g_ctx[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_tile_sums) != cudaSuccess || !p) return SPH_ERR_CUDA;
         g_addr[dev] = static_cast<uint32_t *>(p);
+        g_ctx[dev] = current_context();   // the lookup makes the context current if none was
     }
     *out = g_addr[dev];
     return SPH_OK;
@@ -148,10 +176,17 @@ extern "C" int sph_cell_offsets_static(const uint32_t *counts, uint64_t n, uint3
 {
     if (!offsets || (n && !counts)) return SPH_ERR_INPUT;
     if (n > SPH_SCAN_STATIC_MAX) return SPH_ERR_UNSUPPORTED;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (s) {
+        // the scratch used is the current device's: the stream must be on it
+        int sd = -1, cd = -1;
+        if (cudaStreamGetDevice(s, &sd) != cudaSuccess || cudaGetDevice(&cd) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        if (sd != cd) return SPH_ERR_INPUT;
+    }
     uint32_t *sums = nullptr;
     const int st = scratch_address(&sums);
     if (st != SPH_OK) return st;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const uint32_t ntiles = (uint32_t)((n + SCAN_TILE - 1) / SCAN_TILE);
     if (ntiles == 0) {
         // no counts: the single offset is 0

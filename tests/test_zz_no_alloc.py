@@ -60,9 +60,41 @@ def test_static_scan_large_random_counts_twice():
 
 
 def test_static_scan_rejects_sizes_beyond_its_scratch():
+    # buffers sized for the n + 1 words the call would touch, so that the
+    # call stays inside them even if the size check were wrong
     lib = _abi.load_library()
     dev = torch.device("cuda", 0)
-    d = torch.zeros(16, dtype=torch.int32, device=dev)
-    rc = lib.sph_cell_offsets_static(C.c_void_p(d.data_ptr()), SCAN_STATIC_MAX + 1,
-                                     C.c_void_p(d.data_ptr()), None)
+    n = SCAN_STATIC_MAX + 1
+    d_counts = torch.zeros(n, dtype=torch.int32, device=dev)
+    d_off = torch.zeros(n + 1, dtype=torch.int32, device=dev)
+    rc = lib.sph_cell_offsets_static(C.c_void_p(d_counts.data_ptr()), n,
+                                     C.c_void_p(d_off.data_ptr()), None)
     assert rc == UNSUPPORTED
+    torch.cuda.synchronize(dev)
+    assert int(d_off.abs().sum().item()) == 0   # nothing written
+
+
+def test_static_scan_warm_call_allocates_no_device_memory():
+    """After a first call, a call on 16 million counts leaves the device's
+    free memory unchanged (the caller's buffers are made beforehand)."""
+    lib = _abi.load_library()
+    dev = torch.device("cuda", 0)
+    counts = numpy.ones(SCAN_STATIC_MAX, dtype=numpy.uint32)
+    d_counts = torch.from_numpy(counts.view(numpy.int32)).to(dev)
+    d_off = torch.empty(counts.size + 1, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def call():
+        rc = lib.sph_cell_offsets_static(C.c_void_p(d_counts.data_ptr()), counts.size,
+                                         C.c_void_p(d_off.data_ptr()),
+                                         C.c_void_p(stream.cuda_stream))
+        assert rc == 0, rc
+        torch.cuda.synchronize(dev)
+
+    call()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    call()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
+    assert int(d_off[-1].item()) == SCAN_STATIC_MAX
+

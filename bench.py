@@ -200,20 +200,26 @@ def time_adjoint(device, stream, n=50000, steps=2000, ckpt=100):
             "grad_v0_norm": float(numpy.linalg.norm(gv))}
 
 
-def time_ensemble(device, stream, nboxes=256, steps=200, err_steps=100):
+def time_ensemble(device, stream, nboxes=256, steps=200, err_steps=100, rank=0, world=1,
+                  barrier=None, max_over_ranks=None):
     """The batched ensemble (256 independent x-y periodic shear boxes with
     uniform particle counts in [500, 20000], radii U[0.009, 0.011] m,
-    per-box normal stress U[10, 80] kPa and mu U[0.3, 0.6]) stepped by one
-    handle: every step is one CUDA graph whose launches cover all boxes.
-    Reports the FP32-mixed ensemble throughput (launch variant picked by
-    sph_autotune) and, per box, the mixed form's error against the FP64
-    form: force relative L2 after one step and the largest position
-    difference after err_steps steps, relative to the mean radius."""
+    per-box normal stress U[10, 80] kPa and mu U[0.3, 0.6]), its boxes
+    shared out over the ranks by particle count (ensemble.partition, no
+    data-path exchange): each rank makes and steps its own boxes in one
+    handle, every step one CUDA graph whose launches cover all of them.
+    Reports the FP32-mixed ensemble throughput (all ranks' spheres over the
+    slowest rank's time; launch variant and shape picked by sph_autotune)
+    and, per box, the mixed form's error against the FP64 form: force
+    relative L2 after one step and the largest position difference after
+    err_steps steps, relative to the mean radius (the largest over ranks)."""
     import numpy
     import torch
-    from sphere_b200 import scenes
+    from sphere_b200 import ensemble, scenes
     from sphere_b200.runner import Stepper
-    sims = scenes.shear_ensemble(nboxes=nboxes, seed=0, device=device)
+    all_counts = scenes.ensemble_counts(nboxes=nboxes, seed=0)
+    mine = ensemble.partition(all_counts, world)[rank]
+    sims = scenes.shear_ensemble(nboxes=nboxes, seed=0, device=device, subset=mine)
     counts = [int(q.np[0]) for q in sims]
     n = sum(counts)
     st = Stepper(sims, precision="mixed", length="reference", device=device)
@@ -225,12 +231,18 @@ def time_ensemble(device, stream, nboxes=256, steps=200, err_steps=100):
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    if barrier:
+        barrier()
     start.record(stream)
     st.step_async(steps)
     end.record(stream)
     end.synchronize()
     code = st.sync(raise_on_error=False)
     ms = start.elapsed_time(end)
+    if barrier:
+        barrier()
+    if max_over_ranks:
+        ms = max_over_ranks(ms)
     st.close()
     # per-box error of the mixed form against the FP64 form
     a = Stepper(sims, precision="fp64", length="reference", device=device)
@@ -256,17 +268,24 @@ def time_ensemble(device, stream, nboxes=256, steps=200, err_steps=100):
         xerr.append(float(numpy.max(numpy.abs(xa.x[o:o + k, :3] - xb.x[o:o + k, :3]))) /
                     float(numpy.mean(q.radius)))
         o += k
+    fmax, xmax = max(ferr), max(xerr)
+    if max_over_ranks:
+        fmax, xmax = max_over_ranks(fmax), max_over_ranks(xmax)
+    total = sum(all_counts)
     return {"workload": "%d independent x-y periodic shear boxes, %d..%d spheres each "
                         "(%d in total), radii U[0.009, 0.011] m, porosity ~0.40, normal "
-                        "stress U[10, 80] kPa, mu U[0.3, 0.6], FP32-mixed, one handle"
-                        % (nboxes, min(counts), max(counts), n),
-            "value": n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
-            "steps": steps, "spheres": n, "variant": variant, "variant_ms_per_step": variant_ms,
+                        "stress U[10, 80] kPa, mu U[0.3, 0.6], FP32-mixed, one handle per rank"
+                        % (nboxes, min(all_counts), max(all_counts), total),
+            "value": total * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "spheres": total, "ranks": world,
+            "scaling": "strong" if world > 1 else None,
+            "boxes_on_rank0": len(mine), "spheres_on_rank0": n,
+            "variant": variant, "variant_ms_per_step": variant_ms,
             "tuning": {"variant": tuning[0], "list_step_shape": tuning[1]},
             "device_status": code,
-            "per_box_force_rel_l2_max": max(ferr), "per_box_force_rel_l2_median":
+            "per_box_force_rel_l2_max": fmax, "per_box_force_rel_l2_median_rank0":
                 float(numpy.median(ferr)),
-            "per_box_dx_over_rmean_max_after_%d_steps" % err_steps: max(xerr)}
+            "per_box_dx_over_rmean_max_after_%d_steps" % err_steps: xmax}
 
 
 def time_bonded(device, stream, n=200000, nbonds=300000, steps=200):
@@ -695,8 +714,10 @@ def main():
     if rank == 0 and not args.no_adjoint:
         adj = time_adjoint(local, stream)
     ens = None
-    if rank == 0 and not args.no_ensemble:
-        ens = time_ensemble(local, stream)
+    if not args.no_ensemble:
+        # every rank steps its share of the boxes (all ranks take part)
+        ens = time_ensemble(local, stream, rank=rank, world=world, barrier=barrier,
+                            max_over_ranks=max_over_ranks)
     bonded = None
     if rank == 0 and not args.no_bonded:
         bonded = time_bonded(local, stream)

@@ -142,7 +142,11 @@ int sph_create(const SphBox *boxes, uint32_t nboxes, int precision,
 
 /* Copy particle (and bond, may be NULL when no box has bonds) state to the
  * device; contact lists are emptied and tangential histories zeroed.
- * Replaces transferToGlobalDeviceMemory (src/device.cu:660-746). */
+ * Replaces transferToGlobalDeviceMemory (src/device.cu:660-746).  The
+ * input is checked as checkValues does (src/sphere.cpp:145-345) while the
+ * copies run; when a check fails (SPH_ERR_INPUT) the handle holds no
+ * particle state until an upload succeeds (sph_step: SPH_ERR_STATE).  The
+ * caller's arrays are only read during the call. */
 int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b);
 
 /* Run `nsteps` iterations of the DEM::startTime loop body for fluid == 0

@@ -652,46 +652,54 @@ __global__ void k_image_codes(StepArgs A, uint64_t ns)
     A.slots[q] = b | (sph::shift_code(sx, sy) << sph::CODE_SHIFT);
 }
 
+// Staging for the [np][3] host layouts: one slot of 3 np doubles per
+// 3-vector field (five fields), so that every field's copy and repacking
+// can be queued before a single synchronisation.
+constexpr int STAGE_SLOTS = 5;
+
 static int ensure_stage(SphHandle *h)
 {
     if (h->stage) return SPH_OK;
-    return dalloc(h, &h->stage, 3 * h->ntot);
+    return dalloc(h, &h->stage, (uint64_t)STAGE_SLOTS * 3 * h->ntot);
 }
 
-static int put3(SphHandle *h, double4 *dst, const double *src, uint64_t n)
+// Queue on stream s: the host [n][3] field src into slot `slot` of the
+// staging array, then repacked into dst (zeros when src is NULL).
+static int put3(SphHandle *h, double4 *dst, const double *src, uint64_t n, int slot,
+                cudaStream_t s)
 {
     if (!src || n == 0) {
-        CUDA_TRY(h, cudaMemset(dst, 0, sizeof(double4) * (n ? n : 1)));
+        CUDA_TRY(h, cudaMemsetAsync(dst, 0, sizeof(double4) * (n ? n : 1), s));
         return SPH_OK;
     }
     int st;
     if ((st = ensure_stage(h)) != SPH_OK) return st;
-    CUDA_TRY(h, cudaMemcpyAsync(h->stage, src, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
-                                h->stream));
-    k_unpack3<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(dst, h->stage, n);
+    double *stage = h->stage + (size_t)slot * 3 * n;
+    CUDA_TRY(h, cudaMemcpyAsync(stage, src, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+    k_unpack3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dst, stage, n);
     CUDA_TRY(h, cudaGetLastError());
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return SPH_OK;
 }
 
-static int get3(SphHandle *h, double *dst, const double4 *src, uint64_t n,
-                cudaStream_t cs = nullptr)
+// Queue on stream s: src repacked into staging slot `slot`, then copied to
+// the host [n][3] array dst (nothing when dst is NULL).
+static int get3(SphHandle *h, double *dst, const double4 *src, uint64_t n, int slot,
+                cudaStream_t s)
 {
     if (!dst || n == 0) return SPH_OK;
     int st;
     if ((st = ensure_stage(h)) != SPH_OK) return st;
-    cudaStream_t s = cs ? cs : h->stream;
-    k_pack3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(h->stage, src, n);
+    double *stage = h->stage + (size_t)slot * 3 * n;
+    k_pack3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(stage, src, n);
     CUDA_TRY(h, cudaGetLastError());
-    CUDA_TRY(h, cudaMemcpyAsync(dst, h->stage, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(h, cudaStreamSynchronize(s));
+    CUDA_TRY(h, cudaMemcpyAsync(dst, stage, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s));
     return SPH_OK;
 }
 
-static int put1(SphHandle *h, double *dst, const double *src, uint64_t n)
+static int put1(SphHandle *h, double *dst, const double *src, uint64_t n, cudaStream_t s)
 {
-    if (src) CUDA_TRY(h, cudaMemcpy(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice));
-    else CUDA_TRY(h, cudaMemset(dst, 0, sizeof(double) * (n ? n : 1)));
+    if (src) CUDA_TRY(h, cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    else CUDA_TRY(h, cudaMemsetAsync(dst, 0, sizeof(double) * (n ? n : 1), s));
     return SPH_OK;
 }
 
@@ -703,28 +711,39 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
     if (n > 0 && (!p->x || !p->vel)) return fail(h, SPH_ERR_INPUT, "x and vel are required");
     if (nb > 0 && (!b || !b->pairs)) return fail(h, SPH_ERR_INPUT, "bond pairs are required");
     int st;
-    std::vector<double> rmax_in, rmin_in;
-    if ((st = check_particles(h, p, rmax_in, rmin_in)) != SPH_OK) return st;
     StepArgs &A = h->A;
-    cudaStreamSynchronize(h->stream);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    // The copies are queued first and run while the host checks the same
+    // input (src/sphere.cpp:145-345 checkValues); a check that fails leaves
+    // the handle without a state (sph_step refuses until an upload succeeds).
+    h->uploaded = false;
+    invalidate_pair(h);
+    const cudaStream_t cs = h->stream;
     if (n > 0) {
-        CUDA_TRY(h, cudaMemcpy(A.x, p->x, sizeof(double4) * n, cudaMemcpyHostToDevice));
-        CUDA_TRY(h, cudaMemcpy(A.vel, p->vel, sizeof(double4) * n, cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpyAsync(A.x, p->x, sizeof(double4) * n, cudaMemcpyHostToDevice, cs));
+        CUDA_TRY(h, cudaMemcpyAsync(A.vel, p->vel, sizeof(double4) * n, cudaMemcpyHostToDevice, cs));
     }
-    if ((st = put3(h, A.xyzsum, p->xyzsum, n)) || (st = put3(h, A.force, p->force, n)) ||
-        (st = put3(h, A.angpos, p->angpos, n)) || (st = put3(h, A.angvel, p->angvel, n)) ||
-        (st = put3(h, A.torque, p->torque, n)) || (st = put1(h, A.es_dot, p->es_dot, n)) ||
-        (st = put1(h, A.es, p->es, n)) || (st = put1(h, A.ev_dot, p->ev_dot, n)) ||
-        (st = put1(h, A.ev, p->ev, n)) || (st = put1(h, A.p, p->p, n)))
+    if ((st = put3(h, A.xyzsum, p->xyzsum, n, 0, cs)) || (st = put3(h, A.force, p->force, n, 1, cs)) ||
+        (st = put3(h, A.angpos, p->angpos, n, 2, cs)) || (st = put3(h, A.angvel, p->angvel, n, 3, cs)) ||
+        (st = put3(h, A.torque, p->torque, n, 4, cs)) || (st = put1(h, A.es_dot, p->es_dot, n, cs)) ||
+        (st = put1(h, A.es, p->es, n, cs)) || (st = put1(h, A.ev_dot, p->ev_dot, n, cs)) ||
+        (st = put1(h, A.ev, p->ev, n, cs)) || (st = put1(h, A.p, p->p, n, cs))) {
+        cudaStreamSynchronize(cs);
         return st;
-    CUDA_TRY(h, cudaMemset(A.acc, 0, sizeof(double4) * (n ? n : 1)));
-    CUDA_TRY(h, cudaMemset(A.angacc, 0, sizeof(double4) * (n ? n : 1)));
-    CUDA_TRY(h, cudaMemset(A.wf_pp, 0, sizeof(double) * (n ? n : 1)));
-    CUDA_TRY(h, cudaMemset(A.tau_pp, 0, sizeof(double) * (n ? n : 1)));
+    }
+    CUDA_TRY(h, cudaMemsetAsync(A.acc, 0, sizeof(double4) * (n ? n : 1), cs));
+    CUDA_TRY(h, cudaMemsetAsync(A.angacc, 0, sizeof(double4) * (n ? n : 1), cs));
+    CUDA_TRY(h, cudaMemsetAsync(A.wf_pp, 0, sizeof(double) * (n ? n : 1), cs));
+    CUDA_TRY(h, cudaMemsetAsync(A.tau_pp, 0, sizeof(double) * (n ? n : 1), cs));
     // src/device.cu:458-464: empty contact lists; histories start at zero
     if (n) {
-        CUDA_TRY(h, cudaMemset(A.slots, 0xff, sizeof(uint32_t) * n * sph::NC));
-        CUDA_TRY(h, cudaMemset(A.hist, 0, sizeof(double4) * n * sph::NC));
+        CUDA_TRY(h, cudaMemsetAsync(A.slots, 0xff, sizeof(uint32_t) * n * sph::NC, cs));
+        CUDA_TRY(h, cudaMemsetAsync(A.hist, 0, sizeof(double4) * n * sph::NC, cs));
+    }
+    std::vector<double> rmax_in, rmin_in;
+    if ((st = check_particles(h, p, rmax_in, rmin_in)) != SPH_OK) {
+        cudaStreamSynchronize(cs);
+        return st;
     }
 
     // bonds (local indexes) and the per-particle list of bond endpoints in
@@ -821,12 +840,14 @@ int sph_upload(SphHandle *h, const SphParticles *p, const SphBonds *b)
             d.vrange = (half > 0.0 && R >= 1 && R <= 3) ? R : 0;
         }
     }
-    CUDA_TRY(h, cudaMemcpy(A.boxes, h->dbox.data(), sizeof(DevBox) * h->nbox, cudaMemcpyHostToDevice));
-    CUDA_TRY(h, cudaMemset(A.err, 0, sizeof(uint32_t)));
-    CUDA_TRY(h, cudaMemset(A.vflag, 0, 2 * sizeof(uint32_t)));
-    CUDA_TRY(h, cudaMemset(A.vflag, 1, 1));   // build the lists in the first step
+    CUDA_TRY(h, cudaMemcpyAsync(A.boxes, h->dbox.data(), sizeof(DevBox) * h->nbox,
+                                cudaMemcpyHostToDevice, cs));
+    CUDA_TRY(h, cudaMemsetAsync(A.err, 0, sizeof(uint32_t), cs));
+    CUDA_TRY(h, cudaMemsetAsync(A.vflag, 0, 2 * sizeof(uint32_t), cs));
+    CUDA_TRY(h, cudaMemsetAsync(A.vflag, 1, 1, cs));   // build the lists in the first step
+    // the caller's buffers are read only during the call
+    CUDA_TRY(h, cudaStreamSynchronize(cs));
     h->uploaded = true;
-    invalidate_pair(h);
     return SPH_OK;
 }
 
@@ -1126,23 +1147,30 @@ static int download_from(SphHandle *h, const StepArgs &S, cudaStream_t cs, SphPa
                          SphBonds *b)
 {
     const uint64_t n = h->ntot, nb = h->nbonds;
+    const cudaStream_t s = cs ? cs : h->stream;
     auto d2h = [&](void *dst, const void *src, size_t bytes) -> cudaError_t {
-        if (!cs) return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
-        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, cs);
-        return e == cudaSuccess ? cudaStreamSynchronize(cs) : e;
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
     };
     int st;
     if (p) {
-        if (p->x && n) CUDA_TRY(h, d2h(p->x, S.x, sizeof(double4) * n));
-        if (p->vel && n) CUDA_TRY(h, d2h(p->vel, S.vel, sizeof(double4) * n));
-        if ((st = get3(h, p->xyzsum, S.xyzsum, n, cs)) || (st = get3(h, p->force, S.force, n, cs)) ||
-            (st = get3(h, p->angpos, S.angpos, n, cs)) || (st = get3(h, p->angvel, S.angvel, n, cs)) ||
-            (st = get3(h, p->torque, S.torque, n, cs)))
+        // every particle array queued on s (the 3-vector fields repacked in
+        // their own staging slots), one synchronisation
+        if (p->x && n) CUDA_TRY(h, cudaMemcpyAsync(p->x, S.x, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+        if (p->vel && n)
+            CUDA_TRY(h, cudaMemcpyAsync(p->vel, S.vel, sizeof(double4) * n, cudaMemcpyDeviceToHost, s));
+        if ((st = get3(h, p->xyzsum, S.xyzsum, n, 0, s)) || (st = get3(h, p->force, S.force, n, 1, s)) ||
+            (st = get3(h, p->angpos, S.angpos, n, 2, s)) || (st = get3(h, p->angvel, S.angvel, n, 3, s)) ||
+            (st = get3(h, p->torque, S.torque, n, 4, s))) {
+            cudaStreamSynchronize(s);
             return st;
+        }
         double *dst[5] = {p->es_dot, p->es, p->ev_dot, p->ev, p->p};
         double *src[5] = {S.es_dot, S.es, S.ev_dot, S.ev, S.p};
         for (int k = 0; k < 5; ++k)
-            if (dst[k] && n) CUDA_TRY(h, d2h(dst[k], src[k], sizeof(double) * n));
+            if (dst[k] && n)
+                CUDA_TRY(h, cudaMemcpyAsync(dst[k], src[k], sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(h, cudaStreamSynchronize(s));
     }
     if (b && nb) {
         std::vector<uint2> pairs(nb);

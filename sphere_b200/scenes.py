@@ -302,30 +302,49 @@ def _shear_setup(s, sigma0, mu, k_n=1.16e9, gamma_n=1.0e3, top_vel=0.01, steps=5
 
 
 def shear_ensemble(nboxes=256, seed=0, device=-1, counts=(500, 20000), r_range=(0.009, 0.011),
-                   porosity=0.40, sweeps=2000, inflate=2.0e-7, steps=2000):
+                   porosity=0.40, sweeps=2000, inflate=2.0e-7, steps=2000, subset=None):
     """The batched ensemble: nboxes independent x-y periodic shear boxes
     with particle counts uniform in [counts], radii U[r_range], packed to
     ~porosity on the GPU in one handle (FCC start, sph_relax of all boxes
     at once, radii grown by 1 + inflate), each with its own normal stress
-    U[10, 80] kPa and friction mu U[0.3, 0.6] (_shear_setup)."""
+    U[10, 80] kPa and friction mu U[0.3, 0.6] (_shear_setup).  subset: the
+    indexes of the boxes to make (the others are drawn but not packed); a
+    box is the same whichever subset it is made in (boxes relax
+    independently), so ranks can each make their own share."""
     from .runner import Stepper
     rng = numpy.random.default_rng(seed)
-    sims = []
+    starts = []
     for b in range(nboxes):
         n = int(rng.integers(counts[0], counts[1] + 1))
         r = rng.uniform(r_range[0], r_range[1], n)
         s, _H = _fcc_start(n, rng, r, porosity, 0.5, float(r.mean()), "box%03d" % b)
-        sims.append(s)
-    st = Stepper(sims, device=device)
-    st.upload()
-    st.relax(sweeps, alpha=0.6, z_top=1e300)
-    st.to_sims()
-    st.close()
-    for s in sims:
+        starts.append(s)
+    setup = [(float(rng.uniform(1.0e4, 8.0e4)), float(rng.uniform(0.3, 0.6))) for _ in range(nboxes)]
+    keep = list(range(nboxes)) if subset is None else [int(b) for b in subset]
+    sims = [starts[b] for b in keep]
+    if sims:
+        st = Stepper(sims, device=device)
+        st.upload()
+        st.relax(sweeps, alpha=0.6, z_top=1e300)
+        st.to_sims()
+        st.close()
+    for b, s in zip(keep, sims):
         s.radius *= 1.0 + inflate
-        _shear_setup(s, sigma0=float(rng.uniform(1.0e4, 8.0e4)), mu=float(rng.uniform(0.3, 0.6)),
-                     steps=steps)
+        _shear_setup(s, sigma0=setup[b][0], mu=setup[b][1], steps=steps)
     return sims
+
+
+def ensemble_counts(nboxes=256, seed=0, counts=(500, 20000)):
+    """The particle counts of shear_ensemble's boxes (the same draws, no
+    packing), to partition the boxes before they are made."""
+    rng = numpy.random.default_rng(seed)
+    out = []
+    for _ in range(nboxes):
+        n = int(rng.integers(counts[0], counts[1] + 1))
+        out.append(n)
+        rng.uniform(0.0, 1.0, n)          # the radii
+        rng.uniform(-1.0, 1.0, (n, 3))    # the FCC start's jitter
+    return out
 
 
 def sheared_dense_pack(n=1000000, seed=0, device=-1, sweeps=3000, relax=None):

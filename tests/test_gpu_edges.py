@@ -48,6 +48,10 @@ def test_bad_positions_are_refused_at_upload():
         with pytest.raises(SphereError) as e:
             st.upload()
         assert e.value.status == _status("SPH_ERR_INPUT")
+        # the refused input leaves no state to step
+        with pytest.raises(SphereError) as e:
+            st.step(1)
+        assert e.value.status == _status("SPH_ERR_STATE")
         st.close()
 
 

@@ -43,7 +43,8 @@ typedef enum SphStatus {
     SPH_ERR_NAN = 5,          /* a non-finite particle position */
     SPH_ERR_NOMEM = 6,        /* device or host allocation failed */
     SPH_ERR_STATE = 7,        /* call out of order (e.g. step before upload) */
-    SPH_ERR_UNSUPPORTED = 8   /* feature outside this library's scope */
+    SPH_ERR_UNSUPPORTED = 8,  /* feature outside this library's scope */
+    SPH_ERR_TIMEOUT = 9       /* a device-side wait gave up (the step's state is undefined) */
 } SphStatus;
 
 /* Arithmetic of the step. */
@@ -326,13 +327,27 @@ int sph_set_variant(SphHandle *h, int variant);
  * of list entries whose partner data each thread has in flight (staged in
  * shared memory) -- 0: 128 x 4, 1: 128 x 5, 2: 128 x 6, 3: 64 x 8,
  * 4: 256 x 2, 5: 64 x 8 staging 4, 6: 64 x 8 staging 6, 7: 128 x 4
- * staging 4, 8: 64 x 10 staging 3 (SPH_PAIR_SHAPES); the results do not
- * depend on it.  sph_autotune tries every shape of variant 4 and reports
+ * staging 4, 8: 64 x 10 staging 3, 9: persistent 64 x 8, 10: persistent
+ * 128 x 4 (SPH_PAIR_SHAPES); the results do not depend on it.  sph_autotune tries every shape of variant 4 and reports
  * the best in ms_per_step[4]; sph_get_tuning returns the variant and shape
  * in use. */
-#define SPH_PAIR_SHAPES 9
+#define SPH_PAIR_SHAPES 11
 int sph_set_launch_shape(SphHandle *h, int shape);
 int sph_get_tuning(const SphHandle *h, int *variant, int *shape);
+
+/* Shapes 9 (64 x 8) and 10 (128 x 4) of the list step are persistent: one
+ * cooperative launch per step whose blocks (all resident) take the spheres
+ * in turn, then meet at a grid-wide barrier, sum the wall forces, meet
+ * again and advance the walls.  A block waits at a barrier at most 1 s; a
+ * wait that runs out raises SPH_ERR_TIMEOUT (the launch ends, the device
+ * stays usable, the handle needs sph_upload).  sph_barrier_check runs
+ * `rounds` such barriers among `blocks` resident blocks of 32 threads on
+ * the current device, each waiting for `expected` arrivals for at most
+ * limit_s seconds: SPH_OK when they all open, SPH_ERR_TIMEOUT when
+ * expected > blocks (no barrier can open; every block gives up after the
+ * limit), SPH_ERR_INPUT for blocks outside 1 .. the number of SMs or a
+ * limit outside (0, 10] s. */
+int sph_barrier_check(uint32_t blocks, uint32_t expected, uint32_t rounds, double limit_s);
 
 /* Output snapshot, the output path of the reference's loop
  * (transferFromGlobalDeviceMemory before each output file,

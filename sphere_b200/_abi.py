@@ -24,7 +24,7 @@ SPH_ERR_UNSUPPORTED = 8
 STATUS_NAMES = {
     0: "SPH_OK", 1: "SPH_ERR_INPUT", 2: "SPH_ERR_CUDA", 3: "SPH_ERR_NC_OVERFLOW",
     4: "SPH_ERR_OUT_OF_GRID", 5: "SPH_ERR_NAN", 6: "SPH_ERR_NOMEM",
-    7: "SPH_ERR_STATE", 8: "SPH_ERR_UNSUPPORTED",
+    7: "SPH_ERR_STATE", 8: "SPH_ERR_UNSUPPORTED", 9: "SPH_ERR_TIMEOUT",
 }
 
 PREC_FP64 = 0
@@ -235,6 +235,8 @@ def load_library():
     lib.sph_set_launch_shape.restype = C.c_int
     lib.sph_get_tuning.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.sph_get_tuning.restype = C.c_int
+    lib.sph_barrier_check.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double]
+    lib.sph_barrier_check.restype = C.c_int
     lib.sph_set_neighbor_lists.restype = C.c_int
     lib.sph_adjoint_forward.argtypes = [H, C.c_uint64, C.c_uint32, _dp]
     lib.sph_cell_offsets_static.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]

@@ -170,18 +170,19 @@ static int ensure_pair(SphHandle *h)
         (st = dalloc(h, &P.live[0], n)) || (st = dalloc(h, &P.live[1], n)) ||
         (st = dalloc(h, &P.order[0], n)) || (st = dalloc(h, &P.order[1], n)) ||
         (st = dalloc(h, &P.hist[0], 3 * n * sph::VL_MAX)) ||
-        (st = dalloc(h, &P.hist[1], 3 * n * sph::VL_MAX)) || (st = dalloc(h, &words, 3)) ||
+        (st = dalloc(h, &P.hist[1], 3 * n * sph::VL_MAX)) || (st = dalloc(h, &words, 5)) ||
         (st = dalloc(h, &P.chunk_part, cbox.size())) || (st = dalloc(h, &chunk_box, cbox.size())) ||
         (st = dalloc(h, &box_chunk0, h->nbox)))
         return st;
     P.pp = words;
     P.lsel = words + 1;
     P.from_rows = words + 2;
+    P.bar = words + 3;
     P.chunk_box = chunk_box;
     P.box_chunk0 = box_chunk0;
     P.nchunks = (uint32_t)cbox.size();
     P.chunk_log2 = sph::PAIR_CHUNK_LOG2;
-    CUDA_TRY(h, cudaMemset(words, 0, 3 * sizeof(uint32_t)));
+    CUDA_TRY(h, cudaMemset(words, 0, 5 * sizeof(uint32_t)));
     for (int b = 0; b < 2; ++b) {
         CUDA_TRY(h, cudaMemset(P.cnt[b], 0, sizeof(uint32_t) * n));
         CUDA_TRY(h, cudaMemset(P.live[b], 0, sizeof(uint64_t) * n));
@@ -336,6 +337,7 @@ const char *sph_status_string(int status)
     case SPH_ERR_NOMEM: return "out of memory";
     case SPH_ERR_STATE: return "call out of order";
     case SPH_ERR_UNSUPPORTED: return "unsupported";
+    case SPH_ERR_TIMEOUT: return "a device-side wait gave up (grid barrier time limit)";
     default: return "unknown status";
     }
 }
@@ -963,7 +965,8 @@ static int collect_errors(SphHandle *h)
     CUDA_TRY(h, cudaMemcpy(&bits, h->A.err, sizeof bits, cudaMemcpyDeviceToHost));
     CUDA_TRY(h, cudaMemset(h->A.err, 0, sizeof(uint32_t)));
     if (!bits) return SPH_OK;
-    static const int order[] = {SPH_ERR_NAN, SPH_ERR_OUT_OF_GRID, SPH_ERR_INPUT, SPH_ERR_NC_OVERFLOW};
+    static const int order[] = {SPH_ERR_TIMEOUT, SPH_ERR_NAN, SPH_ERR_OUT_OF_GRID, SPH_ERR_INPUT,
+                                SPH_ERR_NC_OVERFLOW};
     for (int code : order)
         if (bits & (1u << code)) return fail(h, code, sph_status_string(code));
     return fail(h, SPH_ERR_CUDA, "unknown device error bits");
@@ -1338,7 +1341,8 @@ int sph_snapshot_read(SphHandle *h, SphParticles *p, SphBonds *b, SphBox *boxes)
     CUDA_TRY(h, cudaStreamSynchronize(h->snap_stream));
     if (boxes) boxes_from(h, d, boxes);
     if (!bits) return SPH_OK;
-    static const int order[] = {SPH_ERR_NAN, SPH_ERR_OUT_OF_GRID, SPH_ERR_INPUT, SPH_ERR_NC_OVERFLOW};
+    static const int order[] = {SPH_ERR_TIMEOUT, SPH_ERR_NAN, SPH_ERR_OUT_OF_GRID, SPH_ERR_INPUT,
+                                SPH_ERR_NC_OVERFLOW};
     for (int code : order)
         if (bits & (1u << code)) return fail(h, code, sph_status_string(code));
     return SPH_OK;
@@ -1424,6 +1428,26 @@ int sph_set_contacts(SphHandle *h, const uint32_t *contacts, const double *delta
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     invalidate_pair(h);
     return SPH_OK;
+}
+
+int sph_barrier_check(uint32_t blocks, uint32_t expected, uint32_t rounds, double limit_s)
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return SPH_ERR_CUDA;
+    if (blocks == 0 || (int)blocks > sms || !(limit_s > 0.0) || limit_s > 10.0 || expected == 0)
+        return SPH_ERR_INPUT;
+    uint32_t *d = nullptr;
+    if (cudaMalloc(&d, 3 * sizeof(uint32_t)) != cudaSuccess) return SPH_ERR_NOMEM;
+    int st = sph::barrier_check(blocks, expected, rounds, (unsigned long long)(limit_s * 1e9), d,
+                                d + 2, nullptr);
+    uint32_t err = 0;
+    if (st == SPH_OK && cudaMemcpy(&err, d + 2, sizeof err, cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = SPH_ERR_CUDA;
+    cudaFree(d);
+    if (st != SPH_OK) return st;
+    return err & (1u << SPH_ERR_TIMEOUT) ? SPH_ERR_TIMEOUT : SPH_OK;
 }
 
 uint64_t sph_total_cells(const SphHandle *h) { return h ? h->ncells : 0; }

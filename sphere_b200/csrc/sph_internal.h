@@ -110,6 +110,7 @@ struct PairArgs {
     uint32_t *order[2];
     uint32_t *pp, *lsel;
     uint32_t *from_rows;       // != 0: the next rebuild takes histories from A.slots / A.hist
+    uint32_t *bar;             // grid-barrier words of the persistent shapes: count, generation
     double *chunk_part;        // [nchunks]
     const uint32_t *chunk_box; // box of each chunk
     uint32_t nchunks;
@@ -117,7 +118,16 @@ struct PairArgs {
     const uint32_t *box_chunk0;   // first chunk of each box
 };
 constexpr int PAIR_CHUNK_LOG2 = 11;
-constexpr int PAIR_SHAPES = 9;
+
+// A grid-wide barrier among the blocks of one cooperative launch: arrival
+// count and generation words in device memory, and the longest a block
+// waits before it gives up (SPH_ERR_TIMEOUT).
+struct GridSync {
+    uint32_t *count, *gen;
+    unsigned long long limit_ns;
+};
+constexpr unsigned long long BARRIER_LIMIT_NS = 1000000000ull;   // 1 s
+constexpr int PAIR_SHAPES = 11;
 constexpr int PAIR_ORDER_GROUP = 128;   // launch shapes of the list-step kernel (sph_pair.cu)
 
 // Overlap search of one box (sph_overlaps): positions and velocities, the
@@ -214,6 +224,11 @@ int pair_load(const StepArgs &A, const PairArgs &P, cudaStream_t st);
 int pair_flush(const StepArgs &A, const PairArgs &P, cudaStream_t st);
 int pair_count_live(const StepArgs &A, const PairArgs &P, cudaStream_t st,
                     unsigned long long *d_count);
+// Self-check of the grid barrier (sph_barrier_check): `rounds` barriers of
+// `expected` arrivals among `blocks` resident blocks; error bits in *err.
+int barrier_check(uint32_t blocks, uint32_t expected, uint32_t rounds,
+                  unsigned long long limit_ns, uint32_t *d_words, uint32_t *d_err,
+                  cudaStream_t st);
 // Sort and neighbour lists for a rebuild of the list step's lists
 // (sph_kernels.cu): the positions of the current state (xr[*pp]) into A.x,
 // the cell sort, and the lists into the buffers not in use

@@ -275,18 +275,16 @@ __device__ __forceinline__ void finish_sphere(const StepArgs &A, const PairArgs 
     integrate_pair(A, P, B, i, nxt, xa, vel, wa, acc.F, acc.T);
 }
 
-// One step of the list form, one thread per sphere: the sphere's list
+// One sphere of the list step (thread slot t of the ordering): its list
 // entries in order, each tested with the exact FP64 overlap test and, for a
 // touching pair, the contact law with the entry's history (the loads of the
 // next entry -- partner state and, when its pair touched, its history --
 // issued before the current entry is computed); then walls, sums and the
 // integration of the sphere.
-template <int LM, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_pair_step(StepArgs A, PairArgs P)
+template <int LM>
+__device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P, uint32_t t,
+                                            uint32_t cur, uint32_t nxt, uint32_t ls)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= A.ntot) return;
-    const uint32_t cur = *P.pp, nxt = cur ^ 1u, ls = *P.lsel;
     const uint32_t i = P.order[ls][t];
     const double4 *__restrict__ xr = P.xr[cur];
     const float4 *__restrict__ vw = P.vw[cur];
@@ -355,6 +353,15 @@ __global__ void __launch_bounds__(NT, MINB) k_pair_step(StepArgs A, PairArgs P)
         hb = hq;
     }
     finish_sphere<LM>(A, P, B, i, nxt, ls, xa, wa, acc, live_old, live_new);
+}
+
+template <int LM, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_pair_step(StepArgs A, PairArgs P)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.ntot) return;
+    const uint32_t cur = *P.pp;
+    pair_sphere<LM>(A, P, t, cur, cur ^ 1u, *P.lsel);
 }
 
 // cp.async (global -> shared, issued per thread, completion per thread by
@@ -473,39 +480,36 @@ __global__ void __launch_bounds__(NT, MINB) k_pair_step_async(StepArgs A, PairAr
 // and the warps' sums in warp order (FP64, the same order every step).
 constexpr int CHUNK_THREADS = 256;
 
-__global__ void __launch_bounds__(CHUNK_THREADS) k_pair_chunks(StepArgs A, PairArgs P)
+// The wall-force sum of chunk c by the calling block (blockDim.x threads, a
+// multiple of 32, at most 1024): each thread adds its strided share in
+// index order, then a fixed shuffle tree and the warps' sums in warp order.
+__device__ __forceinline__ void chunk_sum(const StepArgs &A, const PairArgs &P, uint32_t c,
+                                          double *s_w)
 {
-    grid_dependency_wait();
-    __shared__ double s_w[CHUNK_THREADS / 32];
-    const uint32_t c = blockIdx.x;
     const uint32_t bx = P.chunk_box[c];
     const DevBox &B = A.boxes[bx];
     const uint32_t start = (c - P.box_chunk0[bx]) << P.chunk_log2;
     const uint32_t end = min(B.np, start + (1u << P.chunk_log2));
     double s = 0.0;
     if (B.nw > 0)
-        for (uint32_t k = start + threadIdx.x; k < end; k += CHUNK_THREADS) s += A.wf_pp[B.p_base + k];
+        for (uint32_t k = start + threadIdx.x; k < end; k += blockDim.x) s += A.wf_pp[B.p_base + k];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __syncthreads();
     if ((threadIdx.x & 31u) == 0) s_w[threadIdx.x >> 5] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int w = 0; w < CHUNK_THREADS / 32; ++w) t += s_w[w];
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) t += s_w[w];
         P.chunk_part[c] = t;
     }
 }
 
-// Per box: the chunks' sums in chunk order (FP64), then integrateWalls and
-// the time bookkeeping (advance_box); block 0 then hands the ping-pong
-// state to the next step.
-constexpr int PBOX_THREADS = 128;
-
-__global__ void __launch_bounds__(PBOX_THREADS) k_pair_box(StepArgs A, PairArgs P)
+// Box bx by the calling block: its chunks' sums in a fixed order (FP64),
+// then integrateWalls and the time bookkeeping (advance_box).
+__device__ __forceinline__ void box_sum_advance(const StepArgs &A, const PairArgs &P, uint32_t bx,
+                                                double *s_w)
 {
-    grid_dependency_wait();
-    __shared__ double s_w[PBOX_THREADS / 32];
-    const uint32_t bx = blockIdx.x;
     DevBox &B = A.boxes[bx];
     bool any = false;
     for (uint32_t w = 0; w < B.nw; ++w) any = any || B.wmode[w] != 0;
@@ -513,17 +517,111 @@ __global__ void __launch_bounds__(PBOX_THREADS) k_pair_box(StepArgs A, PairArgs 
     if (B.np > 0 && any) {
         const uint32_t c0 = P.box_chunk0[bx];
         const uint32_t nch = (B.np + (1u << P.chunk_log2) - 1) >> P.chunk_log2;
-        for (uint32_t k = threadIdx.x; k < nch; k += PBOX_THREADS) s += P.chunk_part[c0 + k];
+        for (uint32_t k = threadIdx.x; k < nch; k += blockDim.x) s += P.chunk_part[c0 + k];
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __syncthreads();
     if ((threadIdx.x & 31u) == 0) s_w[threadIdx.x >> 5] = s;
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    double fsum = 0.0;
-    for (int w = 0; w < PBOX_THREADS / 32; ++w) fsum += s_w[w];
-    advance_box(B, fsum);
-    if (bx == 0) *P.pp ^= 1u;
+    if (threadIdx.x == 0) {
+        double fsum = 0.0;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) fsum += s_w[w];
+        advance_box(B, fsum);
+    }
+}
+
+__global__ void __launch_bounds__(CHUNK_THREADS) k_pair_chunks(StepArgs A, PairArgs P)
+{
+    grid_dependency_wait();
+    __shared__ double s_w[32];
+    chunk_sum(A, P, blockIdx.x, s_w);
+}
+
+// Per box: the chunks' sums, integrateWalls, time; block 0 then hands the
+// ping-pong state to the next step.
+constexpr int PBOX_THREADS = 128;
+
+__global__ void __launch_bounds__(PBOX_THREADS) k_pair_box(StepArgs A, PairArgs P)
+{
+    grid_dependency_wait();
+    __shared__ double s_w[32];
+    box_sum_advance(A, P, blockIdx.x, s_w);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *P.pp ^= 1u;
+}
+
+// A grid-wide barrier with a time limit: the blocks of one launch (all
+// resident: the launch is cooperative) count in, the last one opens the
+// next generation; a block that waits longer than G.limit_ns raises
+// SPH_ERR_TIMEOUT and returns false (its kernel then ends, and so do the
+// others, at this barrier or the next), so a block that never arrives does
+// not hang the device.
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool grid_barrier(const GridSync &G, uint32_t nblocks, uint32_t *err)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile uint32_t *gen = G.gen;
+        const uint32_t g = *gen;
+        __threadfence();
+        if (atomicAdd(G.count, 1u) == nblocks - 1u) {
+            atomicExch(G.count, 0u);
+            __threadfence();
+            atomicAdd(G.gen, 1u);
+        } else {
+            const unsigned long long t0 = now_ns();
+            while (*gen == g) {
+                if (now_ns() - t0 > G.limit_ns) {
+                    ok = 0;
+                    raise_flag(err, SPH_ERR_TIMEOUT);
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// The list step as one persistent, cooperative launch: the blocks take the
+// spheres in turn (slots t = block + k * grid), then, after a grid barrier,
+// the chunks' wall-force sums, and after another the boxes (walls, time)
+// and the hand-over of the ping-pong state.  The same arithmetic and order
+// of sums as k_pair_step + k_pair_chunks + k_pair_box.
+template <int LM, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_pair_persist(StepArgs A, PairArgs P, GridSync G)
+{
+    __shared__ double s_w[32];
+    const uint32_t cur = *P.pp, nxt = cur ^ 1u, ls = *P.lsel;
+    for (uint32_t base = blockIdx.x * NT; base < A.ntot; base += gridDim.x * NT) {
+        const uint32_t t = base + threadIdx.x;
+        if (t < A.ntot) pair_sphere<LM>(A, P, t, cur, nxt, ls);
+    }
+    if (!grid_barrier(G, gridDim.x, A.err)) return;
+    for (uint32_t c = blockIdx.x; c < P.nchunks; c += gridDim.x) chunk_sum(A, P, c, s_w);
+    if (!grid_barrier(G, gridDim.x, A.err)) return;
+    for (uint32_t bx = blockIdx.x; bx < A.nboxes; bx += gridDim.x) box_sum_advance(A, P, bx, s_w);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *P.pp ^= 1u;
+}
+
+// Self-check of the barrier: `rounds` barriers among the launch's blocks,
+// counting `expected` arrivals per barrier (fewer blocks than expected: no
+// barrier opens and every block gives up after the limit).
+__global__ void k_barrier_check(GridSync G, uint32_t expected, uint32_t rounds, uint32_t *err)
+{
+    for (uint32_t r = 0; r < rounds; ++r)
+        if (!grid_barrier(G, expected, err)) return;
 }
 
 // Rebuild request -> the condition of the rebuild node.
@@ -737,6 +835,39 @@ void launch_staged(const StepArgs &A, const PairArgs &P, cudaStream_t st)
     k_pair_step_async<LM, NT, MINB, D><<<blocks_for(A.ntot, NT), NT, sm, st>>>(A, P);
 }
 
+// The persistent kernel: as many blocks as can be resident at once (at
+// most one per NT spheres), launched cooperatively (the launch fails rather
+// than run blocks that could not all be resident); the barrier's count is
+// cleared before each launch.
+template <int LM, int NT, int MINB>
+void launch_persistent(const StepArgs &A, const PairArgs &P, cudaStream_t st)
+{
+    static int per_sm = -1, sms = 0;
+    if (per_sm < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_persist<LM, NT, MINB>, NT, 0);
+    }
+    const unsigned need = blocks_for(A.ntot, NT);
+    const unsigned cap = (unsigned)(per_sm > 0 ? per_sm : 1) * (unsigned)sms;
+    GridSync G;
+    G.count = P.bar;
+    G.gen = P.bar + 1;
+    G.limit_ns = BARRIER_LIMIT_NS;
+    cudaMemsetAsync(P.bar, 0, sizeof(uint32_t), st);
+    cudaLaunchConfig_t c = {};
+    c.gridDim = dim3(need < cap ? need : cap);
+    c.blockDim = dim3(NT);
+    c.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    c.attrs = at;
+    c.numAttrs = 1;
+    cudaLaunchKernelEx(&c, k_pair_persist<LM, NT, MINB>, A, P, G);
+}
+
 template <int LM>
 void launch_pair_lm(const StepArgs &A, const PairArgs &P, int shape, cudaStream_t st)
 {
@@ -749,6 +880,8 @@ void launch_pair_lm(const StepArgs &A, const PairArgs &P, int shape, cudaStream_
     case 6: launch_staged<LM, 64, 8, 6>(A, P, st); break;
     case 7: launch_staged<LM, 128, 4, 4>(A, P, st); break;
     case 8: launch_staged<LM, 64, 10, 3>(A, P, st); break;
+    case 9: launch_persistent<LM, 64, 8>(A, P, st); break;
+    case 10: launch_persistent<LM, 128, 4>(A, P, st); break;
     default: k_pair_step<LM, 128, 4><<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, P); break;
     }
 }
@@ -824,6 +957,17 @@ int launch_step_pair(const StepArgs &A, const PairArgs &P, const StepConfig &cfg
     }
     mark(prof, st, "k_pair_cond");
     launch_pair_kernel(A, P, cfg, st);
+    if (cfg.pair_shape >= 9) {
+        // the persistent shapes do the wall stage themselves
+        mark(prof, st, "k_pair_persist");
+        if (launches) *launches += nl + 1;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            fprintf(stderr, "sphere_b200: list-step launch failed: %s\n", cudaGetErrorString(e));
+            return SPH_ERR_CUDA;
+        }
+        return SPH_OK;
+    }
     mark(prof, st, "k_pair_step");
     const bool pdl = prof == nullptr;
     if (cfg.any_walls) {
@@ -841,6 +985,31 @@ int launch_step_pair(const StepArgs &A, const PairArgs &P, const StepConfig &cfg
         return SPH_ERR_CUDA;
     }
     return SPH_OK;
+}
+
+int barrier_check(uint32_t blocks, uint32_t expected, uint32_t rounds,
+                  unsigned long long limit_ns, uint32_t *d_words, uint32_t *d_err,
+                  cudaStream_t st)
+{
+    if (cudaMemsetAsync(d_words, 0, 2 * sizeof(uint32_t), st) != cudaSuccess ||
+        cudaMemsetAsync(d_err, 0, sizeof(uint32_t), st) != cudaSuccess)
+        return SPH_ERR_CUDA;
+    GridSync G;
+    G.count = d_words;
+    G.gen = d_words + 1;
+    G.limit_ns = limit_ns;
+    cudaLaunchConfig_t c = {};
+    c.gridDim = dim3(blocks);
+    c.blockDim = dim3(32);
+    c.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    c.attrs = at;
+    c.numAttrs = 1;
+    if (cudaLaunchKernelEx(&c, k_barrier_check, G, expected, rounds, d_err) != cudaSuccess)
+        return SPH_ERR_CUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
 }
 
 int pair_load(const StepArgs &A, const PairArgs &P, cudaStream_t st)

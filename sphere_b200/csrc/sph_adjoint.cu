@@ -254,12 +254,30 @@ __global__ void __launch_bounds__(128) k_adj_contacts(AdjArgs J)
         const d3 Fb = mk(lacc[0] / m, lacc[1] / m, lacc[2] / m);
         const d3 Tb = mk(lalp[0] / I, lalp[1] / I, lalp[2] / I);
         d3 xab = d3z(), vab = d3z(), wab = d3z();
-        for (int s = 0; s < NC; ++s) {
+        // A slot that is empty after this step's contact search holds no
+        // history adjoint: the step after wrote one only to slots that held
+        // a contact at its start, i.e. at the end of this step, and those
+        // were occupied after this step's search.  So only the occupied
+        // slots are read and written.
+        uint32_t occ = 0;
+        {
+            const uint4 *rp = reinterpret_cast<const uint4 *>(J.rows_post + (size_t)i * NC);
+#pragma unroll
+            for (int q4 = 0; q4 < NC / 4; ++q4) {
+                const uint4 w4 = rp[q4];
+                occ |= (w4.x != EMPTY ? 1u : 0u) << (4 * q4);
+                occ |= (w4.y != EMPTY ? 1u : 0u) << (4 * q4 + 1);
+                occ |= (w4.z != EMPTY ? 1u : 0u) << (4 * q4 + 2);
+                occ |= (w4.w != EMPTY ? 1u : 0u) << (4 * q4 + 3);
+            }
+        }
+        for (uint32_t m = occ; m; m &= m - 1u) {
+            const int s = __ffs(m) - 1;
             const size_t q = (size_t)i * NC + s;
             const uint32_t w = J.rows_post[q];
             const double4 dbo = J.lH[q];
             double4 h0b_out = make_double4(0.0, 0.0, 0.0, 0.0);
-            if (w != EMPTY) {
+            {
                 const uint32_t b = w & ID_MASK;
                 int sx, sy;
                 decode_shift(w >> CODE_SHIFT, sx, sy);

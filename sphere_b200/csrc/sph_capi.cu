@@ -1660,10 +1660,10 @@ int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_para
         release();
         return fail(h, SPH_ERR_NOMEM, "adjoint buffers do not fit in device memory");
     }
-    double4 *lnext[5], *lcur[5];
+    double4 *lnext[5], *lnext0[5], *lcur0[5];
     for (int k = 0; k < 5; ++k) {
-        lnext[k] = lbuf + (size_t)k * n;
-        lcur[k] = lbuf + (size_t)(5 + k) * n;
+        lnext0[k] = lnext[k] = lbuf + (size_t)k * n;
+        lcur0[k] = lbuf + (size_t)(5 + k) * n;
     }
     std::vector<double4> seed(n ? n : 1);
     for (uint32_t i = 0; i < n; ++i)
@@ -1677,40 +1677,103 @@ int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_para
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(lnext[0], seed.data(), n4, cudaMemcpyHostToDevice, h->stream);
     cudaEventRecord(ev[0], h->stream);
+    // Each segment's recompute (the steps from its checkpoint, each step's
+    // start state and contact rows copied to the tape) and its reverse (the
+    // steps' adjoint kernels, last step first) are captured once as CUDA
+    // graphs and launched for every segment of that shape: the tape
+    // offsets are the same in every segment, the reverse differs only in
+    // the segment's length, in whether it holds the run's first step (whose
+    // previous accelerations are zero) and in which of the two adjoint
+    // buffers it starts from.
+    struct SegGraph {
+        uint64_t ns;
+        int kind;   // recompute: -1; reverse: first * 2 + parity
+        cudaGraph_t g;
+        cudaGraphExec_t ge;
+    };
+    std::vector<SegGraph> graphs;
+    auto seg_graph = [&](uint64_t ns, int kind, cudaGraphExec_t *out) -> int {
+        for (const SegGraph &q : graphs)
+            if (q.ns == ns && q.kind == kind) {
+                *out = q.ge;
+                return SPH_OK;
+            }
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) return SPH_ERR_CUDA;
+        (void)cudaGetLastError();
+        if (cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        int rst = SPH_OK;
+        if (kind < 0) {
+            for (uint64_t k = 0; k < ns && rst == SPH_OK; ++k) {
+                char *t = tape + step_tape * k;
+                cudaMemcpyAsync(t, h->A.x, n4, cudaMemcpyDeviceToDevice, h->own);
+                cudaMemcpyAsync(t + n4, h->A.vel, n4, cudaMemcpyDeviceToDevice, h->own);
+                cudaMemcpyAsync(t + 2 * n4, h->A.angvel, n4, cudaMemcpyDeviceToDevice, h->own);
+                StepArgs Ar = h->A;
+                Ar.tape_rows_pre = (uint32_t *)(t + 3 * n4);
+                Ar.tape_rows_post = Ar.tape_rows_pre + (size_t)n * sph::NC;
+                Ar.tape_hist = (double4 *)(Ar.tape_rows_post + (size_t)n * sph::NC);
+                uint64_t nl = 0;
+                rst = sph::launch_step(Ar, h->cfg, h->own, &nl);
+            }
+        } else {
+            const bool first = (kind >> 1) != 0;
+            double4 *ln[5], *lc[5];
+            for (int q = 0; q < 5; ++q) {
+                ln[q] = (kind & 1) ? lcur0[q] : lnext0[q];
+                lc[q] = (kind & 1) ? lnext0[q] : lcur0[q];
+            }
+            for (uint64_t k = ns; k-- > 0 && rst == SPH_OK;) {
+                const char *t = tape + step_tape * k;
+                const double4 *tx = (const double4 *)t, *tv = tx + n, *tw = tv + n;
+                const uint32_t *rpre = (const uint32_t *)(t + 3 * n4);
+                const uint32_t *rpost = rpre + (size_t)n * sph::NC;
+                const double4 *th = (const double4 *)(rpost + (size_t)n * sph::NC);
+                // the iteration index matters only as "the run's first step or not"
+                const uint64_t it = first && k == 0 ? 0 : 1;
+                rst = sph::adjoint_step(h->A.boxes, n, it, tx, tv, tw, rpre, rpost, th, ln, lc,
+                                        lH, dscal, h->own);
+                for (int q = 0; q < 5; ++q) std::swap(ln[q], lc[q]);
+            }
+        }
+        SegGraph q{ns, kind, nullptr, nullptr};
+        const cudaError_t ec = cudaStreamEndCapture(h->own, &q.g);
+        if (rst != SPH_OK || ec != cudaSuccess) {
+            if (q.g) cudaGraphDestroy(q.g);
+            return rst != SPH_OK ? rst : SPH_ERR_CUDA;
+        }
+        if (cudaGraphInstantiate(&q.ge, q.g, 0) != cudaSuccess) {
+            cudaGraphDestroy(q.g);
+            return SPH_ERR_CUDA;
+        }
+        graphs.push_back(q);
+        *out = q.ge;
+        return SPH_OK;
+    };
+    int parity = 0;   // 1: the step after the last reversed one is in lcur0
     for (uint64_t sgm = nseg; e == cudaSuccess && sgm-- > 0;) {
-        // recompute the segment from its checkpoint, recording the tape
         copy_state(h, h->adj_snaps, sgm, false);
         const uint64_t ns = std::min<uint64_t>(ckpt, nsteps - sgm * ckpt);
-        for (uint64_t k = 0; k < ns; ++k) {
-            char *t = tape + step_tape * k;
-            cudaMemcpyAsync(t, h->A.x, n4, cudaMemcpyDeviceToDevice, h->stream);
-            cudaMemcpyAsync(t + n4, h->A.vel, n4, cudaMemcpyDeviceToDevice, h->stream);
-            cudaMemcpyAsync(t + 2 * n4, h->A.angvel, n4, cudaMemcpyDeviceToDevice, h->stream);
-            StepArgs Ar = h->A;
-            Ar.tape_rows_pre = (uint32_t *)(t + 3 * n4);
-            Ar.tape_rows_post = Ar.tape_rows_pre + (size_t)n * sph::NC;
-            Ar.tape_hist = (double4 *)(Ar.tape_rows_post + (size_t)n * sph::NC);
-            uint64_t nl = 0;
-            if ((st = sph::launch_step(Ar, h->cfg, h->stream, &nl)) != SPH_OK) break;
-            h->launches += nl;
+        cudaGraphExec_t gr = nullptr, gb = nullptr;
+        const bool first = sgm == 0 && h->adj_iter0 == 0;
+        if ((st = seg_graph(ns, -1, &gr)) != SPH_OK ||
+            (st = seg_graph(ns, (first ? 2 : 0) + parity, &gb)) != SPH_OK)
+            break;
+        if (cudaGraphLaunch(gr, h->stream) != cudaSuccess || cudaGraphLaunch(gb, h->stream) != cudaSuccess) {
+            st = SPH_ERR_CUDA;
+            break;
         }
-        if (st != SPH_OK) break;
-        // reverse the segment's steps
-        for (uint64_t k = ns; k-- > 0;) {
-            const char *t = tape + step_tape * k;
-            const double4 *tx = (const double4 *)t, *tv = tx + n, *tw = tv + n;
-            const uint32_t *rpre = (const uint32_t *)(t + 3 * n4);
-            const uint32_t *rpost = rpre + (size_t)n * sph::NC;
-            const double4 *th = (const double4 *)(rpost + (size_t)n * sph::NC);
-            st = sph::adjoint_step(h->A.boxes, n, h->adj_iter0 + sgm * ckpt + k, tx, tv, tw, rpre,
-                                   rpost, th, lnext, lcur, lH, dscal, h->stream);
-            h->launches += 2;
-            if (st != SPH_OK) break;
-            for (int q = 0; q < 5; ++q) std::swap(lnext[q], lcur[q]);
-        }
-        if (st != SPH_OK) break;
+        h->launches += ns * (h->launches_per_step + 2);
+        if (ns & 1) parity ^= 1;
     }
+    // the adjoints of the run's initial state
+    for (int q = 0; q < 5; ++q) lnext[q] = parity ? lcur0[q] : lnext0[q];
     cudaEventRecord(ev[1], h->stream);
+    cudaStreamSynchronize(h->stream);
+    for (const SegGraph &q : graphs) {
+        cudaGraphExecDestroy(q.ge);
+        cudaGraphDestroy(q.g);
+    }
     // leave the handle at the forward's final state
     copy_state(h, h->adj_snaps, nseg, false);
     double scal[3] = {0, 0, 0};

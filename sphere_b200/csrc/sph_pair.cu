@@ -85,6 +85,20 @@ __device__ __forceinline__ double len_rn(d3 v)
     return (double)__fsqrt_rn(__double2float_rn(d));
 }
 
+// A sphere's sums in the list step: force and torque in FP64 (they drive
+// the FP64 integration, where the contacts' forces largely cancel), the
+// energy rates and pressure in FP32 (stored in FP32; es and ev accumulate
+// them in FP64).
+struct MixedAcc {
+    d3 F, T;
+    float es_dot, ev_dot, p;
+    __device__ __forceinline__ void addF(d3 v) { F = vadd(F, v); }
+    __device__ __forceinline__ void addT(d3 v) { T = vadd(T, v); }
+    __device__ __forceinline__ void addEs(double v) { es_dot += (float)v; }
+    __device__ __forceinline__ void addEv(double v) { ev_dot += (float)v; }
+    __device__ __forceinline__ void addP(double v) { p += (float)v; }
+};
+
 __device__ __forceinline__ MixedPair mixed_pair_f(d3 x_ab, double x_length, double delta, float4 va,
                                                   float4 vb, float4 wa, float4 wb, double ra,
                                                   double rb)
@@ -107,7 +121,7 @@ __device__ __forceinline__ MixedPair mixed_pair_f(d3 x_ab, double x_length, doub
 // is returned.  Reads each wall from the box table where it is used.
 template <int LM>
 __device__ __forceinline__ double walls_pair(const DevBox &B, double4 xa, d3 vel_a, d3 angvel_a,
-                                             Acc &acc)
+                                             MixedAcc &acc)
 {
     const SphParams &Pm = B.P;
     const double dt = B.dt, r = xa.w;
@@ -257,7 +271,7 @@ __device__ __forceinline__ void integrate_pair(const StepArgs &A, const PairArgs
 template <int LM>
 __device__ __forceinline__ void finish_sphere(const StepArgs &A, const PairArgs &P,
                                               const DevBox &B, uint32_t i, uint32_t nxt,
-                                              uint32_t ls, double4 xa, float4 wa, Acc &acc,
+                                              uint32_t ls, double4 xa, float4 wa, MixedAcc &acc,
                                               unsigned long long live_old,
                                               unsigned long long live_new)
 {
@@ -268,9 +282,9 @@ __device__ __forceinline__ void finish_sphere(const StepArgs &A, const PairArgs 
     const double w0_force = walls_pair<LM>(B, xa, xyz(vel), mk(wa.x, wa.y, wa.z), acc);
     P.force[i] = make_float4((float)acc.F.x, (float)acc.F.y, (float)acc.F.z, 0.f);
     P.torque[i] = make_float4((float)acc.T.x, (float)acc.T.y, (float)acc.T.z, 0.f);
-    P.epp[i] = make_float4((float)acc.es_dot, (float)acc.ev_dot, (float)acc.p, 0.f);
+    P.epp[i] = make_float4(acc.es_dot, acc.ev_dot, acc.p, 0.f);
     const double2 e0 = P.eacc[i];
-    P.eacc[i] = make_double2(e0.x + acc.es_dot * dt, e0.y + acc.ev_dot * dt);
+    P.eacc[i] = make_double2(e0.x + (double)acc.es_dot * dt, e0.y + (double)acc.ev_dot * dt);
     if (B.nw > 0) A.wf_pp[i] = w0_force;
     integrate_pair(A, P, B, i, nxt, xa, vel, wa, acc.F, acc.T);
 }
@@ -302,12 +316,12 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
     const float4 va = vw[2 * i], wa = vw[2 * i + 1];
     const double dt = B.dt;
 
-    Acc acc;
+    MixedAcc acc;
     acc.F = mk(0.0, 0.0, 0.0);
     acc.T = mk(0.0, 0.0, 0.0);
-    acc.es_dot = 0.0;
-    acc.ev_dot = 0.0;
-    acc.p = 0.0;
+    acc.es_dot = 0.f;
+    acc.ev_dot = 0.f;
+    acc.p = 0.f;
     // entry k's partner state and history are loaded during entry k - 1,
     // entry k's partner id during entry k - 2 (the row holds VL_MAX >= 2
     // ids; those at or past n are not used)
@@ -442,12 +456,12 @@ __global__ void __launch_bounds__(NT, MINB) k_pair_step_async(StepArgs A, PairAr
     const float4 va = vw[2 * i], wa = vw[2 * i + 1];
     const double dt = B.dt;
 
-    Acc acc;
+    MixedAcc acc;
     acc.F = mk(0.0, 0.0, 0.0);
     acc.T = mk(0.0, 0.0, 0.0);
-    acc.es_dot = 0.0;
-    acc.ev_dot = 0.0;
-    acc.p = 0.0;
+    acc.es_dot = 0.f;
+    acc.ev_dot = 0.f;
+    acc.p = 0.f;
     for (uint32_t k = 0; k < n; ++k) {
         cp_async_wait<D - 1>();
         const int q = (int)(k % D);

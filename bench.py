@@ -727,9 +727,15 @@ def main():
     long_run = None
     if rank == 0 and not args.no_long_run and "mixed" in res and "fp64" in res:
         # the mixed form's error against the FP64 form over the workload's
-        # whole run (5,000 steps of the same pack): wall stress, porosity
+        # whole run (5,000 steps of the same pack): wall stress, porosity;
+        # in the launch variant timed above, beside the floor of the chaotic
+        # flow (FP64 against FP64 from positions moved by 1e-15 relative)
         from sphere_b200.mixed_error import compare_precisions
-        long_run = compare_precisions(s, slices=50, device=local, cuda_stream=stream.cuda_stream)
+        long_run = compare_precisions(s, slices=50, device=local, cuda_stream=stream.cuda_stream,
+                                      variant=res["mixed"]["tuning"]["variant"])
+        long_run["fp64_floor"] = compare_precisions(s, slices=50, device=local,
+                                                    cuda_stream=stream.cuda_stream,
+                                                    precision="fp64", perturb=1e-15)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -328,10 +328,13 @@ int sph_set_variant(SphHandle *h, int variant);
  * shared memory) -- 0: 128 x 4, 1: 128 x 5, 2: 128 x 6, 3: 64 x 8,
  * 4: 256 x 2, 5: 64 x 8 staging 4, 6: 64 x 8 staging 6, 7: 128 x 4
  * staging 4, 8: 64 x 10 staging 3, 9: persistent 64 x 8, 10: persistent
- * 128 x 4 (SPH_PAIR_SHAPES); the results do not depend on it.  sph_autotune tries every shape of variant 4 and reports
- * the best in ms_per_step[4]; sph_get_tuning returns the variant and shape
- * in use. */
-#define SPH_PAIR_SHAPES 11
+ * 128 x 4; shapes 11 and 12 load each list entry at its turn instead of
+ * one entry ahead (fewer registers, more resident warps) -- 11: 64 x 10,
+ * 12: 64 x 12 (SPH_PAIR_SHAPES).  The results do
+ * not depend on the shape.  sph_autotune tries every shape of variant 4
+ * and reports the best in ms_per_step[4]; sph_get_tuning returns the
+ * variant and shape in use. */
+#define SPH_PAIR_SHAPES 13
 int sph_set_launch_shape(SphHandle *h, int shape);
 int sph_get_tuning(const SphHandle *h, int *variant, int *shape);
 

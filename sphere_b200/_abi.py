@@ -9,6 +9,7 @@ import os
 NC = 32
 MAXWALLS = 6
 TUNE_VARIANTS = 5   # SPH_TUNE_VARIANTS: launch variants sph_autotune times
+PAIR_SHAPES = 13    # SPH_PAIR_SHAPES: launch shapes of the list step (variant 4)
 BIN_VERSION = 2.15
 
 SPH_OK = 0

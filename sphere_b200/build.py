@@ -4,8 +4,10 @@
 
 Each .cu file is compiled separately: the FP64 step (sph_kernels.cu) and the
 C ABI without FMA contraction (-fmad=false) so that FP64 results reproduce
-the reference's arithmetic bit for bit, the FP32-mixed step (sph_mixed.cu)
-with contraction.  ptxas resource usage is written to
+the reference's arithmetic bit for bit, the FP32-mixed split step
+(sph_mixed.cu) with contraction, the list step (sph_pair.cu) without it, so
+that its launch shapes, compiled under different register budgets, give the
+same bits.  ptxas resource usage is written to
 sphere_b200/_build/ptxas.log.
 """
 import os
@@ -26,7 +28,7 @@ SOURCES = [
     ("sph_kernels.cu", ["-fmad=false"]),
     ("sph_capi.cu", ["-fmad=false"]),
     ("sph_mixed.cu", ["-fmad=true"]),
-    ("sph_pair.cu", ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
+    ("sph_pair.cu", ["-fmad=false", "-ftz=true"]),
     ("sph_adjoint.cu", ["-fmad=false"]),
     ("sph_noalloc.cu", []),
     ("sph_render.cu", ["-fmad=false"]),
@@ -44,8 +46,9 @@ def build(verbose=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
     objs = []
     log = []
+    # the sources, the public header, and this file (its flags)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + \
-        [os.path.join(ROOT, "include", "sphere_b200.h")]
+        [os.path.join(ROOT, "include", "sphere_b200.h"), os.path.abspath(__file__)]
     newest_dep = max(os.path.getmtime(d) for d in deps)
     for src, flags in SOURCES:
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))

@@ -127,7 +127,10 @@ struct GridSync {
     unsigned long long limit_ns;
 };
 constexpr unsigned long long BARRIER_LIMIT_NS = 1000000000ull;   // 1 s
-constexpr int PAIR_SHAPES = 11;
+constexpr int PAIR_SHAPES = 13;
+// Shapes 9 and 10 are the persistent kernel, which does the wall stage
+// itself; every other shape is followed by k_pair_chunks and k_pair_box.
+inline bool pair_shape_persistent(int shape) { return shape == 9 || shape == 10; }
 constexpr int PAIR_ORDER_GROUP = 128;   // launch shapes of the list-step kernel (sph_pair.cu)
 
 // Overlap search of one box (sph_overlaps): positions and velocities, the

@@ -27,7 +27,26 @@ __device__ __forceinline__ f3 fcross(f3 a, f3 b)
 {
     return fk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
-__device__ __forceinline__ float flen(f3 v) { return sqrtf(fdot(v, v)); }
+// FP32 square root and reciprocal of the laws: the GPU's approximate
+// special-function instructions (sqrt.approx.ftz.f32, rcp.approx.ftz.f32;
+// relative error of a few 2^-23), written as PTX.  Each is one defined
+// instruction, so every kernel that inlines the laws gets the same bits
+// from it whatever its register budget (a correctly rounded division or an
+// approximate one left to the compiler is a sequence the code generator may
+// lay out differently per kernel), at one special-function operation each.
+__device__ __forceinline__ float fsqrt_a(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float frcp_a(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float flen(f3 v) { return fsqrt_a(fdot(v, v)); }
 __device__ __forceinline__ f3 tof(d3 v) { return fk((float)v.x, (float)v.y, (float)v.z); }
 __device__ __forceinline__ d3 tod(f3 v) { return mk((double)v.x, (double)v.y, (double)v.z); }
 __device__ __forceinline__ f3 xyzf(double4 v) { return fk((float)v.x, (float)v.y, (float)v.z); }
@@ -44,7 +63,7 @@ __device__ __forceinline__ MixedPair mixed_pair(d3 x_ab, double x_length, double
                                                 double rb)
 {
     MixedPair q;
-    const float inv = 1.0f / (float)x_length;
+    const float inv = frcp_a((float)x_length);
     q.n = fmul(inv, tof(x_ab));
     q.vel_linear = tof(vsub(vel_a, vel_b));
     q.angvel_a = angvel_a;
@@ -90,7 +109,7 @@ __device__ __forceinline__ d3 contact_linear_mixed(const SphParams &P, double dt
     const f3 f_n = fmul(fnm, n);
     const float f_n_length = fabsf(fnm);
     a.addEv((double)(0.5f * gn * vel_n * vel_n));
-    const f3 f_c = fmul(-(float)P.kappa * sqrtf(q.ra * q.rb), n);
+    const f3 f_c = fmul(-(float)P.kappa * fsqrt_a(q.ra * q.rb), n);
     f3 f_t = fk(0.f, 0.f, 0.f);
     d3 delta_t = mk(0.0, 0.0, 0.0);
     if (delta_t0_nonzero || vel_t_length > 0.0f) {
@@ -101,15 +120,15 @@ __device__ __forceinline__ d3 contact_linear_mixed(const SphParams &P, double dt
         const float f_t_limit = (float)P.mu_s * fnc;
         a.addEv((double)(0.5f * gt * vel_t_length * vel_t_length));
         if (f_t_length > f_t_limit) {
-            const f3 t = fmul(1.0f / f_t_length, f_t);
+            const f3 t = fmul(frcp_a(f_t_length), f_t);
             f_t = fmul(f_t_limit, t);
-            delta_t = tod(fmul(-1.0f / k_t, fadd(fmul((float)P.mu_d * fnc, t), fmul(gt, vel_t))));
-            a.addEs((double)(0.5f * flen(fmul((float)dt * f_t_limit, vel_t)) / (float)dt));
+            delta_t = tod(fmul(-frcp_a(k_t), fadd(fmul((float)P.mu_d * fnc, t), fmul(gt, vel_t))));
+            a.addEs((double)(0.5f * flen(fmul((float)dt * f_t_limit, vel_t)) * frcp_a((float)dt)));
         }
     }
     a.addF(tod(fadd(fadd(f_n, f_t), f_c)));
     a.addT(tod(fcross(fmul(-(q.ra + delta * 0.5f), n), f_t)));
-    a.addP((double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra)));
+    a.addP((double)(f_n_length * frcp_a(4.0f * 3.14159265358979f * q.ra * q.ra)));
     return delta_t;
 }
 
@@ -121,7 +140,7 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
 {
     const f3 n = q.n;
     const float delta = q.delta;
-    const float d12 = sqrtf(fabsf(delta)), d14 = sqrtf(d12), d32 = delta * d12;
+    const float d12 = fsqrt_a(fabsf(delta)), d14 = fsqrt_a(d12), d32 = delta * d12;
     const f3 vel_ab = fadd(fadd(q.vel_linear, fmul(q.ra + delta * 0.5f, fcross(n, q.angvel_a))),
                            fmul(q.rb + delta * 0.5f, fcross(n, q.angvel_b)));
     const f3 angvel_ab = fsub(q.angvel_a, q.angvel_b);
@@ -139,7 +158,7 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
     a.addEv((double)(gn * vel_n_ab * vel_n_ab));
     if (fdot(f_n, n) < 0.0f) f_n = fk(0.f, 0.f, 0.f);
     const float f_n_length = flen(f_n);
-    const f3 f_c = fmul(-(float)P.kappa * sqrtf(q.ra * q.rb), n);
+    const f3 f_c = fmul(-(float)P.kappa * fsqrt_a(q.ra * q.rb), n);
     f3 f_t = fk(0.f, 0.f, 0.f);
     f3 T_res = fk(0.f, 0.f, 0.f);
     d3 delta_t = mk(0.0, 0.0, 0.0);
@@ -151,8 +170,8 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
         f_t = fadd(f_t_elast, f_t_visc);
         const float f_t_length = flen(f_t);
         if (f_t_length > f_t_limit) {
-            f_t = fmul(f_t_limit / f_t_length, f_t);
-            delta_t = tod(fmul(1.0f / (-k_t * d12), fadd(f_t, fmul(gt * d14, vel_t_ab))));
+            f_t = fmul(f_t_limit * frcp_a(f_t_length), f_t);
+            delta_t = tod(fmul(frcp_a(-k_t * d12), fadd(f_t, fmul(gt * d14, vel_t_ab))));
             a.addEs(sqrt(dot(vsub(delta_t0, delta_t), vsub(delta_t0, delta_t))) * (double)k_t / dt);
         } else {
             delta_t = vadd(delta_t0, muls(tod(vel_t_ab), dt));
@@ -160,11 +179,11 @@ __device__ __forceinline__ d3 contact_hertz_mixed(const SphParams &P, double dt,
     }
     if (angvel_ab_length > 0.0f)
         T_res = fmul(-fminf((float)P.gamma_r * q.ra * angvel_ab_length,
-                            (float)P.mu_r * q.ra * f_n_length) / angvel_ab_length,
+                            (float)P.mu_r * q.ra * f_n_length) * frcp_a(angvel_ab_length),
                      angvel_ab);
     a.addF(tod(fadd(fadd(f_n, f_t), f_c)));
     a.addT(tod(fadd(fmul(-(q.ra + delta * 0.5f), fcross(n, f_t)), T_res)));
-    a.addP((double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra)));
+    a.addP((double)(f_n_length * frcp_a(4.0f * 3.14159265358979f * q.ra * q.ra)));
     return delta_t;
 }
 
@@ -185,18 +204,18 @@ __device__ __forceinline__ void contact_linear_viscous_mixed(const SphParams &P,
     f3 f_n = fmul(fmaxf(0.0f, -k_n * delta - (float)P.gamma_n * vel_n_ab), n);
     if (fdot(f_n, n) < 0.0f) f_n = fk(0.f, 0.f, 0.f);
     const float f_n_length = flen(f_n);
-    const f3 f_c = fmul(-kappa * sqrtf(q.ra * q.rb), n);
+    const f3 f_c = fmul(-kappa * fsqrt_a(q.ra * q.rb), n);
     f3 f_t = fk(0.f, 0.f, 0.f);
     if (vel_t_ab_length > 0.0f) {
         const float f_t_visc = (float)P.gamma_t * vel_t_ab_length;
         const float fnc = flen(fsub(f_n, f_c));
         const float f_t_limit = vel_t_ab_length > 0.001f ? (float)P.mu_d * fnc : (float)P.mu_s * fnc;
         const float mag = f_t_visc < f_t_limit ? f_t_visc : f_t_limit;
-        f_t = fmul(-mag / vel_t_ab_length, vel_t_ab);
+        f_t = fmul(-mag * frcp_a(vel_t_ab_length), vel_t_ab);
     }
     a.addF(tod(fadd(fadd(f_n, f_t), f_c)));
     a.addT(tod(fmul(-(q.ra + delta * 0.5f), fcross(n, f_t))));
-    a.addP((double)(f_n_length / (4.0f * 3.14159265358979f * q.ra * q.ra)));
+    a.addP((double)(f_n_length * frcp_a(4.0f * 3.14159265358979f * q.ra * q.ra)));
 }
 
 }  // namespace sph

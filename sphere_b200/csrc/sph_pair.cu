@@ -34,10 +34,15 @@
 // more than half the skin since the last build: a conditional graph node
 // whose body is the cell sort, the list build and the history carry-over
 // (launch_step_pair), set by k_pair_cond from the flag the integration
-// raises.  Compiled with FMA contraction and with FP32 division and square
-// root to within an ulp or two (the contact laws' FP32 part); the overlap
-// test is written with explicitly rounded operations so that it matches the
-// FP64 form.
+// raises.  Every launch shape gives the same bits: the code generator may
+// fuse a multiply and an add, or lay out an approximate division,
+// differently in one shape than in another (it decides under each shape's
+// register budget), so the file is compiled without FMA contraction, the
+// contact laws' FP32 square roots and reciprocals are single approximate
+// instructions written as PTX (sph_mixed_laws.cuh), and any other FP32
+// division or square root is correctly rounded.  The overlap test is
+// written with explicitly rounded operations so that it matches the FP64
+// form.
 #include <cstdint>
 #include <cstdio>
 
@@ -104,7 +109,7 @@ __device__ __forceinline__ MixedPair mixed_pair_f(d3 x_ab, double x_length, doub
                                                   double rb)
 {
     MixedPair q;
-    const float inv = 1.0f / (float)x_length;
+    const float inv = frcp_a((float)x_length);
     q.n = fmul(inv, tof(x_ab));
     q.vel_linear = fk(va.x - vb.x, va.y - vb.y, va.z - vb.z);
     q.angvel_a = fk(wa.x, wa.y, wa.z);
@@ -291,11 +296,13 @@ __device__ __forceinline__ void finish_sphere(const StepArgs &A, const PairArgs 
 
 // One sphere of the list step (thread slot t of the ordering): its list
 // entries in order, each tested with the exact FP64 overlap test and, for a
-// touching pair, the contact law with the entry's history (the loads of the
-// next entry -- partner state and, when its pair touched, its history --
-// issued before the current entry is computed); then walls, sums and the
-// integration of the sphere.
-template <int LM>
+// touching pair, the contact law with the entry's history; then walls, sums
+// and the integration of the sphere.  AHEAD: the loads of the next entry --
+// partner state and, when its pair touched, its history -- are issued before
+// the current entry is computed (more loads in flight per thread, about 20
+// more registers); without it each entry is loaded at its turn and the
+// latency is hidden by more resident warps.  Both give the same bits.
+template <int LM, bool AHEAD = true>
 __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P, uint32_t t,
                                             uint32_t cur, uint32_t nxt, uint32_t ls)
 {
@@ -322,6 +329,29 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
     acc.es_dot = 0.f;
     acc.ev_dot = 0.f;
     acc.p = 0.f;
+    if (!AHEAD) {
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t b = lst[k];
+            const double4 xb = xr[b];
+            const float4 vb = vw[2 * b], wb = vw[2 * b + 1];
+            d3 hb = mk(0.0, 0.0, 0.0);
+            if ((live_old >> k) & 1ull) hb = mk(hist[3 * k], hist[3 * k + 1], hist[3 * k + 2]);
+            const d3 x_ab = centre_line(B, xa, xb, nullptr);
+            const double x_ab_length = len_rn<LM>(x_ab);
+            const double delta_n = __dsub_rn(x_ab_length, __dadd_rn(xa.w, xb.w));
+            if (delta_n < 0.0) {
+                const MixedPair q = mixed_pair_f(x_ab, x_ab_length, delta_n, va, vb, wa, wb, xa.w, xb.w);
+                const d3 nd = B.P.contactmodel == 2 ? contact_linear_mixed(B.P, dt, acc, q, hb)
+                                                    : contact_hertz_mixed(B.P, dt, acc, q, hb);
+                hist[3 * k] = nd.x;
+                hist[3 * k + 1] = nd.y;
+                hist[3 * k + 2] = nd.z;
+                live_new |= 1ull << k;
+            }
+        }
+        finish_sphere<LM>(A, P, B, i, nxt, ls, xa, wa, acc, live_old, live_new);
+        return;
+    }
     // entry k's partner state and history are loaded during entry k - 1,
     // entry k's partner id during entry k - 2 (the row holds VL_MAX >= 2
     // ids; those at or past n are not used)
@@ -369,13 +399,13 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
     finish_sphere<LM>(A, P, B, i, nxt, ls, xa, wa, acc, live_old, live_new);
 }
 
-template <int LM, int NT, int MINB>
+template <int LM, int NT, int MINB, bool AHEAD = true>
 __global__ void __launch_bounds__(NT, MINB) k_pair_step(StepArgs A, PairArgs P)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= A.ntot) return;
     const uint32_t cur = *P.pp;
-    pair_sphere<LM>(A, P, t, cur, cur ^ 1u, *P.lsel);
+    pair_sphere<LM, AHEAD>(A, P, t, cur, cur ^ 1u, *P.lsel);
 }
 
 // cp.async (global -> shared, issued per thread, completion per thread by
@@ -896,6 +926,8 @@ void launch_pair_lm(const StepArgs &A, const PairArgs &P, int shape, cudaStream_
     case 8: launch_staged<LM, 64, 10, 3>(A, P, st); break;
     case 9: launch_persistent<LM, 64, 8>(A, P, st); break;
     case 10: launch_persistent<LM, 128, 4>(A, P, st); break;
+    case 11: k_pair_step<LM, 64, 10, false><<<blocks_for(A.ntot, 64), 64, 0, st>>>(A, P); break;
+    case 12: k_pair_step<LM, 64, 12, false><<<blocks_for(A.ntot, 64), 64, 0, st>>>(A, P); break;
     default: k_pair_step<LM, 128, 4><<<blocks_for(A.ntot, 128), 128, 0, st>>>(A, P); break;
     }
 }
@@ -971,7 +1003,7 @@ int launch_step_pair(const StepArgs &A, const PairArgs &P, const StepConfig &cfg
     }
     mark(prof, st, "k_pair_cond");
     launch_pair_kernel(A, P, cfg, st);
-    if (cfg.pair_shape >= 9) {
+    if (pair_shape_persistent(cfg.pair_shape)) {
         // the persistent shapes do the wall stage themselves
         mark(prof, st, "k_pair_persist");
         if (launches) *launches += nl + 1;

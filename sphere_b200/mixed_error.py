@@ -9,6 +9,7 @@ while the steps run (sph_step_async_states), and at the end the porosity
 profile (sph_porosity, the reference's `porosity` program) and the
 positions are read back.
 """
+import copy
 import math
 
 import numpy
@@ -16,11 +17,13 @@ import numpy
 from .runner import Stepper
 
 
-def _run(sim, precision, nsteps, slices, device, cuda_stream, max_slices=0):
+def _run(sim, precision, nsteps, slices, device, cuda_stream, max_slices=0, variant=None):
     st = Stepper([sim], precision=precision, length="reference", device=device)
     try:
         if cuda_stream is not None:
             st.set_stream(cuda_stream)
+        if variant is not None:
+            st.set_variant(variant)
         st.upload()
         nbs = st.box_state_bytes()
         states = numpy.zeros((nsteps, nbs), dtype=numpy.uint8)
@@ -44,10 +47,25 @@ def _run(sim, precision, nsteps, slices, device, cuda_stream, max_slices=0):
             "status": int(code)}
 
 
-def compare_precisions(sim, nsteps=None, slices=50, device=-1, cuda_stream=None):
+def perturbed(sim, rel, seed=0):
+    """A copy of sim whose sphere positions are multiplied by 1 +- rel
+    (a seeded random sign per coordinate)."""
+    q = copy.deepcopy(sim)
+    x = numpy.asarray(q.x)
+    sign = numpy.random.default_rng(seed).choice([-1.0, 1.0], size=x[:, :3].shape)
+    x[:, :3] *= 1.0 + rel * sign
+    q.x = x
+    return q
+
+
+def compare_precisions(sim, nsteps=None, slices=50, device=-1, cuda_stream=None,
+                       precision="mixed", variant=None, perturb=0.0, seed=0):
     """Run `sim` (one box with a stress-controlled top wall, wmode 1) for
-    nsteps steps (default: time_total / dt) in the FP64 and FP32-mixed
-    forms and return the mixed form's differences:
+    nsteps steps (default: time_total / dt) in the FP64 form and in
+    `precision` (the FP32-mixed form by default; launch variant `variant`,
+    None for the handle's default; its start positions multiplied by
+    1 +- perturb, a seeded sign per coordinate, when perturb > 0) and
+    return the second run's differences from the first:
 
     * wall stress (wall force / x-y area): the largest difference over the
       run relative to the applied stress w_sigma0 and to the FP64 series'
@@ -63,13 +81,20 @@ def compare_precisions(sim, nsteps=None, slices=50, device=-1, cuda_stream=None)
       slabs thicker than 2 r_max allow): the largest absolute difference;
     * sphere positions at the end: the largest difference relative to the
       mean radius.
+
+    A sheared pack is chaotic: any difference, a rounding or a move of one
+    part in 1e15 of the start positions, grows until the two runs are
+    different realisations of the same flow.  precision="fp64" with
+    perturb=1e-15 measures that floor: the differences two FP64 runs
+    show for no other reason.
     """
     if int(sim.nw[0]) < 1 or int(sim.wmode[0]) != 1:
         raise ValueError("compare_precisions wants a stress-controlled top wall (wmode 1)")
     if nsteps is None:
         nsteps = int(round(float(sim.time_total[0]) / float(sim.time_dt[0])))
     d = _run(sim, "fp64", nsteps, None, device, cuda_stream, max_slices=slices)
-    m = _run(sim, "mixed", nsteps, d["slices"], device, cuda_stream)
+    second = perturbed(sim, perturb, seed) if perturb > 0.0 else sim
+    m = _run(second, precision, nsteps, d["slices"], device, cuda_stream, variant=variant)
     area = float(sim.L[0]) * float(sim.L[1])
     sigma0 = float(sim.w_sigma0[0])
     r = sim.radius
@@ -83,6 +108,7 @@ def compare_precisions(sim, nsteps=None, slices=50, device=-1, cuda_stream=None)
     return {
         "steps": nsteps,
         "spheres": int(sim.np[0]),
+        "second_run": {"precision": precision, "variant": variant, "perturb": perturb},
         "status": [d["status"], m["status"]],
         "times_equal": bool(numpy.array_equal(d["t"], m["t"])),
         "wall_stress_max_diff_over_sigma0": float(numpy.abs(sm - sd).max() / sigma0),

@@ -56,3 +56,10 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_abi, "lib_path", lambda: str(tmp_path / "absent.so"))
     with pytest.raises(RuntimeError, match="missing"):
         _abi.load_library()
+
+
+def test_header_constants_match_the_mirror():
+    text = open(os.path.join(ROOT, "include", "sphere_b200.h")).read()
+    defs = dict(re.findall(r"#define\s+(SPH_[A-Z_]+)\s+(\d+)", text))
+    assert int(defs["SPH_TUNE_VARIANTS"]) == _abi.TUNE_VARIANTS
+    assert int(defs["SPH_PAIR_SHAPES"]) == _abi.PAIR_SHAPES

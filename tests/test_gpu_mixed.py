@@ -77,20 +77,29 @@ def test_mixed_positions_after_100_steps():
 
 
 def test_mixed_wall_stress_and_porosity_over_a_long_run():
-    # a 20,000-sphere sheared dense pack (the benchmark's scene at a
-    # smaller size: 20 kPa on the top wall, top layer sheared), 2,000 steps
+    """A 20,000-sphere sheared dense pack (the benchmark's scene at a
+    smaller size: 20 kPa on the top wall, top layer sheared), 2,000 steps,
+    in the mixed form's default variant and in the list step, against the
+    FP64 form.  The flow is chaotic, so the bound is the floor two FP64
+    runs show when one starts from positions moved by one part in 1e15:
+    measured on this scene over four such moves, mean stress over the
+    second half 1.7e-5 to 8.6e-5, RMS 1.9e-3 to 2.0e-3, positions 9.0e-4 r
+    to 1.1e-3 r at the end; the mixed form within a few times that."""
     import json
     from sphere_b200 import scenes
     from sphere_b200.mixed_error import compare_precisions
     s = scenes.sheared_dense_pack(n=20000, seed=3, device=0, sweeps=1500)
-    e = compare_precisions(s, nsteps=2000, slices=20, device=0)
-    print(json.dumps(e))
-    assert e["status"] == [0, 0]
-    assert e["times_equal"]
-    # measured on this scene: mean 5.6e-6, RMS 2.0e-3, bulk porosity
-    # 1.3e-9, profile 2.8e-7, positions 8.9e-4 r
-    assert e["wall_stress_mean_rel_diff_second_half"] < 1e-4
-    assert e["wall_stress_rms_diff_over_rms"] < 2e-2
-    assert e["bulk_porosity_max_abs_diff"] < 1e-7
-    assert e["porosity_profile_max_abs_diff"] < 1e-5
-    assert e["positions_max_diff_over_rmean"] < 1e-2
+    floor = [compare_precisions(s, nsteps=2000, slices=20, device=0, precision="fp64",
+                                perturb=1e-15, seed=k) for k in (0, 1)]
+    print(json.dumps(floor))
+    top = {k: max(f[k] for f in floor) for k in floor[0] if isinstance(floor[0][k], float)}
+    for variant in (None, 4):
+        e = compare_precisions(s, nsteps=2000, slices=20, device=0, variant=variant)
+        print(json.dumps(e))
+        assert e["status"] == [0, 0]
+        assert e["times_equal"]
+        assert e["wall_stress_mean_rel_diff_second_half"] < 5e-4
+        assert e["wall_stress_rms_diff_over_rms"] < 2.0 * top["wall_stress_rms_diff_over_rms"]
+        assert e["positions_max_diff_over_rmean"] < 3.0 * top["positions_max_diff_over_rmean"]
+        assert e["bulk_porosity_max_abs_diff"] < max(1e-7, 10.0 * top["bulk_porosity_max_abs_diff"])
+        assert e["porosity_profile_max_abs_diff"] < max(1e-5, 10.0 * top["porosity_profile_max_abs_diff"])

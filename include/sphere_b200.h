@@ -435,6 +435,71 @@ int sph_struct_sizes(uint64_t *sizes);
 #define SPH_SCAN_STATIC_MAX 16777216u
 int sph_cell_offsets_static(const uint32_t *counts, uint64_t n, uint32_t *offsets, void *stream);
 
+/* Darcy flow coupling (fluid == 1, cfd_solver == 1): the Darcy struct of
+ * src/datatypes.h:157-190 without its arrays, plus the output interval.
+ * Boundary codes as the reference's: 0 fixed pressure (Dirichlet), 1 no
+ * flow (Neumann), 2 periodic, 4 prescribed flux (bot/top only). */
+typedef struct SphDarcy {
+    double mu;            /* fluid dynamic viscosity */
+    double rho_f;         /* fluid density */
+    double beta_f;        /* adiabatic fluid compressibility */
+    double k_c;           /* Kozeny-Carman permeability prefactor */
+    double c_phi;         /* porosity scaling coefficient */
+    double tolerance;     /* largest normalized residual of a converged solve */
+    double p_mod_A;       /* top pressure modulation: amplitude, */
+    double p_mod_f;       /* frequency */
+    double p_mod_phi;     /* and phase */
+    double bc_bot_flux;   /* normal flux through the bottom (bc_bot == 4) */
+    double bc_top_flux;   /* and the top (bc_top == 4) */
+    double file_dt;       /* time.file_dt: the output interval */
+    uint32_t maxiter;     /* Jacobi iterations per fluid step at most */
+    uint32_t ndem;        /* DEM steps per fluid step */
+    int32_t bc_xn, bc_xp, bc_yn, bc_yp, bc_bot, bc_top;
+    int32_t free_slip_bot, free_slip_top;   /* kept for the .bin file only */
+} SphDarcy;
+
+/* Turn the Darcy coupling on for a one-box FP64 handle and set its state.
+ * The fluid grid is the box's cell grid (nx, ny, nz = grid.num, not
+ * adaptive); p, phi, dphi and p_constant hold nx*ny*nz cells and v three
+ * doubles per cell, x fastest (the .bin fluid block order,
+ * src/file_io.cpp:347-404); f_p is [np][3] (may be NULL: zero).  Replaces
+ * initDarcyMem + initDarcyMemDev + transferDarcyToGlobalDeviceMemory and
+ * the start-of-run set-up of DEM::startTime (src/darcy.cpp:17-36,
+ * src/darcy.cuh:17-104, src/device.cu:1003-1016).  From then on every step
+ * runs the Darcy part of the step loop (src/device.cu:1891-2419) between
+ * interact and integrate: the pressure force on the spheres, and every ndem
+ * steps the porosities, permeabilities, the Jacobi solve of the pressure
+ * (on the device: no host round trip per iteration) and the velocities.
+ * The file clock and the host's copy of the top wall position that the
+ * reference keeps (refreshed at each output) are kept on the device from
+ * this call on, so that results do not depend on how the steps are split
+ * into calls.  SPH_ERR_UNSUPPORTED for more than one box, the FP32-mixed
+ * form or an adaptive grid. */
+int sph_darcy_set(SphHandle *h, const SphDarcy *d, const double *p, const double *v,
+                  const double *phi, const double *dphi, const int32_t *p_constant,
+                  const double *f_p);
+
+/* The fluid state after the steps run so far (any pointer may be NULL):
+ * p, phi, dphi, k [cells], v [cells][3], f_p [np][3].  Replaces
+ * transferDarcyFromGlobalDeviceMemory (src/darcy.cuh:106-129). */
+int sph_darcy_get(SphHandle *h, double *p, double *v, double *phi, double *dphi, double *k,
+                  double *f_p);
+
+/* The Jacobi solves since the last call, one entry per fluid step: the
+ * step (iter + 1, as the reference's conv.log writes it), the iterations
+ * run (the last nijac) and whether the solve converged.  Up to
+ * SPH_DARCY_LOG entries are kept between calls (older ones are dropped);
+ * *n receives the number written (at most cap).  The reference writes
+ * "step nijac" to output/<sid>-conv.log for converged solves at every
+ * tenth step and for every solve that did not converge
+ * (src/device.cu:2349-2370). */
+#define SPH_DARCY_LOG 4096u
+int sph_darcy_log(SphHandle *h, uint64_t *step, uint32_t *iterations, uint32_t *converged,
+                  uint32_t cap, uint32_t *n);
+
+/* sizeof(SphDarcy), for binding checks. */
+int sph_darcy_struct_size(uint64_t *size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,7 @@ import subprocess
 
 import numpy
 
-from sphere_b200._abi import NC, SphBox, box_from_sim
+from sphere_b200._abi import NC, SphBox, SphDarcy, box_from_sim, darcy_from_sim
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBS = {
@@ -28,6 +28,20 @@ ENTRY = {"oracle": "or_step", "ref": "ref_step"}
 _dp = C.POINTER(C.c_double)
 _up = C.POINTER(C.c_uint32)
 _bp = C.POINTER(C.c_uint8)
+
+
+class OrDarcy(C.Structure):
+    _fields_ = [
+        ("prm", SphDarcy),
+        ("p", _dp), ("p_old", _dp), ("p_new", _dp), ("dp_expl", _dp), ("phi", _dp),
+        ("dphi", _dp), ("norm", _dp), ("k", _dp), ("div_v_p", _dp),
+        ("v", _dp), ("vp_avg", _dp), ("grad_k", _dp), ("grad_p", _dp),
+        ("p_constant", C.POINTER(C.c_int32)),
+        ("f_p", _dp),
+        ("p_top_orig", C.c_double), ("filetimeclock", C.c_double), ("wall_w_host", C.c_double),
+        ("wall0_iz", C.c_uint32), ("log_cap", C.c_uint32), ("log_n", C.c_uint32),
+        ("log_step", C.POINTER(C.c_uint64)), ("log_iters", _up), ("log_ok", _up),
+    ]
 
 
 class OrState(C.Structure):
@@ -46,6 +60,7 @@ class OrState(C.Structure):
         ("x_sorted", _dp), ("vel_sorted", _dp), ("angvel_sorted", _dp),
         ("walls_force_pp", _dp), ("walls_force_partial", _dp),
         ("tau_eff_x_pp", _dp), ("tau_eff_x_partial", _dp),
+        ("darcy", C.POINTER(OrDarcy)),
     ]
 
 
@@ -158,12 +173,68 @@ class CpuRun(object):
         st.nthreads = int(nthreads)
         for name, _t in OrState._fields_:
             if name in ("box", "length_mode", "velocity_state", "iter", "error_flags",
-                        "nthreads", "walls_acc"):
+                        "nthreads", "walls_acc", "darcy"):
                 continue
             a = getattr(self, name)
             ct = dict(OrState._fields_)[name]
             setattr(st, name, a.ctypes.data_as(ct))
         self.state = st
+        self.darcy = None
+        if getattr(s, "fluid", False):
+            self._darcy_init(s)
+
+    # ---------------------------------------------------------- Darcy
+    _CELL1 = ("p", "p_old", "p_new", "dp_expl", "phi", "dphi", "norm", "k", "div_v_p")
+    _CELL3 = ("v", "vp_avg", "grad_k", "grad_p")
+
+    def _darcy_init(self, s, log_cap=100000):
+        """Ghost-padded fluid fields of a Darcy sim ([z+2, y+2, x+2](, 3))
+        and the start-of-run set-up (or_darcy_start)."""
+        num = [int(v) for v in s.num]
+        self.num = num
+        shape = (num[2] + 2, num[1] + 2, num[0] + 2)
+        f = {}
+        for name in self._CELL1:
+            f[name] = numpy.zeros(shape)
+        for name in self._CELL3:
+            f[name] = numpy.zeros(shape + (3,))
+        f["p_constant"] = numpy.zeros(shape, dtype=numpy.int32)
+        inner = (slice(1, -1), slice(1, -1), slice(1, -1))
+        t = lambda a: numpy.asarray(a).transpose((2, 1, 0) + tuple(range(3, numpy.ndim(a))))
+        f["p"][inner] = t(s.p_f)
+        f["v"][inner] = t(s.v_f)
+        f["phi"][inner] = t(s.phi)
+        f["dphi"][inner] = t(numpy.asarray(s.dphi, dtype=numpy.float64) * s.time_dt * s.ndem)
+        f["p_constant"][inner] = t(s.p_f_constant)
+        f["f_p"] = numpy.zeros((max(self.n, 1), 4))
+        if self.n:
+            f["f_p"][:self.n, :3] = numpy.asarray(s.f_p, dtype=numpy.float64).reshape(-1, 3)
+        f["log_step"] = numpy.zeros(log_cap, dtype=numpy.uint64)
+        f["log_iters"] = numpy.zeros(log_cap, dtype=numpy.uint32)
+        f["log_ok"] = numpy.zeros(log_cap, dtype=numpy.uint32)
+        d = OrDarcy()
+        d.prm = darcy_from_sim(s)
+        for name, ct in OrDarcy._fields_:
+            if name in f:
+                setattr(d, name, f[name].ctypes.data_as(ct))
+        d.log_cap = log_cap
+        self.fluid = f
+        self.darcy = d
+        self.state.darcy = C.pointer(d)
+        lib = C.CDLL(LIBS["oracle"])
+        lib.or_darcy_start.argtypes = [C.POINTER(OrState)]
+        lib.or_darcy_start(C.byref(self.state))
+
+    def fluid_cells(self, name):
+        """A fluid field without its ghost layer, in the sim's [x, y, z](, 3)
+        layout."""
+        a = self.fluid[name][1:-1, 1:-1, 1:-1]
+        return numpy.ascontiguousarray(a.transpose((2, 1, 0) + tuple(range(3, a.ndim))))
+
+    def darcy_log(self):
+        n = int(self.darcy.log_n)
+        return (self.fluid["log_step"][:n].copy(), self.fluid["log_iters"][:n].copy(),
+                self.fluid["log_ok"][:n].copy())
 
     def step(self, nsteps=1):
         """Run nsteps steps; returns the accumulated error-flag bits."""

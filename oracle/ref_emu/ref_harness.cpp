@@ -36,6 +36,9 @@
 #include "cohesion.cuh"
 #include "contactsearch.cuh"
 #include "integration.cuh"
+/* the reference's Darcy kernels (src/darcy.cuh) and the helpers they take
+ * from src/navierstokes.cuh, extracted by oracle/Makefile */
+#include "darcy_kernels.inc"
 
 #include <ucontext.h>
 #include <algorithm>
@@ -127,6 +130,152 @@ static void launch_fibers(unsigned grid, unsigned block, const std::function<voi
 }
 
 static inline Float4 *F4(double *p) { return reinterpret_cast<Float4 *>(p); }
+/* src/darcy.cpp:64-76 DEM::d_idx */
+static inline unsigned d_idx_host(unsigned nx, unsigned ny, int x, int y, int z)
+{
+    return (x + 1) + (nx + 2) * (y + 1) + (nx + 2) * (ny + 2) * (z + 1);
+}
+static inline Float3 *F3(double *p) { return reinterpret_cast<Float3 *>(p); }
+
+/* 3-D launch on the fluid grid (src/device.cu:865-869: 8 x 8 x 8 threads
+ * per block, blocks covering grid.num), blocks and threads in order.  None
+ * of the Darcy kernels reads what another thread of the same launch
+ * writes, so the order is immaterial. */
+static void launch_fluid(const std::function<void()> &body)
+{
+    const unsigned gx = (devC_grid.num[0] + 7) / 8, gy = (devC_grid.num[1] + 7) / 8;
+    const unsigned gz = (devC_grid.num[2] + 7) / 8;
+    gridDim = dim3(gx, gy, gz);
+    blockDim = dim3(8, 8, 8);
+    for (unsigned bz = 0; bz < gz; ++bz)
+        for (unsigned by = 0; by < gy; ++by)
+            for (unsigned bx = 0; bx < gx; ++bx) {
+                blockIdx = make_uint3(bx, by, bz);
+                for (unsigned tz = 0; tz < 8; ++tz)
+                    for (unsigned ty = 0; ty < 8; ++ty)
+                        for (unsigned tx = 0; tx < 8; ++tx) {
+                            threadIdx = make_uint3(tx, ty, tz);
+                            body();
+                        }
+            }
+}
+
+/* The Darcy part of the step loop, src/device.cu:1891-2419, with the
+ * host's residual check (src/darcy.cpp:266-293, every nijacnorm = 10
+ * iterations, src/debug.h:16) and conv.log bookkeeping as entries of the
+ * state's log; a NaN residual raises SPH_ERR_NAN instead of exit(1). */
+static void ref_darcy(OrState *s, unsigned iter, unsigned blocksPerGrid, unsigned threadsPerBlock,
+                      Float4 *dev_x, Float4 *dev_x_sorted, Float4 *dev_vel_sorted, Float4 *dev_force)
+{
+    OrDarcy *D = s->darcy;
+    const SphDarcy &d = D->prm;
+    const unsigned np = s->box.np;
+    const unsigned nx = devC_grid.num[0], ny = devC_grid.num[1], nz = devC_grid.num[2];
+    if (s->box.walls.nw > 0 && (s->box.walls.wmode[0] == 1 || s->box.walls.wmode[0] == 3))
+        D->wall0_iz = D->wall_w_host / (devC_grid.L[2] / devC_grid.num[2]);
+    const unsigned wall0_iz = D->wall0_iz;
+    Float *p = D->p, *p_old = D->p_old, *p_new = D->p_new, *dp_expl = D->dp_expl;
+    Float *phi = D->phi, *dphi = D->dphi, *norm = D->norm, *k = D->k, *div_v_p = D->div_v_p;
+    Float3 *v = F3(D->v), *vp_avg = F3(D->vp_avg), *grad_k = F3(D->grad_k), *grad_p = F3(D->grad_p);
+    int *p_constant = D->p_constant;
+    if (np > 0) {
+        launch_fluid([&] { setDarcyGhostNodes<Float>(p, d.bc_xn, d.bc_xp, d.bc_yn, d.bc_yp, d.bc_bot, d.bc_top); });
+        launch_fluid([&] { findDarcyPressureGradient(p, grad_p); });
+        launch_fluid([&] { setDarcyGhostNodes<Float3>(grad_p, d.bc_xn, d.bc_xp, d.bc_yn, d.bc_yp, d.bc_bot, d.bc_top); });
+        launch_seq(blocksPerGrid, threadsPerBlock,
+                   [&] {
+                       findDarcyPressureForceLinear(dev_x, grad_p, phi, wall0_iz, d.rho_f, d.bc_top,
+                                                    dev_force, F4(D->f_p));
+                   },
+                   false);
+    }
+    if ((iter % d.ndem) != 0) return;
+    launch_fluid([&] {
+        findDarcyPorositiesLinear(s->cell_start, s->cell_end, dev_x_sorted, dev_vel_sorted, iter,
+                                  d.ndem, np, d.c_phi, phi, dphi, div_v_p, vp_avg);
+    });
+    if (devC_grid.periodic == 2) {
+        launch_fluid([&] { copyDarcyPorositiesToEdges(phi, dphi, div_v_p, vp_avg); });
+        launch_fluid([&] { copyDarcyPorositiesToBottom(phi, dphi, div_v_p, vp_avg); });
+    }
+    if ((d.p_mod_A > 1.0e-5 || d.p_mod_A < -1.0e-5) && d.p_mod_f > 1.0e-7) {
+        const Float new_pressure =
+            D->p_top_orig + d.p_mod_A * sin(2.0 * M_PI * d.p_mod_f * s->box.t_current + d.p_mod_phi);
+        /* the launch grid's threads past nx or ny write too; keep those
+         * writes inside the array */
+        std::vector<Float> pad((size_t)(nx + 2) * (ny + 2) * (nz + 2) + 16 * (nx + ny + 64), 0.0);
+        std::memcpy(pad.data(), p, sizeof(Float) * (size_t)(nx + 2) * (ny + 2) * (nz + 2));
+        launch_fluid([&] { setDarcyTopPressure(new_pressure, pad.data(), wall0_iz); });
+        std::memcpy(p, pad.data(), sizeof(Float) * (size_t)(nx + 2) * (ny + 2) * (nz + 2));
+        launch_fluid([&] { setDarcyTopWallPressure(new_pressure, wall0_iz, p); });
+    }
+    launch_fluid([&] { findDarcyPermeabilities(d.k_c, phi, k); });
+    launch_fluid([&] { setDarcyGhostNodes<Float>(phi, d.bc_xn, d.bc_xp, d.bc_yn, d.bc_yp, d.bc_bot, d.bc_top); });
+    launch_fluid([&] { setDarcyGhostNodes<Float>(k, d.bc_xn, d.bc_xp, d.bc_yn, d.bc_yp, d.bc_bot, d.bc_top); });
+    launch_fluid([&] { findDarcyPermeabilityGradients(k, grad_k); });
+    if (iter == 0) {
+        launch_fluid([&] { setDarcyNormZero(norm); });
+        launch_fluid([&] { copyValues<Float>(p, p_old); });
+    }
+    if (d.bc_bot == 4 || d.bc_top == 4)
+        launch_fluid([&] { setDarcyGhostNodesFlux<Float>(p, d.bc_bot, d.bc_top, d.bc_bot_flux, d.bc_top_flux, k, d.mu); });
+    unsigned nijac = 0, ok = 0;
+    for (nijac = 0; nijac < d.maxiter; ++nijac) {
+        if (nijac == 0) launch_fluid([&] { copyValues<Float>(p, p_old); });
+        launch_fluid([&] { setDarcyGhostNodes<Float>(p, d.bc_xn, d.bc_xp, d.bc_yn, d.bc_yp, d.bc_bot, d.bc_top); });
+        if (nijac == 0)
+            launch_fluid([&] {
+                firstDarcySolution(p, k, phi, dphi, div_v_p, vp_avg, grad_k, d.beta_f, d.mu, d.bc_xn,
+                                   d.bc_xp, d.bc_yn, d.bc_yp, d.bc_bot, d.bc_top, d.ndem, wall0_iz,
+                                   p_constant, dp_expl);
+            });
+        launch_fluid([&] {
+            updateDarcySolution(p_old, dp_expl, p, k, phi, dphi, div_v_p, vp_avg, grad_k, d.beta_f, d.mu,
+                                d.bc_xn, d.bc_xp, d.bc_yn, d.bc_yp, d.bc_bot, d.bc_top, d.ndem, wall0_iz,
+                                p_constant, p_new, norm);
+        });
+        if (d.bc_top == 1) {
+            /* a wall at or above the top of the grid indexes past the padded
+             * array: the kernel runs on a copy with room to spare, whose
+             * part past the array is dropped (reads there see zeros) */
+            const size_t nc = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+            std::vector<Float> pad(nc + (size_t)(nx + 2) * (ny + 2) * 16, 0.0);
+            std::memcpy(pad.data(), p, sizeof(Float) * nc);
+            launch_fluid([&] { setDarcyTopWallFixedFlow(wall0_iz, pad.data()); });
+            std::memcpy(p, pad.data(), sizeof(Float) * nc);
+        }
+        if (d.bc_bot == 4 || d.bc_top == 4)
+            launch_fluid([&] { setDarcyGhostNodesFlux<Float>(p, d.bc_bot, d.bc_top, d.bc_bot_flux, d.bc_top_flux, k, d.mu); });
+        launch_fluid([&] { copyValues<Float>(p_new, p); });
+        if (nijac % 10 == 0) {
+            double max_norm_res = -1.0e9;
+            bool nan = false;
+            for (unsigned z = 0; z < nz && !nan; ++z)
+                for (unsigned y = 0; y < ny && !nan; ++y)
+                    for (unsigned x = 0; x < nx; ++x) {
+                        const double r = fabs(norm[d_idx_host(nx, ny, x, y, z)]);
+                        if (r != r) { nan = true; break; }
+                        if (r > max_norm_res) max_norm_res = r;
+                    }
+            if (nan) {
+                s->error_flags |= 1 << SPH_ERR_NAN;
+                break;
+            }
+            if (max_norm_res <= d.tolerance) { ok = 1; break; }
+        }
+        if (nijac == d.maxiter - 1) break;
+    }
+    if (D->log_n < D->log_cap) {
+        D->log_step[D->log_n] = (uint64_t)iter + 1;
+        D->log_iters[D->log_n] = nijac;
+        D->log_ok[D->log_n] = ok;
+        D->log_n++;
+    }
+    if (D->filetimeclock + s->box.dt < d.file_dt)
+        launch_fluid([&] { setDarcyZeros<Float>(dphi); });
+    launch_fluid([&] { setDarcyGhostNodes<Float>(p, d.bc_xn, d.bc_xp, d.bc_yn, d.bc_yp, d.bc_bot, d.bc_top); });
+    launch_fluid([&] { findDarcyVelocities(p, phi, k, d.mu, v); });
+}
 
 extern "C" int ref_step(OrState *s, uint64_t nsteps)
 {
@@ -262,6 +411,10 @@ extern "C" int ref_step(OrState *s, uint64_t nsteps)
                            },
                            false);
         }
+        /* device.cu:1891-2419 */
+        if (s->darcy)
+            ref_darcy(s, iter, blocksPerGrid, threadsPerBlock, dev_x, dev_x_sorted, dev_vel_sorted,
+                      dev_force);
         if (np > 0) {
             /* device.cu:2427-2452 */
             if (nw > 0 && w_mode[0] == 3) {
@@ -310,6 +463,15 @@ extern "C" int ref_step(OrState *s, uint64_t nsteps)
         }
         /* device.cu:2536-2538 */
         s->box.t_current += s->box.dt;
+        /* device.cu:2537, 2569, 2672: the file clock; the output's transfer
+         * (device.cu:805) refreshes the host copy of the walls */
+        if (s->darcy) {
+            s->darcy->filetimeclock += s->box.dt;
+            if (s->darcy->filetimeclock >= s->darcy->prm.file_dt) {
+                s->darcy->filetimeclock = 0.0;
+                if (nw > 0) s->darcy->wall_w_host = w_nx[0].w;
+            }
+        }
         s->iter++;
     }
     s->velocity_state = velocity_state;

@@ -45,6 +45,8 @@
 
 #define NC SPH_NC
 static const double PI = 3.14159265358979; /* src/constants.h:15 */
+/* M_PI of the C library, which src/darcy.cuh uses */
+static const double OR_DARCY_PI = 3.14159265358979323846;
 
 typedef struct { double x, y, z; } v3;
 static inline v3 mk(double x, double y, double z) { v3 r; r.x = x; r.y = y; r.z = z; return r; }
@@ -762,6 +764,576 @@ static void integrate_walls(const Ctx *c, OrState *s, double t_current)
     }
 }
 
+/* ------------------------------------------------------------------ Darcy */
+
+/* The Darcy coupling (fluid == 1, cfd_solver == 1), src/darcy.cuh and the
+ * Darcy part of the step loop, src/device.cu:1891-2419.  Each function is
+ * one kernel, run over the cells (or spheres) in launch order; none reads a
+ * value that another thread of the same launch writes, except where
+ * noted, so the order of the threads does not matter. */
+
+typedef struct {
+    OrDarcy *d;
+    const SphDarcy *P;
+    int nx, ny, nz;
+    double dx, dy, dz;
+} Dc;
+
+static void ctx_init(Ctx *c, OrState *s);
+
+/* darcy.cuh:146-157 d_idx (navierstokes.cuh:231-240 idx is the same) */
+static inline uint32_t d_idx(const Dc *c, int x, int y, int z)
+{
+    return (uint32_t)(x + 1) + (uint32_t)(c->nx + 2) * (uint32_t)(y + 1) +
+           (uint32_t)(c->nx + 2) * (uint32_t)(c->ny + 2) * (uint32_t)(z + 1);
+}
+
+/* darcy.cuh:346-349 sphereVolume: 4/3 pi r^3 with the C library's M_PI */
+static inline double sphere_volume(double r) { return 4.0 / 3.0 * OR_DARCY_PI * pow(r, 3); }
+
+/* darcy.cuh:356-385 weight / weightDist of the vector between the points */
+static inline double weight_dist(v3 x, double dx, double dy, double dz)
+{
+    const v3 dist = mk(fabs(x.x), fabs(x.y), fabs(x.z));
+    if (dist.x < dx && dist.y < dy && dist.z < dz)
+        return (1.0 - dist.x / dx) * (1.0 - dist.y / dy) * (1.0 - dist.z / dz);
+    return 0.0;
+}
+
+/* darcy.cuh:212-285 setDarcyGhostNodes (m doubles per cell) */
+static void darcy_ghost(const Dc *c, double *f, int m)
+{
+    const SphDarcy *P = c->P;
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                double val[3];
+                memcpy(val, f + (size_t)m * d_idx(c, x, y, z), sizeof(double) * m);
+#define PUT(X, Y, Z) memcpy(f + (size_t)m * d_idx(c, X, Y, Z), val, sizeof(double) * m)
+                if (x == 0 && P->bc_xn == 0) PUT(-1, y, z);
+                if (x == 1 && P->bc_xn == 1) PUT(-1, y, z);
+                if (x == 0 && P->bc_xn == 2) PUT(nx, y, z);
+                if (x == nx - 1 && P->bc_xp == 0) PUT(nx, y, z);
+                if (x == nx - 2 && P->bc_xp == 1) PUT(nx, y, z);
+                if (x == nx - 1 && P->bc_xp == 2) PUT(-1, y, z);
+                if (y == 0 && P->bc_yn == 0) PUT(x, -1, z);
+                if (y == 1 && P->bc_yn == 1) PUT(x, -1, z);
+                if (y == 0 && P->bc_yn == 2) PUT(x, ny, z);
+                if (y == ny - 1 && P->bc_yp == 0) PUT(x, ny, z);
+                if (y == ny - 2 && P->bc_yp == 1) PUT(x, ny, z);
+                if (y == ny - 1 && P->bc_yp == 2) PUT(x, -1, z);
+                if (z == 0 && P->bc_bot == 0) PUT(x, y, -1);
+                if (z == 1 && P->bc_bot == 1) PUT(x, y, -1);
+                if (z == 0 && P->bc_bot == 2) PUT(x, y, nz);
+                if (z == nz - 1 && P->bc_top == 0) PUT(x, y, nz);
+                if (z == nz - 2 && P->bc_top == 1) PUT(x, y, nz);
+                if (z == nz - 1 && P->bc_top == 2) PUT(x, y, -1);
+#undef PUT
+            }
+}
+
+/* darcy.cuh:288-329 setDarcyGhostNodesFlux */
+static void darcy_ghost_flux(const Dc *c, double *f, const double *k, double L2)
+{
+    const SphDarcy *P = c->P;
+    if (!(P->bc_bot == 4 || P->bc_top == 4)) return;
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const double p = f[d_idx(c, x, y, z)];
+                const double kk = k[d_idx(c, x, y, z)];
+                const double dz = L2 / nz;
+                double q_z = 0.;
+                if (z == 0) q_z = P->bc_bot_flux;
+                else if (z == nz - 1) q_z = P->bc_top_flux;
+                const double p_ghost = -P->mu / kk * q_z * dz + p;
+                if (z == 0 && P->bc_bot == 4) f[d_idx(c, x, y, -1)] = p_ghost;
+                if (z == nz - 1 && P->bc_top == 4) f[d_idx(c, x, y, nz)] = p_ghost;
+            }
+}
+
+/* darcy.cuh:1101-1157 findDarcyPressureGradient (also
+ * findDarcyPermeabilityGradients, :1535-1593: the same central difference) */
+static void darcy_gradient(const Dc *c, const double *f, double *g)
+{
+    for (int z = 0; z < c->nz; ++z)
+        for (int y = 0; y < c->ny; ++y)
+            for (int x = 0; x < c->nx; ++x) {
+                const double xn = f[d_idx(c, x - 1, y, z)], xp = f[d_idx(c, x + 1, y, z)];
+                const double yn = f[d_idx(c, x, y - 1, z)], yp = f[d_idx(c, x, y + 1, z)];
+                const double zn = f[d_idx(c, x, y, z - 1)], zp = f[d_idx(c, x, y, z + 1)];
+                double *o = g + 3 * (size_t)d_idx(c, x, y, z);
+                o[0] = (xp - xn) / (c->dx + c->dx);
+                o[1] = (yp - yn) / (c->dy + c->dy);
+                o[2] = (zp - zn) / (c->dz + c->dz);
+            }
+}
+
+/* darcy.cuh:1160-1318 findDarcyPressureForceLinear, per sphere (original
+ * order): the pressure gradient interpolated from the 27 cells around the
+ * sphere's cell, times the sphere volume, plus buoyancy; added to the
+ * sphere's force.  The index sums are unsigned as in the reference (a
+ * sphere in the bottom layer compares 0xffffffff with wall0_iz - 1). */
+static void darcy_force(const Ctx *c, const Dc *dc, OrState *s)
+{
+    const OrDarcy *D = dc->d;
+    const SphDarcy *P = dc->P;
+    const uint32_t nx = c->num[0], ny = c->num[1], nz = c->num[2];
+    for (unsigned i = 0; i < c->np; ++i) {
+        const double *x = s->x + 4 * (size_t)i;
+        const v3 x3 = mk(x[0], x[1], x[2]);
+        const uint32_t i_x = (uint32_t)floor((x[0] - c->origo[0]) / (c->L[0] / c->num[0]));
+        const uint32_t i_y = (uint32_t)floor((x[1] - c->origo[1]) / (c->L[1] / c->num[1]));
+        const uint32_t i_z = (uint32_t)floor((x[2] - c->origo[2]) / (c->L[2] / c->num[2]));
+        if (!(x[0] >= c->origo[0] && x[1] >= c->origo[1] && x[2] >= c->origo[2]) || i_x >= nx ||
+            i_y >= ny || i_z >= nz) {
+            /* outside the grid (the reference reads past its arrays): no
+             * pressure force */
+            FLAG(s, SPH_ERR_OUT_OF_GRID);
+            memset(D->f_p + 4 * (size_t)i, 0, 32);
+            continue;
+        }
+        const double dx = c->L[0] / nx, dy = c->L[1] / ny, dz = c->L[2] / nz;
+        const v3 X = mk(i_x * dx + 0.5 * dx, i_y * dy + 0.5 * dy, i_z * dz + 0.5 * dz);
+        v3 grad_p = mk(0., 0., 0.);
+        for (int d_iz = -1; d_iz < 2; d_iz++)
+            for (int d_iy = -1; d_iy < 2; d_iy++)
+                for (int d_ix = -1; d_ix < 2; d_ix++) {
+                    const int ix_n = (int)(i_x + (uint32_t)d_ix);
+                    const int iy_n = (int)(i_y + (uint32_t)d_iy);
+                    const int iz_n = (int)(i_z + (uint32_t)d_iz);
+                    v3 gpi = ld3(D->grad_p + 3 * (size_t)d_idx(dc, ix_n, iy_n, iz_n));
+                    if ((ix_n == -1 && iy_n == -1) || (ix_n == -1 && iz_n == -1) ||
+                        (iy_n == -1 && iz_n == -1) || (ix_n == (int)nx && iy_n == (int)ny) ||
+                        (ix_n == (int)nx && iz_n == (int)nz) ||
+                        (iy_n == (int)ny && iz_n == (int)nz) ||
+                        (ix_n == (int)nx && iy_n == -1) || (ix_n == (int)nx && iz_n == -1) ||
+                        (iy_n == (int)ny && ix_n == -1) || (iy_n == (int)ny && iz_n == -1) ||
+                        (iz_n == (int)nz && ix_n == -1) || (iz_n == (int)nz && iy_n == -1))
+                        gpi = mk(0., 0., 0.);
+                    if (P->bc_top == 0 && i_z + (uint32_t)d_iz >= D->wall0_iz - 1u) gpi.z = 0.0;
+                    const v3 n = mk(dx * d_ix, dy * d_iy, dz * d_iz);
+                    const double w = weight_dist(vsub(x3, vadd(X, n)), dx, dy, dz);
+                    grad_p = vadd(grad_p, smul(w, gpi));
+                }
+        const double v = sphere_volume(x[3]);
+        const SphParams *Pm = c->P;
+        v3 f_p = vsub(muls(smul(-1.0, grad_p), v),
+                      smul(P->rho_f * v, mk(Pm->g[0], Pm->g[1], Pm->g[2])));
+        if (P->bc_top == 0 && i_z >= D->wall0_iz) f_p.z = 0.0;
+        double *F = s->force + 4 * (size_t)i;
+        F[0] += f_p.x;
+        F[1] += f_p.y;
+        F[2] += f_p.z;
+        F[3] += 0.0;
+        double *o = D->f_p + 4 * (size_t)i;
+        o[0] = f_p.x;
+        o[1] = f_p.y;
+        o[2] = f_p.z;
+        o[3] = 0.0;
+    }
+}
+
+/* darcy.cuh:392-730 findDarcyPorositiesLinear: per cell, the solid volume
+ * of the spheres in the 27 cells around it weighted by the trilinear hat
+ * centred on the cell, now and after an Euler step of the positions; the
+ * sphere-weighted mean sphere velocity.  Spheres in sorted order. */
+static void darcy_porosities(const Ctx *c, const Dc *dc, OrState *s, uint64_t iteration)
+{
+    OrDarcy *D = dc->d;
+    const double c_phi = dc->P->c_phi;
+    const int nx = dc->nx, ny = dc->ny, nz = dc->nz;
+    const double dx = dc->dx, dy = dc->dy, dz = dc->dz;
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const uint32_t cellidx = d_idx(dc, x, y, z);
+                if (c->np == 0) {
+                    D->phi[cellidx] = 0.9;
+                    D->dphi[cellidx] = 0.0;
+                    continue;
+                }
+                double solid_volume = 0.0, solid_volume_new = 0.0;
+                const v3 X = mk(x * dx + 0.5 * dx, y * dy + 0.5 * dy, z * dz + 0.5 * dz);
+                v3 vp_avg_num = mk(0.0, 0.0, 0.0);
+                double vp_avg_denum = 0.0;
+                const double phi_0 = D->phi[cellidx];
+                for (int z_dim = -1; z_dim < 2; ++z_dim)
+                    for (int y_dim = -1; y_dim < 2; ++y_dim)
+                        for (int x_dim = -1; x_dim < 2; ++x_dim) {
+                            int t[3] = {x + x_dim, y + y_dim, z + z_dim};
+                            if (t[2] == -1) t[2] = 1;
+                            if (c->periodic == 2) {
+                                if (t[1] == -1) t[1] = 1;
+                                if (t[1] == (int)c->num[1]) t[1] = (int)c->num[1] - 2;
+                            }
+                            v3 distmod = mk(0.0, 0.0, 0.0);
+                            if (find_dist_mod(c, t, &distmod) == -1) continue;
+                            const uint32_t cellID = (uint32_t)t[0] + (uint32_t)t[1] * c->num[0] +
+                                                    (c->num[0] * c->num[1]) * (uint32_t)t[2];
+                            const uint32_t start = s->cell_start[cellID];
+                            if (start == 0xffffffffu) continue;
+                            const uint32_t end = s->cell_end[cellID];
+                            for (uint32_t i = start; i < end; ++i) {
+                                double xr[4], vv[4];
+                                memcpy(xr, s->x_sorted + 4 * (size_t)i, 32);
+                                memcpy(vv, s->vel_sorted + 4 * (size_t)i, 32);
+                                v3 dist = mk(X.x - xr[0], X.y - xr[1], X.z - xr[2]);
+                                dist = vadd(dist, distmod);
+                                const double sw = weight_dist(dist, dx, dy, dz);
+                                const double vol_p = sphere_volume(xr[3]);
+                                solid_volume += sw * vol_p;
+                                vp_avg_num = vadd(vp_avg_num, smul(sw * vol_p, mk(vv[0], vv[1], vv[2])));
+                                vp_avg_denum += sw * vol_p;
+                                for (int q = 0; q < 4; ++q) xr[q] += vv[q] * c->dt;
+                                dist = vadd(mk(X.x - xr[0], X.y - xr[1], X.z - xr[2]), distmod);
+                                solid_volume_new += weight_dist(dist, dx, dy, dz) * vol_p;
+                            }
+                        }
+                double cell_volume = dx * dy * dz;
+                if (z == nz - 1) cell_volume *= 0.875;
+                const double phi = fmin(0.9, fmax(0.1, 1.0 - solid_volume / cell_volume));
+                const double phi_new = fmin(0.9, fmax(0.1, 1.0 - solid_volume_new / cell_volume));
+                double dphi;
+                v3 vp_avg;
+                if (iteration == 0) {
+                    dphi = 0.0;
+                    vp_avg = mk(0.0, 0.0, 0.0);
+                } else {
+                    dphi = 0.5 * (phi_new - phi_0);
+                    vp_avg = divs(vp_avg_num, fmax(1.0e-16, vp_avg_denum));
+                }
+                D->phi[cellidx] = phi * c_phi;
+                D->dphi[cellidx] = dphi * c_phi;
+                D->vp_avg[3 * (size_t)cellidx] = vp_avg.x;
+                D->vp_avg[3 * (size_t)cellidx + 1] = vp_avg.y;
+                D->vp_avg[3 * (size_t)cellidx + 2] = vp_avg.z;
+            }
+}
+
+/* darcy.cuh:733-807 copyDarcyPorositiesToEdges / ToBottom (periodic == 2):
+ * phi, dphi, div_v_p and vp_avg of the y edge layers from the layer inside
+ * them, then of the bottom layer from the layer above it */
+static void darcy_copy_cell(const Dc *dc, uint32_t w, uint32_t r)
+{
+    OrDarcy *D = dc->d;
+    D->phi[w] = D->phi[r];
+    D->dphi[w] = D->dphi[r];
+    D->div_v_p[w] = D->div_v_p[r];
+    memcpy(D->vp_avg + 3 * (size_t)w, D->vp_avg + 3 * (size_t)r, 24);
+}
+
+static void darcy_copy_edges(const Dc *dc)
+{
+    for (int z = 0; z < dc->nz; ++z)
+        for (int y = 0; y < dc->ny; ++y)
+            for (int x = 0; x < dc->nx; ++x) {
+                if (!(y == 0 || y == dc->ny - 1)) continue;
+                int y_read = 0;
+                if (y == 0) y_read = 1;
+                if (y == dc->ny - 1) y_read = dc->ny - 2;
+                darcy_copy_cell(dc, d_idx(dc, x, y, z), d_idx(dc, x, y_read, z));
+            }
+}
+
+static void darcy_copy_bottom(const Dc *dc)
+{
+    for (int y = 0; y < dc->ny; ++y)
+        for (int x = 0; x < dc->nx; ++x) darcy_copy_cell(dc, d_idx(dc, x, y, 0), d_idx(dc, x, y, 1));
+}
+
+/* darcy.cuh:1414-1435 setDarcyTopPressure: the condition reads
+ * (x < nx && y < ny && z == nz - 1) || z == wall0_iz, so at z == wall0_iz
+ * every thread of the launch grid (8 x 8 x 8 blocks covering the cells,
+ * src/device.cu:865-869) writes, also those past nx or ny (their index
+ * lands in other cells of the padded array); then :1438-1459
+ * setDarcyTopWallPressure at z == wall0_iz */
+static void darcy_top_pressure(const Dc *dc, double new_pressure)
+{
+    OrDarcy *D = dc->d;
+    const int gx = (dc->nx + 7) / 8 * 8, gy = (dc->ny + 7) / 8 * 8, gz = (dc->nz + 7) / 8 * 8;
+    const uint64_t ncell = (uint64_t)(dc->nx + 2) * (dc->ny + 2) * (dc->nz + 2);
+    for (int z = 0; z < gz; ++z)
+        for (int y = 0; y < gy; ++y)
+            for (int x = 0; x < gx; ++x) {
+                if ((x < dc->nx && y < dc->ny && z == dc->nz - 1) || (uint32_t)z == D->wall0_iz) {
+                    const uint32_t k = d_idx(dc, x, y, z);
+                    if (k < ncell) D->p[k] = new_pressure;
+                }
+            }
+    for (int z = 0; z < gz; ++z)
+        for (int y = 0; y < dc->ny; ++y)
+            for (int x = 0; x < dc->nx; ++x)
+                if ((uint32_t)z == D->wall0_iz) D->p[d_idx(dc, x, y, z)] = new_pressure;
+}
+
+/* darcy.cuh:1462-1482 setDarcyTopWallFixedFlow: p at z = wall0_iz + 1 from
+ * z = wall0_iz - 1 */
+static void darcy_top_fixed_flow(const Dc *dc)
+{
+    OrDarcy *D = dc->d;
+    const int gz = (dc->nz + 7) / 8 * 8;
+    const uint64_t ncell = (uint64_t)(dc->nx + 2) * (dc->ny + 2) * (dc->nz + 2);
+    for (int z = 0; z < gz; ++z)
+        for (int y = 0; y < dc->ny; ++y)
+            for (int x = 0; x < dc->nx; ++x)
+                if ((uint32_t)z == D->wall0_iz + 1u) {
+                    /* cells past the padded array (a wall at or above the
+                     * top of the grid) are skipped */
+                    const uint32_t w = d_idx(dc, x, y, z), r = d_idx(dc, x, y, z - 2);
+                    if (w < ncell && r < ncell) D->p[w] = D->p[r];
+                }
+}
+
+/* darcy.cuh:1485-1532 findDarcyPermeabilities (Kozeny-Carman, capped) */
+static void darcy_permeabilities(const Dc *dc)
+{
+    OrDarcy *D = dc->d;
+    for (int z = 0; z < dc->nz; ++z)
+        for (int y = 0; y < dc->ny; ++y)
+            for (int x = 0; x < dc->nx; ++x) {
+                const uint32_t ci = d_idx(dc, x, y, z);
+                double phi = D->phi[ci];
+                if (phi > 0.9999) phi = 0.9999;
+                double k = dc->P->k_c * pow(phi, 3) / pow(1.0 - phi, 2);
+                k = fmin(2.7e-10, k);
+                D->k[ci] = k;
+            }
+}
+
+/* darcy.cuh:1644-1923 firstDarcySolution (explicit) and :1926-2226
+ * updateDarcySolution (the Jacobi update): the pressure change of the
+ * diffusion term (harmonic means of k across faces) and of the porosity
+ * forcing, zero at Dirichlet boundaries (the +y test compares y with
+ * nx - 1, as written) and in cells of constant pressure */
+static double darcy_dp(const Dc *dc, const Ctx *c, int x, int y, int z, const double *pf)
+{
+    const OrDarcy *D = dc->d;
+    const SphDarcy *P = dc->P;
+    const int nx = dc->nx, ny = dc->ny, nz = dc->nz;
+    const double dx = dc->dx, dy = dc->dy, dz = dc->dz;
+    const uint32_t ci = d_idx(dc, x, y, z);
+    const double phi_xn = D->phi[d_idx(dc, x - 1, y, z)], phi = D->phi[ci];
+    const double phi_xp = D->phi[d_idx(dc, x + 1, y, z)];
+    const double phi_yn = D->phi[d_idx(dc, x, y - 1, z)], phi_yp = D->phi[d_idx(dc, x, y + 1, z)];
+    const double phi_zn = D->phi[d_idx(dc, x, y, z - 1)], phi_zp = D->phi[d_idx(dc, x, y, z + 1)];
+    const double dphi = D->dphi[ci];
+    const v3 vp_avg = ld3(D->vp_avg + 3 * (size_t)ci);
+    const int p_constant = D->p_constant[ci];
+    double p_xn = pf[d_idx(dc, x - 1, y, z)];
+    const double p = pf[ci];
+    double p_xp = pf[d_idx(dc, x + 1, y, z)];
+    double p_yn = pf[d_idx(dc, x, y - 1, z)], p_yp = pf[d_idx(dc, x, y + 1, z)];
+    double p_zn = pf[d_idx(dc, x, y, z - 1)], p_zp = pf[d_idx(dc, x, y, z + 1)];
+    const double k_xn = D->k[d_idx(dc, x - 1, y, z)], k = D->k[ci];
+    const double k_xp = D->k[d_idx(dc, x + 1, y, z)];
+    const double k_yn = D->k[d_idx(dc, x, y - 1, z)], k_yp = D->k[d_idx(dc, x, y + 1, z)];
+    const double k_zn = D->k[d_idx(dc, x, y, z - 1)], k_zp = D->k[d_idx(dc, x, y, z + 1)];
+    if (x == 0 && P->bc_xn == 1) p_xn = p;
+    if (x == nx - 1 && P->bc_xp == 1) p_xp = p;
+    if (y == 0 && P->bc_yn == 1) p_yn = p;
+    if (y == ny - 1 && P->bc_yp == 1) p_yp = p;
+    if (z == 0 && P->bc_bot == 1) p_zn = p;
+    if (z == nz - 1 && P->bc_top == 1) p_zp = p;
+    const v3 grad_phi = mk((phi_xp - phi_xn) / (dx + dx), (phi_yp - phi_yn) / (dy + dy),
+                           (phi_zp - phi_zn) / (dz + dz));
+    const double div_k_grad_p =
+        (2. * k_xp * k / (k_xp + k) * (p_xp - p) / dx - 2. * k_xn * k / (k_xn + k) * (p - p_xn) / dx) / dx +
+        (2. * k_yp * k / (k_yp + k) * (p_yp - p) / dy - 2. * k_yn * k / (k_yn + k) * (p - p_yn) / dy) / dy +
+        (2. * k_zp * k / (k_zp + k) * (p_zp - p) / dz - 2. * k_zn * k / (k_zn + k) * (p - p_zn) / dz) / dz;
+    const double ndt = P->ndem * c->dt;
+    double dp = ndt / (P->beta_f * phi * P->mu) * div_k_grad_p -
+                (ndt / (P->beta_f * phi * (1.0 - phi))) * (dphi / ndt + dot(vp_avg, grad_phi));
+    if ((P->bc_bot == 0 && z == 0) || (P->bc_top == 0 && z == nz - 1) ||
+        ((uint32_t)z >= D->wall0_iz && P->bc_top == 0) || (P->bc_xn == 0 && x == 0) ||
+        (P->bc_xp == 0 && x == nx - 1) || (P->bc_yn == 0 && y == 0) ||
+        (P->bc_yp == 0 && y == nx - 1) || p_constant == 1)
+        dp = 0.0;
+    return dp;
+}
+
+/* darcy.cuh:2267-2325 findDarcyVelocities */
+static void darcy_velocities(const Dc *dc)
+{
+    OrDarcy *D = dc->d;
+    const double mu = dc->P->mu;
+    for (int z = 0; z < dc->nz; ++z)
+        for (int y = 0; y < dc->ny; ++y)
+            for (int x = 0; x < dc->nx; ++x) {
+                const uint32_t ci = d_idx(dc, x, y, z);
+                const double xn = D->p[d_idx(dc, x - 1, y, z)], xp = D->p[d_idx(dc, x + 1, y, z)];
+                const double yn = D->p[d_idx(dc, x, y - 1, z)], yp = D->p[d_idx(dc, x, y + 1, z)];
+                const double zn = D->p[d_idx(dc, x, y, z - 1)], zp = D->p[d_idx(dc, x, y, z + 1)];
+                const double k = D->k[ci], phi = D->phi[ci];
+                const v3 grad_p = mk((xp - xn) / (dc->dx + dc->dx), (yp - yn) / (dc->dy + dc->dy),
+                                     (zp - zn) / (dc->dz + dc->dz));
+                const v3 v = divs(smul(-k / mu, grad_p), phi);
+                D->v[3 * (size_t)ci] = v.x;
+                D->v[3 * (size_t)ci + 1] = v.y;
+                D->v[3 * (size_t)ci + 2] = v.z;
+            }
+}
+
+static void darcy_interior_copy(const Dc *dc, const double *src, double *dst)
+{
+    for (int z = 0; z < dc->nz; ++z)
+        for (int y = 0; y < dc->ny; ++y)
+            for (int x = 0; x < dc->nx; ++x) dst[d_idx(dc, x, y, z)] = src[d_idx(dc, x, y, z)];
+}
+
+static void dc_init(Dc *dc, const Ctx *c, OrDarcy *D)
+{
+    dc->d = D;
+    dc->P = &D->prm;
+    dc->nx = (int)c->num[0];
+    dc->ny = (int)c->num[1];
+    dc->nz = (int)c->num[2];
+    dc->dx = c->L[0] / c->num[0];
+    dc->dy = c->L[1] / c->num[1];
+    dc->dz = c->L[2] / c->num[2];
+}
+
+void or_darcy_start(OrState *s)
+{
+    OrDarcy *D = s->darcy;
+    if (!D) return;
+    Ctx c;
+    ctx_init(&c, s);
+    Dc dc;
+    dc_init(&dc, &c, D);
+    /* device.cu:1009-1015 */
+    D->p_top_orig = D->p[d_idx(&dc, 0, 0, dc.nz - 1)] -
+                    D->prm.p_mod_A * sin(2.0 * OR_DARCY_PI * D->prm.p_mod_f * s->box.t_current +
+                                         D->prm.p_mod_phi);
+    D->filetimeclock = 0.0;
+    D->wall_w_host = s->box.walls.nw > 0 ? s->box.walls.nx[0][3] : 0.0;
+    D->wall0_iz = 10000000u;
+    D->log_n = 0;
+}
+
+static void darcy_log(OrDarcy *D, uint64_t step, uint32_t iters, uint32_t ok)
+{
+    if (D->log_n < D->log_cap) {
+        D->log_step[D->log_n] = step;
+        D->log_iters[D->log_n] = iters;
+        D->log_ok[D->log_n] = ok;
+        D->log_n++;
+    }
+}
+
+/* device.cu:1891-2419: the Darcy part of one step, after interact and
+ * bonds, before the shear-stress sums and integrate.  The Jacobi loop's
+ * residual check (every nijacnorm = 10 iterations, src/debug.h:16) takes
+ * the largest |norm| over the cells (darcy.cpp:266-293); a NaN raises
+ * SPH_ERR_NAN and ends the solve (the reference exits). */
+static void darcy_step(const Ctx *c, OrState *s)
+{
+    OrDarcy *D = s->darcy;
+    const SphDarcy *P = &D->prm;
+    Dc dc;
+    dc_init(&dc, c, D);
+    const uint64_t iter = s->iter;
+    /* device.cu:1901-1904 wall0_iz from the host's copy of wall 0 */
+    if (c->nw > 0 && (s->box.walls.wmode[0] == 1 || s->box.walls.wmode[0] == 3))
+        D->wall0_iz = (uint32_t)(D->wall_w_host / (c->L[2] / c->num[2]));
+    if (c->np > 0) {
+        darcy_ghost(&dc, D->p, 1);
+        darcy_gradient(&dc, D->p, D->grad_p);
+        darcy_ghost(&dc, D->grad_p, 3);
+        darcy_force(c, &dc, s);
+    }
+    if (iter % P->ndem != 0) return;
+    darcy_porosities(c, &dc, s, iter);
+    if (c->periodic == 2) {
+        darcy_copy_edges(&dc);
+        darcy_copy_bottom(&dc);
+    }
+    if ((P->p_mod_A > 1.0e-5 || P->p_mod_A < -1.0e-5) && P->p_mod_f > 1.0e-7) {
+        const double new_pressure =
+            D->p_top_orig + P->p_mod_A * sin(2.0 * OR_DARCY_PI * P->p_mod_f * s->box.t_current +
+                                              P->p_mod_phi);
+        darcy_top_pressure(&dc, new_pressure);
+    }
+    darcy_permeabilities(&dc);
+    darcy_ghost(&dc, D->phi, 1);
+    darcy_ghost(&dc, D->k, 1);
+    darcy_gradient(&dc, D->k, D->grad_k);
+    if (iter == 0) {
+        for (int z = 0; z < dc.nz; ++z)
+            for (int y = 0; y < dc.ny; ++y)
+                for (int x = 0; x < dc.nx; ++x) D->norm[d_idx(&dc, x, y, z)] = 0.0;
+        darcy_interior_copy(&dc, D->p, D->p_old);
+    }
+    darcy_ghost_flux(&dc, D->p, D->k, c->L[2]);
+    uint32_t nijac = 0, ok = 0;
+    for (nijac = 0; nijac < P->maxiter; ++nijac) {
+        if (nijac == 0) darcy_interior_copy(&dc, D->p, D->p_old);
+        darcy_ghost(&dc, D->p, 1);
+        if (nijac == 0)
+            for (int z = 0; z < dc.nz; ++z)
+                for (int y = 0; y < dc.ny; ++y)
+                    for (int x = 0; x < dc.nx; ++x)
+                        D->dp_expl[d_idx(&dc, x, y, z)] = darcy_dp(&dc, c, x, y, z, D->p);
+        for (int z = 0; z < dc.nz; ++z)
+            for (int y = 0; y < dc.ny; ++y)
+                for (int x = 0; x < dc.nx; ++x) {
+                    const uint32_t ci = d_idx(&dc, x, y, z);
+                    const double dp_impl = darcy_dp(&dc, c, x, y, z, D->p);
+                    const double epsilon = 0.5;
+                    const double p = D->p[ci];
+                    double p_new = D->p_old[ci] + (1.0 - epsilon) * D->dp_expl[ci] + epsilon * dp_impl;
+                    const double theta = 0.05;
+                    p_new = p * (1.0 - theta) + p_new * theta;
+                    D->p_new[ci] = p_new;
+                    D->norm[ci] = (p_new - p) / (p + 1.0e-16);
+                }
+        if (P->bc_top == 1) darcy_top_fixed_flow(&dc);
+        darcy_ghost_flux(&dc, D->p, D->k, c->L[2]);
+        darcy_interior_copy(&dc, D->p_new, D->p);
+        if (nijac % 10 == 0) {
+            double max_norm_res = -1.0e9;
+            int nan = 0;
+            for (int z = 0; z < dc.nz && !nan; ++z)
+                for (int y = 0; y < dc.ny && !nan; ++y)
+                    for (int x = 0; x < dc.nx; ++x) {
+                        const double r = fabs(D->norm[d_idx(&dc, x, y, z)]);
+                        if (r != r) { nan = 1; break; }
+                        if (r > max_norm_res) max_norm_res = r;
+                    }
+            if (nan) {
+                FLAG(s, SPH_ERR_NAN);
+                break;
+            }
+            if (max_norm_res <= P->tolerance) {
+                ok = 1;
+                break;
+            }
+        }
+        if (nijac == P->maxiter - 1) break;
+    }
+    darcy_log(D, iter + 1, nijac, ok);
+    if (D->filetimeclock + c->dt < P->file_dt)
+        for (int z = 0; z < dc.nz; ++z)
+            for (int y = 0; y < dc.ny; ++y)
+                for (int x = 0; x < dc.nx; ++x) D->dphi[d_idx(&dc, x, y, z)] = 0.0;
+    darcy_ghost(&dc, D->p, 1);
+    darcy_velocities(&dc);
+}
+
+/* device.cu:2537 and 2569-2672: the host's file clock, and the host copy of
+ * the walls refreshed by the output's transfer from the device */
+static void darcy_clock(const Ctx *c, OrState *s)
+{
+    OrDarcy *D = s->darcy;
+    D->filetimeclock += c->dt;
+    if (D->filetimeclock >= D->prm.file_dt) {
+        D->filetimeclock = 0.0;
+        if (c->nw > 0) D->wall_w_host = s->box.walls.nx[0][3];
+    }
+}
+
 /* --------------------------------------------------------------- step loop */
 
 static void ctx_init(Ctx *c, OrState *s)
@@ -836,6 +1408,7 @@ int or_step(OrState *s, uint64_t nsteps)
             interact(&c, s);
             if (s->box.nb0 > 0) bonds_linear(&c, s, s->bonds_broken);
         }
+        if (s->darcy) darcy_step(&c, s);
         if (np > 0) {
             if (c.nw > 0 && s->box.walls.wmode[0] == 3) {
                 find_shear_stress(&c, s);
@@ -851,6 +1424,7 @@ int or_step(OrState *s, uint64_t nsteps)
             if (c.nw > 0) integrate_walls(&c, s, s->box.t_current);
         }
         s->box.t_current += s->box.dt;
+        if (s->darcy) darcy_clock(&c, s);
         s->iter++;
     }
     return s->error_flags;

@@ -47,7 +47,30 @@ typedef struct OrState {
     double *walls_force_pp;                             /* [nw*np] */
     double *walls_force_partial;                        /* [ceil(np/256)] */
     double *tau_eff_x_pp, *tau_eff_x_partial;           /* [np], [ceil(np/256)] */
+    struct OrDarcy *darcy;                              /* NULL: fluid == 0 */
 } OrState;
+
+/* Darcy coupling (fluid == 1, cfd_solver == 1).  Cell fields are padded
+ * with one ghost layer on every side, (nx+2)(ny+2)(nz+2) cells indexed
+ * (x+1) + (nx+2)(y+1) + (nx+2)(ny+2)(z+1) (src/darcy.cpp:64-76); vector
+ * fields hold three doubles per cell (Float3).  The file clock and the
+ * host's copy of the top wall position (refreshed when an output is
+ * written) are the reference's host variables (src/device.cu:918, 1001,
+ * 1903, 2537, 2569-2672).  The log keeps one entry per fluid step. */
+typedef struct OrDarcy {
+    SphDarcy prm;
+    double *p, *p_old, *p_new, *dp_expl, *phi, *dphi, *norm, *k, *div_v_p;
+    double *v, *vp_avg, *grad_k, *grad_p;
+    int32_t *p_constant;
+    double *f_p;              /* [np][4] */
+    double p_top_orig;
+    double filetimeclock;
+    double wall_w_host;
+    uint32_t wall0_iz;
+    uint32_t log_cap, log_n;
+    uint64_t *log_step;
+    uint32_t *log_iters, *log_ok;
+} OrDarcy;
 
 /* Run nsteps iterations of the fluid == 0 step loop.  Returns the OR of the
  * error flags raised (0 = clean). */
@@ -78,6 +101,9 @@ void or_relax(double *x4, uint32_t np, const double origo[3], const double L[3],
               const uint32_t num[3], int periodic, uint32_t sweeps, double alpha, double z_top,
               int nthreads, double *max_ov);
 int ref_step(OrState *s, uint64_t nsteps);
+/* Darcy set-up at the start of a run (src/device.cu:1003-1016): p_top_orig
+ * from the top cell's pressure, the host wall copy from wall 0. */
+void or_darcy_start(OrState *s);
 
 #ifdef __cplusplus
 }

@@ -6,6 +6,8 @@ their sizes against the library (``sph_struct_sizes``).
 import ctypes as C
 import os
 
+import numpy
+
 NC = 32
 MAXWALLS = 6
 TUNE_VARIANTS = 5   # SPH_TUNE_VARIANTS: launch variants sph_autotune times
@@ -85,6 +87,52 @@ class SphParticles(C.Structure):
 class SphBonds(C.Structure):
     _fields_ = [("pairs", _up), ("delta_n", _dp), ("delta_t", _dp),
                 ("omega_n", _dp), ("omega_t", _dp)]
+
+
+class SphDarcy(C.Structure):
+    _fields_ = [("mu", C.c_double), ("rho_f", C.c_double), ("beta_f", C.c_double),
+                ("k_c", C.c_double), ("c_phi", C.c_double), ("tolerance", C.c_double),
+                ("p_mod_A", C.c_double), ("p_mod_f", C.c_double), ("p_mod_phi", C.c_double),
+                ("bc_bot_flux", C.c_double), ("bc_top_flux", C.c_double),
+                ("file_dt", C.c_double),
+                ("maxiter", C.c_uint32), ("ndem", C.c_uint32),
+                ("bc_xn", C.c_int32), ("bc_xp", C.c_int32), ("bc_yn", C.c_int32),
+                ("bc_yp", C.c_int32), ("bc_bot", C.c_int32), ("bc_top", C.c_int32),
+                ("free_slip_bot", C.c_int32), ("free_slip_top", C.c_int32)]
+
+
+DARCY_LOG = 4096   # SPH_DARCY_LOG
+
+
+def darcy_from_sim(s):
+    """The SphDarcy of a sim object with a Darcy fluid (cfd_solver 1)."""
+    d = SphDarcy()
+    for name in ("mu", "rho_f", "beta_f", "k_c", "c_phi", "p_mod_A", "p_mod_f", "p_mod_phi",
+                 "bc_bot_flux", "bc_top_flux"):
+        setattr(d, name, float(numpy.asarray(getattr(s, name)).ravel()[0]))
+    d.tolerance = float(numpy.asarray(s.tolerance).ravel()[0])
+    d.file_dt = float(s.time_file_dt[0])
+    d.maxiter = int(numpy.asarray(s.maxiter).ravel()[0])
+    d.ndem = int(numpy.asarray(s.ndem).ravel()[0])
+    for name in ("bc_xn", "bc_xp", "bc_yn", "bc_yp", "bc_bot", "bc_top", "free_slip_bot",
+                 "free_slip_top"):
+        setattr(d, name, int(numpy.asarray(getattr(s, name)).ravel()[0]))
+    return d
+
+
+def cells_to_file(a):
+    """A sim's cell array [nx, ny, nz(, k)] in the .bin order (x fastest)."""
+    a = numpy.asarray(a)
+    axes = (2, 1, 0) + tuple(range(3, a.ndim))
+    return numpy.ascontiguousarray(a.transpose(axes))
+
+
+def cells_from_file(flat, num, k=None):
+    """The inverse of cells_to_file: [nx, ny, nz(, k)] from x-fastest data."""
+    shape = (int(num[2]), int(num[1]), int(num[0])) + ((k,) if k else ())
+    a = numpy.asarray(flat).reshape(shape)
+    axes = (2, 1, 0) + tuple(range(3, a.ndim))
+    return numpy.ascontiguousarray(a.transpose(axes))
 
 
 def dptr(a):
@@ -242,6 +290,16 @@ def load_library():
     lib.sph_adjoint_forward.argtypes = [H, C.c_uint64, C.c_uint32, _dp]
     lib.sph_cell_offsets_static.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
     lib.sph_cell_offsets_static.restype = C.c_int
+    lib.sph_darcy_set.argtypes = [H, C.POINTER(SphDarcy), _dp, _dp, _dp, _dp,
+                                  C.POINTER(C.c_int32), _dp]
+    lib.sph_darcy_set.restype = C.c_int
+    lib.sph_darcy_get.argtypes = [H, _dp, _dp, _dp, _dp, _dp, _dp]
+    lib.sph_darcy_get.restype = C.c_int
+    lib.sph_darcy_log.argtypes = [H, C.POINTER(C.c_uint64), _up, _up, C.c_uint32,
+                                  C.POINTER(C.c_uint32)]
+    lib.sph_darcy_log.restype = C.c_int
+    lib.sph_darcy_struct_size.argtypes = [C.POINTER(C.c_uint64)]
+    lib.sph_darcy_struct_size.restype = C.c_int
     lib.sph_adjoint_forward.restype = C.c_int
     lib.sph_adjoint_backward.argtypes = [H, _dp, _dp, _dp, _dp]
     lib.sph_adjoint_backward.restype = C.c_int

@@ -4,11 +4,14 @@ Layout: python/sphere.py:1355-1553 (writebin) and :965-1353 (readbin),
 src/file_io.cpp:30-731 (C++ readbin/writebin).  Files are little-endian;
 every block below is written in the order the reference writes it.  The
 writer produces files byte-identical to python/sphere.py:writebin for
-simulations without a fluid; the reader accepts versions >= 2.1 (older
-optional fields default as in python/sphere.py:readbin).  Fluid blocks
-(the Navier-Stokes / Darcy coupling) are outside this package's scope.
+simulations without a fluid and with a Darcy fluid (cfd_solver 1); the
+reader accepts versions >= 2.1 (older optional fields default as in
+python/sphere.py:readbin).  The Navier-Stokes fluid block (cfd_solver 0) is
+not supported.
 """
 import numpy
+
+from ._abi import cells_from_file, cells_to_file
 
 VERSION = 2.15
 
@@ -29,11 +32,63 @@ class _Reader(object):
         return a
 
 
-def read_bin(target, sim, verbose=False, fluid=False):
+def _read_darcy(r, s, n):
+    """The Darcy fluid block (python/sphere.py:1157-1345 readbin,
+    src/file_io.cpp:347-404).  dphi is stored in the file as the change per
+    fluid step; the sim holds it per unit time, divided by time_dt * ndem
+    with the ndem the sim held before this read, as the reference's reader
+    divides."""
+    version = float(s.version[0])
+    if version >= 2.0:
+        s.cfd_solver = r.take(numpy.int32, 1)
+    else:
+        s.cfd_solver = numpy.zeros(1, dtype=numpy.int32)
+    if int(s.cfd_solver[0]) != 1:
+        raise NotImplementedError("the Navier-Stokes fluid block (cfd_solver %d) is not supported"
+                                  % int(s.cfd_solver[0]))
+    num = [int(v) for v in s.num]
+    ncell = num[0] * num[1] * num[2]
+    ndem_before = numpy.asarray(getattr(s, "ndem", numpy.array(1)))
+    s.mu = r.take(numpy.float64, 1)
+    blk = r.take(numpy.float64, ncell * 6).reshape(ncell, 6)
+    s.v_f = cells_from_file(blk[:, 0:3], num, 3)
+    s.p_f = cells_from_file(blk[:, 3], num)
+    s.phi = cells_from_file(blk[:, 4], num)
+    s.dphi = cells_from_file(blk[:, 5], num) / (s.time_dt * ndem_before)
+    s.rho_f = r.take(numpy.float64, 1)
+    s.p_mod_A = r.take(numpy.float64, 1)
+    s.p_mod_f = r.take(numpy.float64, 1)
+    s.p_mod_phi = r.take(numpy.float64, 1)
+    if version >= 2.12:
+        for name in ("bc_xn", "bc_xp", "bc_yn", "bc_yp"):
+            setattr(s, name, r.take(numpy.int32, 1))
+    for name in ("bc_bot", "bc_top", "free_slip_bot", "free_slip_top"):
+        setattr(s, name, r.take(numpy.int32, 1))
+    if version >= 2.11:
+        s.bc_bot_flux = r.take(numpy.float64, 1)
+        s.bc_top_flux = r.take(numpy.float64, 1)
+    else:
+        s.bc_bot_flux = numpy.zeros(1, dtype=numpy.float64)
+        s.bc_top_flux = numpy.zeros(1, dtype=numpy.float64)
+    if version >= 2.15:
+        s.p_f_constant = cells_from_file(r.take(numpy.int32, ncell), num)
+    else:
+        s.p_f_constant = numpy.zeros(num, dtype=numpy.int32)
+    s.tolerance = r.take(numpy.float64, 1)
+    s.maxiter = r.take(numpy.uint32, 1)
+    s.ndem = r.take(numpy.uint32, 1)
+    s.c_phi = r.take(numpy.float64, 1)
+    s.f_p = r.take(numpy.float64, n * 3).reshape(n, 3)
+    s.beta_f = r.take(numpy.float64, 1)
+    s.k_c = r.take(numpy.float64, 1)
+
+
+def read_bin(target, sim, verbose=False, fluid=None):
     """Read a sphere .bin file into the attributes of `sim`
-    (python/sphere.py:965 readbin)."""
-    if fluid:
-        raise NotImplementedError("fluid (Navier-Stokes/Darcy) blocks are not supported")
+    (python/sphere.py:965 readbin).  As in the reference, whether the file
+    holds a fluid block is the sim's `fluid` flag (or `fluid` when given)."""
+    if fluid is None:
+        fluid = bool(getattr(sim, "fluid", False))
     if verbose:
         print("Input file: {0}".format(target))
     with open(target, "rb") as fh:
@@ -120,6 +175,9 @@ def read_bin(target, sim, verbose=False, fluid=False):
     s.bonds_delta_t = r.take(numpy.float64, nb0 * nd).reshape(nb0, nd)
     s.bonds_omega_n = r.take(numpy.float64, nb0)
     s.bonds_omega_t = r.take(numpy.float64, nb0 * nd).reshape(nb0, nd)
+    if fluid:
+        s.fluid = True
+        _read_darcy(r, s, n)
     if s.version[0] >= 1.02:
         s.color = r.take(numpy.int32, n)
     else:
@@ -140,11 +198,47 @@ def _i32(a):
     return numpy.ascontiguousarray(numpy.asarray(a).astype(numpy.int32)).tobytes()
 
 
-def encode_bin(sim):
-    """Bytes of `sim` in the .bin layout of python/sphere.py:1355 writebin."""
+def _encode_darcy(s, w, dphi_raw=None):
+    """The Darcy fluid block in the order of python/sphere.py:1471-1539 and
+    src/file_io.cpp:656-716.  dphi goes to the file as dphi * time_dt * ndem
+    (the reference's Python writer); dphi_raw, when given, is written as it
+    is (the values of the solver, as its C++ writer writes them)."""
+    if int(numpy.asarray(s.cfd_solver).ravel()[0]) != 1:
+        raise NotImplementedError("the Navier-Stokes fluid block (cfd_solver 0) is not supported")
+    n = int(s.np[0])
+    w(_i32(numpy.asarray(s.cfd_solver).ravel()[:1]))
+    w(_f64(s.mu))
+    if dphi_raw is None:
+        dphi_raw = numpy.asarray(s.dphi, dtype=numpy.float64) * s.time_dt * s.ndem
+    num = [int(v) for v in s.num]
+    ncell = num[0] * num[1] * num[2]
+    blk = numpy.empty((ncell, 6))
+    blk[:, 0:3] = cells_to_file(s.v_f).reshape(ncell, 3)
+    blk[:, 3] = cells_to_file(s.p_f).reshape(ncell)
+    blk[:, 4] = cells_to_file(s.phi).reshape(ncell)
+    blk[:, 5] = cells_to_file(dphi_raw).reshape(ncell)
+    w(blk.tobytes())
+    for name in ("rho_f", "p_mod_A", "p_mod_f", "p_mod_phi"):
+        w(_f64(getattr(s, name)))
+    for name in ("bc_xn", "bc_xp", "bc_yn", "bc_yp", "bc_bot", "bc_top", "free_slip_bot",
+                 "free_slip_top"):
+        w(_i32(getattr(s, name)))
+    w(_f64(s.bc_bot_flux))
+    w(_f64(s.bc_top_flux))
+    w(_i32(cells_to_file(s.p_f_constant).reshape(ncell)))
+    w(_f64(numpy.asarray(s.tolerance).ravel()[:1]))
+    w(_u32(numpy.asarray(s.maxiter).ravel()[:1]))
+    w(_u32(numpy.asarray(s.ndem).ravel()[:1]))
+    w(_f64(s.c_phi))
+    w(_f64(numpy.asarray(s.f_p, dtype=numpy.float64).reshape(-1, 3)[:n]))
+    w(_f64(s.beta_f))
+    w(_f64(s.k_c))
+
+
+def encode_bin(sim, dphi_raw=None):
+    """Bytes of `sim` in the .bin layout of python/sphere.py:1355 writebin
+    (with the Darcy fluid block when sim.fluid)."""
     s = sim
-    if getattr(s, "fluid", False):
-        raise NotImplementedError("fluid (Navier-Stokes/Darcy) blocks are not supported")
     n = int(s.np[0])
     nd = int(s.nd[0])
     out = []
@@ -209,13 +303,15 @@ def encode_bin(sim):
     w(_f64(numpy.asarray(s.bonds_delta_t).reshape(-1, 3)[:nb0]))
     w(_f64(numpy.asarray(s.bonds_omega_n).reshape(-1)[:nb0]))
     w(_f64(numpy.asarray(s.bonds_omega_t).reshape(-1, 3)[:nb0]))
+    if getattr(s, "fluid", False):
+        _encode_darcy(s, w, dphi_raw)
     w(_i32(s.color))
     return b"".join(out)
 
 
-def write_bin(target, sim):
+def write_bin(target, sim, dphi_raw=None):
     """Write `sim` to `target` (python/sphere.py:1355 writebin layout)."""
-    data = encode_bin(sim)
+    data = encode_bin(sim, dphi_raw)
     with open(target, "wb") as fh:
         fh.write(data)
     return len(data)

@@ -29,6 +29,7 @@ SOURCES = [
     ("sph_capi.cu", ["-fmad=false"]),
     ("sph_mixed.cu", ["-fmad=true"]),
     ("sph_pair.cu", ["-fmad=false", "-ftz=true"]),
+    ("sph_darcy.cu", ["-fmad=false"]),
     ("sph_adjoint.cu", ["-fmad=false"]),
     ("sph_noalloc.cu", []),
     ("sph_render.cu", ["-fmad=false"]),

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -95,6 +96,14 @@ struct SphHandle {
     // into graphs with conditional nodes; the list step then reads its
     // rebuild request on the host each step
     bool eager = false;
+    // the Darcy coupling (sph_darcy_set): its device fields and state
+    // (D.st null until set), the host mirror of the device's step count
+    // (the top-pressure ring index), the Jacobi log entries read so far and
+    // the top pressure at the start of the run
+    sph::DarcyArgs D{};
+    bool darcy_on = false;
+    uint64_t darcy_qstep = 0, darcy_log_tail = 0;
+    double darcy_p_top_orig = 0.0;
 };
 
 static int fail(SphHandle *h, int code, const std::string &msg)
@@ -312,6 +321,13 @@ static void init_dev_box(DevBox &d, const SphBox &b)
 }
 
 extern "C" {
+
+int sph_darcy_struct_size(uint64_t *size)
+{
+    if (!size) return SPH_ERR_INPUT;
+    *size = sizeof(SphDarcy);
+    return SPH_OK;
+}
 
 int sph_struct_sizes(uint64_t *sizes)
 {
@@ -868,12 +884,16 @@ static int capture_step(SphHandle *h, sph::Prof *prof, cudaGraph_t *g, cudaGraph
     cfg.fork = h->ev_fork;
     cfg.join = h->ev_join;
     const bool pair = pair_active(h);
-    if (pair && !h->side) {
-        // the list step captures its rebuild body on the side stream
+    if ((pair || h->darcy_on) && !h->side) {
+        // the list step captures its rebuild body, the Darcy coupling its
+        // Jacobi loop's body, on the side stream
         CUDA_TRY(h, cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
         CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
         CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     }
+    cfg.side = h->side;
+    cfg.fork = h->ev_fork;
+    cfg.join = h->ev_join;
     if (pair) {
         int st = ensure_pair(h);
         if (st != SPH_OK) return st;
@@ -981,10 +1001,60 @@ int sph_step(SphHandle *h, uint64_t nsteps)
     return collect_errors(h);
 }
 
+// The Darcy top pressure of the next n (<= DARCY_RING) queued steps
+// (device.cu:2000-2008: p_top_orig + A sin(2 pi f t + phi) with the host's
+// time and the C library's sin) into the device ring, in stream order.
+static int fill_darcy_pmod(SphHandle *h, uint64_t n)
+{
+    const SphDarcy &d = h->D.prm;
+    std::vector<double> v(n);
+    double t = h->t_host[0];
+    for (uint64_t j = 0; j < n; ++j) {
+        v[j] = h->darcy_p_top_orig + d.p_mod_A * sin(2.0 * 3.14159265358979323846 * d.p_mod_f * t +
+                                                     d.p_mod_phi);
+        t += h->boxes[0].dt;
+    }
+    double *ring = const_cast<double *>(h->D.pmod);
+    uint64_t done = 0;
+    while (done < n) {
+        const uint64_t slot = (h->darcy_qstep + done) % sph::DARCY_RING;
+        const uint64_t len = std::min<uint64_t>(n - done, sph::DARCY_RING - slot);
+        CUDA_TRY(h, cudaMemcpyAsync(ring + slot, v.data() + done, sizeof(double) * len,
+                                    cudaMemcpyHostToDevice, h->stream));
+        done += len;
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->darcy_qstep += n;
+    return SPH_OK;
+}
+
+static int queue_steps_now(SphHandle *h, uint64_t nsteps, uint8_t *states);
+static int drop_graphs(SphHandle *h);
+
 // Queue nsteps steps on the handle's stream; with states, the box table
 // after step s is copied to states + s * (nbox * sizeof(DevBox)) as soon as
-// that step's wall stage has run.
+// that step's wall stage has run.  With a modulated Darcy top pressure the
+// steps are queued in runs of at most DARCY_RING, each after its pressures.
 static int queue_steps(SphHandle *h, uint64_t nsteps, uint8_t *states)
+{
+    if (!h->darcy_on) return queue_steps_now(h, nsteps, states);
+    if (!h->D.pmod) {
+        h->darcy_qstep += nsteps;
+        return queue_steps_now(h, nsteps, states);
+    }
+    const size_t bytes = sizeof(DevBox) * h->nbox;
+    uint64_t done = 0;
+    while (done < nsteps) {
+        const uint64_t n = std::min<uint64_t>(nsteps - done, sph::DARCY_RING);
+        int st = fill_darcy_pmod(h, n);
+        if (st == SPH_OK) st = queue_steps_now(h, n, states ? states + done * bytes : nullptr);
+        if (st != SPH_OK) return st;
+        done += n;
+    }
+    return SPH_OK;
+}
+
+static int queue_steps_now(SphHandle *h, uint64_t nsteps, uint8_t *states)
 {
     int st;
     if (h->eager) {
@@ -1139,6 +1209,189 @@ int sph_advance(SphHandle *h, double time_total, double file_dt, double *time_cu
     *filetimeclock = ftc;
     if (steps_done) *steps_done = k;
     return st;
+}
+
+// ------------------------------------------------------------------ Darcy
+
+int sph_darcy_set(SphHandle *h, const SphDarcy *d, const double *p, const double *v,
+                  const double *phi, const double *dphi, const int32_t *p_constant,
+                  const double *f_p)
+{
+    if (!h || !d || !p || !v || !phi || !dphi) return SPH_ERR_INPUT;
+    if (h->nbox != 1 || h->precision != SPH_PREC_FP64)
+        return fail(h, SPH_ERR_UNSUPPORTED, "the Darcy coupling runs one box in the FP64 form");
+    const SphBox &b0 = h->boxes[0];
+    if (b0.grid.adaptive)
+        return fail(h, SPH_ERR_UNSUPPORTED, "the Darcy coupling on an adaptive grid");
+    if (d->ndem == 0) return fail(h, SPH_ERR_INPUT, "ndem must be at least 1");
+    for (int k = 0; k < 3; ++k)
+        if (b0.grid.num[k] < 1) return fail(h, SPH_ERR_INPUT, "empty fluid grid");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const int nx = (int)b0.grid.num[0], ny = (int)b0.grid.num[1], nz = (int)b0.grid.num[2];
+    const uint64_t ncell = (uint64_t)(nx + 2) * (ny + 2) * (nz + 2);
+    if (ncell >= 0xffffffffull) return fail(h, SPH_ERR_UNSUPPORTED, "fluid grid too large");
+    sph::DarcyArgs &D = h->D;
+    if (!D.st) {
+        int st;
+        double **f1[] = {&D.p, &D.p_old, &D.p_new, &D.dp_expl, &D.phi, &D.dphi, &D.norm, &D.k,
+                         &D.div_v_p};
+        for (double **f : f1)
+            if ((st = dalloc(h, f, ncell)) != SPH_OK) return st;
+        double **f3[] = {&D.v, &D.vp_avg, &D.grad_k, &D.grad_p};
+        for (double **f : f3)
+            if ((st = dalloc(h, f, 3 * ncell)) != SPH_OK) return st;
+        if ((st = dalloc(h, &D.p_constant, ncell)) != SPH_OK ||
+            (st = dalloc(h, &D.f_p, h->ntot)) != SPH_OK || (st = dalloc(h, &D.st, 1)) != SPH_OK ||
+            (st = dalloc(h, &D.log_step, SPH_DARCY_LOG)) != SPH_OK ||
+            (st = dalloc(h, &D.log_iters, SPH_DARCY_LOG)) != SPH_OK ||
+            (st = dalloc(h, &D.log_ok, SPH_DARCY_LOG)) != SPH_OK)
+            return st;
+    }
+    const bool modulated = (d->p_mod_A > 1.0e-5 || d->p_mod_A < -1.0e-5) && d->p_mod_f > 1.0e-7;
+    if (modulated && !D.pmod) {
+        double *ring = nullptr;
+        int st = dalloc(h, &ring, sph::DARCY_RING);
+        if (st != SPH_OK) return st;
+        D.pmod = ring;
+    }
+    D.prm = *d;
+    D.periodic = b0.grid.periodic;
+    D.nx = nx;
+    D.ny = ny;
+    D.nz = nz;
+    D.dx = b0.grid.L[0] / b0.grid.num[0];
+    D.dy = b0.grid.L[1] / b0.grid.num[1];
+    D.dz = b0.grid.L[2] / b0.grid.num[2];
+    D.ncell = (uint32_t)ncell;
+    if (!modulated) D.pmod = nullptr;
+    // the fields with zero ghost layers, x fastest inside
+    auto pad = [&](const double *src, int m) {
+        std::vector<double> out((size_t)m * ncell, 0.0);
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y)
+                for (int x = 0; x < nx; ++x) {
+                    const size_t c = (size_t)(x + 1) + (size_t)(nx + 2) * (y + 1) +
+                                     (size_t)(nx + 2) * (ny + 2) * (z + 1);
+                    const size_t i = (size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z);
+                    for (int k = 0; k < m; ++k) out[(size_t)m * c + k] = src[(size_t)m * i + k];
+                }
+        return out;
+    };
+    const std::vector<double> hp = pad(p, 1), hv = pad(v, 3), hphi = pad(phi, 1), hd = pad(dphi, 1);
+    std::vector<int32_t> hc(ncell, 0);
+    if (p_constant)
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y)
+                for (int x = 0; x < nx; ++x)
+                    hc[(size_t)(x + 1) + (size_t)(nx + 2) * (y + 1) + (size_t)(nx + 2) * (ny + 2) * (z + 1)] =
+                        p_constant[(size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z)];
+    std::vector<double4> hf(h->ntot ? h->ntot : 1, make_double4(0.0, 0.0, 0.0, 0.0));
+    if (f_p)
+        for (uint64_t i = 0; i < h->ntot; ++i) hf[i] = make_double4(f_p[3 * i], f_p[3 * i + 1], f_p[3 * i + 2], 0.0);
+    const size_t B1 = sizeof(double) * ncell;
+    CUDA_TRY(h, cudaMemcpy(D.p, hp.data(), B1, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(D.v, hv.data(), 3 * B1, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(D.phi, hphi.data(), B1, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(D.dphi, hd.data(), B1, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(D.p_constant, hc.data(), sizeof(int32_t) * ncell, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(D.f_p, hf.data(), sizeof(double4) * (h->ntot ? h->ntot : 1), cudaMemcpyHostToDevice));
+    double *zero1[] = {D.p_old, D.p_new, D.dp_expl, D.norm, D.k, D.div_v_p};
+    for (double *f : zero1) CUDA_TRY(h, cudaMemset(f, 0, B1));
+    double *zero3[] = {D.vp_avg, D.grad_k, D.grad_p};
+    for (double *f : zero3) CUDA_TRY(h, cudaMemset(f, 0, 3 * B1));
+    // the start of the run (device.cu:1001, 1009-1015, 918): the top
+    // pressure at t = time.current, the file clock, the host's copy of the
+    // top wall as the device holds it now
+    DevBox b;
+    CUDA_TRY(h, cudaMemcpy(&b, h->A.boxes, sizeof(DevBox), cudaMemcpyDeviceToHost));
+    h->darcy_p_top_orig = hp[(size_t)1 + (size_t)(nx + 2) * 1 + (size_t)(nx + 2) * (ny + 2) * nz] -
+                          d->p_mod_A * sin(2.0 * 3.14159265358979323846 * d->p_mod_f * h->t_host[0] +
+                                           d->p_mod_phi);
+    sph::DarcyState ds{};
+    ds.filetimeclock = 0.0;
+    ds.wall_w_host = b.nw > 0 ? b.wnx[0][3] : 0.0;
+    ds.wall0_iz = 10000000u;
+    CUDA_TRY(h, cudaMemcpy(D.st, &ds, sizeof ds, cudaMemcpyHostToDevice));
+    h->darcy_qstep = 0;
+    h->darcy_log_tail = 0;
+    h->darcy_on = true;
+    h->cfg.darcy = &h->D;
+    h->cfg.unfused = true;
+    return drop_graphs(h);
+}
+
+int sph_darcy_get(SphHandle *h, double *p, double *v, double *phi, double *dphi, double *k,
+                  double *f_p)
+{
+    if (!h) return SPH_ERR_INPUT;
+    if (!h->darcy_on) return fail(h, SPH_ERR_STATE, "sph_darcy_get before sph_darcy_set");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const sph::DarcyArgs &D = h->D;
+    const int nx = D.nx, ny = D.ny, nz = D.nz;
+    const size_t ncell = D.ncell;
+    auto get = [&](double *dst, const double *src, int m) -> int {
+        if (!dst) return SPH_OK;
+        std::vector<double> buf((size_t)m * ncell);
+        CUDA_TRY(h, cudaMemcpy(buf.data(), src, sizeof(double) * m * ncell, cudaMemcpyDeviceToHost));
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y)
+                for (int x = 0; x < nx; ++x) {
+                    const size_t c = (size_t)(x + 1) + (size_t)(nx + 2) * (y + 1) +
+                                     (size_t)(nx + 2) * (ny + 2) * (z + 1);
+                    const size_t i = (size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z);
+                    for (int q = 0; q < m; ++q) dst[(size_t)m * i + q] = buf[(size_t)m * c + q];
+                }
+        return SPH_OK;
+    };
+    int st;
+    if ((st = get(p, D.p, 1)) || (st = get(v, D.v, 3)) || (st = get(phi, D.phi, 1)) ||
+        (st = get(dphi, D.dphi, 1)) || (st = get(k, D.k, 1)))
+        return st;
+    if (f_p && h->ntot) {
+        std::vector<double4> hf(h->ntot);
+        CUDA_TRY(h, cudaMemcpy(hf.data(), D.f_p, sizeof(double4) * h->ntot, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < h->ntot; ++i) {
+            f_p[3 * i] = hf[i].x;
+            f_p[3 * i + 1] = hf[i].y;
+            f_p[3 * i + 2] = hf[i].z;
+        }
+    }
+    return SPH_OK;
+}
+
+int sph_darcy_log(SphHandle *h, uint64_t *step, uint32_t *iterations, uint32_t *converged,
+                  uint32_t cap, uint32_t *n)
+{
+    if (!h || !n || (cap && (!step || !iterations || !converged))) return SPH_ERR_INPUT;
+    *n = 0;
+    if (!h->darcy_on) return fail(h, SPH_ERR_STATE, "sph_darcy_log before sph_darcy_set");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    const sph::DarcyArgs &D = h->D;
+    sph::DarcyState ds;
+    CUDA_TRY(h, cudaMemcpy(&ds, D.st, sizeof ds, cudaMemcpyDeviceToHost));
+    const uint64_t head = ds.log_head;
+    uint64_t first = h->darcy_log_tail;
+    if (head - first > SPH_DARCY_LOG) first = head - SPH_DARCY_LOG;
+    const uint64_t count = std::min<uint64_t>(head - first, cap);
+    if (count) {
+        std::vector<uint64_t> a(SPH_DARCY_LOG);
+        std::vector<uint32_t> b(SPH_DARCY_LOG), c(SPH_DARCY_LOG);
+        CUDA_TRY(h, cudaMemcpy(a.data(), D.log_step, sizeof(uint64_t) * SPH_DARCY_LOG, cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, cudaMemcpy(b.data(), D.log_iters, sizeof(uint32_t) * SPH_DARCY_LOG, cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, cudaMemcpy(c.data(), D.log_ok, sizeof(uint32_t) * SPH_DARCY_LOG, cudaMemcpyDeviceToHost));
+        for (uint64_t j = 0; j < count; ++j) {
+            const size_t slot = (size_t)((first + j) % SPH_DARCY_LOG);
+            step[j] = a[slot];
+            iterations[j] = b[slot];
+            converged[j] = c[slot];
+        }
+    }
+    h->darcy_log_tail = first + count;
+    *n = (uint32_t)count;
+    return SPH_OK;
 }
 
 }  // extern "C"
@@ -1586,6 +1839,7 @@ int sph_adjoint_forward(SphHandle *h, uint64_t nsteps, uint32_t ckpt, double *fo
 {
     if (!h || nsteps == 0 || ckpt == 0) return SPH_ERR_INPUT;
     if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_adjoint_forward before sph_upload");
+    if (h->darcy_on) return fail(h, SPH_ERR_UNSUPPORTED, "the adjoint of the Darcy coupling");
     const SphBox &b0 = h->boxes[0];
     if (h->nbox != 1 || h->precision != SPH_PREC_FP64 || h->lenmode != SPH_LEN_FP64 ||
         b0.params.contactmodel != 2 || b0.params.E > 0.001 || b0.params.kappa != 0.0 ||
@@ -1892,6 +2146,9 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
 {
     if (!h || steps == 0) return SPH_ERR_INPUT;
     if (!h->uploaded) return fail(h, SPH_ERR_STATE, "sph_autotune before sph_upload");
+    if (h->darcy_on)
+        return fail(h, SPH_ERR_UNSUPPORTED, "sph_autotune with the Darcy coupling (its timed "
+                                            "steps would advance the fluid)");
     cudaSetDevice(h->device);
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     {

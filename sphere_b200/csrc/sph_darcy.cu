@@ -1,0 +1,782 @@
+// sph_darcy.cu -- the Darcy flow coupling of the FP64 step (fluid == 1,
+// cfd_solver == 1): src/darcy.cuh and the Darcy part of the step loop,
+// src/device.cu:1891-2419.
+//
+// The fluid grid is the box's cell grid.  Every step with spheres adds the
+// fluid's pressure force (the pressure gradient interpolated to the sphere
+// times its volume, plus buoyancy) to the sphere forces between interact
+// and integrate.  Every ndem steps the fluid is updated: porosities from
+// the sorted spheres (a trilinear hat per cell, now and after an Euler step
+// of the positions), Kozeny-Carman permeabilities, and the pressure from a
+// relaxed Jacobi iteration of the diffusion equation with the porosity
+// change as forcing, then the Darcy velocities.
+//
+// Design for the GPU: the reference runs the Jacobi loop from the host,
+// four launches and a device synchronisation per iteration and a copy of
+// the whole residual field to the host every tenth; here the loop is a
+// conditional WHILE node of the step's CUDA graph, the residual maximum is
+// reduced on the device (atomicMax of the bit pattern of |r|, exact and
+// order-free) and the loop's condition is set by a one-thread kernel at the
+// end of each iteration, so a step with its fluid solve is one graph launch
+// with no host round trip.  The copy of the new pressure and the next
+// iteration's ghost layer are one kernel (each cell writes its value and
+// the ghost cells that copy it).  Which steps update the fluid
+// (iter % ndem) and the top wall's cell (wall0_iz, from the reference's
+// host copy of the wall, refreshed at outputs) are decided on the device,
+// which keeps the reference's host file clock, so the results do not
+// depend on how the steps are split into calls.  The modulated top
+// pressure is computed on the host with the C library's sin, as the
+// reference computes it, into a ring read by step index.
+//
+// Arithmetic: the kernels keep the reference's expressions and operand
+// order and the file is compiled without FMA contraction, so the results
+// equal the reference's bit for bit.  pow(r, 3) and pow(1 - phi, 2) are the
+// correctly rounded cube and square (FMA-exact products), which the C
+// library's pow returns.  Two writes of the reference depend on its launch
+// grid and are reproduced: setDarcyTopPressure's condition reads
+// (x < nx && y < ny && z == nz - 1) || z == wall0_iz, so at z == wall0_iz
+// every thread of its 8 x 8 x 8 blocks writes, also those past nx or ny
+// (their index lands on other cells of the padded array; writes past the
+// array are dropped); and the Dirichlet test of the +y side compares y
+// with nx - 1.
+#include <cstdint>
+#include <cstdio>
+
+#include "sph_device.cuh"
+#include "sph_internal.h"
+
+namespace sph {
+
+namespace {
+
+constexpr int DARCY_THREADS = 256;
+constexpr double DARCY_PI = 3.14159265358979323846;   // M_PI, which src/darcy.cuh uses
+
+inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// darcy.cuh:146-157 d_idx
+__device__ __forceinline__ uint32_t d_idx(const DarcyArgs &D, int x, int y, int z)
+{
+    return (uint32_t)(x + 1) + (uint32_t)(D.nx + 2) * (uint32_t)(y + 1) +
+           (uint32_t)(D.nx + 2) * (uint32_t)(D.ny + 2) * (uint32_t)(z + 1);
+}
+
+// Cell c of the interior (x fastest) as coordinates.
+__device__ __forceinline__ bool cell_of(const DarcyArgs &D, uint32_t c, int &x, int &y, int &z)
+{
+    const uint32_t nxy = (uint32_t)D.nx * (uint32_t)D.ny;
+    if (c >= nxy * (uint32_t)D.nz) return false;
+    z = (int)(c / nxy);
+    const uint32_t r = c - (uint32_t)z * nxy;
+    y = (int)(r / (uint32_t)D.nx);
+    x = (int)(r - (uint32_t)y * (uint32_t)D.nx);
+    return true;
+}
+
+// The correctly rounded r^3 and r^2: the rounding error of each product is
+// kept exactly by an FMA and added before the last rounding.
+__device__ __forceinline__ double cube_rn(double r)
+{
+    const double p = __dmul_rn(r, r);
+    const double e = __fma_rn(r, r, -p);
+    const double hi = __dmul_rn(p, r);
+    const double lo = __fma_rn(p, r, -hi);
+    return __dadd_rn(hi, __fma_rn(e, r, lo));
+}
+
+// darcy.cuh:346-349 sphereVolume
+__device__ __forceinline__ double sphere_volume(double r)
+{
+    const double c = 4.0 / 3.0 * DARCY_PI;
+    return c * cube_rn(r);
+}
+
+// darcy.cuh:356-385 weight / weightDist, of the vector between the points
+__device__ __forceinline__ double weight_dist(d3 x, double dx, double dy, double dz)
+{
+    const d3 dist = mk(fabs(x.x), fabs(x.y), fabs(x.z));
+    if (dist.x < dx && dist.y < dy && dist.z < dz)
+        return (1.0 - dist.x / dx) * (1.0 - dist.y / dy) * (1.0 - dist.z / dz);
+    return 0.0;
+}
+
+__device__ __forceinline__ d3 ld3(const double *p) { return mk(p[0], p[1], p[2]); }
+__device__ __forceinline__ void st3(double *p, d3 v)
+{
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+}
+
+// darcy.cuh:212-285 setDarcyGhostNodes for cell (x, y, z) holding val (M
+// doubles): the ghost cells that copy this cell.
+template <int M>
+__device__ __forceinline__ void put_ghosts(const DarcyArgs &D, double *f, int x, int y, int z,
+                                           const double *val)
+{
+    const SphDarcy &P = D.prm;
+    const int nx = D.nx, ny = D.ny, nz = D.nz;
+    auto put = [&](int X, int Y, int Z) {
+        double *o = f + (size_t)M * d_idx(D, X, Y, Z);
+#pragma unroll
+        for (int m = 0; m < M; ++m) o[m] = val[m];
+    };
+    if (x == 0 && P.bc_xn == 0) put(-1, y, z);
+    if (x == 1 && P.bc_xn == 1) put(-1, y, z);
+    if (x == 0 && P.bc_xn == 2) put(nx, y, z);
+    if (x == nx - 1 && P.bc_xp == 0) put(nx, y, z);
+    if (x == nx - 2 && P.bc_xp == 1) put(nx, y, z);
+    if (x == nx - 1 && P.bc_xp == 2) put(-1, y, z);
+    if (y == 0 && P.bc_yn == 0) put(x, -1, z);
+    if (y == 1 && P.bc_yn == 1) put(x, -1, z);
+    if (y == 0 && P.bc_yn == 2) put(x, ny, z);
+    if (y == ny - 1 && P.bc_yp == 0) put(x, ny, z);
+    if (y == ny - 2 && P.bc_yp == 1) put(x, ny, z);
+    if (y == ny - 1 && P.bc_yp == 2) put(x, -1, z);
+    if (z == 0 && P.bc_bot == 0) put(x, y, -1);
+    if (z == 1 && P.bc_bot == 1) put(x, y, -1);
+    if (z == 0 && P.bc_bot == 2) put(x, y, nz);
+    if (z == nz - 1 && P.bc_top == 0) put(x, y, nz);
+    if (z == nz - 2 && P.bc_top == 1) put(x, y, nz);
+    if (z == nz - 1 && P.bc_top == 2) put(x, y, -1);
+}
+
+// Whether this step updates the fluid (set by k_darcy_begin).
+__device__ __forceinline__ bool fluid_step(const DarcyArgs &D) { return D.st->active != 0u; }
+
+// ------------------------------------------------------------ every step
+
+// device.cu:1901-1904 (wall0_iz from the host copy of wall 0) and the
+// choice of the fluid-update steps (iter % ndem == 0)
+__global__ void k_darcy_begin(StepArgs A, DarcyArgs D)
+{
+    const DevBox &B = A.boxes[0];
+    DarcyState *s = D.st;
+    if (B.nw > 0 && (B.wmode[0] == 1 || B.wmode[0] == 3))
+        s->wall0_iz = (uint32_t)(s->wall_w_host / (B.L[2] / B.num[2]));
+    s->active = (B.iter % D.prm.ndem) == 0 ? 1u : 0u;
+}
+
+// setDarcyGhostNodes for M-double fields: one thread per interior cell
+template <int M>
+__global__ void k_darcy_ghost(DarcyArgs D, double *f, int gated)
+{
+    if (gated && !fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    double val[M];
+    const double *src = f + (size_t)M * d_idx(D, x, y, z);
+#pragma unroll
+    for (int m = 0; m < M; ++m) val[m] = src[m];
+    put_ghosts<M>(D, f, x, y, z, val);
+}
+
+// darcy.cuh:1101-1157 findDarcyPressureGradient (and :1535-1593
+// findDarcyPermeabilityGradients): central differences
+__global__ void k_darcy_grad(DarcyArgs D, const double *f, double *g, int gated)
+{
+    if (gated && !fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    const double xn = f[d_idx(D, x - 1, y, z)], xp = f[d_idx(D, x + 1, y, z)];
+    const double yn = f[d_idx(D, x, y - 1, z)], yp = f[d_idx(D, x, y + 1, z)];
+    const double zn = f[d_idx(D, x, y, z - 1)], zp = f[d_idx(D, x, y, z + 1)];
+    st3(g + 3 * (size_t)d_idx(D, x, y, z),
+        mk((xp - xn) / (D.dx + D.dx), (yp - yn) / (D.dy + D.dy), (zp - zn) / (D.dz + D.dz)));
+}
+
+// darcy.cuh:1160-1318 findDarcyPressureForceLinear, per sphere: the index
+// sums are unsigned as the reference's (a sphere in the bottom layer
+// compares 0xffffffff with wall0_iz - 1)
+__global__ void k_darcy_force(StepArgs A, DarcyArgs D)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.ntot) return;
+    const DevBox &B = A.boxes[0];
+    const SphDarcy &P = D.prm;
+    const uint32_t wall0_iz = D.st->wall0_iz;
+    const double4 x = A.x[i];
+    const d3 x3 = mk(x.x, x.y, x.z);
+    const uint32_t i_x = (uint32_t)floor((x.x - B.origo[0]) / (B.L[0] / B.num[0]));
+    const uint32_t i_y = (uint32_t)floor((x.y - B.origo[1]) / (B.L[1] / B.num[1]));
+    const uint32_t i_z = (uint32_t)floor((x.z - B.origo[2]) / (B.L[2] / B.num[2]));
+    const uint32_t nx = B.num[0], ny = B.num[1], nz = B.num[2];
+    if (!(x.x >= B.origo[0] && x.y >= B.origo[1] && x.z >= B.origo[2]) || i_x >= nx ||
+        i_y >= ny || i_z >= nz) {
+        // a sphere outside the grid (the reference reads past its arrays):
+        // no pressure force
+        raise_flag(A.err, SPH_ERR_OUT_OF_GRID);
+        D.f_p[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        return;
+    }
+    const double dx = B.L[0] / nx, dy = B.L[1] / ny, dz = B.L[2] / nz;
+    const d3 X = mk(i_x * dx + 0.5 * dx, i_y * dy + 0.5 * dy, i_z * dz + 0.5 * dz);
+    d3 grad_p = mk(0., 0., 0.);
+    for (int d_iz = -1; d_iz < 2; d_iz++)
+        for (int d_iy = -1; d_iy < 2; d_iy++)
+            for (int d_ix = -1; d_ix < 2; d_ix++) {
+                const int ix_n = (int)(i_x + (uint32_t)d_ix);
+                const int iy_n = (int)(i_y + (uint32_t)d_iy);
+                const int iz_n = (int)(i_z + (uint32_t)d_iz);
+                d3 gpi = ld3(D.grad_p + 3 * (size_t)d_idx(D, ix_n, iy_n, iz_n));
+                if ((ix_n == -1 && iy_n == -1) || (ix_n == -1 && iz_n == -1) ||
+                    (iy_n == -1 && iz_n == -1) || (ix_n == (int)nx && iy_n == (int)ny) ||
+                    (ix_n == (int)nx && iz_n == (int)nz) || (iy_n == (int)ny && iz_n == (int)nz) ||
+                    (ix_n == (int)nx && iy_n == -1) || (ix_n == (int)nx && iz_n == -1) ||
+                    (iy_n == (int)ny && ix_n == -1) || (iy_n == (int)ny && iz_n == -1) ||
+                    (iz_n == (int)nz && ix_n == -1) || (iz_n == (int)nz && iy_n == -1))
+                    gpi = mk(0., 0., 0.);
+                if (P.bc_top == 0 && i_z + (uint32_t)d_iz >= wall0_iz - 1u) gpi.z = 0.0;
+                const d3 n = mk(dx * d_ix, dy * d_iy, dz * d_iz);
+                const double w = weight_dist(vsub(x3, vadd(X, n)), dx, dy, dz);
+                grad_p = vadd(grad_p, smul(w, gpi));
+            }
+    const double v = sphere_volume(x.w);
+    d3 f_p = vsub(muls(smul(-1.0, grad_p), v), smul(P.rho_f * v, mk(B.P.g[0], B.P.g[1], B.P.g[2])));
+    if (P.bc_top == 0 && i_z >= wall0_iz) f_p.z = 0.0;
+    const double4 F = A.force[i];
+    A.force[i] = make_double4(F.x + f_p.x, F.y + f_p.y, F.z + f_p.z, F.w + 0.0);
+    D.f_p[i] = make_double4(f_p.x, f_p.y, f_p.z, 0.0);
+}
+
+// ------------------------------------------------- the fluid update steps
+
+// darcy.cuh:392-730 findDarcyPorositiesLinear: per cell, the solid volume
+// of the spheres of the 27 cells around it under the trilinear hat centred
+// on the cell, now and after an Euler step of the positions; the
+// volume-weighted mean sphere velocity.  Spheres in sorted order.
+__global__ void k_darcy_porosity(StepArgs A, DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    const DevBox &B = A.boxes[0];
+    const uint32_t cellidx = d_idx(D, x, y, z);
+    if (A.ntot == 0) {
+        D.phi[cellidx] = 0.9;
+        D.dphi[cellidx] = 0.0;
+        return;
+    }
+    const double dx = D.dx, dy = D.dy, dz = D.dz;
+    const double dt = B.dt;
+    double solid_volume = 0.0, solid_volume_new = 0.0;
+    const d3 X = mk(x * dx + 0.5 * dx, y * dy + 0.5 * dy, z * dz + 0.5 * dz);
+    d3 vp_avg_num = mk(0.0, 0.0, 0.0);
+    double vp_avg_denum = 0.0;
+    const double phi_0 = D.phi[cellidx];
+    for (int z_dim = -1; z_dim < 2; ++z_dim)
+        for (int y_dim = -1; y_dim < 2; ++y_dim)
+            for (int x_dim = -1; x_dim < 2; ++x_dim) {
+                int tx = x + x_dim, ty = y + y_dim, tz = z + z_dim;
+                if (tz == -1) tz = 1;
+                if (B.periodic == 2) {
+                    if (ty == -1) ty = 1;
+                    if (ty == (int)B.num[1]) ty = (int)B.num[1] - 2;
+                }
+                int sx, sy;
+                if (!image_cell(B, tx, ty, tz, sx, sy)) continue;
+                const d3 distmod = shift_vec(B, sx, sy);
+                const uint32_t cell = B.cell_base + (uint32_t)tx + (uint32_t)ty * B.num[0] +
+                                      (B.num[0] * B.num[1]) * (uint32_t)tz;
+                const uint32_t start = A.cell_off[cell], end = start + A.cell_count[cell];
+                for (uint32_t a = start; a < end; ++a) {
+                    double4 xr = A.xs[a];
+                    const double4 vv = A.vs[a];
+                    d3 dist = vadd(mk(X.x - xr.x, X.y - xr.y, X.z - xr.z), distmod);
+                    const double sw = weight_dist(dist, dx, dy, dz);
+                    const double vol_p = sphere_volume(xr.w);
+                    solid_volume += sw * vol_p;
+                    vp_avg_num = vadd(vp_avg_num, smul(sw * vol_p, mk(vv.x, vv.y, vv.z)));
+                    vp_avg_denum += sw * vol_p;
+                    xr.x += vv.x * dt;
+                    xr.y += vv.y * dt;
+                    xr.z += vv.z * dt;
+                    dist = vadd(mk(X.x - xr.x, X.y - xr.y, X.z - xr.z), distmod);
+                    solid_volume_new += weight_dist(dist, dx, dy, dz) * vol_p;
+                }
+            }
+    double cell_volume = dx * dy * dz;
+    if (z == D.nz - 1) cell_volume *= 0.875;
+    const double phi = fmin(0.9, fmax(0.1, 1.0 - solid_volume / cell_volume));
+    const double phi_new = fmin(0.9, fmax(0.1, 1.0 - solid_volume_new / cell_volume));
+    double dphi;
+    d3 vp_avg;
+    if (B.iter == 0) {
+        dphi = 0.0;
+        vp_avg = mk(0.0, 0.0, 0.0);
+    } else {
+        dphi = 0.5 * (phi_new - phi_0);
+        vp_avg = divs(vp_avg_num, fmax(1.0e-16, vp_avg_denum));
+    }
+    D.phi[cellidx] = phi * D.prm.c_phi;
+    D.dphi[cellidx] = dphi * D.prm.c_phi;
+    st3(D.vp_avg + 3 * (size_t)cellidx, vp_avg);
+}
+
+// darcy.cuh:733-807 copyDarcyPorositiesToEdges, then ...ToBottom
+// (periodic == 2): phi, dphi, div_v_p, vp_avg of the y edge layers from
+// the layer inside each, then of the bottom layer from the layer above
+__device__ __forceinline__ void copy_cell(const DarcyArgs &D, uint32_t w, uint32_t r)
+{
+    D.phi[w] = D.phi[r];
+    D.dphi[w] = D.dphi[r];
+    D.div_v_p[w] = D.div_v_p[r];
+    st3(D.vp_avg + 3 * (size_t)w, ld3(D.vp_avg + 3 * (size_t)r));
+}
+
+__global__ void k_darcy_edges(DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    if (!(y == 0 || y == D.ny - 1)) return;
+    int y_read = 0;
+    if (y == 0) y_read = 1;
+    if (y == D.ny - 1) y_read = D.ny - 2;
+    copy_cell(D, d_idx(D, x, y, z), d_idx(D, x, y_read, z));
+}
+
+__global__ void k_darcy_bottom(DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    if (z != 0) return;
+    copy_cell(D, d_idx(D, x, y, 0), d_idx(D, x, y, 1));
+}
+
+// darcy.cuh:1414-1459 setDarcyTopPressure then setDarcyTopWallPressure:
+// one thread per thread of the reference's launch grid (blocks of
+// 8 x 8 x 8 covering the cells)
+__global__ void k_darcy_top_pressure(DarcyArgs D, int gx, int gy, int gz, int wall_pass)
+{
+    if (!fluid_step(D)) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint32_t)gx * (uint32_t)gy * (uint32_t)gz) return;
+    const int z = (int)(t / ((uint32_t)gx * (uint32_t)gy));
+    const uint32_t r = t - (uint32_t)z * (uint32_t)gx * (uint32_t)gy;
+    const int y = (int)(r / (uint32_t)gx), x = (int)(r - (uint32_t)y * (uint32_t)gx);
+    const DarcyState *s = D.st;
+    const double new_pressure = D.pmod[s->qstep % DARCY_RING];
+    const uint32_t wall0_iz = s->wall0_iz;
+    if (!wall_pass) {
+        if ((x < D.nx && y < D.ny && z == D.nz - 1) || (uint32_t)z == wall0_iz) {
+            const uint32_t k = d_idx(D, x, y, z);
+            if (k < D.ncell) D.p[k] = new_pressure;
+        }
+    } else if (x < D.nx && y < D.ny && (uint32_t)z == wall0_iz) {
+        D.p[d_idx(D, x, y, z)] = new_pressure;
+    }
+}
+
+// darcy.cuh:1485-1532 findDarcyPermeabilities (Kozeny-Carman, capped)
+__global__ void k_darcy_perm(DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    const uint32_t ci = d_idx(D, x, y, z);
+    double phi = D.phi[ci];
+    if (phi > 0.9999) phi = 0.9999;
+    const double q = 1.0 - phi;
+    double k = D.prm.k_c * cube_rn(phi) / __dmul_rn(q, q);
+    k = fmin(2.7e-10, k);
+    D.k[ci] = k;
+}
+
+// darcy.cuh:288-329 setDarcyGhostNodesFlux (bc 4 at the bottom or top)
+__global__ void k_darcy_flux(StepArgs A, DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    const SphDarcy &P = D.prm;
+    const double p = D.p[d_idx(D, x, y, z)];
+    const double k = D.k[d_idx(D, x, y, z)];
+    const double dz = A.boxes[0].L[2] / D.nz;
+    double q_z = 0.;
+    if (z == 0) q_z = P.bc_bot_flux;
+    else if (z == D.nz - 1) q_z = P.bc_top_flux;
+    const double p_ghost = -P.mu / k * q_z * dz + p;
+    if (z == 0 && P.bc_bot == 4) D.p[d_idx(D, x, y, -1)] = p_ghost;
+    if (z == D.nz - 1 && P.bc_top == 4) D.p[d_idx(D, x, y, D.nz)] = p_ghost;
+}
+
+// Before the Jacobi loop (device.cu:2193-2254): p_old = p (copyValues)
+// and the ghost layer of p
+__global__ void k_darcy_pre(DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    const uint32_t ci = d_idx(D, x, y, z);
+    const double val = D.p[ci];
+    D.p_old[ci] = val;
+    put_ghosts<1>(D, D.p, x, y, z, &val);
+}
+
+// darcy.cuh:1644-1923 firstDarcySolution and :1926-2226
+// updateDarcySolution: the pressure change of the diffusion term (harmonic
+// means of k across the faces) and of the porosity forcing, zero at
+// Dirichlet boundaries, above the wall and in cells of constant pressure
+__device__ double darcy_dp(const DarcyArgs &D, double dt, int x, int y, int z)
+{
+    const SphDarcy &P = D.prm;
+    const int nx = D.nx, ny = D.ny, nz = D.nz;
+    const double dx = D.dx, dy = D.dy, dz = D.dz;
+    const uint32_t ci = d_idx(D, x, y, z);
+    const double phi_xn = D.phi[d_idx(D, x - 1, y, z)], phi = D.phi[ci];
+    const double phi_xp = D.phi[d_idx(D, x + 1, y, z)];
+    const double phi_yn = D.phi[d_idx(D, x, y - 1, z)], phi_yp = D.phi[d_idx(D, x, y + 1, z)];
+    const double phi_zn = D.phi[d_idx(D, x, y, z - 1)], phi_zp = D.phi[d_idx(D, x, y, z + 1)];
+    const double dphi = D.dphi[ci];
+    const d3 vp_avg = ld3(D.vp_avg + 3 * (size_t)ci);
+    const int p_constant = D.p_constant[ci];
+    const double *pf = D.p;
+    double p_xn = pf[d_idx(D, x - 1, y, z)];
+    const double p = pf[ci];
+    double p_xp = pf[d_idx(D, x + 1, y, z)];
+    double p_yn = pf[d_idx(D, x, y - 1, z)], p_yp = pf[d_idx(D, x, y + 1, z)];
+    double p_zn = pf[d_idx(D, x, y, z - 1)], p_zp = pf[d_idx(D, x, y, z + 1)];
+    const double k_xn = D.k[d_idx(D, x - 1, y, z)], k = D.k[ci];
+    const double k_xp = D.k[d_idx(D, x + 1, y, z)];
+    const double k_yn = D.k[d_idx(D, x, y - 1, z)], k_yp = D.k[d_idx(D, x, y + 1, z)];
+    const double k_zn = D.k[d_idx(D, x, y, z - 1)], k_zp = D.k[d_idx(D, x, y, z + 1)];
+    if (x == 0 && P.bc_xn == 1) p_xn = p;
+    if (x == nx - 1 && P.bc_xp == 1) p_xp = p;
+    if (y == 0 && P.bc_yn == 1) p_yn = p;
+    if (y == ny - 1 && P.bc_yp == 1) p_yp = p;
+    if (z == 0 && P.bc_bot == 1) p_zn = p;
+    if (z == nz - 1 && P.bc_top == 1) p_zp = p;
+    const d3 grad_phi = mk((phi_xp - phi_xn) / (dx + dx), (phi_yp - phi_yn) / (dy + dy),
+                           (phi_zp - phi_zn) / (dz + dz));
+    const double div_k_grad_p =
+        (2. * k_xp * k / (k_xp + k) * (p_xp - p) / dx - 2. * k_xn * k / (k_xn + k) * (p - p_xn) / dx) / dx +
+        (2. * k_yp * k / (k_yp + k) * (p_yp - p) / dy - 2. * k_yn * k / (k_yn + k) * (p - p_yn) / dy) / dy +
+        (2. * k_zp * k / (k_zp + k) * (p_zp - p) / dz - 2. * k_zn * k / (k_zn + k) * (p - p_zn) / dz) / dz;
+    const double ndt = P.ndem * dt;
+    double dp = ndt / (P.beta_f * phi * P.mu) * div_k_grad_p -
+                (ndt / (P.beta_f * phi * (1.0 - phi))) * (dphi / ndt + dot(vp_avg, grad_phi));
+    if ((P.bc_bot == 0 && z == 0) || (P.bc_top == 0 && z == nz - 1) ||
+        ((uint32_t)z >= D.st->wall0_iz && P.bc_top == 0) || (P.bc_xn == 0 && x == 0) ||
+        (P.bc_xp == 0 && x == nx - 1) || (P.bc_yn == 0 && y == 0) ||
+        (P.bc_yp == 0 && y == nx - 1) || p_constant == 1)
+        dp = 0.0;
+    return dp;
+}
+
+__global__ void k_darcy_first(StepArgs A, DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    D.dp_expl[d_idx(D, x, y, z)] = darcy_dp(D, A.boxes[0].dt, x, y, z);
+}
+
+// The start of the Jacobi loop: the iteration count, the residual
+// maximum, and the loop's first condition (run when this step updates the
+// fluid and maxiter > 0).
+template <bool GRAPH>
+__global__ void k_darcy_loop_begin(DarcyArgs D, cudaGraphConditionalHandle hc)
+{
+    DarcyState *s = D.st;
+    s->nijac = 0;
+    s->maxnorm = 0ull;
+    s->nan = 0u;
+    s->go = (s->active && D.prm.maxiter > 0) ? 1u : 0u;
+    if (GRAPH) cudaGraphSetConditional(hc, s->go);
+}
+
+// One Jacobi update (updateDarcySolution): p_new and the normalised
+// residual; every tenth iteration (src/debug.h:16 nijacnorm) the largest
+// |residual| over the cells goes to the state (as the bits of a
+// non-negative double, which order as the values do), a NaN to its flag.
+__global__ void k_darcy_update(StepArgs A, DarcyArgs D)
+{
+    int x, y, z;
+    const bool in = cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z);
+    DarcyState *s = D.st;
+    const bool check = (s->nijac % 10u) == 0u;
+    double r = 0.0;
+    if (in) {
+        const uint32_t ci = d_idx(D, x, y, z);
+        const double dp_impl = darcy_dp(D, A.boxes[0].dt, x, y, z);
+        const double epsilon = 0.5;
+        const double p = D.p[ci];
+        double p_new = D.p_old[ci] + (1.0 - epsilon) * D.dp_expl[ci] + epsilon * dp_impl;
+        const double theta = 0.05;
+        p_new = p * (1.0 - theta) + p_new * theta;
+        const double res_norm = (p_new - p) / (p + 1.0e-16);
+        D.p_new[ci] = p_new;
+        D.norm[ci] = res_norm;
+        r = fabs(res_norm);
+    }
+    if (!check) return;
+    const bool isnan_r = in && r != r;
+    unsigned long long bits = in && !isnan_r ? (unsigned long long)__double_as_longlong(r) : 0ull;
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long b = __shfl_xor_sync(0xffffffffu, bits, o);
+        bits = b > bits ? b : bits;
+    }
+    const unsigned anynan = __any_sync(0xffffffffu, isnan_r);
+    if ((threadIdx.x & 31) == 0) {
+        if (bits) atomicMax(&s->maxnorm, bits);
+        if (anynan) s->nan = 1u;
+    }
+}
+
+// darcy.cuh:1462-1482 setDarcyTopWallFixedFlow (bc_top == 1): p at
+// z = wall0_iz + 1 from z = wall0_iz - 1, over the reference's launch grid
+// (z < 8 ceil(nz / 8))
+__global__ void k_darcy_fixed_flow(DarcyArgs D, int gz)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nxy = (uint32_t)D.nx * (uint32_t)D.ny;
+    if (t >= nxy) return;
+    const int y = (int)(t / (uint32_t)D.nx), x = (int)(t - (uint32_t)y * (uint32_t)D.nx);
+    const uint32_t z = D.st->wall0_iz + 1u;
+    if (z >= (uint32_t)gz) return;
+    // cells past the padded array (a wall at or above the top of the grid)
+    // are skipped
+    const uint32_t w = d_idx(D, x, y, (int)z), r = d_idx(D, x, y, (int)z - 2);
+    if (w < D.ncell && r < D.ncell) D.p[w] = D.p[r];
+}
+
+// copyValues(p_new -> p) and the ghost layer of the new p (the reference's
+// setDarcyGhostNodes at the start of the next iteration, or after the
+// loop): each cell writes its value and the ghost cells that copy it
+__global__ void k_darcy_copy_ghost(DarcyArgs D)
+{
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    const uint32_t ci = d_idx(D, x, y, z);
+    const double val = D.p_new[ci];
+    D.p[ci] = val;
+    put_ghosts<1>(D, D.p, x, y, z, &val);
+}
+
+// The end of a Jacobi iteration (device.cu:2333-2375): every tenth
+// iteration, stop when the largest residual is within the tolerance (or a
+// residual was NaN: SPH_ERR_NAN); stop after maxiter iterations; log the
+// solve when it stops; set the loop's condition.
+template <bool GRAPH>
+__global__ void k_darcy_check(StepArgs A, DarcyArgs D, cudaGraphConditionalHandle hc)
+{
+    DarcyState *s = D.st;
+    const uint32_t nijac = s->nijac;
+    uint32_t stop = 0, ok = 0;
+    if (nijac % 10u == 0u) {
+        if (s->nan) {
+            raise_flag(A.err, SPH_ERR_NAN);
+            stop = 1;
+        } else if (__longlong_as_double((long long)s->maxnorm) <= D.prm.tolerance) {
+            stop = 1;
+            ok = 1;
+        }
+        s->maxnorm = 0ull;
+    }
+    if (!stop && nijac == D.prm.maxiter - 1u) stop = 1;
+    if (stop) {
+        const unsigned long long h = s->log_head;
+        const uint32_t slot = (uint32_t)(h % SPH_DARCY_LOG);
+        D.log_step[slot] = A.boxes[0].iter + 1;
+        D.log_iters[slot] = nijac;
+        D.log_ok[slot] = ok;
+        s->log_head = h + 1;
+        s->go = 0u;
+    } else {
+        s->nijac = nijac + 1;
+        s->go = 1u;
+    }
+    if (GRAPH) cudaGraphSetConditional(hc, s->go);
+}
+
+// After the loop: dphi zeroed unless an output follows this step
+// (device.cu:2379-2386, the host file clock), then findDarcyVelocities
+// (darcy.cuh:2267-2325) from the pressure whose ghost layer the loop's
+// last copy wrote
+__global__ void k_darcy_post(StepArgs A, DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    int x, y, z;
+    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
+    const uint32_t ci = d_idx(D, x, y, z);
+    if (D.st->filetimeclock + A.boxes[0].dt < D.prm.file_dt) D.dphi[ci] = 0.0;
+    const double *p = D.p;
+    const double xn = p[d_idx(D, x - 1, y, z)], xp = p[d_idx(D, x + 1, y, z)];
+    const double yn = p[d_idx(D, x, y - 1, z)], yp = p[d_idx(D, x, y + 1, z)];
+    const double zn = p[d_idx(D, x, y, z - 1)], zp = p[d_idx(D, x, y, z + 1)];
+    const double k = D.k[ci], phi = D.phi[ci];
+    const d3 grad_p = mk((xp - xn) / (D.dx + D.dx), (yp - yn) / (D.dy + D.dy), (zp - zn) / (D.dz + D.dz));
+    st3(D.v + 3 * (size_t)ci, divs(smul(-k / D.prm.mu, grad_p), phi));
+}
+
+// After the step's wall stage (device.cu:2537, 2569, 2672, 805): the file
+// clock; at an output the host copy of wall 0 is refreshed; the step count
+__global__ void k_darcy_tick(StepArgs A, DarcyArgs D)
+{
+    const DevBox &B = A.boxes[0];
+    DarcyState *s = D.st;
+    s->filetimeclock += B.dt;
+    if (s->filetimeclock >= D.prm.file_dt) {
+        s->filetimeclock = 0.0;
+        if (B.nw > 0) s->wall_w_host = B.wnx[0][3];
+    }
+    s->qstep += 1;
+}
+
+static inline void record(cudaEvent_t ev, cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal);
+    else cudaEventRecord(ev, st);
+}
+
+static inline void mark(Prof *prof, cudaStream_t st, const char *name)
+{
+    if (!prof || prof->n >= Prof::MAX) return;
+    prof->name[prof->n] = name;
+    record(prof->ev[prof->n + 1], st);
+    prof->n++;
+}
+
+// The kernels of one Jacobi iteration.
+template <bool GRAPH>
+void jacobi_body(const StepArgs &A, const DarcyArgs &D, cudaStream_t st,
+                 cudaGraphConditionalHandle hc, uint64_t &nl)
+{
+    const uint32_t ncells = (uint32_t)D.nx * D.ny * D.nz;
+    const unsigned gc = blocks_for(ncells, DARCY_THREADS);
+    k_darcy_update<<<gc, DARCY_THREADS, 0, st>>>(A, D);
+    nl += 1;
+    if (D.prm.bc_top == 1) {
+        const int gz = (D.nz + 7) / 8 * 8;
+        k_darcy_fixed_flow<<<blocks_for((uint64_t)D.nx * D.ny, DARCY_THREADS), DARCY_THREADS, 0, st>>>(D, gz);
+        nl += 1;
+    }
+    if (D.prm.bc_bot == 4 || D.prm.bc_top == 4) {
+        k_darcy_flux<<<gc, DARCY_THREADS, 0, st>>>(A, D);
+        nl += 1;
+    }
+    k_darcy_copy_ghost<<<gc, DARCY_THREADS, 0, st>>>(D);
+    k_darcy_check<GRAPH><<<1, 1, 0, st>>>(A, D, hc);
+    nl += 2;
+}
+
+}  // namespace
+
+int launch_darcy(const StepArgs &A, const DarcyArgs &D, const StepConfig &cfg, cudaStream_t st,
+                 uint64_t *launches, Prof *prof)
+{
+    uint64_t nl = 0;
+    const SphDarcy &P = D.prm;
+    const uint32_t ncells = (uint32_t)D.nx * D.ny * D.nz;
+    const unsigned gc = blocks_for(ncells, DARCY_THREADS);
+    k_darcy_begin<<<1, 1, 0, st>>>(A, D);
+    nl += 1;
+    if (A.ntot > 0) {
+        k_darcy_ghost<1><<<gc, DARCY_THREADS, 0, st>>>(D, D.p, 0);
+        k_darcy_grad<<<gc, DARCY_THREADS, 0, st>>>(D, D.p, D.grad_p, 0);
+        k_darcy_ghost<3><<<gc, DARCY_THREADS, 0, st>>>(D, D.grad_p, 0);
+        k_darcy_force<<<blocks_for(A.ntot, DARCY_THREADS), DARCY_THREADS, 0, st>>>(A, D);
+        mark(prof, st, "k_darcy_force");
+        nl += 4;
+    }
+    // the fluid update: every kernel returns at once unless iter % ndem == 0
+    k_darcy_porosity<<<gc, DARCY_THREADS, 0, st>>>(A, D);
+    nl += 1;
+    if (D.periodic == 2) {
+        k_darcy_edges<<<gc, DARCY_THREADS, 0, st>>>(D);
+        k_darcy_bottom<<<gc, DARCY_THREADS, 0, st>>>(D);
+        nl += 2;
+    }
+    if (D.pmod) {
+        const int gx = (D.nx + 7) / 8 * 8, gy = (D.ny + 7) / 8 * 8, gz = (D.nz + 7) / 8 * 8;
+        const unsigned gt = blocks_for((uint64_t)gx * gy * gz, DARCY_THREADS);
+        k_darcy_top_pressure<<<gt, DARCY_THREADS, 0, st>>>(D, gx, gy, gz, 0);
+        k_darcy_top_pressure<<<gt, DARCY_THREADS, 0, st>>>(D, gx, gy, gz, 1);
+        nl += 2;
+    }
+    k_darcy_perm<<<gc, DARCY_THREADS, 0, st>>>(D);
+    k_darcy_ghost<1><<<gc, DARCY_THREADS, 0, st>>>(D, D.phi, 1);
+    k_darcy_ghost<1><<<gc, DARCY_THREADS, 0, st>>>(D, D.k, 1);
+    k_darcy_grad<<<gc, DARCY_THREADS, 0, st>>>(D, D.k, D.grad_k, 1);
+    nl += 4;
+    if (P.bc_bot == 4 || P.bc_top == 4) {
+        k_darcy_flux<<<gc, DARCY_THREADS, 0, st>>>(A, D);
+        nl += 1;
+    }
+    k_darcy_pre<<<gc, DARCY_THREADS, 0, st>>>(D);
+    k_darcy_first<<<gc, DARCY_THREADS, 0, st>>>(A, D);
+    nl += 2;
+    mark(prof, st, "k_darcy_fluid");
+    // the Jacobi loop: a WHILE node under capture, a host loop otherwise
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return SPH_ERR_CUDA;
+    if (cs == cudaStreamCaptureStatusActive) {
+        if (!cfg.side) return SPH_ERR_CUDA;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        cudaGraphConditionalHandle hc;
+        if (cudaGraphConditionalHandleCreate(&hc, g, 0u, cudaGraphCondAssignDefault) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        k_darcy_loop_begin<true><<<1, 1, 0, st>>>(D, hc);
+        nl += 1;
+        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = hc;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, g, deps, nd, &np) != cudaSuccess) return SPH_ERR_CUDA;
+        if (cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) !=
+            cudaSuccess)
+            return SPH_ERR_CUDA;
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        if (cudaStreamBeginCaptureToGraph(cfg.side, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return SPH_ERR_CUDA;
+        uint64_t nb = 0;
+        jacobi_body<true>(A, D, cfg.side, hc, nb);
+        cudaGraph_t done = nullptr;
+        if (cudaStreamEndCapture(cfg.side, &done) != cudaSuccess) return SPH_ERR_CUDA;
+        nl += 1;
+    } else {
+        cudaGraphConditionalHandle none = 0;
+        k_darcy_loop_begin<false><<<1, 1, 0, st>>>(D, none);
+        nl += 1;
+        for (;;) {
+            uint32_t go = 0;
+            if (cudaMemcpyAsync(&go, &D.st->go, sizeof go, cudaMemcpyDeviceToHost, st) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return SPH_ERR_CUDA;
+            if (!go) break;
+            jacobi_body<false>(A, D, st, none, nl);
+        }
+    }
+    mark(prof, st, "k_darcy_jacobi");
+    k_darcy_post<<<gc, DARCY_THREADS, 0, st>>>(A, D);
+    nl += 1;
+    mark(prof, st, "k_darcy_post");
+    if (launches) *launches += nl;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "sphere_b200: Darcy launch failed: %s\n", cudaGetErrorString(e));
+        return SPH_ERR_CUDA;
+    }
+    return SPH_OK;
+}
+
+void launch_darcy_tick(const StepArgs &A, const DarcyArgs &D, cudaStream_t st)
+{
+    k_darcy_tick<<<1, 1, 0, st>>>(A, D);
+}
+
+}  // namespace sph

@@ -156,6 +156,39 @@ struct OverlapArgs {
 // STEP_TAIL: the wall stage alone.
 enum StepPhase { STEP_WHOLE = 0, STEP_HEAD = 1, STEP_OVERLAP = 2, STEP_TAIL = 3 };
 
+// The Darcy coupling (fluid == 1, cfd_solver == 1, sph_darcy.cu).  Cell
+// fields are padded with one ghost layer on every side, (nx+2)(ny+2)(nz+2)
+// cells indexed (x+1) + (nx+2)(y+1) + (nx+2)(ny+2)(z+1) as the reference's
+// (src/darcy.cpp:64-76); vector fields hold three doubles per cell.
+constexpr uint32_t DARCY_RING = 65536;   // queued top pressures (steps)
+struct DarcyState {
+    double filetimeclock;          // the reference's host file clock
+    double wall_w_host;            // its host copy of walls.nx[0].w (refreshed at outputs)
+    unsigned long long maxnorm;    // bits of the largest |norm| of a checked iteration
+    unsigned long long qstep;      // steps run since sph_darcy_set (top-pressure ring index)
+    unsigned long long log_head;   // Jacobi log entries written
+    uint32_t wall0_iz;             // src/device.cu:1001, 1903
+    uint32_t active;               // this step runs the fluid update (iter % ndem == 0)
+    uint32_t nijac;                // Jacobi iteration of the running solve
+    uint32_t go;                   // the solve continues (the loop's condition)
+    uint32_t nan;                  // a checked residual was NaN
+};
+struct DarcyArgs {
+    SphDarcy prm;
+    int periodic;                  // grid.periodic of the box
+    int nx, ny, nz;
+    double dx, dy, dz;
+    uint32_t ncell;                // padded cells
+    double *p, *p_old, *p_new, *dp_expl, *phi, *dphi, *norm, *k, *div_v_p;
+    double *v, *vp_avg, *grad_k, *grad_p;
+    int32_t *p_constant;
+    double4 *f_p;
+    DarcyState *st;
+    const double *pmod;            // top pressure per queued step (DARCY_RING), null: no modulation
+    uint64_t *log_step;            // the Jacobi log, a ring of SPH_DARCY_LOG entries
+    uint32_t *log_iters, *log_ok;
+};
+
 struct StepConfig {
     int lenmode;
     bool unfused;     // some box has a shear-stress (wmode 3) top wall
@@ -166,6 +199,7 @@ struct StepConfig {
     int phase = STEP_WHOLE;
     cudaStream_t side = nullptr;                       // STEP_OVERLAP only
     cudaEvent_t fork = nullptr, join = nullptr;        // STEP_OVERLAP only
+    const DarcyArgs *darcy = nullptr;                  // the Darcy coupling, null: off
 };
 
 // Per-kernel timing of an un-graphed step (the counterpart of the
@@ -177,6 +211,13 @@ struct Prof {
     const char *name[MAX];
     int n = 0;
 };
+
+// The Darcy part of a step (between interact and integrate; needs
+// cfg.side under stream capture for the Jacobi loop's body) and the file
+// clock after the step's wall stage (sph_darcy.cu).
+int launch_darcy(const StepArgs &A, const DarcyArgs &D, const StepConfig &cfg, cudaStream_t st,
+                 uint64_t *launches, Prof *prof);
+void launch_darcy_tick(const StepArgs &A, const DarcyArgs &D, cudaStream_t st);
 
 // Enqueue one step on `st`; adds the number of kernel launches to
 // *launches.  Capturable in a CUDA graph (events in prof become event-record

@@ -985,6 +985,11 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
             interact(A, st, gi, false, cfg.lenmode,
                      cfg.variant == SPLIT_VARIANT ? 1 : cfg.variant);
             mark(prof, st, "k_interact");
+            if (cfg.darcy) {
+                // device.cu:1891-2419, between interact and integrate
+                const int ds = launch_darcy(A, *cfg.darcy, cfg, st, &nl, prof);
+                if (ds != SPH_OK) return ds;
+            }
             k_shear_stress<<<blocks_for(A.ntot, 256), 256, 0, st>>>(A);
             k_block_sums<<<A.npartials, 256, 0, st>>>(A, A.tau_pp, A.tau_partial, 1);
             k_tau_final<<<A.nboxes, BOX_THREADS, 0, st>>>(A);
@@ -996,7 +1001,16 @@ int launch_step_with(const StepArgs &A, const StepConfig &cfg, cudaStream_t st,
     } else if (overlap) {
         cudaStreamWaitEvent(st, cfg.join, 0);
     }
+    if (A.ntot == 0 && cfg.darcy) {
+        // a fluid without spheres (the reference's pure-fluid runs)
+        const int ds = launch_darcy(A, *cfg.darcy, cfg, st, &nl, prof);
+        if (ds != SPH_OK) return ds;
+    }
     if (cfg.phase == STEP_WHOLE) wall_stage(st);
+    if (cfg.darcy) {
+        launch_darcy_tick(A, *cfg.darcy, st);
+        nl += 1;
+    }
     if (launches) *launches += nl;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

@@ -145,12 +145,70 @@ class Stepper(object):
             pass
 
     def upload(self):
+        """Copy the sims' state to the device; a sim with a Darcy fluid also
+        starts its fluid (sph_darcy_set), as the reference sets it up at the
+        start of a run."""
         self.hp = HostParticles.from_sims(self.sims)
         self.hb = HostBonds.from_sims(self.sims)
         ps = self.hp.struct()
         bs = self.hb.struct()
         self._check(self.lib.sph_upload(self.h, C.byref(ps), C.byref(bs) if self.nbonds else None),
                     "sph_upload")
+        if len(self.sims) == 1 and getattr(self.sims[0], "fluid", False):
+            self.darcy_set(self.sims[0])
+
+    # ------------------------------------------------------------ Darcy
+    def darcy_set(self, s):
+        """Start the Darcy coupling from the fluid of sim s (sph_darcy_set).
+        dphi goes in as the solver holds it, dphi * time_dt * ndem (what the
+        reference's writer puts in its input file)."""
+        self._darcy = _abi.darcy_from_sim(s)
+        self._num = [int(v) for v in s.num]
+        f = lambda a, t=numpy.float64: numpy.ascontiguousarray(_abi.cells_to_file(numpy.asarray(a, dtype=t)))
+        p = f(s.p_f)
+        v = f(s.v_f)
+        phi = f(s.phi)
+        dphi = f(numpy.asarray(s.dphi, dtype=numpy.float64) * s.time_dt * s.ndem)
+        pc = f(s.p_f_constant, numpy.int32)
+        fp = numpy.ascontiguousarray(numpy.asarray(s.f_p, dtype=numpy.float64).reshape(-1, 3))
+        self._check(self.lib.sph_darcy_set(self.h, C.byref(self._darcy), _abi.dptr(p), _abi.dptr(v),
+                                           _abi.dptr(phi), _abi.dptr(dphi),
+                                           pc.ctypes.data_as(C.POINTER(C.c_int32)),
+                                           _abi.dptr(fp) if fp.size else None),
+                    "sph_darcy_set")
+
+    def darcy_get(self):
+        """The fluid after the steps so far, in a sim's [x, y, z](, 3)
+        layout: p_f, v_f, phi, dphi (as the solver holds it, per fluid
+        step), k and f_p ([np, 3])."""
+        num = self._num
+        ncell = num[0] * num[1] * num[2]
+        p = numpy.empty(ncell)
+        v = numpy.empty(ncell * 3)
+        phi = numpy.empty(ncell)
+        dphi = numpy.empty(ncell)
+        k = numpy.empty(ncell)
+        fp = numpy.empty((self.ntot, 3))
+        self._check(self.lib.sph_darcy_get(self.h, _abi.dptr(p), _abi.dptr(v), _abi.dptr(phi),
+                                           _abi.dptr(dphi), _abi.dptr(k),
+                                           _abi.dptr(fp) if self.ntot else None), "sph_darcy_get")
+        return {"p_f": _abi.cells_from_file(p, num), "v_f": _abi.cells_from_file(v, num, 3),
+                "phi": _abi.cells_from_file(phi, num), "dphi_raw": _abi.cells_from_file(dphi, num),
+                "k": _abi.cells_from_file(k, num), "f_p": fp}
+
+    def darcy_log(self):
+        """The Jacobi solves since the last call: (step, iterations,
+        converged) arrays (sph_darcy_log)."""
+        cap = _abi.DARCY_LOG
+        step = numpy.zeros(cap, dtype=numpy.uint64)
+        it = numpy.zeros(cap, dtype=numpy.uint32)
+        ok = numpy.zeros(cap, dtype=numpy.uint32)
+        n = C.c_uint32(0)
+        self._check(self.lib.sph_darcy_log(self.h, step.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                           _abi.uptr(it), _abi.uptr(ok), cap, C.byref(n)),
+                    "sph_darcy_log")
+        k = int(n.value)
+        return step[:k].copy(), it[:k].copy(), ok[:k].copy()
 
     def step(self, nsteps=1, raise_on_error=True):
         st = self.lib.sph_step(self.h, int(nsteps))
@@ -437,6 +495,13 @@ class Stepper(object):
             _abi.sim_from_box(s, b)
             o += k
             ob += kb
+        if state is None and len(self.sims) == 1 and getattr(self.sims[0], "fluid", False):
+            s = self.sims[0]
+            f = self.darcy_get()
+            s.p_f, s.v_f, s.phi, s.f_p = f["p_f"], f["v_f"], f["phi"], f["f_p"]
+            # as a sim reading the output file holds it (per unit time)
+            s.dphi = f["dphi_raw"] / (s.time_dt * s.ndem)
+            self.dphi_raw = f["dphi_raw"]
         return self.sims
 
 
@@ -524,6 +589,8 @@ def run_sim(s, root="..", verbose=True, device=-1, precision="fp64", length="ref
     if int(s.time_step_count[0]) == 0:
         binio.write_bin(os.path.join(outdir, s.sid + ".output00000.bin"), s)
     st = Stepper([s], precision=precision, length=length, device=device)
+    if getattr(s, "fluid", False):
+        return _run_fluid(st, s, outdir, status_path, verbose)
     try:
         st.upload()
         _write_status(status_path, s)
@@ -587,90 +654,21 @@ def run_sim(s, root="..", verbose=True, device=-1, precision="fp64", length="ref
         st.close()
 
 
-# src/sphere.cpp:145-345 checkValues (host side, before any device work)
-def check_values(s):
-    if int(s.nd[0]) != 3:
-        return "Error: nd = %d, ND = 3" % int(s.nd[0])
-    if s.time_current[0] > s.time_total[0] or s.time_current[0] < 0.0:
-        return "Error: time.current = %g s, time.total = %g s" % (s.time_current[0], s.time_total[0])
-    if (numpy.asarray(s.origo) < 0.0).any():
-        return "Error: Negative values in grid.origo are known to cause problems."
-    if (numpy.asarray(s.L) <= 0.0).any():
-        return "Error: grid.L must be positive"
-    if (numpy.asarray(s.num) <= 0).any():
-        return "Error: grid.num must be positive"
-    if s.periodic[0] == 2 and s.num[0] < 3:
-        return "Error: When 1st dimension boundaries are periodic, there must be at least 3 cells in that dimension."
-    if s.periodic[0] == 1 and (s.num[0] < 3 or s.num[1] < 3):
-        return ("Error: When 1st and 2nd dimension boundaries are periodic, there must be at "
-                "least 3 cells in each of those dimensions.")
-    n = int(s.np[0])
-    if n:
-        if (s.radius <= 0.0).any():
-            return "Error: Particle %d has a radius of %g m." % (int(numpy.argmax(s.radius <= 0.0)),
-                                                                  float(s.radius.min()))
-        if numpy.isnan(s.x).any() or numpy.isnan(s.vel).any() or numpy.isnan(s.fixvel).any():
-            return "Error: NaN particle position or velocity"
-        out = (s.x < numpy.asarray(s.origo)).any(axis=1) | (s.x > numpy.asarray(s.L)).any(axis=1)
-        if out.any():
-            return "Error: Particle %d is outside of the computational grid" % int(numpy.argmax(out))
-        if s.nw[0] > 0 and s.w_x[0] < max(0.0, float(s.x[:, 2].max())):
-            return "Error: One or more particles have centres above the upper, dynamic wall"
-    if s.k_n[0] <= 0.0:
-        return "Error: k_n = %g N/m" % s.k_n[0]
-    if s.E[0] < 0.0:
-        return "Error: E = %g N/m^3" % s.E[0]
-    if s.rho[0] <= 0.0:
-        return "Error: rho = %g kg/m3" % s.rho[0]
-    return None
+def _run_fluid(st, s, outdir, status_path, verbose):
+    """run() with a Darcy fluid: the output-cadence loop of sph_advance
+    (src/device.cu:1031, 2536-2537, 2569), each output with the fluid fields
+    as the reference's writer stores them (dphi per fluid step), and
+    output/<sid>-conv.log with the reference's lines (src/device.cu:2349-2370:
+    "step iterations" for converged solves at every tenth step and for every
+    solve that did not converge)."""
+    conv = open(os.path.join(outdir, s.sid + "-conv.log"), "w")
 
+    def log():
+        step, iters, ok = st.darcy_log()
+        for a, b, c in zip(step, iters, ok):
+            if (c and (int(a) - 1) % 10 == 0) or not c:
+                conv.write("%d\t%d\n" % (int(a), int(b)))
 
-def report_values(s):
-    """The `--dry` report of src/sphere.cpp:349-466."""
-    print("  - Number of dimensions: nd = %d" % s.nd[0])
-    print("  - Number of particles:  np = %d" % s.np[0])
-    print("  - Compiled for double precision")
-    print("  - Timestep length:      time.dt         = %g s" % s.time_dt[0])
-    print("  - Start at time:        time.current    = %g s" % s.time_current[0])
-    print("  - Total sim. time:      time.total      = %g s" % s.time_total[0])
-    print("  - File output interval: time.file_dt    = %g s" % s.time_file_dt[0])
-    print("  - Start at step count:  time.step_count = %d" % s.time_step_count[0])
-    cm = int(s.contactmodel[0])
-    names = {1: "Linear-elastic-viscous (n), visco-frictional (t)",
-             2: "Linear-elastic-visco-frictional", 3: "Nonlinear-elastic-visco-frictional"}
-    print("  - Contact model: " + names.get(cm, "unknown (%d)" % cm))
-    print("  - Using Young's modulus for contact stiffness" if s.E[0] > 0.01 else
-          "  - Using global value for contact stiffness")
-    print("  - Number of dynamic walls: %d" % s.nw[0])
-    print("  - Grid: %d * %d * %d cells" % tuple(int(v) for v in s.num))
-    print("  - Domain size: %g * %g * %g m" % tuple(float(v) for v in s.L))
-    print("  - No. of particle bonds: %d" % s.nb0[0])
-
-
-def _write_status(path, s):
-    with open(path, "w") as fh:
-        cur = float(s.time_current[0])
-        tot = float(s.time_total[0])
-        fh.write("%2.4e %2.4e %d\n" % (cur, 100.0 * cur / tot if tot else 0.0,
-                                       int(s.time_step_count[0])))
-
-
-def run_sim(s, root="..", verbose=True, device=-1, precision="fp64", length="reference"):
-    """Run `s` to time_total, writing the reference's output files.  Returns
-    0 or the SphStatus of the first failure (as the binary's exit status)."""
-    msg = check_values(s)
-    if msg:
-        print(msg)
-        return 1
-    # the caller's object keeps its input state, as with the reference binary
-    s = copy.deepcopy(s)
-    outdir = os.path.join(root, "output")
-    os.makedirs(outdir, exist_ok=True)
-    status_path = os.path.join(outdir, s.sid + ".status.dat")
-    # device.cu:840-842: output file 0 before the first step
-    if int(s.time_step_count[0]) == 0:
-        binio.write_bin(os.path.join(outdir, s.sid + ".output00000.bin"), s)
-    st = Stepper([s], precision=precision, length=length, device=device)
     try:
         st.upload()
         _write_status(status_path, s)
@@ -680,13 +678,13 @@ def run_sim(s, root="..", verbose=True, device=-1, precision="fp64", length="ref
         ftc = 0.0
         status = 0
         while cur <= total:
-            code, cur, ftc, done = st.advance(total, file_dt, cur, ftc)
+            # at most SPH_DARCY_LOG steps per call, so that no log entry is lost
+            code, cur, ftc, done = st.advance(total, file_dt, cur, ftc, _abi.DARCY_LOG)
+            log()
             if code != 0:
                 status = code
                 if verbose:
                     print("sphere_b200: " + st._msg(st.h))
-                # an overflowing contact list is reported and the run goes on
-                # (the reference ignores it); anything else ends the run
                 if code != _abi.SPH_ERR_NC_OVERFLOW or done == 0:
                     break
             if ftc >= file_dt:
@@ -694,13 +692,13 @@ def run_sim(s, root="..", verbose=True, device=-1, precision="fp64", length="ref
                 s.time_current[0] = cur
                 s.time_step_count[0] += 1
                 binio.write_bin(os.path.join(outdir, "%s.output%05d.bin" %
-                                             (s.sid, int(s.time_step_count[0]))), s)
+                                             (s.sid, int(s.time_step_count[0]))), s,
+                                dphi_raw=st.dphi_raw)
                 _write_status(status_path, s)
                 ftc = 0.0
-        st.to_sims()
-        s.time_current[0] = cur
         if verbose:
             print("  - Last output file number: %d" % int(s.time_step_count[0]))
         return status
     finally:
+        conv.close()
         st.close()

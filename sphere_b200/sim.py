@@ -41,8 +41,6 @@ class sim(object):
     """DEM simulation object (python/sphere.py:33 ``class sim``)."""
 
     def __init__(self, sid='unnamed', np=0, nd=3, nw=0, fluid=False, cfd_solver=0):
-        if fluid:
-            raise NotImplementedError("fluid coupling is outside sphere_b200")
         self.version = numpy.ones(1, dtype=numpy.float64) * VERSION
         self.nd = numpy.ones(1, dtype=numpy.int32) * int(nd)
         self.np = numpy.ones(1, dtype=numpy.uint32) * int(np)
@@ -119,6 +117,171 @@ class sim(object):
         self.bonds_omega_t = numpy.zeros((0, d), dtype=numpy.float64)
         self.fluid = False
         self.color = numpy.zeros(n, dtype=numpy.int32)
+        if fluid:
+            # the Darcy solver's fields (python/sphere.py:310-440); the
+            # Navier-Stokes solver (cfd_solver 0) is not built
+            self.fluid = True
+            self.cfd_solver = numpy.ones(1, dtype=numpy.int32) * int(cfd_solver)
+            self._darcy_defaults(0.0)
+
+    # ------------------------------------------------------------- fluid
+    def _darcy_defaults(self, p):
+        """The Darcy fields with their defaults on the current grid."""
+        num = tuple(int(v) for v in self.num)
+        n = int(self.np[0])
+        self.mu = numpy.zeros(1, dtype=numpy.float64)
+        self.rho_f = numpy.ones(1, dtype=numpy.float64) * 1.0e3
+        self.p_f = numpy.ones(num, dtype=numpy.float64) * p
+        self.v_f = numpy.zeros(num + (int(self.nd[0]),), dtype=numpy.float64)
+        self.phi = numpy.ones(num, dtype=numpy.float64)
+        self.dphi = numpy.zeros(num, dtype=numpy.float64)
+        self.p_mod_A = numpy.zeros(1, dtype=numpy.float64)
+        self.p_mod_f = numpy.zeros(1, dtype=numpy.float64)
+        self.p_mod_phi = numpy.zeros(1, dtype=numpy.float64)
+        for name in ("bc_xn", "bc_xp", "bc_yn", "bc_yp"):
+            setattr(self, name, numpy.ones(1, dtype=numpy.int32) * 2)
+        self.bc_bot = numpy.zeros(1, dtype=numpy.int32)
+        self.bc_top = numpy.zeros(1, dtype=numpy.int32)
+        self.free_slip_bot = numpy.ones(1, dtype=numpy.int32)
+        self.free_slip_top = numpy.ones(1, dtype=numpy.int32)
+        self.bc_bot_flux = numpy.zeros(1, dtype=numpy.float64)
+        self.bc_top_flux = numpy.zeros(1, dtype=numpy.float64)
+        self.p_f_constant = numpy.zeros(num, dtype=numpy.int32)
+        self.tolerance = numpy.array(1.0e-3)
+        self.maxiter = numpy.array(1e4)
+        self.ndem = numpy.array(1)
+        self.c_phi = numpy.ones(1, dtype=numpy.float64)
+        self.f_p = numpy.zeros((n, int(self.nd[0])), dtype=numpy.float64)
+        self.beta_f = numpy.ones(1, dtype=numpy.float64) * 4.5e-10
+        self.k_c = numpy.ones(1, dtype=numpy.float64) * 4.6e-10
+
+    def initFluid(self, mu=8.9e-4, rho=1.0e3, p=0.0, hydrostatic=False, cfd_solver=0):
+        """Fluid arrays and viscosity on the current grid
+        (python/sphere.py:3395).  Only the Darcy solver (cfd_solver = 1) is
+        built here.  With hydrostatic=True the cells below the top wall (or
+        below the top of the grid) get the hydrostatic pressure of the
+        fluid column above them, p at the top."""
+        if int(cfd_solver) != 1:
+            raise NotImplementedError("only the Darcy fluid solver (cfd_solver = 1) is built; "
+                                      "the Navier-Stokes solver (cfd_solver = 0) is not")
+        self.fluid = True
+        self.cfd_solver = numpy.ones(1, dtype=numpy.int32)
+        self._darcy_defaults(p)
+        self.mu = numpy.ones(1, dtype=numpy.float64) * mu
+        self.rho_f = numpy.ones(1, dtype=numpy.float64) * rho
+        if hydrostatic:
+            dz = self.L[2] / self.num[2]
+            if int(self.nw[0]) == 1:
+                wall0_iz = int(self.w_x[0] / (self.L[2] / self.num[2]))
+                self.p_f[:, :, wall0_iz:] = p
+                top = self.w_x[0]
+                layers = numpy.arange(wall0_iz - 1)
+            else:
+                top = self.L[2]
+                layers = numpy.arange(self.num[2] - 1)
+            for iz in layers:
+                depth = top - (dz * iz + 0.5 * dz)
+                self.p_f[:, :, iz] = p + (depth - dz) * rho * -self.g[2]
+
+    def _check_darcy(self, what):
+        if not self.fluid or int(numpy.asarray(self.cfd_solver).ravel()[0]) != 1:
+            raise Exception(what + '() is only relevant for the Darcy solver (cfd_solver = 1)')
+
+    # boundary conditions of the fluid (python/sphere.py:3527-3685):
+    # 0 fixed pressure, 1 no flow, 2 periodic (x, y) / no slip (z), 4 flux
+    def setFluidBottomNoFlow(self):
+        self.bc_bot[0] = 1
+
+    def setFluidBottomNoFlowNoSlip(self):
+        self.bc_bot[0] = 2
+
+    def setFluidBottomFixedPressure(self):
+        self.bc_bot[0] = 0
+
+    def setFluidBottomFixedFlux(self, specific_flux):
+        self.bc_bot[0] = 4
+        self.bc_bot_flux[0] = specific_flux
+
+    def setFluidTopNoFlow(self):
+        self.bc_top[0] = 1
+
+    def setFluidTopNoFlowNoSlip(self):
+        self.bc_top[0] = 2
+
+    def setFluidTopFixedPressure(self):
+        self.bc_top[0] = 0
+
+    def setFluidTopFixedFlux(self, specific_flux):
+        self.bc_top[0] = 4
+        self.bc_top_flux[0] = specific_flux
+
+    def _sides(self, names, code):
+        for name in names:
+            getattr(self, name)[0] = code
+
+    def setFluidXFixedPressure(self):
+        self._sides(("bc_xn", "bc_xp"), 0)
+
+    def setFluidXNoFlow(self):
+        self._sides(("bc_xn", "bc_xp"), 1)
+
+    def setFluidXPeriodic(self):
+        self._sides(("bc_xn", "bc_xp"), 2)
+
+    def setFluidYFixedPressure(self):
+        self._sides(("bc_yn", "bc_yp"), 0)
+
+    def setFluidYNoFlow(self):
+        self._sides(("bc_yn", "bc_yp"), 1)
+
+    def setFluidYPeriodic(self):
+        self._sides(("bc_yn", "bc_yp"), 2)
+
+    def setPermeabilityPrefactor(self, k_c, verbose=False):
+        """Kozeny-Carman prefactor k_c of k = k_c phi^3 / (1 - phi)^2
+        (python/sphere.py:3701)."""
+        self._check_darcy('setPermeabilityPrefactor')
+        self.k_c[0] = k_c
+
+    def setPermeabilityGrainSize(self, verbose=False):
+        """k_c from the mean grain diameter, d^2 / 180 (python/sphere.py:3687)."""
+        self.setPermeabilityPrefactor(numpy.mean(self.radius * 2.0) ** 2.0 / 180.0, verbose)
+
+    def setFluidCompressibility(self, beta_f):
+        self._check_darcy('setFluidCompressibility')
+        self.beta_f[0] = beta_f
+
+    def setFluidViscosity(self, mu):
+        self.mu[0] = mu
+
+    def setFluidDensity(self, rho_f):
+        self.rho_f[0] = rho_f
+
+    def setFluidPressureModulation(self, A, f, phi=0.0, plot=False):
+        """Top pressure p_top + A sin(2 pi f t + phi) (python/sphere.py:6219)."""
+        self.p_mod_A[0] = A
+        self.p_mod_f[0] = f
+        self.p_mod_phi[0] = phi
+
+    def disableFluidPressureModulation(self):
+        self.setFluidPressureModulation(A=0.0, f=0.0)
+
+    def setTolerance(self, tolerance):
+        self.tolerance = numpy.asarray(tolerance)
+
+    def setMaxIterations(self, maxiter):
+        self.maxiter = numpy.asarray(maxiter)
+
+    def setDEMstepsPerCFDstep(self, ndem):
+        self.ndem = numpy.asarray(ndem)
+
+    def findPermeabilities(self):
+        """Cell permeabilities from the porosities as the solver finds them
+        (src/darcy.cuh:1485-1532)."""
+        self._check_darcy('findPermeabilities')
+        phi = numpy.minimum(numpy.asarray(self.phi, dtype=numpy.float64), 0.9999)
+        self.k = numpy.minimum(2.7e-10, self.k_c * phi ** 3 / (1.0 - phi) ** 2)
+        return self.k
 
     # ------------------------------------------------------------ identity
     def id(self, sid=''):
@@ -152,6 +315,8 @@ class sim(object):
         self.ev = numpy.append(self.ev, ev)
         self.p = numpy.append(self.p, p)
         self.color = numpy.append(self.color, color)
+        if self.fluid:
+            self.f_p = numpy.append(self.f_p, [numpy.zeros(3)], axis=0)
 
     _PER_PARTICLE = ("x", "radius", "vel", "xyzsum", "fixvel", "force", "angpos", "angvel",
                      "torque", "es_dot", "es", "ev_dot", "ev", "p", "color")
@@ -165,6 +330,8 @@ class sim(object):
         self.np = self.np - idx.size
         for name in self._PER_PARTICLE:
             setattr(self, name, numpy.delete(getattr(self, name), i, axis=0))
+        if self.fluid:
+            self.f_p = numpy.delete(self.f_p, i, axis=0)
 
     def deleteAllParticles(self):
         self.np[0] = 0
@@ -181,6 +348,8 @@ class sim(object):
         for name in ("es_dot", "es", "ev_dot", "ev", "p"):
             setattr(self, name, numpy.zeros(0))
         self.color = numpy.zeros(0, dtype=numpy.int32)
+        if self.fluid:
+            self.f_p = numpy.zeros((0, 3))
 
     # ----------------------------------------------------------------- I/O
     def readbin(self, targetbin, verbose=True, bonds=True, sigma0mod=True, esysparticle=False):
@@ -543,8 +712,10 @@ class sim(object):
             else:
                 k_max = numpy.max([self.k_n[:], self.k_t[:]])
             self.time_dt[0] = epsilon / (numpy.sqrt(k_max / m_min))
-        else:
+        elif not self.fluid:
             raise Exception('Error: Could not automatically set a time step.')
+        if self.fluid:
+            self.time_dt[0] = numpy.min([self.largestFluidTimeStep(), self.time_dt[0]])
         self.time_current[0] = current
         self.time_total[0] = total
         self.time_file_dt[0] = file_dt
@@ -552,6 +723,29 @@ class sim(object):
 
     def dry(self):
         self.fluid = False
+
+    def wet(self):
+        """Total fluid saturation with the default fluid
+        (python/sphere.py:3386): initFluid() with its defaults."""
+        self.fluid = True
+        self.initFluid()
+
+    def largestFluidTimeStep(self, safety=0.5, v_max=-1.0):
+        """The largest stable fluid time step (python/sphere.py:2067): for
+        the Darcy solver the advective (CFL) limit, the smallest cell width
+        over the largest fluid speed (1e-7 m/s when the fluid is at rest)."""
+        if not self.fluid:
+            return None
+        v = numpy.asarray(self.v_f, dtype=numpy.float64).reshape(-1, 3)
+        v_max_obs = numpy.amax(numpy.sqrt((v * v).sum(axis=1))) if v.size else 0.0
+        if v_max_obs == 0:
+            v_max_obs = 1.0e-7
+        if v_max < 0.0:
+            v_max = v_max_obs
+        dx_min = numpy.min(self.L / self.num)
+        self._check_darcy('largestFluidTimeStep')
+        self.cellSize()
+        return dx_min / v_max
 
     def defaultParams(self, mu_s=0.5, mu_d=0.5, mu_r=0.0, rho=2600, k_n=1.16e9, k_t=1.16e9,
                       k_r=0, gamma_n=0.0, gamma_t=0.0, gamma_r=0.0, gamma_wn=1.0e4,

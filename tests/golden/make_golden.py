@@ -110,6 +110,28 @@ def bin_scenes(S):
     s.uniaxialStrainRate(wvel=-0.002)
     s.initTemporal(total=0.01, file_dt=0.002)
     out["bonds"] = s
+    numpy.random.seed(5)
+    s = S(np=24, nw=0, sid="golden_darcy", fluid=True)
+    s.generateRadii(psd='uni', mean=0.01, variance=0.001)
+    s.periodicBoundariesXY()
+    s.initRandomGridPos(gridnum=numpy.array([8, 8, 16]))
+    s.consolidate(normal_stress=1.0e4)
+    s.initFluid(mu=1.0e-3, rho=1.0e3, p=1.0e3, hydrostatic=True, cfd_solver=1)
+    s.setFluidBottomNoFlow()
+    s.setFluidTopFixedFlux(2.0e-5)
+    s.setFluidXNoFlow()
+    s.setPermeabilityPrefactor(1.0e-9, verbose=False)
+    s.setFluidCompressibility(1.0e-8)
+    s.setFluidPressureModulation(A=100.0, f=2.0, phi=0.25)
+    s.setDEMstepsPerCFDstep(3)
+    s.setTolerance(1.0e-4)
+    s.setMaxIterations(500)
+    s.p_f_constant[0, 1, 2] = 1
+    s.dphi[:, :, 1] = 0.5
+    s.v_f[:, :, :, 2] = -1.0e-3
+    s.f_p[:, 2] = 0.25
+    s.initTemporal(total=0.01, file_dt=0.002)
+    out["darcy"] = s
     return out
 
 

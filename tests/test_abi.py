@@ -63,3 +63,10 @@ def test_header_constants_match_the_mirror():
     defs = dict(re.findall(r"#define\s+(SPH_[A-Z_]+)\s+(\d+)", text))
     assert int(defs["SPH_TUNE_VARIANTS"]) == _abi.TUNE_VARIANTS
     assert int(defs["SPH_PAIR_SHAPES"]) == _abi.PAIR_SHAPES
+
+
+def test_darcy_struct_size_matches_ctypes():
+    lib = _abi.load_library()
+    n = C.c_uint64(0)
+    assert lib.sph_darcy_struct_size(C.byref(n)) == 0
+    assert n.value == C.sizeof(_abi.SphDarcy)

@@ -1,7 +1,8 @@
 """The .bin v2.15 format against golden files written by the reference's own
 python/sphere.py (tests/golden/bin_*.bin, see tests/golden/make_golden.py):
 the same seeded scenes built with sphere_b200.sim must encode to the same
-bytes, and every golden file must read back and re-encode unchanged."""
+bytes, and every golden file must read back and re-encode unchanged.  The
+darcy scene carries the Darcy fluid block (cfd_solver 1)."""
 import os
 
 import numpy
@@ -24,18 +25,25 @@ def _scenes():
     return mod.bin_scenes(sim)
 
 
-@pytest.mark.parametrize("name", ["grid", "consolidate", "shear", "bonds"])
+@pytest.mark.parametrize("name", ["grid", "consolidate", "shear", "bonds", "darcy"])
 def test_setup_and_writer_match_reference_bytes(name):
     ours = _scenes()[name]
     golden = open(os.path.join(GOLDEN, "bin_%s.bin" % name), "rb").read()
     assert binio.encode_bin(ours) == golden
 
 
-@pytest.mark.parametrize("name", ["grid", "consolidate", "shear", "bonds"])
+@pytest.mark.parametrize("name", ["grid", "consolidate", "shear", "bonds", "darcy"])
 def test_reader_round_trip(name, tmp_path):
     path = os.path.join(GOLDEN, "bin_%s.bin" % name)
-    s = sim()
+    # as in the reference, the sim says whether the file has a fluid block
+    s = sim(fluid=(name == "darcy"))
     s.readbin(path, verbose=False)
+    if name == "darcy":
+        # the reader divides dphi by time_dt * ndem with the ndem the sim
+        # held before the read (1), the writer multiplies by the file's (3),
+        # as the reference's own reader and writer do: every other byte
+        # round-trips, and dphi does with the scale the writer applies
+        s.dphi = s.dphi / s.ndem
     assert binio.encode_bin(s) == open(path, "rb").read()
     s.writebin(folder=str(tmp_path), verbose=False)
     assert open(os.path.join(str(tmp_path), s.sid + ".bin"), "rb").read() == open(path, "rb").read()
@@ -60,3 +68,24 @@ def test_reads_reference_output_files(fname, n):
     assert s.x.shape == (n, 3) and (s.radius > 0).all()
     assert numpy.isfinite(s.x).all()
     assert s.version[0] == binio.VERSION
+
+
+def test_darcy_reader_scales_dphi_and_fields(tmp_path):
+    """The fluid fields of the Darcy golden scene read back in the sim's
+    [x, y, z] layout, dphi divided by time_dt * ndem as the reference's
+    reader divides (with the ndem the sim held before the read)."""
+    ours = _scenes()["darcy"]
+    s = sim(fluid=True)
+    s.readbin(os.path.join(GOLDEN, "bin_darcy.bin"), verbose=False)
+    assert numpy.array_equal(s.p_f, ours.p_f) and numpy.array_equal(s.v_f, ours.v_f)
+    assert numpy.array_equal(s.p_f_constant, ours.p_f_constant)
+    raw = ours.dphi * ours.time_dt * ours.ndem
+    assert numpy.array_equal(s.dphi, raw / (s.time_dt * 1))
+    assert int(s.ndem) == 3 and int(s.maxiter) == 500 and int(s.bc_bot[0]) == 1
+    assert numpy.array_equal(s.f_p, ours.f_p)
+
+
+def test_navier_stokes_block_is_not_supported(tmp_path):
+    s = sim(fluid=True)
+    with pytest.raises(NotImplementedError):
+        s.initFluid(cfd_solver=0)

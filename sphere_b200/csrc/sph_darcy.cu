@@ -13,14 +13,16 @@
 //
 // Design for the GPU: the reference runs the Jacobi loop from the host,
 // four launches and a device synchronisation per iteration and a copy of
-// the whole residual field to the host every tenth; here the loop is a
-// conditional WHILE node of the step's CUDA graph, the residual maximum is
-// reduced on the device (atomicMax of the bit pattern of |r|, exact and
-// order-free) and the loop's condition is set by a one-thread kernel at the
-// end of each iteration, so a step with its fluid solve is one graph launch
-// with no host round trip.  The copy of the new pressure and the next
-// iteration's ghost layer are one kernel (each cell writes its value and
-// the ghost cells that copy it).  Which steps update the fluid
+// the whole residual field to the host every tenth; here the whole loop is
+// one cooperative launch (k_darcy_jacobi): each iteration is the update,
+// a grid barrier, the copy of the new pressure with the flux ghosts and the
+// next iteration's ghost layer (each cell writes its value and the ghost
+// cells that copy it), and a barrier; every tenth iteration each block
+// reduces the largest |residual| of its cells (the bits of a non-negative
+// double, which order as the values do) and every block takes the same
+// stop decision from all blocks' values.  The barriers are bounded
+// (SPH_ERR_TIMEOUT).  A step with its fluid solve is one graph launch with
+// no host round trip.  Which steps update the fluid
 // (iter % ndem) and the top wall's cell (wall0_iz, from the reference's
 // host copy of the wall, refreshed at outputs) are decided on the device,
 // which keeps the reference's host file clock, so the results do not
@@ -44,12 +46,14 @@
 
 #include "sph_device.cuh"
 #include "sph_internal.h"
+#include "sph_sync.cuh"
 
 namespace sph {
 
 namespace {
 
 constexpr int DARCY_THREADS = 256;
+constexpr int JACOBI_THREADS = 512;   // the Jacobi loop: one block per SM
 constexpr double DARCY_PI = 3.14159265358979323846;   // M_PI, which src/darcy.cuh uses
 
 inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
@@ -419,7 +423,16 @@ __global__ void k_darcy_pre(DarcyArgs D)
 // updateDarcySolution: the pressure change of the diffusion term (harmonic
 // means of k across the faces) and of the porosity forcing, zero at
 // Dirichlet boundaries, above the wall and in cells of constant pressure
-__device__ double darcy_dp(const DarcyArgs &D, double dt, int x, int y, int z)
+template <bool CG>
+__device__ __forceinline__ double ldp(const double *p, uint32_t i)
+{
+    return CG ? __ldcg(p + i) : p[i];
+}
+
+// CG: the pressures are read past L1 (inside the persistent loop, where
+// other blocks wrote them since the last barrier)
+template <bool CG>
+__device__ double darcy_dp(const DarcyArgs &D, const double *pf, double dt, int x, int y, int z)
 {
     const SphDarcy &P = D.prm;
     const int nx = D.nx, ny = D.ny, nz = D.nz;
@@ -432,12 +445,11 @@ __device__ double darcy_dp(const DarcyArgs &D, double dt, int x, int y, int z)
     const double dphi = D.dphi[ci];
     const d3 vp_avg = ld3(D.vp_avg + 3 * (size_t)ci);
     const int p_constant = D.p_constant[ci];
-    const double *pf = D.p;
-    double p_xn = pf[d_idx(D, x - 1, y, z)];
-    const double p = pf[ci];
-    double p_xp = pf[d_idx(D, x + 1, y, z)];
-    double p_yn = pf[d_idx(D, x, y - 1, z)], p_yp = pf[d_idx(D, x, y + 1, z)];
-    double p_zn = pf[d_idx(D, x, y, z - 1)], p_zp = pf[d_idx(D, x, y, z + 1)];
+    double p_xn = ldp<CG>(pf, d_idx(D, x - 1, y, z));
+    const double p = ldp<CG>(pf, ci);
+    double p_xp = ldp<CG>(pf, d_idx(D, x + 1, y, z));
+    double p_yn = ldp<CG>(pf, d_idx(D, x, y - 1, z)), p_yp = ldp<CG>(pf, d_idx(D, x, y + 1, z));
+    double p_zn = ldp<CG>(pf, d_idx(D, x, y, z - 1)), p_zp = ldp<CG>(pf, d_idx(D, x, y, z + 1));
     const double k_xn = D.k[d_idx(D, x - 1, y, z)], k = D.k[ci];
     const double k_xp = D.k[d_idx(D, x + 1, y, z)];
     const double k_yn = D.k[d_idx(D, x, y - 1, z)], k_yp = D.k[d_idx(D, x, y + 1, z)];
@@ -470,125 +482,167 @@ __global__ void k_darcy_first(StepArgs A, DarcyArgs D)
     if (!fluid_step(D)) return;
     int x, y, z;
     if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
-    D.dp_expl[d_idx(D, x, y, z)] = darcy_dp(D, A.boxes[0].dt, x, y, z);
+    D.dp_expl[d_idx(D, x, y, z)] = darcy_dp<false>(D, D.p, A.boxes[0].dt, x, y, z);
 }
 
-// The start of the Jacobi loop: the iteration count, the residual
-// maximum, and the loop's first condition (run when this step updates the
-// fluid and maxiter > 0).
-template <bool GRAPH>
-__global__ void k_darcy_loop_begin(DarcyArgs D, cudaGraphConditionalHandle hc)
+// The Jacobi loop of one fluid step (device.cu:2218-2376) as one
+// cooperative launch, the blocks taking the cells in turn, the pressure in
+// two arrays that alternate (D.p and D.p_new): iteration n reads array
+// n % 2 and writes the other.  Per iteration, per cell:
+//  - updateDarcySolution: the new pressure and its normalised residual;
+//  - setDarcyGhostNodesFlux (bc 4) from the cell's pressure before the
+//    update, into the other array's ghost layer;
+//  - copyValues(p_new -> p) and the ghost layer of the new pressure (the
+//    reference's setDarcyGhostNodes at the start of the next iteration, or
+//    after the loop): the new value into the other array with the ghost
+//    cells that copy it;
+// then a grid barrier.  With bc_top == 1, setDarcyTopWallFixedFlow (p at
+// z = wall0_iz + 1 from z = wall0_iz - 1 in the array just read) runs
+// between two barriers.  Every tenth iteration (src/debug.h:16 nijacnorm)
+// each block's largest |residual| (the bits of a non-negative double,
+// which order as the values do) and whether one was NaN go to per-block
+// slots; after the barrier every block reads all slots and takes the same
+// decision: stop when the largest residual is within the tolerance, or one
+// was NaN (SPH_ERR_NAN); stop after maxiter iterations.  The final
+// pressure ends up in D.p.  The barriers are bounded (SPH_ERR_TIMEOUT); the
+// pressures other blocks write are read past L1.  Block 0 logs the solve.
+__global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, DarcyArgs D, GridSync G)
 {
-    DarcyState *s = D.st;
-    s->nijac = 0;
-    s->maxnorm = 0ull;
-    s->nan = 0u;
-    s->go = (s->active && D.prm.maxiter > 0) ? 1u : 0u;
-    if (GRAPH) cudaGraphSetConditional(hc, s->go);
-}
-
-// One Jacobi update (updateDarcySolution): p_new and the normalised
-// residual; every tenth iteration (src/debug.h:16 nijacnorm) the largest
-// |residual| over the cells goes to the state (as the bits of a
-// non-negative double, which order as the values do), a NaN to its flag.
-__global__ void k_darcy_update(StepArgs A, DarcyArgs D)
-{
-    int x, y, z;
-    const bool in = cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z);
-    DarcyState *s = D.st;
-    const bool check = (s->nijac % 10u) == 0u;
-    double r = 0.0;
-    if (in) {
-        const uint32_t ci = d_idx(D, x, y, z);
-        const double dp_impl = darcy_dp(D, A.boxes[0].dt, x, y, z);
-        const double epsilon = 0.5;
-        const double p = D.p[ci];
-        double p_new = D.p_old[ci] + (1.0 - epsilon) * D.dp_expl[ci] + epsilon * dp_impl;
-        const double theta = 0.05;
-        p_new = p * (1.0 - theta) + p_new * theta;
-        const double res_norm = (p_new - p) / (p + 1.0e-16);
-        D.p_new[ci] = p_new;
-        D.norm[ci] = res_norm;
-        r = fabs(res_norm);
-    }
-    if (!check) return;
-    const bool isnan_r = in && r != r;
-    unsigned long long bits = in && !isnan_r ? (unsigned long long)__double_as_longlong(r) : 0ull;
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long b = __shfl_xor_sync(0xffffffffu, bits, o);
-        bits = b > bits ? b : bits;
-    }
-    const unsigned anynan = __any_sync(0xffffffffu, isnan_r);
-    if ((threadIdx.x & 31) == 0) {
-        if (bits) atomicMax(&s->maxnorm, bits);
-        if (anynan) s->nan = 1u;
-    }
-}
-
-// darcy.cuh:1462-1482 setDarcyTopWallFixedFlow (bc_top == 1): p at
-// z = wall0_iz + 1 from z = wall0_iz - 1, over the reference's launch grid
-// (z < 8 ceil(nz / 8))
-__global__ void k_darcy_fixed_flow(DarcyArgs D, int gz)
-{
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ unsigned long long s_max[JACOBI_THREADS / 32];
+    __shared__ uint32_t s_nan[JACOBI_THREADS / 32];
+    __shared__ int s_stop, s_ok, s_bad;
+    DarcyState *st = D.st;
+    const SphDarcy &P = D.prm;
+    if (!(st->active && P.maxiter > 0)) return;   // the same in every block
+    const uint32_t ncells = (uint32_t)D.nx * (uint32_t)D.ny * (uint32_t)D.nz;
     const uint32_t nxy = (uint32_t)D.nx * (uint32_t)D.ny;
-    if (t >= nxy) return;
-    const int y = (int)(t / (uint32_t)D.nx), x = (int)(t - (uint32_t)y * (uint32_t)D.nx);
-    const uint32_t z = D.st->wall0_iz + 1u;
-    if (z >= (uint32_t)gz) return;
-    // cells past the padded array (a wall at or above the top of the grid)
-    // are skipped
-    const uint32_t w = d_idx(D, x, y, (int)z), r = d_idx(D, x, y, (int)z - 2);
-    if (w < D.ncell && r < D.ncell) D.p[w] = D.p[r];
-}
-
-// copyValues(p_new -> p) and the ghost layer of the new p (the reference's
-// setDarcyGhostNodes at the start of the next iteration, or after the
-// loop): each cell writes its value and the ghost cells that copy it
-__global__ void k_darcy_copy_ghost(DarcyArgs D)
-{
-    int x, y, z;
-    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
-    const uint32_t ci = d_idx(D, x, y, z);
-    const double val = D.p_new[ci];
-    D.p[ci] = val;
-    put_ghosts<1>(D, D.p, x, y, z, &val);
-}
-
-// The end of a Jacobi iteration (device.cu:2333-2375): every tenth
-// iteration, stop when the largest residual is within the tolerance (or a
-// residual was NaN: SPH_ERR_NAN); stop after maxiter iterations; log the
-// solve when it stops; set the loop's condition.
-template <bool GRAPH>
-__global__ void k_darcy_check(StepArgs A, DarcyArgs D, cudaGraphConditionalHandle hc)
-{
-    DarcyState *s = D.st;
-    const uint32_t nijac = s->nijac;
-    uint32_t stop = 0, ok = 0;
-    if (nijac % 10u == 0u) {
-        if (s->nan) {
-            raise_flag(A.err, SPH_ERR_NAN);
-            stop = 1;
-        } else if (__longlong_as_double((long long)s->maxnorm) <= D.prm.tolerance) {
-            stop = 1;
-            ok = 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
+    const double dt = A.boxes[0].dt;
+    const bool flux = P.bc_bot == 4 || P.bc_top == 4;
+    const int gz = (D.nz + 7) / 8 * 8;
+    const uint32_t wall0_iz = st->wall0_iz;
+    const double dzf = A.boxes[0].L[2] / D.nz;
+    double *const buf[2] = {D.p, D.p_new};
+    uint32_t nijac = 0;
+    int ok = 0, bad = 0;
+    for (;;) {
+        double *pc = buf[nijac & 1u];
+        double *pn = buf[(nijac & 1u) ^ 1u];
+        const bool check = (nijac % 10u) == 0u;
+        unsigned long long bmax = 0ull;
+        uint32_t bnan = 0u;
+        for (uint32_t c = first; c < ncells; c += stride) {
+            int x, y, z;
+            cell_of(D, c, x, y, z);
+            const uint32_t ci = d_idx(D, x, y, z);
+            const double dp_impl = darcy_dp<true>(D, pc, dt, x, y, z);
+            const double epsilon = 0.5;
+            const double p = __ldcg(pc + ci);
+            double p_new = D.p_old[ci] + (1.0 - epsilon) * D.dp_expl[ci] + epsilon * dp_impl;
+            const double theta = 0.05;
+            p_new = p * (1.0 - theta) + p_new * theta;
+            const double res_norm = (p_new - p) / (p + 1.0e-16);
+            if (flux) {
+                const double k = D.k[ci];
+                double q_z = 0.;
+                if (z == 0) q_z = P.bc_bot_flux;
+                else if (z == D.nz - 1) q_z = P.bc_top_flux;
+                const double p_ghost = -P.mu / k * q_z * dzf + p;
+                if (z == 0 && P.bc_bot == 4) __stcg(pn + d_idx(D, x, y, -1), p_ghost);
+                if (z == D.nz - 1 && P.bc_top == 4) __stcg(pn + d_idx(D, x, y, D.nz), p_ghost);
+            }
+            __stcg(pn + ci, p_new);
+            put_ghosts<1>(D, pn, x, y, z, &p_new);
+            if (check) {
+                const double r = fabs(res_norm);
+                if (r != r) {
+                    bnan = 1u;
+                } else {
+                    const unsigned long long b = (unsigned long long)__double_as_longlong(r);
+                    bmax = b > bmax ? b : bmax;
+                }
+            }
         }
-        s->maxnorm = 0ull;
+        if (check) {
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long b = __shfl_xor_sync(0xffffffffu, bmax, o);
+                bmax = b > bmax ? b : bmax;
+            }
+            const uint32_t anynan = __any_sync(0xffffffffu, bnan != 0u) ? 1u : 0u;
+            if ((threadIdx.x & 31) == 0) {
+                s_max[threadIdx.x >> 5] = bmax;
+                s_nan[threadIdx.x >> 5] = anynan;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned long long m = 0ull;
+                uint32_t nn = 0u;
+                for (int w = 0; w < JACOBI_THREADS / 32; ++w) {
+                    m = s_max[w] > m ? s_max[w] : m;
+                    nn |= s_nan[w];
+                }
+                __stcg(D.part_max + blockIdx.x, m);
+                __stcg(D.part_nan + blockIdx.x, nn);
+            }
+        }
+        if (P.bc_top == 1) {
+            // after every cell has read the array it writes; cells past the
+            // padded array (a wall at or above the top of the grid) are
+            // skipped
+            if (!grid_barrier_acqrel(G, gridDim.x, A.err)) return;
+            const uint32_t z = wall0_iz + 1u;
+            if (z < (uint32_t)gz)
+                for (uint32_t t = first; t < nxy; t += stride) {
+                    const int y = (int)(t / (uint32_t)D.nx), x = (int)(t - (uint32_t)y * (uint32_t)D.nx);
+                    const uint32_t w = d_idx(D, x, y, (int)z), r = d_idx(D, x, y, (int)z - 2);
+                    if (w < D.ncell && r < D.ncell) __stcg(pc + w, __ldcg(pc + r));
+                }
+        }
+        if (!grid_barrier_acqrel(G, gridDim.x, A.err)) return;
+        if (threadIdx.x == 0) {
+            int stop = 0, good = 0, nanseen = 0;
+            if (check) {
+                unsigned long long m = 0ull;
+                uint32_t nn = 0u;
+                for (uint32_t b = 0; b < gridDim.x; ++b) {
+                    const unsigned long long v = __ldcg(D.part_max + b);
+                    m = v > m ? v : m;
+                    nn |= __ldcg(D.part_nan + b);
+                }
+                if (nn) {
+                    stop = 1;
+                    nanseen = 1;
+                } else if (__longlong_as_double((long long)m) <= P.tolerance) {
+                    stop = 1;
+                    good = 1;
+                }
+            }
+            if (!stop && nijac == P.maxiter - 1u) stop = 1;
+            s_stop = stop;
+            s_ok = good;
+            s_bad = nanseen;
+        }
+        __syncthreads();
+        if (s_stop) {
+            ok = s_ok;
+            bad = s_bad;
+            if (pn != D.p)   // the result in D.p (every cell: the ghost layer too)
+                for (uint32_t c = first; c < D.ncell; c += stride) __stcg(D.p + c, __ldcg(pn + c));
+            break;
+        }
+        ++nijac;
     }
-    if (!stop && nijac == D.prm.maxiter - 1u) stop = 1;
-    if (stop) {
-        const unsigned long long h = s->log_head;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (bad) raise_flag(A.err, SPH_ERR_NAN);
+        const unsigned long long h = st->log_head;
         const uint32_t slot = (uint32_t)(h % SPH_DARCY_LOG);
         D.log_step[slot] = A.boxes[0].iter + 1;
         D.log_iters[slot] = nijac;
-        D.log_ok[slot] = ok;
-        s->log_head = h + 1;
-        s->go = 0u;
-    } else {
-        s->nijac = nijac + 1;
-        s->go = 1u;
+        D.log_ok[slot] = (uint32_t)ok;
+        st->log_head = h + 1;
+        st->nijac = nijac;
     }
-    if (GRAPH) cudaGraphSetConditional(hc, s->go);
 }
 
 // After the loop: dphi zeroed unless an output follows this step
@@ -641,29 +695,6 @@ static inline void mark(Prof *prof, cudaStream_t st, const char *name)
     prof->n++;
 }
 
-// The kernels of one Jacobi iteration.
-template <bool GRAPH>
-void jacobi_body(const StepArgs &A, const DarcyArgs &D, cudaStream_t st,
-                 cudaGraphConditionalHandle hc, uint64_t &nl)
-{
-    const uint32_t ncells = (uint32_t)D.nx * D.ny * D.nz;
-    const unsigned gc = blocks_for(ncells, DARCY_THREADS);
-    k_darcy_update<<<gc, DARCY_THREADS, 0, st>>>(A, D);
-    nl += 1;
-    if (D.prm.bc_top == 1) {
-        const int gz = (D.nz + 7) / 8 * 8;
-        k_darcy_fixed_flow<<<blocks_for((uint64_t)D.nx * D.ny, DARCY_THREADS), DARCY_THREADS, 0, st>>>(D, gz);
-        nl += 1;
-    }
-    if (D.prm.bc_bot == 4 || D.prm.bc_top == 4) {
-        k_darcy_flux<<<gc, DARCY_THREADS, 0, st>>>(A, D);
-        nl += 1;
-    }
-    k_darcy_copy_ghost<<<gc, DARCY_THREADS, 0, st>>>(D);
-    k_darcy_check<GRAPH><<<1, 1, 0, st>>>(A, D, hc);
-    nl += 2;
-}
-
 }  // namespace
 
 int launch_darcy(const StepArgs &A, const DarcyArgs &D, const StepConfig &cfg, cudaStream_t st,
@@ -711,55 +742,36 @@ int launch_darcy(const StepArgs &A, const DarcyArgs &D, const StepConfig &cfg, c
     k_darcy_first<<<gc, DARCY_THREADS, 0, st>>>(A, D);
     nl += 2;
     mark(prof, st, "k_darcy_fluid");
-    // the Jacobi loop: a WHILE node under capture, a host loop otherwise
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return SPH_ERR_CUDA;
-    if (cs == cudaStreamCaptureStatusActive) {
-        if (!cfg.side) return SPH_ERR_CUDA;
-        cudaGraph_t g = nullptr;
-        const cudaGraphNode_t *deps = nullptr;
-        size_t nd = 0;
-        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd) != cudaSuccess)
-            return SPH_ERR_CUDA;
-        cudaGraphConditionalHandle hc;
-        if (cudaGraphConditionalHandleCreate(&hc, g, 0u, cudaGraphCondAssignDefault) != cudaSuccess)
-            return SPH_ERR_CUDA;
-        k_darcy_loop_begin<true><<<1, 1, 0, st>>>(D, hc);
-        nl += 1;
-        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd) != cudaSuccess)
-            return SPH_ERR_CUDA;
-        cudaGraphNodeParams np = {};
-        np.type = cudaGraphNodeTypeConditional;
-        np.conditional.handle = hc;
-        np.conditional.type = cudaGraphCondTypeWhile;
-        np.conditional.size = 1;
-        cudaGraphNode_t node;
-        if (cudaGraphAddNode(&node, g, deps, nd, &np) != cudaSuccess) return SPH_ERR_CUDA;
-        if (cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) !=
-            cudaSuccess)
-            return SPH_ERR_CUDA;
-        cudaGraph_t body = np.conditional.phGraph_out[0];
-        if (cudaStreamBeginCaptureToGraph(cfg.side, body, nullptr, nullptr, 0,
-                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            return SPH_ERR_CUDA;
-        uint64_t nb = 0;
-        jacobi_body<true>(A, D, cfg.side, hc, nb);
-        cudaGraph_t done = nullptr;
-        if (cudaStreamEndCapture(cfg.side, &done) != cudaSuccess) return SPH_ERR_CUDA;
-        nl += 1;
-    } else {
-        cudaGraphConditionalHandle none = 0;
-        k_darcy_loop_begin<false><<<1, 1, 0, st>>>(D, none);
-        nl += 1;
-        for (;;) {
-            uint32_t go = 0;
-            if (cudaMemcpyAsync(&go, &D.st->go, sizeof go, cudaMemcpyDeviceToHost, st) !=
-                    cudaSuccess ||
-                cudaStreamSynchronize(st) != cudaSuccess)
-                return SPH_ERR_CUDA;
-            if (!go) break;
-            jacobi_body<false>(A, D, st, none, nl);
+    // the Jacobi loop: one cooperative launch, as many blocks as can be
+    // resident at once (at most one per JACOBI_THREADS cells); the launch
+    // fails rather than run blocks that could not all be resident
+    {
+        static int per_sm = -1, sms = 0;
+        if (per_sm < 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_darcy_jacobi, JACOBI_THREADS, 0);
         }
+        unsigned cap = (unsigned)(per_sm > 0 ? per_sm : 1) * (unsigned)sms;
+        const unsigned need = blocks_for(ncells, JACOBI_THREADS);
+        if (cap > DARCY_PARTS) cap = DARCY_PARTS;
+        GridSync G;
+        G.count = D.bar;
+        G.gen = D.bar + 1;
+        G.limit_ns = BARRIER_LIMIT_NS;
+        cudaMemsetAsync(D.bar, 0, sizeof(uint32_t), st);
+        cudaLaunchConfig_t c = {};
+        c.gridDim = dim3(need < cap ? need : cap);
+        c.blockDim = dim3(JACOBI_THREADS);
+        c.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        c.attrs = at;
+        c.numAttrs = 1;
+        if (cudaLaunchKernelEx(&c, k_darcy_jacobi, A, D, G) != cudaSuccess) return SPH_ERR_CUDA;
+        nl += 2;
     }
     mark(prof, st, "k_darcy_jacobi");
     k_darcy_post<<<gc, DARCY_THREADS, 0, st>>>(A, D);

@@ -164,14 +164,11 @@ constexpr uint32_t DARCY_RING = 65536;   // queued top pressures (steps)
 struct DarcyState {
     double filetimeclock;          // the reference's host file clock
     double wall_w_host;            // its host copy of walls.nx[0].w (refreshed at outputs)
-    unsigned long long maxnorm;    // bits of the largest |norm| of a checked iteration
     unsigned long long qstep;      // steps run since sph_darcy_set (top-pressure ring index)
     unsigned long long log_head;   // Jacobi log entries written
     uint32_t wall0_iz;             // src/device.cu:1001, 1903
     uint32_t active;               // this step runs the fluid update (iter % ndem == 0)
-    uint32_t nijac;                // Jacobi iteration of the running solve
-    uint32_t go;                   // the solve continues (the loop's condition)
-    uint32_t nan;                  // a checked residual was NaN
+    uint32_t nijac;                // the last iteration of the last solve
 };
 struct DarcyArgs {
     SphDarcy prm;
@@ -187,7 +184,13 @@ struct DarcyArgs {
     const double *pmod;            // top pressure per queued step (DARCY_RING), null: no modulation
     uint64_t *log_step;            // the Jacobi log, a ring of SPH_DARCY_LOG entries
     uint32_t *log_iters, *log_ok;
+    // the Jacobi loop's cooperative launch: barrier words (count, generation)
+    // and the per-block largest |residual| and NaN flag of a checked iteration
+    uint32_t *bar;
+    unsigned long long *part_max;
+    uint32_t *part_nan;
 };
+constexpr uint32_t DARCY_PARTS = 8192;   // blocks of the Jacobi launch at most
 
 struct StepConfig {
     int lenmode;

@@ -50,6 +50,7 @@
 #include "sph_internal.h"
 #include "sph_mixed_laws.cuh"
 #include "sph_step.cuh"
+#include "sph_sync.cuh"
 
 namespace sph {
 
@@ -592,50 +593,6 @@ __global__ void __launch_bounds__(PBOX_THREADS) k_pair_box(StepArgs A, PairArgs 
     __shared__ double s_w[32];
     box_sum_advance(A, P, blockIdx.x, s_w);
     if (blockIdx.x == 0 && threadIdx.x == 0) *P.pp ^= 1u;
-}
-
-// A grid-wide barrier with a time limit: the blocks of one launch (all
-// resident: the launch is cooperative) count in, the last one opens the
-// next generation; a block that waits longer than G.limit_ns raises
-// SPH_ERR_TIMEOUT and returns false (its kernel then ends, and so do the
-// others, at this barrier or the next), so a block that never arrives does
-// not hang the device.
-__device__ __forceinline__ unsigned long long now_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ bool grid_barrier(const GridSync &G, uint32_t nblocks, uint32_t *err)
-{
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        volatile uint32_t *gen = G.gen;
-        const uint32_t g = *gen;
-        __threadfence();
-        if (atomicAdd(G.count, 1u) == nblocks - 1u) {
-            atomicExch(G.count, 0u);
-            __threadfence();
-            atomicAdd(G.gen, 1u);
-        } else {
-            const unsigned long long t0 = now_ns();
-            while (*gen == g) {
-                if (now_ns() - t0 > G.limit_ns) {
-                    ok = 0;
-                    raise_flag(err, SPH_ERR_TIMEOUT);
-                    break;
-                }
-                __nanosleep(128);
-            }
-        }
-        __threadfence();
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
 }
 
 // The list step as one persistent, cooperative launch: the blocks take the

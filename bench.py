@@ -19,7 +19,10 @@ buffers, and (rank 0, N = 1) the CPU baseline: the reference's own step
 kernels compiled for the CPU (oracle/_ref) on a bounded sample.  Rank 0
 also reports the cost of the adjoint (time_adjoint) under "adjoint", the
 batched-ensemble throughput and per-box error (time_ensemble) under
-"ensemble", and the bonded-pack throughput (time_bonded) under "bonded".
+"ensemble", the bonded-pack throughput (time_bonded) under "bonded", the
+FP64 gravity settling (time_settling) under "settling" and the
+Darcy-coupled pack with the reference's CPU kernels beside it (time_darcy)
+under "darcy".
 
 --impl reference times that CPU reference alone (rank 0; other ranks exit).
 
@@ -363,6 +366,70 @@ def time_settling(device, stream, n=10000, steps=1000):
             "device_status": code}
 
 
+def time_darcy(device, stream, n=100000, steps=100, ref_n=5000):
+    """The Darcy-coupled pack (scenes.darcy_pack: a lattice pack of n
+    spheres U[0.009, 0.011] m under a 10 kPa top wall, periodic x-y, in
+    water at hydrostatic pressure, beta_f = 1e-7 1/Pa, grain-size
+    permeability; the fluid on the cell grid), FP64 with the fluid updated
+    every step: steps queued at once and timed with CUDA events on the
+    launching stream, the Jacobi iterations of each step from its log, the
+    per-kernel-group times from the profiled step graphs.  Beside it the
+    reference's own DEM and Darcy kernels on the CPU (oracle/_ref), all host
+    threads, on the same construction at ref_n spheres."""
+    import numpy
+    import torch
+    from sphere_b200 import scenes
+    from sphere_b200.runner import Stepper
+    s = scenes.darcy_pack(n, seed=31)
+    s.time_file_dt[0] = 1.0   # no output inside the timed steps
+    st = Stepper([s], precision="fp64", length="reference", device=device)
+    st.set_stream(stream.cuda_stream)
+    st.upload()
+    st.step(3)     # graphs instantiated, untimed
+    st.upload()    # the timed run starts from the workload's initial state
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    launches0 = st.kernel_launches()
+    start.record(stream)
+    st.step_async(steps)
+    end.record(stream)
+    end.synchronize()
+    code = st.sync(raise_on_error=False)
+    ms = start.elapsed_time(end)
+    launches = st.kernel_launches() - launches0
+    _, iters, ok = st.darcy_log()
+    try:
+        st.profile(True)
+        st.step_async(PROFILE_RING)
+        st.sync(raise_on_error=False)
+        st.step_async(PROFILE_RING)
+        st.sync(raise_on_error=False)
+        kernels = st.profile_read()
+    except Exception as e:
+        kernels = {"error": str(e)}
+    st.profile(False)
+    st.close()
+    cells = int(s.num[0]) * int(s.num[1]) * int(s.num[2])
+    it = float(numpy.mean(iters)) if len(iters) else 0.0
+    sr = scenes.darcy_pack(ref_n, seed=31)
+    sr.time_file_dt[0] = 1.0
+    rate, done, secs, threads, kind, _ = cpu_reference_rate(sr, 20, 10.0)
+    return {"workload": "Darcy-coupled pack: %d spheres U[0.009, 0.011] m (jittered lattice, "
+                        "periodic x-y, 10 kPa top wall) in water (mu = 8.9e-4 Pa s) at "
+                        "hydrostatic pressure, beta_f = 1e-7 1/Pa, k_c = d^2/180, fluid on the "
+                        "%d x %d x %d cell grid updated every step, FP64, %d steps"
+                        % (n, int(s.num[0]), int(s.num[1]), int(s.num[2]), steps),
+            "value": n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "spheres": n, "fluid_cells": cells,
+            "jacobi_iterations_per_step": it, "solves_converged": int(numpy.sum(ok)),
+            "jacobi_cell_iterations_per_s": cells * it * steps / (ms / 1e3),
+            "kernel_ms": kernels, "gpu_launches": launches, "device_status": code,
+            "cpu_reference": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                              "sample": "%d whole steps of the same construction at %d spheres "
+                                        "(%.1f s)" % (done, ref_n, secs)}}
+
+
 def bench_config(args):
     """The `config` object of the JSON line, the same in both arms."""
     return {"workload": WORKLOAD, "spheres_per_gpu": args.n, "length_mode": "reference",
@@ -384,6 +451,12 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-bonded", action="store_true")
     ap.add_argument("--no-settling", action="store_true")
+    ap.add_argument("--no-darcy", action="store_true")
+    ap.add_argument("--darcy-only", action="store_true",
+                    help="run only the Darcy-coupled workload (time_darcy) and print its JSON")
+    ap.add_argument("--darcy-n", type=int, default=100000,
+                    help="spheres of the Darcy-coupled workload")
+    ap.add_argument("--darcy-steps", type=int, default=100)
     ap.add_argument("--ref-n", type=int, default=100000,
                     help="spheres of the reference arm's sample of the workload (the same "
                          "construction, packed on the CPU)")
@@ -403,6 +476,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.darcy_only:
+        import torch
+        torch.cuda.set_device(local)
+        out = time_darcy(local, torch.cuda.Stream(), n=args.darcy_n, steps=args.darcy_steps,
+                         ref_n=min(5000, args.darcy_n))
+        if rank == 0:
+            print(json.dumps(out))
+        return 0
 
     if args.impl == "reference":
         # The reference's own step kernels compiled for the CPU
@@ -724,6 +806,9 @@ def main():
     settling = None
     if rank == 0 and not args.no_settling:
         settling = time_settling(local, stream)
+    darcy = None
+    if rank == 0 and not args.no_darcy:
+        darcy = time_darcy(local, stream, n=args.darcy_n, steps=args.darcy_steps)
     long_run = None
     if rank == 0 and not args.no_long_run and "mixed" in res and "fp64" in res:
         # the mixed form's error against the FP64 form over the workload's
@@ -777,6 +862,8 @@ def main():
         line["bonded"] = bonded
     if settling is not None:
         line["settling"] = settling
+    if darcy is not None:
+        line["darcy"] = darcy
     if long_run is not None:
         line["mixed_error_long_run"] = long_run
     print(json.dumps(line))

@@ -101,6 +101,19 @@ def two_particles(radii=(1.0, 1.0), x0=(5.0, 5.0, 2.0), x1=(5.0, 5.0, 4.05), vel
     return s
 
 
+def darcy_pack(n, seed, periodic=1, nw=1, wmode=1, beta_f=1.0e-7, file_every=7.5, **kw):
+    """A seeded sphere pack (lattice_pack) in a Darcy fluid (cfd_solver 1)
+    at hydrostatic pressure below the top wall: water (mu = 8.9e-4,
+    rho_f = 1e3), compressibility beta_f, the grain-size permeability
+    prefactor (d^2 / 180), an output every file_every steps."""
+    s = lattice_pack(n, seed=seed, periodic=periodic, nw=nw, wmode=wmode, **kw)
+    s.initFluid(cfd_solver=1, mu=8.9e-4, rho=1.0e3, p=0.0, hydrostatic=True)
+    s.setFluidCompressibility(beta_f)
+    s.setPermeabilityGrainSize()
+    s.time_file_dt[0] = s.time_dt[0] * file_every
+    return s
+
+
 def gravity_settling(n=10000, seed=0, steps=1000):
     """Plain FP64 gravity settling of n spheres: radii U[0.010, 0.012] m,
     rho 2600, jittered cubic lattice (spacing 2.5*r_max, jitter +-0.2*r_max)

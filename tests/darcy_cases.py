@@ -29,14 +29,7 @@ def fluid_box(p_top=0.0, dt=1.0e-7, file_every=0.99):
     return s
 
 
-def fluid_pack(n, seed, periodic=1, nw=1, wmode=1, beta_f=1.0e-7, file_every=7.5, **kw):
-    """A seeded sphere pack in a Darcy fluid at hydrostatic pressure."""
-    s = scenes.lattice_pack(n, seed=seed, periodic=periodic, nw=nw, wmode=wmode, **kw)
-    s.initFluid(cfd_solver=1, mu=8.9e-4, rho=1.0e3, p=0.0, hydrostatic=True)
-    s.setFluidCompressibility(beta_f)
-    s.setPermeabilityGrainSize()
-    s.time_file_dt[0] = s.time_dt[0] * file_every
-    return s
+fluid_pack = scenes.darcy_pack
 
 
 def make(name):

@@ -1248,7 +1248,8 @@ int sph_darcy_set(SphHandle *h, const SphDarcy *d, const double *p, const double
             (st = dalloc(h, &D.log_ok, SPH_DARCY_LOG)) != SPH_OK ||
             (st = dalloc(h, &D.bar, 2)) != SPH_OK ||
             (st = dalloc(h, &D.part_max, sph::DARCY_PARTS)) != SPH_OK ||
-            (st = dalloc(h, &D.part_nan, sph::DARCY_PARTS)) != SPH_OK)
+            (st = dalloc(h, &D.part_nan, sph::DARCY_PARTS)) != SPH_OK ||
+            (st = dalloc(h, &D.coef, (uint64_t)sph::DARCY_COEF * nx * ny * nz)) != SPH_OK)
             return st;
         CUDA_TRY(h, cudaMemset(D.bar, 0, 2 * sizeof(uint32_t)));
     }

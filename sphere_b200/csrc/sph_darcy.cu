@@ -423,6 +423,35 @@ __global__ void k_darcy_pre(DarcyArgs D)
 // updateDarcySolution: the pressure change of the diffusion term (harmonic
 // means of k across the faces) and of the porosity forcing, zero at
 // Dirichlet boundaries, above the wall and in cells of constant pressure
+// darcy.cuh:1644-1923 firstDarcySolution and :1926-2226
+// updateDarcySolution: the pressure change
+//   ndt/(beta_f phi mu) div(k grad p) - ndt/(beta_f phi (1 - phi))
+//                                       (dphi/ndt + vp_avg . grad phi),
+// div(k grad p) with the harmonic means of k across the faces, zero at
+// Dirichlet boundaries, at and above the wall with a Dirichlet top, and in
+// cells of constant pressure (the +y test compares y with nx - 1, as
+// written).  Everything but the pressures stays fixed during a solve, so
+// k_darcy_first computes it once per fluid step with the reference's
+// subexpressions (the same roundings): for each face the harmonic mean
+// 2 k_n k / (k_n + k), the factor ndt/(beta_f phi mu), the forcing term,
+// and whether the change is zero; dp_of then gives the change of any
+// pressure field with the reference's remaining operations and order.
+struct DpCoef {
+    double a[6];   // faces xp, xn, yp, yn, zp, zn
+    double c1, f, zero;
+};
+
+__device__ __forceinline__ DpCoef load_coef(const DarcyArgs &D, uint32_t c, uint32_t ncells)
+{
+    DpCoef q;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) q.a[k] = D.coef[(size_t)k * ncells + c];
+    q.c1 = D.coef[(size_t)6 * ncells + c];
+    q.f = D.coef[(size_t)7 * ncells + c];
+    q.zero = D.coef[(size_t)8 * ncells + c];
+    return q;
+}
+
 template <bool CG>
 __device__ __forceinline__ double ldp(const double *p, uint32_t i)
 {
@@ -432,10 +461,40 @@ __device__ __forceinline__ double ldp(const double *p, uint32_t i)
 // CG: the pressures are read past L1 (inside the persistent loop, where
 // other blocks wrote them since the last barrier)
 template <bool CG>
-__device__ double darcy_dp(const DarcyArgs &D, const double *pf, double dt, int x, int y, int z)
+__device__ __forceinline__ double dp_of(const DarcyArgs &D, const DpCoef &q, const double *pf, int x,
+                                        int y, int z)
 {
+    if (q.zero != 0.0) return 0.0;
     const SphDarcy &P = D.prm;
-    const int nx = D.nx, ny = D.ny, nz = D.nz;
+    const double dx = D.dx, dy = D.dy, dz = D.dz;
+    double p_xn = ldp<CG>(pf, d_idx(D, x - 1, y, z));
+    const double p = ldp<CG>(pf, d_idx(D, x, y, z));
+    double p_xp = ldp<CG>(pf, d_idx(D, x + 1, y, z));
+    double p_yn = ldp<CG>(pf, d_idx(D, x, y - 1, z)), p_yp = ldp<CG>(pf, d_idx(D, x, y + 1, z));
+    double p_zn = ldp<CG>(pf, d_idx(D, x, y, z - 1)), p_zp = ldp<CG>(pf, d_idx(D, x, y, z + 1));
+    if (x == 0 && P.bc_xn == 1) p_xn = p;
+    if (x == D.nx - 1 && P.bc_xp == 1) p_xp = p;
+    if (y == 0 && P.bc_yn == 1) p_yn = p;
+    if (y == D.ny - 1 && P.bc_yp == 1) p_yp = p;
+    if (z == 0 && P.bc_bot == 1) p_zn = p;
+    if (z == D.nz - 1 && P.bc_top == 1) p_zp = p;
+    const double div_k_grad_p = (q.a[0] * (p_xp - p) / dx - q.a[1] * (p - p_xn) / dx) / dx +
+                                (q.a[2] * (p_yp - p) / dy - q.a[3] * (p - p_yn) / dy) / dy +
+                                (q.a[4] * (p_zp - p) / dz - q.a[5] * (p - p_zn) / dz) / dz;
+    return q.c1 * div_k_grad_p - q.f;
+}
+
+// The fixed parts of the pressure change of each cell (above), and the
+// explicit change dp_expl from the pressure at the start of the solve.
+__global__ void k_darcy_first(StepArgs A, DarcyArgs D)
+{
+    if (!fluid_step(D)) return;
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    int x, y, z;
+    if (!cell_of(D, c, x, y, z)) return;
+    const uint32_t ncells = (uint32_t)D.nx * (uint32_t)D.ny * (uint32_t)D.nz;
+    const SphDarcy &P = D.prm;
+    const int nx = D.nx, nz = D.nz;
     const double dx = D.dx, dy = D.dy, dz = D.dz;
     const uint32_t ci = d_idx(D, x, y, z);
     const double phi_xn = D.phi[d_idx(D, x - 1, y, z)], phi = D.phi[ci];
@@ -445,44 +504,34 @@ __device__ double darcy_dp(const DarcyArgs &D, const double *pf, double dt, int 
     const double dphi = D.dphi[ci];
     const d3 vp_avg = ld3(D.vp_avg + 3 * (size_t)ci);
     const int p_constant = D.p_constant[ci];
-    double p_xn = ldp<CG>(pf, d_idx(D, x - 1, y, z));
-    const double p = ldp<CG>(pf, ci);
-    double p_xp = ldp<CG>(pf, d_idx(D, x + 1, y, z));
-    double p_yn = ldp<CG>(pf, d_idx(D, x, y - 1, z)), p_yp = ldp<CG>(pf, d_idx(D, x, y + 1, z));
-    double p_zn = ldp<CG>(pf, d_idx(D, x, y, z - 1)), p_zp = ldp<CG>(pf, d_idx(D, x, y, z + 1));
     const double k_xn = D.k[d_idx(D, x - 1, y, z)], k = D.k[ci];
     const double k_xp = D.k[d_idx(D, x + 1, y, z)];
     const double k_yn = D.k[d_idx(D, x, y - 1, z)], k_yp = D.k[d_idx(D, x, y + 1, z)];
     const double k_zn = D.k[d_idx(D, x, y, z - 1)], k_zp = D.k[d_idx(D, x, y, z + 1)];
-    if (x == 0 && P.bc_xn == 1) p_xn = p;
-    if (x == nx - 1 && P.bc_xp == 1) p_xp = p;
-    if (y == 0 && P.bc_yn == 1) p_yn = p;
-    if (y == ny - 1 && P.bc_yp == 1) p_yp = p;
-    if (z == 0 && P.bc_bot == 1) p_zn = p;
-    if (z == nz - 1 && P.bc_top == 1) p_zp = p;
     const d3 grad_phi = mk((phi_xp - phi_xn) / (dx + dx), (phi_yp - phi_yn) / (dy + dy),
                            (phi_zp - phi_zn) / (dz + dz));
-    const double div_k_grad_p =
-        (2. * k_xp * k / (k_xp + k) * (p_xp - p) / dx - 2. * k_xn * k / (k_xn + k) * (p - p_xn) / dx) / dx +
-        (2. * k_yp * k / (k_yp + k) * (p_yp - p) / dy - 2. * k_yn * k / (k_yn + k) * (p - p_yn) / dy) / dy +
-        (2. * k_zp * k / (k_zp + k) * (p_zp - p) / dz - 2. * k_zn * k / (k_zn + k) * (p - p_zn) / dz) / dz;
-    const double ndt = P.ndem * dt;
-    double dp = ndt / (P.beta_f * phi * P.mu) * div_k_grad_p -
-                (ndt / (P.beta_f * phi * (1.0 - phi))) * (dphi / ndt + dot(vp_avg, grad_phi));
-    if ((P.bc_bot == 0 && z == 0) || (P.bc_top == 0 && z == nz - 1) ||
-        ((uint32_t)z >= D.st->wall0_iz && P.bc_top == 0) || (P.bc_xn == 0 && x == 0) ||
-        (P.bc_xp == 0 && x == nx - 1) || (P.bc_yn == 0 && y == 0) ||
-        (P.bc_yp == 0 && y == nx - 1) || p_constant == 1)
-        dp = 0.0;
-    return dp;
-}
-
-__global__ void k_darcy_first(StepArgs A, DarcyArgs D)
-{
-    if (!fluid_step(D)) return;
-    int x, y, z;
-    if (!cell_of(D, blockIdx.x * blockDim.x + threadIdx.x, x, y, z)) return;
-    D.dp_expl[d_idx(D, x, y, z)] = darcy_dp<false>(D, D.p, A.boxes[0].dt, x, y, z);
+    const double ndt = P.ndem * A.boxes[0].dt;
+    DpCoef q;
+    q.a[0] = 2. * k_xp * k / (k_xp + k);
+    q.a[1] = 2. * k_xn * k / (k_xn + k);
+    q.a[2] = 2. * k_yp * k / (k_yp + k);
+    q.a[3] = 2. * k_yn * k / (k_yn + k);
+    q.a[4] = 2. * k_zp * k / (k_zp + k);
+    q.a[5] = 2. * k_zn * k / (k_zn + k);
+    q.c1 = ndt / (P.beta_f * phi * P.mu);
+    q.f = (ndt / (P.beta_f * phi * (1.0 - phi))) * (dphi / ndt + dot(vp_avg, grad_phi));
+    q.zero = ((P.bc_bot == 0 && z == 0) || (P.bc_top == 0 && z == nz - 1) ||
+              ((uint32_t)z >= D.st->wall0_iz && P.bc_top == 0) || (P.bc_xn == 0 && x == 0) ||
+              (P.bc_xp == 0 && x == nx - 1) || (P.bc_yn == 0 && y == 0) ||
+              (P.bc_yp == 0 && y == nx - 1) || p_constant == 1)
+                 ? 1.0
+                 : 0.0;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) D.coef[(size_t)m * ncells + c] = q.a[m];
+    D.coef[(size_t)6 * ncells + c] = q.c1;
+    D.coef[(size_t)7 * ncells + c] = q.f;
+    D.coef[(size_t)8 * ncells + c] = q.zero;
+    D.dp_expl[ci] = dp_of<false>(D, q, D.p, x, y, z);
 }
 
 // The Jacobi loop of one fluid step (device.cu:2218-2376) as one
@@ -518,7 +567,6 @@ __global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, 
     const uint32_t nxy = (uint32_t)D.nx * (uint32_t)D.ny;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
-    const double dt = A.boxes[0].dt;
     const bool flux = P.bc_bot == 4 || P.bc_top == 4;
     const int gz = (D.nz + 7) / 8 * 8;
     const uint32_t wall0_iz = st->wall0_iz;
@@ -536,7 +584,7 @@ __global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, 
             int x, y, z;
             cell_of(D, c, x, y, z);
             const uint32_t ci = d_idx(D, x, y, z);
-            const double dp_impl = darcy_dp<true>(D, pc, dt, x, y, z);
+            const double dp_impl = dp_of<true>(D, load_coef(D, c, ncells), pc, x, y, z);
             const double epsilon = 0.5;
             const double p = __ldcg(pc + ci);
             double p_new = D.p_old[ci] + (1.0 - epsilon) * D.dp_expl[ci] + epsilon * dp_impl;

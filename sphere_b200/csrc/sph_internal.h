@@ -189,7 +189,11 @@ struct DarcyArgs {
     uint32_t *bar;
     unsigned long long *part_max;
     uint32_t *part_nan;
+    // per interior cell (x fastest), field-major, the parts of the pressure
+    // change that stay fixed during a solve (DARCY_COEF doubles per cell)
+    double *coef;
 };
+constexpr int DARCY_COEF = 9;
 constexpr uint32_t DARCY_PARTS = 8192;   // blocks of the Jacobi launch at most
 
 struct StepConfig {

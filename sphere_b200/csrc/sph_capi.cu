@@ -1246,12 +1246,12 @@ int sph_darcy_set(SphHandle *h, const SphDarcy *d, const double *p, const double
             (st = dalloc(h, &D.log_step, SPH_DARCY_LOG)) != SPH_OK ||
             (st = dalloc(h, &D.log_iters, SPH_DARCY_LOG)) != SPH_OK ||
             (st = dalloc(h, &D.log_ok, SPH_DARCY_LOG)) != SPH_OK ||
-            (st = dalloc(h, &D.bar, 2)) != SPH_OK ||
+            (st = dalloc(h, &D.bar, 1)) != SPH_OK ||
             (st = dalloc(h, &D.part_max, sph::DARCY_PARTS)) != SPH_OK ||
             (st = dalloc(h, &D.part_nan, sph::DARCY_PARTS)) != SPH_OK ||
             (st = dalloc(h, &D.coef, (uint64_t)sph::DARCY_COEF * nx * ny * nz)) != SPH_OK)
             return st;
-        CUDA_TRY(h, cudaMemset(D.bar, 0, 2 * sizeof(uint32_t)));
+        CUDA_TRY(h, cudaMemset(D.bar, 0, sizeof(unsigned long long)));
     }
     const bool modulated = (d->p_mod_A > 1.0e-5 || d->p_mod_A < -1.0e-5) && d->p_mod_f > 1.0e-7;
     if (modulated && !D.pmod) {

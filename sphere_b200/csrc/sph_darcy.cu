@@ -112,37 +112,48 @@ __device__ __forceinline__ void st3(double *p, d3 v)
     p[2] = v.z;
 }
 
-// darcy.cuh:212-285 setDarcyGhostNodes for cell (x, y, z) holding val (M
-// doubles): the ghost cells that copy this cell.
+// darcy.cuh:212-285 setDarcyGhostNodes: which ghost cells copy cell
+// (x, y, z), one bit per condition of the reference, six per axis: along an
+// axis of n cells with codes lo (at 0) and hi (at n - 1), bit 0: c == 0 and
+// lo == 0 (ghost -1), 1: c == 1 and lo == 1 (-1), 2: c == 0 and lo == 2
+// (n), 3: c == n - 1 and hi == 0 (n), 4: c == n - 2 and hi == 1 (n), 5:
+// c == n - 1 and hi == 2 (-1).  Bits 0-5 are x, 6-11 y, 12-17 z.
+__device__ __forceinline__ uint32_t ghost_axis(int c, int n, int lo, int hi)
+{
+    return (uint32_t)(c == 0 && lo == 0) | (uint32_t)(c == 1 && lo == 1) << 1 |
+           (uint32_t)(c == 0 && lo == 2) << 2 | (uint32_t)(c == n - 1 && hi == 0) << 3 |
+           (uint32_t)(c == n - 2 && hi == 1) << 4 | (uint32_t)(c == n - 1 && hi == 2) << 5;
+}
+__device__ __forceinline__ uint32_t ghost_bits(const DarcyArgs &D, int x, int y, int z)
+{
+    const SphDarcy &P = D.prm;
+    return ghost_axis(x, D.nx, P.bc_xn, P.bc_xp) | ghost_axis(y, D.ny, P.bc_yn, P.bc_yp) << 6 |
+           ghost_axis(z, D.nz, P.bc_bot, P.bc_top) << 12;
+}
+
+// The cell's value (M doubles) into the ghost cells of its bits (every
+// ghost gets the same value, so their order does not matter).
+template <int M>
+__device__ __forceinline__ void put_ghost_bits(const DarcyArgs &D, double *f, int x, int y, int z,
+                                               uint32_t bits, const double *val)
+{
+    while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        const int axis = b / 6, k = b - 6 * axis;
+        const int n = axis == 0 ? D.nx : axis == 1 ? D.ny : D.nz;
+        const int t = (k == 2 || k == 3 || k == 4) ? n : -1;
+        double *o = f + (size_t)M * d_idx(D, axis == 0 ? t : x, axis == 1 ? t : y, axis == 2 ? t : z);
+#pragma unroll
+        for (int m = 0; m < M; ++m) o[m] = val[m];
+    }
+}
+
 template <int M>
 __device__ __forceinline__ void put_ghosts(const DarcyArgs &D, double *f, int x, int y, int z,
                                            const double *val)
 {
-    const SphDarcy &P = D.prm;
-    const int nx = D.nx, ny = D.ny, nz = D.nz;
-    auto put = [&](int X, int Y, int Z) {
-        double *o = f + (size_t)M * d_idx(D, X, Y, Z);
-#pragma unroll
-        for (int m = 0; m < M; ++m) o[m] = val[m];
-    };
-    if (x == 0 && P.bc_xn == 0) put(-1, y, z);
-    if (x == 1 && P.bc_xn == 1) put(-1, y, z);
-    if (x == 0 && P.bc_xn == 2) put(nx, y, z);
-    if (x == nx - 1 && P.bc_xp == 0) put(nx, y, z);
-    if (x == nx - 2 && P.bc_xp == 1) put(nx, y, z);
-    if (x == nx - 1 && P.bc_xp == 2) put(-1, y, z);
-    if (y == 0 && P.bc_yn == 0) put(x, -1, z);
-    if (y == 1 && P.bc_yn == 1) put(x, -1, z);
-    if (y == 0 && P.bc_yn == 2) put(x, ny, z);
-    if (y == ny - 1 && P.bc_yp == 0) put(x, ny, z);
-    if (y == ny - 2 && P.bc_yp == 1) put(x, ny, z);
-    if (y == ny - 1 && P.bc_yp == 2) put(x, -1, z);
-    if (z == 0 && P.bc_bot == 0) put(x, y, -1);
-    if (z == 1 && P.bc_bot == 1) put(x, y, -1);
-    if (z == 0 && P.bc_bot == 2) put(x, y, nz);
-    if (z == nz - 1 && P.bc_top == 0) put(x, y, nz);
-    if (z == nz - 2 && P.bc_top == 1) put(x, y, nz);
-    if (z == nz - 1 && P.bc_top == 2) put(x, y, -1);
+    put_ghost_bits<M>(D, f, x, y, z, ghost_bits(D, x, y, z), val);
 }
 
 // Whether this step updates the fluid (set by k_darcy_begin).
@@ -420,10 +431,6 @@ __global__ void k_darcy_pre(DarcyArgs D)
 }
 
 // darcy.cuh:1644-1923 firstDarcySolution and :1926-2226
-// updateDarcySolution: the pressure change of the diffusion term (harmonic
-// means of k across the faces) and of the porosity forcing, zero at
-// Dirichlet boundaries, above the wall and in cells of constant pressure
-// darcy.cuh:1644-1923 firstDarcySolution and :1926-2226
 // updateDarcySolution: the pressure change
 //   ndt/(beta_f phi mu) div(k grad p) - ndt/(beta_f phi (1 - phi))
 //                                       (dphi/ndt + vp_avg . grad phi),
@@ -452,36 +459,72 @@ __device__ __forceinline__ DpCoef load_coef(const DarcyArgs &D, uint32_t c, uint
     return q;
 }
 
-template <bool CG>
-__device__ __forceinline__ double ldp(const double *p, uint32_t i)
+// a / b correctly rounded for a divisor b that stays fixed (the cell
+// sizes), from rb = RN(1 / b), by Markstein's correction (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990): q0 = RN(a rb) lies within one
+// ulp of a / b, the remainder r = a - b q0 is exact (one FMA), and
+// RN(q0 + r rb) is the correctly rounded quotient while q0 is a normal
+// number away from the ends of the range.  A zero a gives q0 = +-0, the
+// quotient with its sign (rb has the sign of b); tiny, huge, infinite and
+// NaN q0 take the division itself.  One multiply and two FMAs instead of a
+// division sequence -- and no division at all for the zero differences of
+// a pressure field at rest, which are most of them in a layered pack.
+struct CellInv {
+    double rx, ry, rz;
+};
+__device__ __forceinline__ CellInv cell_inv(const DarcyArgs &D)
 {
-    return CG ? __ldcg(p + i) : p[i];
+    return CellInv{1.0 / D.dx, 1.0 / D.dy, 1.0 / D.dz};
+}
+__device__ __forceinline__ double div_fixed(double a, double b, double rb)
+{
+    const double q0 = __dmul_rn(a, rb);
+    const double aq = fabs(q0);
+    if (aq > 0x1p-900 && aq < 0x1p+1000) return __fma_rn(__fma_rn(-q0, b, a), rb, q0);
+    if (a == 0.0) return q0;
+    return a / b;
 }
 
-// CG: the pressures are read past L1 (inside the persistent loop, where
-// other blocks wrote them since the last barrier)
-template <bool CG>
-__device__ __forceinline__ double dp_of(const DarcyArgs &D, const DpCoef &q, const double *pf, int x,
-                                        int y, int z)
+// The pressure change from the pressures of the cell and its six
+// neighbours (no-flow faces already replaced by the cell's own), with the
+// divisions by the cell sizes as div_fixed (the same quotients).  It is
+// evaluated also for a cell whose change is zero (the value is then
+// dropped), so that the stencil's loads need not wait for the flag.
+__device__ __forceinline__ double dp_stencil(const DarcyArgs &D, const DpCoef &q, const CellInv &iv,
+                                             double p, double p_xn, double p_xp, double p_yn,
+                                             double p_yp, double p_zn, double p_zp)
 {
-    if (q.zero != 0.0) return 0.0;
+    // (a0 (p_xp - p) / dx - a1 (p - p_xn) / dx) / dx + ... (y, z alike)
+    auto axis = [&](double a_p, double a_n, double pp, double pn_, double h, double rh) {
+        const double t1 = div_fixed(a_p * (pp - p), h, rh);
+        const double t2 = div_fixed(a_n * (p - pn_), h, rh);
+        return div_fixed(t1 - t2, h, rh);
+    };
+    const double div_k_grad_p = axis(q.a[0], q.a[1], p_xp, p_xn, D.dx, iv.rx) +
+                                axis(q.a[2], q.a[3], p_yp, p_yn, D.dy, iv.ry) +
+                                axis(q.a[4], q.a[5], p_zp, p_zn, D.dz, iv.rz);
+    const double dp = q.c1 * div_k_grad_p - q.f;
+    return q.zero != 0.0 ? 0.0 : dp;
+}
+
+// The pressure change of cell (x, y, z) for the pressure field pf.
+__device__ __forceinline__ double dp_of(const DarcyArgs &D, const DpCoef &q, const double *pf, int x,
+                                        int y, int z, const CellInv &iv)
+{
     const SphDarcy &P = D.prm;
-    const double dx = D.dx, dy = D.dy, dz = D.dz;
-    double p_xn = ldp<CG>(pf, d_idx(D, x - 1, y, z));
-    const double p = ldp<CG>(pf, d_idx(D, x, y, z));
-    double p_xp = ldp<CG>(pf, d_idx(D, x + 1, y, z));
-    double p_yn = ldp<CG>(pf, d_idx(D, x, y - 1, z)), p_yp = ldp<CG>(pf, d_idx(D, x, y + 1, z));
-    double p_zn = ldp<CG>(pf, d_idx(D, x, y, z - 1)), p_zp = ldp<CG>(pf, d_idx(D, x, y, z + 1));
+    double p_xn = pf[d_idx(D, x - 1, y, z)];
+    const double p = pf[d_idx(D, x, y, z)];
+    double p_xp = pf[d_idx(D, x + 1, y, z)];
+    double p_yn = pf[d_idx(D, x, y - 1, z)], p_yp = pf[d_idx(D, x, y + 1, z)];
+    double p_zn = pf[d_idx(D, x, y, z - 1)], p_zp = pf[d_idx(D, x, y, z + 1)];
     if (x == 0 && P.bc_xn == 1) p_xn = p;
     if (x == D.nx - 1 && P.bc_xp == 1) p_xp = p;
     if (y == 0 && P.bc_yn == 1) p_yn = p;
     if (y == D.ny - 1 && P.bc_yp == 1) p_yp = p;
     if (z == 0 && P.bc_bot == 1) p_zn = p;
     if (z == D.nz - 1 && P.bc_top == 1) p_zp = p;
-    const double div_k_grad_p = (q.a[0] * (p_xp - p) / dx - q.a[1] * (p - p_xn) / dx) / dx +
-                                (q.a[2] * (p_yp - p) / dy - q.a[3] * (p - p_yn) / dy) / dy +
-                                (q.a[4] * (p_zp - p) / dz - q.a[5] * (p - p_zn) / dz) / dz;
-    return q.c1 * div_k_grad_p - q.f;
+    return dp_stencil(D, q, iv, p, p_xn, p_xp, p_yn, p_yp, p_zn, p_zp);
 }
 
 // The fixed parts of the pressure change of each cell (above), and the
@@ -531,7 +574,91 @@ __global__ void k_darcy_first(StepArgs A, DarcyArgs D)
     D.coef[(size_t)6 * ncells + c] = q.c1;
     D.coef[(size_t)7 * ncells + c] = q.f;
     D.coef[(size_t)8 * ncells + c] = q.zero;
-    D.dp_expl[ci] = dp_of<false>(D, q, D.p, x, y, z);
+    D.dp_expl[ci] = dp_of(D, q, D.p, x, y, z, cell_inv(D));
+}
+
+// A cell of the Jacobi loop with what stays fixed for it during a solve:
+// its coordinates and padded index, the coefficients of its pressure
+// change, the part of the new pressure that does not depend on the iterate
+// (p_old + (1 - epsilon) dp_expl, the reference's first two terms), the
+// term of the flux ghost (-mu / k q_z dz, bc 4), and flags: bits 0-17 the
+// ghost cells that copy it (ghost_bits), 18-23 the neighbours (xn, xp, yn,
+// yp, zn, zp) a no-flow face (bc 1) replaces by the cell itself, 24 and 25
+// the flux ghost below and above.
+struct JCell {
+    int x, y, z;
+    uint32_t ci, bits;
+    DpCoef q;
+    double base, flux_t;
+};
+
+constexpr double JACOBI_EPSILON = 0.5;   // darcy.cuh updateDarcySolution
+constexpr double JACOBI_THETA = 0.05;
+
+__device__ __forceinline__ JCell jcell_init(const DarcyArgs &D, uint32_t c, uint32_t ncells, double dzf)
+{
+    const SphDarcy &P = D.prm;
+    JCell j;
+    cell_of(D, c, j.x, j.y, j.z);
+    const int x = j.x, y = j.y, z = j.z;
+    j.ci = d_idx(D, x, y, z);
+    j.q = load_coef(D, c, ncells);
+    j.base = D.p_old[j.ci] + (1.0 - JACOBI_EPSILON) * D.dp_expl[j.ci];
+    uint32_t b = ghost_bits(D, x, y, z);
+    b |= (uint32_t)(x == 0 && P.bc_xn == 1) << 18 | (uint32_t)(x == D.nx - 1 && P.bc_xp == 1) << 19 |
+         (uint32_t)(y == 0 && P.bc_yn == 1) << 20 | (uint32_t)(y == D.ny - 1 && P.bc_yp == 1) << 21 |
+         (uint32_t)(z == 0 && P.bc_bot == 1) << 22 | (uint32_t)(z == D.nz - 1 && P.bc_top == 1) << 23;
+    j.flux_t = 0.0;
+    if (P.bc_bot == 4 || P.bc_top == 4) {
+        // darcy.cuh setDarcyGhostNodesFlux: p_ghost = -mu / k q_z dz + p
+        double q_z = 0.;
+        if (z == 0) q_z = P.bc_bot_flux;
+        else if (z == D.nz - 1) q_z = P.bc_top_flux;
+        j.flux_t = -P.mu / D.k[j.ci] * q_z * dzf;
+        b |= (uint32_t)(z == 0 && P.bc_bot == 4) << 24 | (uint32_t)(z == D.nz - 1 && P.bc_top == 4) << 25;
+    }
+    j.bits = b;
+    return j;
+}
+
+// One Jacobi update of the cell (reads pc, writes pn), and on a checked
+// iteration its normalised residual into the running maximum.
+__device__ __forceinline__ void jcell_update(const DarcyArgs &D, const JCell &j, const double *pc,
+                                             double *pn, const CellInv &iv, bool check,
+                                             unsigned long long &bmax, uint32_t &bnan)
+{
+    const uint32_t sy = (uint32_t)D.nx + 2u, sz = sy * ((uint32_t)D.ny + 2u);
+    const uint32_t ci = j.ci;
+    const double p = __ldcg(pc + ci);
+    double p_xn = __ldcg(pc + ci - 1u), p_xp = __ldcg(pc + ci + 1u);
+    double p_yn = __ldcg(pc + ci - sy), p_yp = __ldcg(pc + ci + sy);
+    double p_zn = __ldcg(pc + ci - sz), p_zp = __ldcg(pc + ci + sz);
+    const uint32_t b = j.bits;
+    if (b & (1u << 18)) p_xn = p;
+    if (b & (1u << 19)) p_xp = p;
+    if (b & (1u << 20)) p_yn = p;
+    if (b & (1u << 21)) p_yp = p;
+    if (b & (1u << 22)) p_zn = p;
+    if (b & (1u << 23)) p_zp = p;
+    const double dp_impl = dp_stencil(D, j.q, iv, p, p_xn, p_xp, p_yn, p_yp, p_zn, p_zp);
+    double p_new = j.base + JACOBI_EPSILON * dp_impl;
+    p_new = p * (1.0 - JACOBI_THETA) + p_new * JACOBI_THETA;
+    if (b & (1u << 24)) __stcg(pn + ci - sz, j.flux_t + p);
+    if (b & (1u << 25)) __stcg(pn + ci + sz, j.flux_t + p);
+    __stcg(pn + ci, p_new);
+    if (b & 0x3ffffu) put_ghost_bits<1>(D, pn, j.x, j.y, j.z, b & 0x3ffffu, &p_new);
+    if (check) {
+        // the normalised residual; a zero change skips the division (its
+        // quotient is +-0 unless the divisor is zero or NaN)
+        const double num = p_new - p, den = p + 1.0e-16;
+        const double r = (num == 0.0 && den == den && den != 0.0) ? 0.0 : fabs(num / den);
+        if (r != r) {
+            bnan = 1u;
+        } else {
+            const unsigned long long v = (unsigned long long)__double_as_longlong(r);
+            bmax = v > bmax ? v : bmax;
+        }
+    }
 }
 
 // The Jacobi loop of one fluid step (device.cu:2218-2376) as one
@@ -549,17 +676,22 @@ __global__ void k_darcy_first(StepArgs A, DarcyArgs D)
 // z = wall0_iz + 1 from z = wall0_iz - 1 in the array just read) runs
 // between two barriers.  Every tenth iteration (src/debug.h:16 nijacnorm)
 // each block's largest |residual| (the bits of a non-negative double,
-// which order as the values do) and whether one was NaN go to per-block
-// slots; after the barrier every block reads all slots and takes the same
-// decision: stop when the largest residual is within the tolerance, or one
-// was NaN (SPH_ERR_NAN); stop after maxiter iterations.  The final
-// pressure ends up in D.p.  The barriers are bounded (SPH_ERR_TIMEOUT); the
-// pressures other blocks write are read past L1.  Block 0 logs the solve.
-__global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, DarcyArgs D, GridSync G)
+// which order as the values do) and whether one was NaN go to the block's
+// slot as it arrives at the barrier; after the barrier each warp reads all
+// slots and takes the same decision as every other warp: stop when the
+// largest residual is within the tolerance, or one was NaN (SPH_ERR_NAN);
+// stop after maxiter iterations.  The final pressure ends up in D.p.  The
+// barrier counts arrivals on a counter that only grows (D.bar, zeroed
+// before the launch) and is bounded (SPH_ERR_TIMEOUT); the pressures other
+// blocks write are read past L1.  Block 0 logs the solve.
+// ONE: every thread has at most one cell, whose fixed state (JCell) it
+// keeps in registers for the whole solve; otherwise each thread takes its
+// cells in turn and gathers their state at every iteration.
+template <bool ONE>
+__global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, DarcyArgs D)
 {
     __shared__ unsigned long long s_max[JACOBI_THREADS / 32];
     __shared__ uint32_t s_nan[JACOBI_THREADS / 32];
-    __shared__ int s_stop, s_ok, s_bad;
     DarcyState *st = D.st;
     const SphDarcy &P = D.prm;
     if (!(st->active && P.maxiter > 0)) return;   // the same in every block
@@ -567,11 +699,17 @@ __global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, 
     const uint32_t nxy = (uint32_t)D.nx * (uint32_t)D.ny;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool flux = P.bc_bot == 4 || P.bc_top == 4;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const int gz = (D.nz + 7) / 8 * 8;
     const uint32_t wall0_iz = st->wall0_iz;
     const double dzf = A.boxes[0].L[2] / D.nz;
     double *const buf[2] = {D.p, D.p_new};
+    const CellInv iv = cell_inv(D);
+    const bool mine = first < ncells;
+    JCell own;
+    if (ONE && mine) own = jcell_init(D, first, ncells, dzf);
+    unsigned long long target = 0ull;   // arrivals the next barrier waits for
+    auto no_arrival_work = [] {};
     uint32_t nijac = 0;
     int ok = 0, bad = 0;
     for (;;) {
@@ -580,37 +718,11 @@ __global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, 
         const bool check = (nijac % 10u) == 0u;
         unsigned long long bmax = 0ull;
         uint32_t bnan = 0u;
-        for (uint32_t c = first; c < ncells; c += stride) {
-            int x, y, z;
-            cell_of(D, c, x, y, z);
-            const uint32_t ci = d_idx(D, x, y, z);
-            const double dp_impl = dp_of<true>(D, load_coef(D, c, ncells), pc, x, y, z);
-            const double epsilon = 0.5;
-            const double p = __ldcg(pc + ci);
-            double p_new = D.p_old[ci] + (1.0 - epsilon) * D.dp_expl[ci] + epsilon * dp_impl;
-            const double theta = 0.05;
-            p_new = p * (1.0 - theta) + p_new * theta;
-            const double res_norm = (p_new - p) / (p + 1.0e-16);
-            if (flux) {
-                const double k = D.k[ci];
-                double q_z = 0.;
-                if (z == 0) q_z = P.bc_bot_flux;
-                else if (z == D.nz - 1) q_z = P.bc_top_flux;
-                const double p_ghost = -P.mu / k * q_z * dzf + p;
-                if (z == 0 && P.bc_bot == 4) __stcg(pn + d_idx(D, x, y, -1), p_ghost);
-                if (z == D.nz - 1 && P.bc_top == 4) __stcg(pn + d_idx(D, x, y, D.nz), p_ghost);
-            }
-            __stcg(pn + ci, p_new);
-            put_ghosts<1>(D, pn, x, y, z, &p_new);
-            if (check) {
-                const double r = fabs(res_norm);
-                if (r != r) {
-                    bnan = 1u;
-                } else {
-                    const unsigned long long b = (unsigned long long)__double_as_longlong(r);
-                    bmax = b > bmax ? b : bmax;
-                }
-            }
+        if (ONE) {
+            if (mine) jcell_update(D, own, pc, pn, iv, check, bmax, bnan);
+        } else {
+            for (uint32_t c = first; c < ncells; c += stride)
+                jcell_update(D, jcell_init(D, c, ncells, dzf), pc, pn, iv, check, bmax, bnan);
         }
         if (check) {
             for (int o = 16; o > 0; o >>= 1) {
@@ -618,27 +730,17 @@ __global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, 
                 bmax = b > bmax ? b : bmax;
             }
             const uint32_t anynan = __any_sync(0xffffffffu, bnan != 0u) ? 1u : 0u;
-            if ((threadIdx.x & 31) == 0) {
-                s_max[threadIdx.x >> 5] = bmax;
-                s_nan[threadIdx.x >> 5] = anynan;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                unsigned long long m = 0ull;
-                uint32_t nn = 0u;
-                for (int w = 0; w < JACOBI_THREADS / 32; ++w) {
-                    m = s_max[w] > m ? s_max[w] : m;
-                    nn |= s_nan[w];
-                }
-                __stcg(D.part_max + blockIdx.x, m);
-                __stcg(D.part_nan + blockIdx.x, nn);
+            if (lane == 0) {
+                s_max[warp] = bmax;
+                s_nan[warp] = anynan;
             }
         }
         if (P.bc_top == 1) {
             // after every cell has read the array it writes; cells past the
             // padded array (a wall at or above the top of the grid) are
             // skipped
-            if (!grid_barrier_acqrel(G, gridDim.x, A.err)) return;
+            target += gridDim.x;
+            if (!grid_sync_count(D.bar, target, BARRIER_LIMIT_NS, A.err, no_arrival_work)) return;
             const uint32_t z = wall0_iz + 1u;
             if (z < (uint32_t)gz)
                 for (uint32_t t = first; t < nxy; t += stride) {
@@ -647,34 +749,47 @@ __global__ void __launch_bounds__(JACOBI_THREADS, 1) k_darcy_jacobi(StepArgs A, 
                     if (w < D.ncell && r < D.ncell) __stcg(pc + w, __ldcg(pc + r));
                 }
         }
-        if (!grid_barrier_acqrel(G, gridDim.x, A.err)) return;
-        if (threadIdx.x == 0) {
-            int stop = 0, good = 0, nanseen = 0;
-            if (check) {
-                unsigned long long m = 0ull;
-                uint32_t nn = 0u;
-                for (uint32_t b = 0; b < gridDim.x; ++b) {
-                    const unsigned long long v = __ldcg(D.part_max + b);
-                    m = v > m ? v : m;
-                    nn |= __ldcg(D.part_nan + b);
-                }
-                if (nn) {
-                    stop = 1;
-                    nanseen = 1;
-                } else if (__longlong_as_double((long long)m) <= P.tolerance) {
-                    stop = 1;
-                    good = 1;
-                }
+        // the block's largest residual goes out with its arrival (thread 0,
+        // after the block barrier that makes the warps' values visible)
+        target += gridDim.x;
+        const bool passed = grid_sync_count(D.bar, target, BARRIER_LIMIT_NS, A.err, [&] {
+            if (!check) return;
+            unsigned long long m = 0ull;
+            uint32_t nn = 0u;
+            for (int w = 0; w < JACOBI_THREADS / 32; ++w) {
+                m = s_max[w] > m ? s_max[w] : m;
+                nn |= s_nan[w];
             }
-            if (!stop && nijac == P.maxiter - 1u) stop = 1;
-            s_stop = stop;
-            s_ok = good;
-            s_bad = nanseen;
+            __stcg(D.part_max + blockIdx.x, m);
+            __stcg(D.part_nan + blockIdx.x, nn);
+        });
+        if (!passed) return;
+        int stop = 0, good = 0, nanseen = 0;
+        if (check) {
+            // every warp reduces all blocks' slots itself: no block barrier
+            unsigned long long m = 0ull;
+            uint32_t nn = 0u;
+            for (uint32_t b = lane; b < gridDim.x; b += 32u) {
+                const unsigned long long v = __ldcg(D.part_max + b);
+                m = v > m ? v : m;
+                nn |= __ldcg(D.part_nan + b);
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long v = __shfl_xor_sync(0xffffffffu, m, o);
+                m = v > m ? v : m;
+            }
+            if (__any_sync(0xffffffffu, nn != 0u)) {
+                stop = 1;
+                nanseen = 1;
+            } else if (__longlong_as_double((long long)m) <= P.tolerance) {
+                stop = 1;
+                good = 1;
+            }
         }
-        __syncthreads();
-        if (s_stop) {
-            ok = s_ok;
-            bad = s_bad;
+        if (!stop && nijac == P.maxiter - 1u) stop = 1;
+        if (stop) {
+            ok = good;
+            bad = nanseen;
             if (pn != D.p)   // the result in D.p (every cell: the ghost layer too)
                 for (uint32_t c = first; c < D.ncell; c += stride) __stcg(D.p + c, __ldcg(pn + c));
             break;
@@ -799,16 +914,15 @@ int launch_darcy(const StepArgs &A, const DarcyArgs &D, const StepConfig &cfg, c
             int dev = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_darcy_jacobi, JACOBI_THREADS, 0);
+            int a = 0, b = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_darcy_jacobi<true>, JACOBI_THREADS, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_darcy_jacobi<false>, JACOBI_THREADS, 0);
+            per_sm = a < b ? a : b;
         }
         unsigned cap = (unsigned)(per_sm > 0 ? per_sm : 1) * (unsigned)sms;
         const unsigned need = blocks_for(ncells, JACOBI_THREADS);
         if (cap > DARCY_PARTS) cap = DARCY_PARTS;
-        GridSync G;
-        G.count = D.bar;
-        G.gen = D.bar + 1;
-        G.limit_ns = BARRIER_LIMIT_NS;
-        cudaMemsetAsync(D.bar, 0, sizeof(uint32_t), st);
+        cudaMemsetAsync(D.bar, 0, sizeof(unsigned long long), st);
         cudaLaunchConfig_t c = {};
         c.gridDim = dim3(need < cap ? need : cap);
         c.blockDim = dim3(JACOBI_THREADS);
@@ -818,7 +932,10 @@ int launch_darcy(const StepArgs &A, const DarcyArgs &D, const StepConfig &cfg, c
         at[0].val.cooperative = 1;
         c.attrs = at;
         c.numAttrs = 1;
-        if (cudaLaunchKernelEx(&c, k_darcy_jacobi, A, D, G) != cudaSuccess) return SPH_ERR_CUDA;
+        const bool one = (uint64_t)c.gridDim.x * JACOBI_THREADS >= ncells;
+        const cudaError_t le = one ? cudaLaunchKernelEx(&c, k_darcy_jacobi<true>, A, D)
+                                   : cudaLaunchKernelEx(&c, k_darcy_jacobi<false>, A, D);
+        if (le != cudaSuccess) return SPH_ERR_CUDA;
         nl += 2;
     }
     mark(prof, st, "k_darcy_jacobi");

@@ -184,9 +184,10 @@ struct DarcyArgs {
     const double *pmod;            // top pressure per queued step (DARCY_RING), null: no modulation
     uint64_t *log_step;            // the Jacobi log, a ring of SPH_DARCY_LOG entries
     uint32_t *log_iters, *log_ok;
-    // the Jacobi loop's cooperative launch: barrier words (count, generation)
-    // and the per-block largest |residual| and NaN flag of a checked iteration
-    uint32_t *bar;
+    // the Jacobi loop's cooperative launch: the arrival counter of its grid
+    // barrier (zeroed before each launch, only grows during it) and the
+    // per-block largest |residual| and NaN flag of a checked iteration
+    unsigned long long *bar;
     unsigned long long *part_max;
     uint32_t *part_nan;
     // per interior cell (x fastest), field-major, the parts of the pressure

@@ -97,4 +97,45 @@ __device__ __forceinline__ bool grid_barrier_acqrel(const GridSync &G, uint32_t 
     return s_ok != 0;
 }
 
+__device__ __forceinline__ unsigned long long ld_acquire_gpu_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// A grid-wide barrier on an arrival counter that only grows (zeroed before
+// the launch): at its n-th barrier (n = 1, 2, ...) each block adds one with
+// a release reduction, which needs no answer, and polls the counter with
+// acquire loads until it reaches n x nblocks.  Against the generation
+// barrier above this saves the load of the generation before the arrival
+// and the last block's publication after it.  `arrive` runs on thread 0
+// between the block barrier and the arrival, so what it writes (and what
+// the block wrote before the barrier) is released with the arrival.  Same
+// time limit and error as above.
+template <class F>
+__device__ __forceinline__ bool grid_sync_count(unsigned long long *ctr, unsigned long long target,
+                                                unsigned long long limit_ns, uint32_t *err, F arrive)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        arrive();
+        asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(ctr) : "memory");
+        const unsigned long long t0 = now_ns();
+        uint32_t polls = 0;
+        while (ld_acquire_gpu_u64(ctr) < target) {
+            if ((++polls & 63u) == 0u && now_ns() - t0 > limit_ns) {
+                ok = 0;
+                raise_flag(err, SPH_ERR_TIMEOUT);
+                break;
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 }  // namespace sph

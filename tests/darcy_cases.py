@@ -29,6 +29,23 @@ def fluid_box(p_top=0.0, dt=1.0e-7, file_every=0.99):
     return s
 
 
+def big_fluid_box():
+    """A pure-fluid box of 46 x 45 x 40 = 82,800 cells: more cells than one
+    Jacobi launch has threads on a B200 (148 blocks of 512), so that threads
+    take their cells in turn; no-flow x sides and a fixed flux at the
+    bottom, a pressure step at the top."""
+    s = sphere_b200.sim(np=0, nd=3, nw=0, sid="cfdbig", fluid=True)
+    s.defaultParams()
+    s.defineWorldBoundaries([4.6, 4.5, 4.0], dx=0.1)
+    s.initFluid(cfd_solver=1)
+    s.initTemporal(total=0.2, file_dt=0.01, dt=1.0e-6)
+    s.time_file_dt[0] = s.time_dt[0] * 0.99
+    s.setFluidXNoFlow()
+    s.setFluidBottomFixedFlux(1.0e-5)
+    s.p_f[:, :, -1] = 1.0
+    return s
+
+
 fluid_pack = scenes.darcy_pack
 
 

@@ -60,6 +60,19 @@ def test_darcy_step_equals_oracle(name):
     compare(hp, fluid, log, oracle_run(s, steps), name)
 
 
+def test_darcy_grid_with_more_cells_than_threads():
+    """82,800 cells: the Jacobi threads take several cells each (the other
+    form of the loop); still the oracle's every bit."""
+    s = darcy_cases.big_fluid_box()
+    hp, fluid, log = gpu_run(s, [3])
+    r = oracle_run(s, 3)
+    for f, g in (("p_f", "p"), ("v_f", "v"), ("phi", "phi"), ("k", "k")):
+        assert numpy.array_equal(fluid[f], r.fluid_cells(g)), f
+    step, iters, ok = r.darcy_log()
+    assert log[1] == iters.tolist() and log[2] == ok.tolist()
+    assert min(iters) > 10
+
+
 @pytest.mark.parametrize("name", ["darcy_pack_wall", "darcy_pack_modulated", "darcy_pack_bcs"])
 def test_darcy_steps_split_into_calls_change_no_bit(name):
     s, steps = darcy_cases.make(name)

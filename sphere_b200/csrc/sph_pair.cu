@@ -520,14 +520,50 @@ __global__ void __launch_bounds__(NT, MINB) k_pair_step_async(StepArgs A, PairAr
     finish_sphere<LM>(A, P, B, i, nxt, ls, xa, wa, acc, live_old, live_new);
 }
 
-// Wall-force sum of one chunk of 2^chunk_log2 spheres of one box: each
-// thread adds its strided share in index order, then a fixed shuffle tree
-// and the warps' sums in warp order (FP64, the same order every step).
+// Wall-force sum of one chunk of 2^chunk_log2 spheres of one box, and the
+// sum of a box's chunks: FP64 sums in a fixed order, the same whatever the
+// block that runs them (the chunk and box kernels, or the persistent
+// kernel with its own block size).
 constexpr int CHUNK_THREADS = 256;
+constexpr int PBOX_THREADS = 128;
 
-// The wall-force sum of chunk c by the calling block (blockDim.x threads, a
-// multiple of 32, at most 1024): each thread adds its strided share in
-// index order, then a fixed shuffle tree and the warps' sums in warp order.
+// The sum of get(0), ..., get(n - 1) in a fixed order for a given V: term k
+// goes to virtual lane k mod V, each lane adds its terms in index order,
+// each group of 32 lanes is reduced by the xor-shuffle tree, and the V / 32
+// group sums are added in order.  The block's threads (blockDim.x, a
+// multiple of 32 dividing V, at least V / 4) play lanes t, t + blockDim.x,
+// ...: thread t of warp w holds lane t + j blockDim.x, whose group is
+// w + j blockDim.x / 32, with the same lane in it.  Thread 0 returns the
+// sum (the others 0).
+template <int V, class G>
+__device__ __forceinline__ double ordered_sum(uint32_t n, G get, double *s_w)
+{
+    constexpr int RMAX = 4;
+    const uint32_t nt = blockDim.x, r = V / nt;
+    double acc[RMAX];
+#pragma unroll
+    for (int j = 0; j < RMAX; ++j) {
+        double s = 0.0;
+        if ((uint32_t)j < r)
+            for (uint32_t k = threadIdx.x + (uint32_t)j * nt; k < n; k += V) s += get(k);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        acc[j] = s;
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31u) == 0) {
+#pragma unroll
+        for (int j = 0; j < RMAX; ++j)
+            if ((uint32_t)j < r) s_w[(threadIdx.x >> 5) + (uint32_t)j * (nt >> 5)] = acc[j];
+    }
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < V / 32; ++w) t += s_w[w];
+    return t;
+}
+
+// The wall-force sum of chunk c by the calling block.
 __device__ __forceinline__ void chunk_sum(const StepArgs &A, const PairArgs &P, uint32_t c,
                                           double *s_w)
 {
@@ -535,19 +571,10 @@ __device__ __forceinline__ void chunk_sum(const StepArgs &A, const PairArgs &P, 
     const DevBox &B = A.boxes[bx];
     const uint32_t start = (c - P.box_chunk0[bx]) << P.chunk_log2;
     const uint32_t end = min(B.np, start + (1u << P.chunk_log2));
-    double s = 0.0;
-    if (B.nw > 0)
-        for (uint32_t k = start + threadIdx.x; k < end; k += blockDim.x) s += A.wf_pp[B.p_base + k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    __syncthreads();
-    if ((threadIdx.x & 31u) == 0) s_w[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (uint32_t w = 0; w < blockDim.x / 32; ++w) t += s_w[w];
-        P.chunk_part[c] = t;
-    }
+    const double *wf = A.wf_pp + B.p_base + start;
+    const double t = ordered_sum<CHUNK_THREADS>(B.nw > 0 ? end - start : 0u,
+                                                [&](uint32_t k) { return wf[k]; }, s_w);
+    if (threadIdx.x == 0) P.chunk_part[c] = t;
 }
 
 // Box bx by the calling block: its chunks' sums in a fixed order (FP64),
@@ -558,22 +585,11 @@ __device__ __forceinline__ void box_sum_advance(const StepArgs &A, const PairArg
     DevBox &B = A.boxes[bx];
     bool any = false;
     for (uint32_t w = 0; w < B.nw; ++w) any = any || B.wmode[w] != 0;
-    double s = 0.0;
-    if (B.np > 0 && any) {
-        const uint32_t c0 = P.box_chunk0[bx];
-        const uint32_t nch = (B.np + (1u << P.chunk_log2) - 1) >> P.chunk_log2;
-        for (uint32_t k = threadIdx.x; k < nch; k += blockDim.x) s += P.chunk_part[c0 + k];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    __syncthreads();
-    if ((threadIdx.x & 31u) == 0) s_w[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double fsum = 0.0;
-        for (uint32_t w = 0; w < blockDim.x / 32; ++w) fsum += s_w[w];
-        advance_box(B, fsum);
-    }
+    uint32_t nch = 0;
+    if (B.np > 0 && any) nch = (B.np + (1u << P.chunk_log2) - 1) >> P.chunk_log2;
+    const double *part = P.chunk_part + P.box_chunk0[bx];
+    const double fsum = ordered_sum<PBOX_THREADS>(nch, [&](uint32_t k) { return part[k]; }, s_w);
+    if (threadIdx.x == 0) advance_box(B, fsum);
 }
 
 __global__ void __launch_bounds__(CHUNK_THREADS) k_pair_chunks(StepArgs A, PairArgs P)
@@ -585,7 +601,6 @@ __global__ void __launch_bounds__(CHUNK_THREADS) k_pair_chunks(StepArgs A, PairA
 
 // Per box: the chunks' sums, integrateWalls, time; block 0 then hands the
 // ping-pong state to the next step.
-constexpr int PBOX_THREADS = 128;
 
 __global__ void __launch_bounds__(PBOX_THREADS) k_pair_box(StepArgs A, PairArgs P)
 {

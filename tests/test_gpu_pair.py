@@ -199,6 +199,36 @@ def test_pair_ensemble_box_by_box():
     b.close()
 
 
+def test_pair_shapes_same_bits_under_a_loaded_wall():
+    """A 6,000-sphere sheared pack with its top wall lowered onto the pack:
+    over a hundred spheres press on it, so the wall-force sums (per chunk of
+    spheres, then per box) add many terms; the persistent shapes run them
+    with their own block sizes and must add them in the same order as the
+    chunk and box kernels."""
+    s = scenes.sheared_dense_pack(n=6000, seed=4, device=0, sweeps=800)
+    # the wall lowered onto the pack's top 2 % (held spheres, overlaps of
+    # about 1e-4 m at most)
+    s.w_x[0] = numpy.quantile(s.x[:, 2] + s.radius, 0.98)
+    out = {}
+    for shape in range(_abi.PAIR_SHAPES):
+        st = Stepper([copy.deepcopy(s)], precision="mixed")
+        st.set_variant(PAIR)
+        st.set_launch_shape(shape)
+        st.upload()
+        st.step(20)
+        hp, _ = st.download()
+        out[shape] = (hp, st.boxes()[0])
+        st.close()
+    a, ba = out[0]
+    # spheres in contact with the top wall (x[:, 3] is the radius)
+    assert numpy.count_nonzero(a.x[:, 2] + a.x[:, 3] > ba.walls.nx[0][3]) > 100
+    for shape, (b, bb) in out.items():
+        assert list(ba.walls.mvfd[0]) == list(bb.walls.mvfd[0]), shape
+        assert list(ba.walls.nx[0]) == list(bb.walls.nx[0]), shape
+        for f in ("x", "vel", "force"):
+            assert numpy.array_equal(getattr(a, f), getattr(b, f)), (shape, f)
+
+
 @pytest.mark.parametrize("name", ["fast_spheres", "periodic_xy_wall_stress"])
 def test_pair_shapes_give_the_same_bits(name):
     """Every launch shape of the list step (register budgets, staged

@@ -706,11 +706,13 @@ def main():
         except Exception:
             pass
         tuning = st.tuning()
+        shape_ms = [round(float(v), 4) for v in st.shape_times()] if variant_ms is not None else []
         st.close()
         ms_step = ms_max / args.steps
         return {"value": world * n * args.steps / (ms_max / 1e3), "ms_per_step": ms_step,
                 "variant": variant, "variant_ms_per_step": variant_ms,
-                "tuning": {"variant": tuning[0], "list_step_shape": tuning[1]},
+                "tuning": {"variant": tuning[0], "list_step_shape": tuning[1],
+                           "list_step_shape_ms": shape_ms},
                 "neighbor_lists": nstats,
                 "roofline": roofline, "kernel_ms": kernels, "live_contacts": contacts,
                 "gpu_launches": launches, "clocks": clk, "device_status": code,

@@ -337,6 +337,11 @@ int sph_set_variant(SphHandle *h, int variant);
 #define SPH_PAIR_SHAPES 13
 int sph_set_launch_shape(SphHandle *h, int shape);
 int sph_get_tuning(const SphHandle *h, int *variant, int *shape);
+/* The last sph_autotune's time per step (ms) of the list step at each
+ * launch shape, into ms[0 .. n-1] (-1: not tried, or past
+ * SPH_PAIR_SHAPES).  sph_autotune times every candidate twice, in two
+ * rounds over all of them, and keeps each one's better time. */
+int sph_get_shape_times(const SphHandle *h, double *ms, int n);
 
 /* Shapes 9 (64 x 8) and 10 (128 x 4) of the list step are persistent: one
  * cooperative launch per step whose blocks (all resident) take the spheres

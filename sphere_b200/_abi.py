@@ -284,6 +284,8 @@ def load_library():
     lib.sph_set_launch_shape.restype = C.c_int
     lib.sph_get_tuning.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.sph_get_tuning.restype = C.c_int
+    lib.sph_get_shape_times.argtypes = [H, _dp, C.c_int]
+    lib.sph_get_shape_times.restype = C.c_int
     lib.sph_barrier_check.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double]
     lib.sph_barrier_check.restype = C.c_int
     lib.sph_set_neighbor_lists.restype = C.c_int

@@ -101,9 +101,15 @@ struct PairArgs {
     float4 *angpos, *acc, *angacc, *force, *torque, *epp;
     double2 *eacc;
     double4 *xyzsum;
+    // the lists and histories, entry-major (entry k of every sphere side by
+    // side): sphere i's entry k at ids[k * nrow + i], its history component
+    // c at hist[(3 k + c) * nrow + i] (nrow = the spheres of the handle), so
+    // that the threads of a warp read entry k of their lists from a few
+    // lines instead of one line each
     uint32_t *ids[2], *cnt[2];
     uint64_t *live[2];
     double *hist[2];
+    uint32_t nrow;
     // the order in which the step kernel's threads take the spheres: within
     // each group of PAIR_ORDER_GROUP consecutive spheres, by list length
     // (built with each list), so that a warp's lists are of similar length

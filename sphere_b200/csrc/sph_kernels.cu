@@ -218,9 +218,12 @@ constexpr int VLIST_THREADS = 128;
 // without repeats.  A sphere that moves less than vskin / 2 (checked in the
 // integration against xref) keeps every sphere it can touch in its list.
 // Runs only when vflag[0] is set; a list that overflows vcap (<= VL_MAX) is
-// marked VL_MAX + 1 and that sphere uses the cell search.
+// marked VL_MAX + 1 and that sphere uses the cell search.  Entry k of
+// sphere i goes to vlist[i * row_stride + k * k_stride] (rows of VL_MAX for
+// the FP64 form's lists, entry-major for the list step's).
 __device__ __forceinline__ void vlist_build_one(const StepArgs &A, uint32_t a, uint32_t *lst,
-                                                uint32_t *vlist, uint32_t *vcount, uint32_t cap)
+                                                uint32_t *vlist, uint32_t *vcount, uint32_t cap,
+                                                uint32_t row_stride, uint32_t k_stride)
 {
     const int RS = VLIST_THREADS;
     const uint32_t i = A.perm[a];
@@ -270,8 +273,8 @@ __device__ __forceinline__ void vlist_build_one(const StepArgs &A, uint32_t a, u
         vcount[i] = VL_MAX + 1;
         return;
     }
-    uint32_t *out = vlist + (size_t)i * VL_MAX;
-    for (int k = 0; k < n; ++k) out[k] = lst[k * RS];
+    uint32_t *out = vlist + (size_t)i * row_stride;
+    for (int k = 0; k < n; ++k) out[(size_t)k * k_stride] = lst[k * RS];
     vcount[i] = (uint32_t)n;
 }
 
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(VLIST_THREADS) k_vlist_build(StepArgs A)
     __shared__ uint32_t s_list[VL_MAX * VLIST_THREADS];
     for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < A.ntot;
          a += gridDim.x * blockDim.x)
-        vlist_build_one(A, a, s_list + threadIdx.x, A.vlist, A.vcount, A.vcap);
+        vlist_build_one(A, a, s_list + threadIdx.x, A.vlist, A.vcount, A.vcap, VL_MAX, 1u);
 }
 
 // The list step's rebuild (sph_pair.cu): its current positions into A.x for
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(VLIST_THREADS) k_pair_vlist(StepArgs A, PairAr
     __shared__ uint32_t s_list[VL_MAX * VLIST_THREADS];
     const uint32_t alt = *P.lsel ^ 1u;
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a < A.ntot) vlist_build_one(A, a, s_list + threadIdx.x, P.ids[alt], P.cnt[alt], VL_MAX);
+    if (a < A.ntot) vlist_build_one(A, a, s_list + threadIdx.x, P.ids[alt], P.cnt[alt], VL_MAX, 1u, P.nrow);
 }
 
 // After the (possible) build: clear the request, count builds.

@@ -91,6 +91,31 @@ __device__ __forceinline__ double len_rn(d3 v)
     return (double)__fsqrt_rn(__double2float_rn(d));
 }
 
+// Sphere i's list and history in their entry-major layout (PairArgs):
+// entry k's id at ids[k * nrow], history component c at
+// hist[(3 k + c) * nrow], from the sphere's own column.
+struct ListRow {
+    const uint32_t *ids;
+    double *hist;
+    size_t nrow;
+    __device__ __forceinline__ ListRow(const PairArgs &P, uint32_t sel, uint32_t i)
+        : ids(P.ids[sel] + i), hist(P.hist[sel] + i), nrow(P.nrow)
+    {
+    }
+    __device__ __forceinline__ uint32_t id(uint32_t k) const { return ids[(size_t)k * nrow]; }
+    __device__ __forceinline__ double *h(uint32_t k, int c) const
+    {
+        return hist + (size_t)(3u * k + (uint32_t)c) * nrow;
+    }
+    __device__ __forceinline__ d3 hist3(uint32_t k) const { return mk(*h(k, 0), *h(k, 1), *h(k, 2)); }
+    __device__ __forceinline__ void put3(uint32_t k, d3 v) const
+    {
+        *h(k, 0) = v.x;
+        *h(k, 1) = v.y;
+        *h(k, 2) = v.z;
+    }
+};
+
 // A sphere's sums in the list step: force and torque in FP64 (they drive
 // the FP64 integration, where the contacts' forces largely cancel), the
 // energy rates and pressure in FP32 (stored in FP32; es and ev accumulate
@@ -318,8 +343,7 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
     }
     const unsigned long long live_old = P.live[ls][i];
     unsigned long long live_new = 0ull;
-    const uint32_t *__restrict__ lst = P.ids[ls] + (size_t)i * VL_MAX;
-    double *__restrict__ hist = P.hist[ls] + (size_t)i * VL_MAX * 3;
+    const ListRow L(P, ls, i);
     const double4 xa = xr[i];
     const float4 va = vw[2 * i], wa = vw[2 * i + 1];
     const double dt = B.dt;
@@ -332,11 +356,11 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
     acc.p = 0.f;
     if (!AHEAD) {
         for (uint32_t k = 0; k < n; ++k) {
-            const uint32_t b = lst[k];
+            const uint32_t b = L.id(k);
             const double4 xb = xr[b];
             const float4 vb = vw[2 * b], wb = vw[2 * b + 1];
             d3 hb = mk(0.0, 0.0, 0.0);
-            if ((live_old >> k) & 1ull) hb = mk(hist[3 * k], hist[3 * k + 1], hist[3 * k + 2]);
+            if ((live_old >> k) & 1ull) hb = L.hist3(k);
             const d3 x_ab = centre_line(B, xa, xb, nullptr);
             const double x_ab_length = len_rn<LM>(x_ab);
             const double delta_n = __dsub_rn(x_ab_length, __dadd_rn(xa.w, xb.w));
@@ -344,9 +368,7 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
                 const MixedPair q = mixed_pair_f(x_ab, x_ab_length, delta_n, va, vb, wa, wb, xa.w, xb.w);
                 const d3 nd = B.P.contactmodel == 2 ? contact_linear_mixed(B.P, dt, acc, q, hb)
                                                     : contact_hertz_mixed(B.P, dt, acc, q, hb);
-                hist[3 * k] = nd.x;
-                hist[3 * k + 1] = nd.y;
-                hist[3 * k + 2] = nd.z;
+                L.put3(k, nd);
                 live_new |= 1ull << k;
             }
         }
@@ -359,13 +381,13 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
     double4 xb = make_double4(0.0, 0.0, 0.0, 0.0);
     float4 vb = make_float4(0.f, 0.f, 0.f, 0.f), wb = vb;
     d3 hb = mk(0.0, 0.0, 0.0);
-    uint32_t b_next = lst[1];
+    uint32_t b_next = L.id(1);
     if (n) {
-        const uint32_t b = lst[0];
+        const uint32_t b = L.id(0);
         xb = xr[b];
         vb = vw[2 * b];
         wb = vw[2 * b + 1];
-        if (live_old & 1ull) hb = mk(hist[0], hist[1], hist[2]);
+        if (live_old & 1ull) hb = L.hist3(0);
     }
     for (uint32_t k = 0; k < n; ++k) {
         double4 xq = xb;
@@ -373,12 +395,12 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
         d3 hq = mk(0.0, 0.0, 0.0);
         if (k + 1 < n) {
             const uint32_t b = b_next;
-            if (k + 2 < n) b_next = lst[k + 2];
+            if (k + 2 < n) b_next = L.id(k + 2);
             xq = xr[b];
             vq = vw[2 * b];
             wq = vw[2 * b + 1];
             if ((live_old >> (k + 1)) & 1ull)
-                hq = mk(hist[3 * (k + 1)], hist[3 * (k + 1) + 1], hist[3 * (k + 1) + 2]);
+                hq = L.hist3(k + 1);
         }
         const d3 x_ab = centre_line(B, xa, xb, nullptr);
         const double x_ab_length = len_rn<LM>(x_ab);
@@ -387,9 +409,7 @@ __device__ __forceinline__ void pair_sphere(const StepArgs &A, const PairArgs &P
             const MixedPair q = mixed_pair_f(x_ab, x_ab_length, delta_n, va, vb, wa, wb, xa.w, xb.w);
             const d3 nd = B.P.contactmodel == 2 ? contact_linear_mixed(B.P, dt, acc, q, hb)
                                                 : contact_hertz_mixed(B.P, dt, acc, q, hb);
-            hist[3 * k] = nd.x;
-            hist[3 * k + 1] = nd.y;
-            hist[3 * k + 2] = nd.z;
+            L.put3(k, nd);
             live_new |= 1ull << k;
         }
         xb = xq;
@@ -461,22 +481,21 @@ __global__ void __launch_bounds__(NT, MINB) k_pair_step_async(StepArgs A, PairAr
     }
     const unsigned long long live_old = P.live[ls][i];
     unsigned long long live_new = 0ull;
-    const uint32_t *__restrict__ lst = P.ids[ls] + (size_t)i * VL_MAX;
-    double *__restrict__ hist = P.hist[ls] + (size_t)i * VL_MAX * 3;
+    const ListRow L(P, ls, i);
     auto stage = [&](uint32_t k) {
         // entry k into slot k % D (an empty commit group past the list's end)
         if (k < n) {
             const int q = (int)(k % D);
-            const uint32_t b = lst[k];
+            const uint32_t b = L.id(k);
             const double4 *gx = xr + b;
             cp_async16(&S.x[q][tx], gx);
             cp_async16(reinterpret_cast<char *>(&S.x[q][tx]) + 16, reinterpret_cast<const char *>(gx) + 16);
             cp_async16(&S.v[q][tx], vw + 2 * b);
             cp_async16(&S.w[q][tx], vw + 2 * b + 1);
             if ((live_old >> k) & 1ull) {
-                cp_async8(&S.h[q][0][tx], hist + 3 * k);
-                cp_async8(&S.h[q][1][tx], hist + 3 * k + 1);
-                cp_async8(&S.h[q][2][tx], hist + 3 * k + 2);
+                cp_async8(&S.h[q][0][tx], L.h(k, 0));
+                cp_async8(&S.h[q][1][tx], L.h(k, 1));
+                cp_async8(&S.h[q][2][tx], L.h(k, 2));
             }
         }
         cp_async_commit();
@@ -507,9 +526,7 @@ __global__ void __launch_bounds__(NT, MINB) k_pair_step_async(StepArgs A, PairAr
             const MixedPair mp = mixed_pair_f(x_ab, x_ab_length, delta_n, va, vb, wa, wb, xa.w, xb.w);
             const d3 nd = B.P.contactmodel == 2 ? contact_linear_mixed(B.P, dt, acc, mp, hb)
                                                 : contact_hertz_mixed(B.P, dt, acc, mp, hb);
-            hist[3 * k] = nd.x;
-            hist[3 * k + 1] = nd.y;
-            hist[3 * k + 2] = nd.z;
+            L.put3(k, nd);
             live_new |= 1ull << k;
         }
         // slot k % D is refilled only after its values were used (the copy
@@ -654,19 +671,18 @@ __global__ void k_pair_remap(StepArgs A, PairArgs P)
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.ntot) return;
     const uint32_t ls = *P.lsel, nw = ls ^ 1u;
-    const uint32_t *nid = P.ids[nw] + (size_t)i * VL_MAX;
+    const ListRow NL(P, nw, i);
     uint32_t nn = P.cnt[nw][i];
     if (nn > (uint32_t)VL_MAX) nn = 0;   // overflowed: raised by the step kernel
-    double *nh = P.hist[nw] + (size_t)i * VL_MAX * 3;
     unsigned long long live = 0ull;
     auto find = [&](uint32_t b) -> int {
         int lo = 0, hi = (int)nn;   // first entry >= b
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
-            if (nid[mid] < b) lo = mid + 1;
+            if (NL.id((uint32_t)mid) < b) lo = mid + 1;
             else hi = mid;
         }
-        return lo < (int)nn && nid[lo] == b ? lo : -1;
+        return lo < (int)nn && NL.id((uint32_t)lo) == b ? lo : -1;
     };
     if (*P.from_rows) {
         for (int s = 0; s < NC; ++s) {
@@ -675,23 +691,18 @@ __global__ void k_pair_remap(StepArgs A, PairArgs P)
             const int k = find(w & ID_MASK);
             if (k < 0) continue;
             const double4 h = A.hist[(size_t)i * NC + s];
-            nh[3 * k] = h.x;
-            nh[3 * k + 1] = h.y;
-            nh[3 * k + 2] = h.z;
+            NL.put3((uint32_t)k, mk(h.x, h.y, h.z));
             live |= 1ull << k;
         }
     } else {
-        const uint32_t *oid = P.ids[ls] + (size_t)i * VL_MAX;
-        const double *oh = P.hist[ls] + (size_t)i * VL_MAX * 3;
+        const ListRow OL(P, ls, i);
         const uint32_t on = min(P.cnt[ls][i], (uint32_t)VL_MAX);
         for (unsigned long long m = P.live[ls][i]; m; m &= m - 1ull) {
             const int ko = __ffsll((long long)m) - 1;
             if ((uint32_t)ko >= on) break;
-            const int k = find(oid[ko]);
+            const int k = find(OL.id((uint32_t)ko));
             if (k < 0) continue;
-            nh[3 * k] = oh[3 * ko];
-            nh[3 * k + 1] = oh[3 * ko + 1];
-            nh[3 * k + 2] = oh[3 * ko + 2];
+            NL.put3((uint32_t)k, OL.hist3((uint32_t)ko));
             live |= 1ull << k;
         }
     }
@@ -780,18 +791,18 @@ __global__ void k_pair_flush(StepArgs A, PairArgs P)
     A.es[i] = ea.x;
     A.ev[i] = ea.y;
     const DevBox &B = A.boxes[box_index(A, i)];
-    const uint32_t *ids = P.ids[ls] + (size_t)i * VL_MAX;
-    const double *h = P.hist[ls] + (size_t)i * VL_MAX * 3;
+    const ListRow L(P, ls, i);
     const uint32_t nn = min(P.cnt[ls][i], (uint32_t)VL_MAX);
     int s = 0;
     for (unsigned long long m = P.live[ls][i]; m && s < NC; m &= m - 1ull) {
         const int k = __ffsll((long long)m) - 1;
         if ((uint32_t)k >= nn) break;
-        const uint32_t b = ids[k];
+        const uint32_t b = L.id((uint32_t)k);
         uint32_t code = 0;
         (void)centre_line(B, xa, P.xr[c][b], &code);
         A.slots[(size_t)i * NC + s] = b | (code << CODE_SHIFT);
-        A.hist[(size_t)i * NC + s] = make_double4(h[3 * k], h[3 * k + 1], h[3 * k + 2], 0.0);
+        const d3 hk = L.hist3((uint32_t)k);
+        A.hist[(size_t)i * NC + s] = make_double4(hk.x, hk.y, hk.z, 0.0);
         ++s;
     }
     for (; s < NC; ++s) {

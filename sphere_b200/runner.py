@@ -325,6 +325,14 @@ class Stepper(object):
         self._check(self.lib.sph_get_tuning(self.h, C.byref(v), C.byref(sh)), "sph_get_tuning")
         return v.value, sh.value
 
+    def shape_times(self):
+        """The last autotune's ms per step of the list step at each launch
+        shape, -1 where not tried (sph_get_shape_times)."""
+        ms = numpy.zeros(_abi.PAIR_SHAPES)
+        self._check(self.lib.sph_get_shape_times(self.h, _abi.dptr(ms), len(ms)),
+                    "sph_get_shape_times")
+        return ms
+
     def adjoint_forward(self, nsteps, ckpt=100):
         """nsteps steps with a checkpoint every ckpt steps kept for
         adjoint_backward (sph_adjoint_forward); returns the device ms."""

@@ -53,50 +53,6 @@ __device__ __forceinline__ bool grid_barrier(const GridSync &G, uint32_t nblocks
     return s_ok != 0;
 }
 
-// The same barrier with release/acquire ordering instead of full fences:
-// the block's threads meet at __syncthreads, thread 0 arrives with an
-// acq_rel atomic (its release orders the block's writes before the
-// barrier, through the block barrier, before the arrival), the last block
-// to arrive resets the count and publishes the next generation with a
-// release store, and the others poll the generation with acquire loads (the
-// block barrier after them orders the block's later reads).  Polls without
-// a sleep; the time limit is read every 64 polls.
-__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p)
-{
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ bool grid_barrier_acqrel(const GridSync &G, uint32_t nblocks, uint32_t *err)
-{
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const uint32_t g = ld_acquire_gpu(G.gen);
-        uint32_t arrived;
-        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(G.count) : "memory");
-        if (arrived == nblocks - 1u) {
-            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(G.count) : "memory");
-            asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(G.gen), "r"(g + 1u) : "memory");
-        } else {
-            const unsigned long long t0 = now_ns();
-            uint32_t polls = 0;
-            while (ld_acquire_gpu(G.gen) == g) {
-                if ((++polls & 63u) == 0u && now_ns() - t0 > G.limit_ns) {
-                    ok = 0;
-                    raise_flag(err, SPH_ERR_TIMEOUT);
-                    break;
-                }
-            }
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
 __device__ __forceinline__ unsigned long long ld_acquire_gpu_u64(const unsigned long long *p)
 {
     unsigned long long v;

@@ -273,7 +273,10 @@ int sph_relax(SphHandle *h, uint32_t sweeps, double alpha, double z_top,
  * tangential histories is recorded, then its steps are reversed with the
  * contact set of each step frozen and each contact law differentiated on
  * the branch it took (normal force on/off, stick/slip).  adjoint_ms gets
- * the device time of recompute + reverse.  Afterwards the handle holds the
+ * the device time of recompute + reverse; the CUDA graphs of the segments
+ * (one per segment length and kind) are captured before that time is
+ * taken, as the forward's step graph is built before forward_ms is taken.
+ * Afterwards the handle holds the
  * forward's final state and the checkpoints are released.
  *
  * Scope: one box, SPH_PREC_FP64 with SPH_LEN_FP64, contact model 2, E = 0,

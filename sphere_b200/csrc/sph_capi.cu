@@ -2202,7 +2202,7 @@ int sph_autotune(SphHandle *h, uint32_t steps, double *ms_per_step, int *chosen)
     for (int t = 0; t < NCAND; ++t) cand_ms[t] = -1.0;
     // the variants, and the list step at each of its launch shapes; two
     // rounds over all of them, each candidate keeping its better time, so
-    // that no candidate is judged on one run alone
+    // that no candidate is picked or dropped on one run alone
     for (int u = 0; u < 2 * NCAND && st == SPH_OK; ++u) {
         const int t = u % NCAND;
         const int v = t < sph::INTERACT_VARIANTS ? t : sph::PAIR_VARIANT;

@@ -81,7 +81,8 @@ def test_darcy_reader_scales_dphi_and_fields(tmp_path):
     assert numpy.array_equal(s.p_f_constant, ours.p_f_constant)
     raw = ours.dphi * ours.time_dt * ours.ndem
     assert numpy.array_equal(s.dphi, raw / (s.time_dt * 1))
-    assert int(s.ndem) == 3 and int(s.maxiter) == 500 and int(s.bc_bot[0]) == 1
+    assert int(numpy.ravel(s.ndem)[0]) == 3 and int(numpy.ravel(s.maxiter)[0]) == 500
+    assert int(s.bc_bot[0]) == 1
     assert numpy.array_equal(s.f_p, ours.f_p)
 
 

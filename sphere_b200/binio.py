@@ -4,10 +4,10 @@ Layout: python/sphere.py:1355-1553 (writebin) and :965-1353 (readbin),
 src/file_io.cpp:30-731 (C++ readbin/writebin).  Files are little-endian;
 every block below is written in the order the reference writes it.  The
 writer produces files byte-identical to python/sphere.py:writebin for
-simulations without a fluid and with a Darcy fluid (cfd_solver 1); the
-reader accepts versions >= 2.1 (older optional fields default as in
-python/sphere.py:readbin).  The Navier-Stokes fluid block (cfd_solver 0) is
-not supported.
+simulations without a fluid, with a Darcy fluid (cfd_solver 1) and with a
+Navier-Stokes fluid (cfd_solver 0: the block is read and written, the
+solver itself is not built); the reader accepts versions >= 2.1 (older
+optional fields default as in python/sphere.py:readbin).
 """
 import numpy
 
@@ -33,19 +33,22 @@ class _Reader(object):
 
 
 def _read_darcy(r, s, n):
-    """The Darcy fluid block (python/sphere.py:1157-1345 readbin,
-    src/file_io.cpp:347-404).  dphi is stored in the file as the change per
-    fluid step; the sim holds it per unit time, divided by time_dt * ndem
-    with the ndem the sim held before this read, as the reference's reader
-    divides."""
+    """The fluid block (python/sphere.py:1157-1345 readbin,
+    src/file_io.cpp:251-404): the cell fields and boundary codes, then the
+    Darcy solver's parameters and pressure force (cfd_solver 1) or the
+    Navier-Stokes solver's parameters and its four per-sphere fluid forces
+    (cfd_solver 0; the fields are kept, the solver is not built).  dphi is
+    stored in the file as the change per fluid step; the sim holds it per
+    unit time, divided by time_dt * ndem with the ndem the sim held before
+    this read, as the reference's reader divides."""
     version = float(s.version[0])
     if version >= 2.0:
         s.cfd_solver = r.take(numpy.int32, 1)
     else:
         s.cfd_solver = numpy.zeros(1, dtype=numpy.int32)
-    if int(s.cfd_solver[0]) != 1:
-        raise NotImplementedError("the Navier-Stokes fluid block (cfd_solver %d) is not supported"
-                                  % int(s.cfd_solver[0]))
+    solver = int(s.cfd_solver[0])
+    if solver not in (0, 1):
+        raise ValueError("Value of cfd_solver not understood (%d)" % solver)
     num = [int(v) for v in s.num]
     ncell = num[0] * num[1] * num[2]
     ndem_before = numpy.asarray(getattr(s, "ndem", numpy.array(1)))
@@ -59,7 +62,7 @@ def _read_darcy(r, s, n):
     s.p_mod_A = r.take(numpy.float64, 1)
     s.p_mod_f = r.take(numpy.float64, 1)
     s.p_mod_phi = r.take(numpy.float64, 1)
-    if version >= 2.12:
+    if version >= 2.12 and solver == 1:   # the sides: Darcy only
         for name in ("bc_xn", "bc_xp", "bc_yn", "bc_yp"):
             setattr(s, name, r.take(numpy.int32, 1))
     for name in ("bc_bot", "bc_top", "free_slip_bot", "free_slip_top"):
@@ -74,6 +77,21 @@ def _read_darcy(r, s, n):
         s.p_f_constant = cells_from_file(r.take(numpy.int32, ncell), num)
     else:
         s.p_f_constant = numpy.zeros(num, dtype=numpy.int32)
+    if version < 2.0:
+        return
+    if solver == 0:
+        s.gamma = r.take(numpy.float64, 1)
+        s.theta = r.take(numpy.float64, 1)
+        s.beta = r.take(numpy.float64, 1)
+        s.tolerance = r.take(numpy.float64, 1)
+        s.maxiter = r.take(numpy.uint32, 1)
+        s.ndem = r.take(numpy.uint32, 1)
+        s.c_phi = r.take(numpy.float64, 1)
+        s.c_v = r.take(numpy.float64, 1)
+        s.dt_dem_fac = r.take(numpy.float64, 1)
+        for name in ("f_d", "f_p", "f_v", "f_sum"):
+            setattr(s, name, r.take(numpy.float64, n * 3).reshape(n, 3))
+        return
     s.tolerance = r.take(numpy.float64, 1)
     s.maxiter = r.take(numpy.uint32, 1)
     s.ndem = r.take(numpy.uint32, 1)
@@ -199,12 +217,17 @@ def _i32(a):
 
 
 def _encode_darcy(s, w, dphi_raw=None):
-    """The Darcy fluid block in the order of python/sphere.py:1471-1539 and
-    src/file_io.cpp:656-716.  dphi goes to the file as dphi * time_dt * ndem
-    (the reference's Python writer); dphi_raw, when given, is written as it
-    is (the values of the solver, as its C++ writer writes them)."""
-    if int(numpy.asarray(s.cfd_solver).ravel()[0]) != 1:
-        raise NotImplementedError("the Navier-Stokes fluid block (cfd_solver 0) is not supported")
+    """The fluid block in the order of python/sphere.py:1471-1539 and
+    src/file_io.cpp:577-716: the Darcy solver's (cfd_solver 1), or the
+    Navier-Stokes solver's (cfd_solver 0: no side codes, then gamma, theta,
+    beta, tolerance, maxiter, ndem, c_phi, c_v, dt_dem_fac and the drag,
+    pressure, viscous and total fluid forces).  dphi goes to the file as
+    dphi * time_dt * ndem (the reference's Python writer); dphi_raw, when
+    given, is written as it is (the values of the solver, as its C++ writer
+    writes them)."""
+    solver = int(numpy.asarray(s.cfd_solver).ravel()[0])
+    if solver not in (0, 1):
+        raise ValueError("Value of cfd_solver not understood (%d)" % solver)
     n = int(s.np[0])
     w(_i32(numpy.asarray(s.cfd_solver).ravel()[:1]))
     w(_f64(s.mu))
@@ -220,12 +243,22 @@ def _encode_darcy(s, w, dphi_raw=None):
     w(blk.tobytes())
     for name in ("rho_f", "p_mod_A", "p_mod_f", "p_mod_phi"):
         w(_f64(getattr(s, name)))
-    for name in ("bc_xn", "bc_xp", "bc_yn", "bc_yp", "bc_bot", "bc_top", "free_slip_bot",
-                 "free_slip_top"):
+    sides = ("bc_xn", "bc_xp", "bc_yn", "bc_yp") if solver == 1 else ()
+    for name in sides + ("bc_bot", "bc_top", "free_slip_bot", "free_slip_top"):
         w(_i32(getattr(s, name)))
     w(_f64(s.bc_bot_flux))
     w(_f64(s.bc_top_flux))
     w(_i32(cells_to_file(s.p_f_constant).reshape(ncell)))
+    if solver == 0:
+        for name in ("gamma", "theta", "beta", "tolerance"):
+            w(_f64(numpy.asarray(getattr(s, name)).ravel()[:1]))
+        w(_u32(numpy.asarray(s.maxiter).ravel()[:1]))
+        w(_u32(numpy.asarray(s.ndem).ravel()[:1]))
+        for name in ("c_phi", "c_v", "dt_dem_fac"):
+            w(_f64(numpy.asarray(getattr(s, name)).ravel()[:1]))
+        for name in ("f_d", "f_p", "f_v", "f_sum"):
+            w(_f64(numpy.asarray(getattr(s, name), dtype=numpy.float64).reshape(-1, 3)[:n]))
+        return
     w(_f64(numpy.asarray(s.tolerance).ravel()[:1]))
     w(_u32(numpy.asarray(s.maxiter).ravel()[:1]))
     w(_u32(numpy.asarray(s.ndem).ravel()[:1]))

@@ -148,6 +148,10 @@ class Stepper(object):
         """Copy the sims' state to the device; a sim with a Darcy fluid also
         starts its fluid (sph_darcy_set), as the reference sets it up at the
         start of a run."""
+        for s in self.sims:
+            if getattr(s, "fluid", False) and int(numpy.asarray(s.cfd_solver).ravel()[0]) != 1:
+                raise NotImplementedError("the Navier-Stokes fluid solver (cfd_solver 0) is not "
+                                          "built; only the Darcy solver (cfd_solver 1) steps")
         self.hp = HostParticles.from_sims(self.sims)
         self.hb = HostBonds.from_sims(self.sims)
         ps = self.hp.struct()
@@ -161,7 +165,11 @@ class Stepper(object):
     def darcy_set(self, s):
         """Start the Darcy coupling from the fluid of sim s (sph_darcy_set).
         dphi goes in as the solver holds it, dphi * time_dt * ndem (what the
-        reference's writer puts in its input file)."""
+        reference's writer puts in its input file).  A Navier-Stokes fluid
+        (cfd_solver 0) is refused: that solver is not built."""
+        if int(numpy.asarray(s.cfd_solver).ravel()[0]) != 1:
+            raise NotImplementedError("the Navier-Stokes fluid solver (cfd_solver 0) is not "
+                                      "built; only the Darcy solver (cfd_solver 1) steps")
         self._darcy = _abi.darcy_from_sim(s)
         self._num = [int(v) for v in s.num]
         f = lambda a, t=numpy.float64: numpy.ascontiguousarray(_abi.cells_to_file(numpy.asarray(a, dtype=t)))
@@ -584,6 +592,9 @@ def _write_status(path, s):
 def run_sim(s, root="..", verbose=True, device=-1, precision="fp64", length="reference"):
     """Run `s` to time_total, writing the reference's output files.  Returns
     0 or the SphStatus of the first failure (as the binary's exit status)."""
+    if getattr(s, "fluid", False) and int(numpy.asarray(s.cfd_solver).ravel()[0]) != 1:
+        raise NotImplementedError("the Navier-Stokes fluid solver (cfd_solver 0) is not built; "
+                                  "only the Darcy solver (cfd_solver 1) steps")
     msg = check_values(s)
     if msg:
         print(msg)

@@ -118,13 +118,54 @@ class sim(object):
         self.fluid = False
         self.color = numpy.zeros(n, dtype=numpy.int32)
         if fluid:
-            # the Darcy solver's fields (python/sphere.py:310-440); the
-            # Navier-Stokes solver (cfd_solver 0) is not built
+            # the fluid fields (python/sphere.py:310-440): those of the Darcy
+            # solver, or of the Navier-Stokes solver (cfd_solver 0), whose
+            # fields and .bin block are kept but whose solver is not built
             self.fluid = True
             self.cfd_solver = numpy.ones(1, dtype=numpy.int32) * int(cfd_solver)
-            self._darcy_defaults(0.0)
+            if int(cfd_solver) == 0:
+                self._ns_defaults(0.0)
+            else:
+                self._darcy_defaults(0.0)
 
     # ------------------------------------------------------------- fluid
+    def _ns_defaults(self, p):
+        """The Navier-Stokes fields with their defaults on the current grid
+        (python/sphere.py:3418-3489 initFluid with cfd_solver 0): the
+        cell fields and boundary codes shared with the Darcy solver, the
+        solver parameters gamma, theta, beta, tolerance, maxiter, ndem,
+        c_phi, c_v, dt_dem_fac and the per-sphere drag, pressure, viscous and
+        total fluid forces."""
+        num = tuple(int(v) for v in self.num)
+        n, nd = int(self.np[0]), int(self.nd[0])
+        self.mu = numpy.zeros(1, dtype=numpy.float64)
+        self.rho_f = numpy.ones(1, dtype=numpy.float64) * 1.0e3
+        self.p_f = numpy.ones(num, dtype=numpy.float64) * p
+        self.v_f = numpy.zeros(num + (nd,), dtype=numpy.float64)
+        self.phi = numpy.ones(num, dtype=numpy.float64)
+        self.dphi = numpy.zeros(num, dtype=numpy.float64)
+        self.p_mod_A = numpy.zeros(1, dtype=numpy.float64)
+        self.p_mod_f = numpy.zeros(1, dtype=numpy.float64)
+        self.p_mod_phi = numpy.zeros(1, dtype=numpy.float64)
+        self.bc_bot = numpy.zeros(1, dtype=numpy.int32)
+        self.bc_top = numpy.zeros(1, dtype=numpy.int32)
+        self.free_slip_bot = numpy.ones(1, dtype=numpy.int32)
+        self.free_slip_top = numpy.ones(1, dtype=numpy.int32)
+        self.bc_bot_flux = numpy.zeros(1, dtype=numpy.float64)
+        self.bc_top_flux = numpy.zeros(1, dtype=numpy.float64)
+        self.p_f_constant = numpy.zeros(num, dtype=numpy.int32)
+        self.gamma = numpy.array(0.0)
+        self.theta = numpy.array(1.0)
+        self.beta = numpy.array(0.0)
+        self.tolerance = numpy.array(1.0e-3)
+        self.maxiter = numpy.array(1e4)
+        self.ndem = numpy.array(1)
+        self.c_phi = numpy.ones(1, dtype=numpy.float64)
+        self.c_v = numpy.ones(1, dtype=numpy.float64)
+        self.dt_dem_fac = numpy.ones(1, dtype=numpy.float64)
+        for name in ("f_d", "f_p", "f_v", "f_sum"):
+            setattr(self, name, numpy.zeros((n, nd), dtype=numpy.float64))
+
     def _darcy_defaults(self, p):
         """The Darcy fields with their defaults on the current grid."""
         num = tuple(int(v) for v in self.num)
@@ -157,16 +198,20 @@ class sim(object):
 
     def initFluid(self, mu=8.9e-4, rho=1.0e3, p=0.0, hydrostatic=False, cfd_solver=0):
         """Fluid arrays and viscosity on the current grid
-        (python/sphere.py:3395).  Only the Darcy solver (cfd_solver = 1) is
-        built here.  With hydrostatic=True the cells below the top wall (or
-        below the top of the grid) get the hydrostatic pressure of the
-        fluid column above them, p at the top."""
-        if int(cfd_solver) != 1:
-            raise NotImplementedError("only the Darcy fluid solver (cfd_solver = 1) is built; "
-                                      "the Navier-Stokes solver (cfd_solver = 0) is not")
+        (python/sphere.py:3395).  cfd_solver 1: the Darcy solver, which
+        run() steps; cfd_solver 0: the Navier-Stokes solver's fields, which
+        can be set up, written and read (its .bin block), but run() refuses
+        them: that solver is not built.  With hydrostatic=True the cells
+        below the top wall (or below the top of the grid) get the hydrostatic
+        pressure of the fluid column above them, p at the top."""
+        if int(cfd_solver) not in (0, 1):
+            raise Exception('Value of cfd_solver not understood (%s)' % cfd_solver)
         self.fluid = True
-        self.cfd_solver = numpy.ones(1, dtype=numpy.int32)
-        self._darcy_defaults(p)
+        self.cfd_solver = numpy.ones(1, dtype=numpy.int32) * int(cfd_solver)
+        if int(cfd_solver) == 0:
+            self._ns_defaults(p)
+        else:
+            self._darcy_defaults(p)
         self.mu = numpy.ones(1, dtype=numpy.float64) * mu
         self.rho_f = numpy.ones(1, dtype=numpy.float64) * rho
         if hydrostatic:
@@ -265,6 +310,16 @@ class sim(object):
 
     def disableFluidPressureModulation(self):
         self.setFluidPressureModulation(A=0.0, f=0.0)
+
+    # the Navier-Stokes solver's parameters (python/sphere.py:6294-6352)
+    def setGamma(self, gamma):
+        self.gamma = numpy.asarray(gamma)
+
+    def setTheta(self, theta):
+        self.theta = numpy.asarray(theta)
+
+    def setBeta(self, beta):
+        self.beta = numpy.asarray(beta)
 
     def setTolerance(self, tolerance):
         self.tolerance = numpy.asarray(tolerance)
@@ -731,9 +786,11 @@ class sim(object):
         self.initFluid()
 
     def largestFluidTimeStep(self, safety=0.5, v_max=-1.0):
-        """The largest stable fluid time step (python/sphere.py:2067): for
-        the Darcy solver the advective (CFL) limit, the smallest cell width
-        over the largest fluid speed (1e-7 m/s when the fluid is at rest)."""
+        """The largest stable fluid time step (python/sphere.py:3167): the
+        advective (CFL) limit, the smallest cell width over the largest
+        fluid speed (1e-7 m/s when the fluid is at rest); for the
+        Navier-Stokes solver the smaller of that and the diffusive limit
+        0.5 dx^2 / mu, times `safety`."""
         if not self.fluid:
             return None
         v = numpy.asarray(self.v_f, dtype=numpy.float64).reshape(-1, 3)
@@ -743,6 +800,9 @@ class sim(object):
         if v_max < 0.0:
             v_max = v_max_obs
         dx_min = numpy.min(self.L / self.num)
+        if int(numpy.asarray(self.cfd_solver).ravel()[0]) == 0:
+            dt_von_neumann = 0.5 * dx_min ** 2 / (self.mu[0] + 1.0e-16)
+            return numpy.min([dt_von_neumann, dx_min / v_max]) * safety
         self._check_darcy('largestFluidTimeStep')
         self.cellSize()
         return dx_min / v_max

@@ -132,6 +132,31 @@ def bin_scenes(S):
     s.f_p[:, 2] = 0.25
     s.initTemporal(total=0.01, file_dt=0.002)
     out["darcy"] = s
+    numpy.random.seed(6)
+    s = S(np=18, nw=0, sid="golden_ns", fluid=True)
+    s.generateRadii(psd='uni', mean=0.01, variance=0.001)
+    s.periodicBoundariesXY()
+    s.initRandomGridPos(gridnum=numpy.array([8, 8, 16]))
+    s.consolidate(normal_stress=1.0e4)
+    s.initFluid(mu=1.0e-3, rho=1.0e3, p=2.0e3, hydrostatic=True, cfd_solver=0)
+    s.setFluidBottomNoFlow()
+    s.setFluidTopFixedPressure()
+    s.setFluidPressureModulation(A=50.0, f=1.0, phi=0.5)
+    s.setGamma(0.1)
+    s.setTheta(0.9)
+    s.setBeta(0.2)
+    s.setTolerance(1.0e-5)
+    s.setMaxIterations(800)
+    s.setDEMstepsPerCFDstep(2)
+    s.p_f_constant[1, 0, 1] = 1
+    s.dphi[:, :, 1] = 0.25
+    s.v_f[:, :, :, 0] = 2.0e-3
+    s.f_d[:, 0] = 0.5
+    s.f_p[:, 1] = -0.25
+    s.f_v[:, 2] = 0.125
+    s.f_sum[:] = s.f_d + s.f_p + s.f_v
+    s.initTemporal(total=0.01, file_dt=0.002)
+    out["ns"] = s
     return out
 
 

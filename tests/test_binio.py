@@ -2,7 +2,8 @@
 python/sphere.py (tests/golden/bin_*.bin, see tests/golden/make_golden.py):
 the same seeded scenes built with sphere_b200.sim must encode to the same
 bytes, and every golden file must read back and re-encode unchanged.  The
-darcy scene carries the Darcy fluid block (cfd_solver 1)."""
+darcy scene carries the Darcy fluid block (cfd_solver 1), the ns scene the
+Navier-Stokes fluid block (cfd_solver 0: read and written, not stepped)."""
 import os
 
 import numpy
@@ -25,20 +26,20 @@ def _scenes():
     return mod.bin_scenes(sim)
 
 
-@pytest.mark.parametrize("name", ["grid", "consolidate", "shear", "bonds", "darcy"])
+@pytest.mark.parametrize("name", ["grid", "consolidate", "shear", "bonds", "darcy", "ns"])
 def test_setup_and_writer_match_reference_bytes(name):
     ours = _scenes()[name]
     golden = open(os.path.join(GOLDEN, "bin_%s.bin" % name), "rb").read()
     assert binio.encode_bin(ours) == golden
 
 
-@pytest.mark.parametrize("name", ["grid", "consolidate", "shear", "bonds", "darcy"])
+@pytest.mark.parametrize("name", ["grid", "consolidate", "shear", "bonds", "darcy", "ns"])
 def test_reader_round_trip(name, tmp_path):
     path = os.path.join(GOLDEN, "bin_%s.bin" % name)
     # as in the reference, the sim says whether the file has a fluid block
-    s = sim(fluid=(name == "darcy"))
+    s = sim(fluid=(name in ("darcy", "ns")))
     s.readbin(path, verbose=False)
-    if name == "darcy":
+    if name in ("darcy", "ns"):
         # the reader divides dphi by time_dt * ndem with the ndem the sim
         # held before the read (1), the writer multiplies by the file's (3),
         # as the reference's own reader and writer do: every other byte
@@ -86,7 +87,25 @@ def test_darcy_reader_scales_dphi_and_fields(tmp_path):
     assert numpy.array_equal(s.f_p, ours.f_p)
 
 
-def test_navier_stokes_block_is_not_supported(tmp_path):
+def test_navier_stokes_fields_read_back():
+    """The Navier-Stokes block's solver parameters and per-sphere fluid
+    forces, as the reference's writer stored them."""
+    ours = _scenes()["ns"]
     s = sim(fluid=True)
+    s.readbin(os.path.join(GOLDEN, "bin_ns.bin"), verbose=False)
+    assert int(s.cfd_solver[0]) == 0 and not hasattr(s, "bc_xn")
+    for name in ("gamma", "theta", "beta", "tolerance", "c_phi", "c_v", "dt_dem_fac"):
+        assert float(numpy.ravel(getattr(s, name))[0]) == float(numpy.ravel(getattr(ours, name))[0]), name
+    assert int(numpy.ravel(s.maxiter)[0]) == 800 and int(numpy.ravel(s.ndem)[0]) == 2
+    for name in ("f_d", "f_p", "f_v", "f_sum"):
+        assert numpy.array_equal(getattr(s, name), getattr(ours, name)), name
+    assert numpy.array_equal(s.p_f, ours.p_f) and numpy.array_equal(s.v_f, ours.v_f)
+
+
+def test_navier_stokes_fluid_is_not_stepped(tmp_path):
+    """The Navier-Stokes solver is not built: run() refuses such a sim
+    before it touches a device."""
+    from sphere_b200 import runner
+    s = _scenes()["ns"]
     with pytest.raises(NotImplementedError):
-        s.initFluid(cfd_solver=0)
+        runner.run_sim(s, root=str(tmp_path), verbose=False)
